@@ -1,0 +1,87 @@
+/* spektralab B200 extensions: entry points with no counterpart in the reference engine's C ABI.
+ *
+ * Conventions are those of spektralab.h: C linkage, no exceptions cross, a negative spk_status and a
+ * message in spk_last_error on failure. Host pointers unless stated.
+ */
+#ifndef SPEKTRALAB_B200_H
+#define SPEKTRALAB_B200_H
+
+#include "spektralab.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- test and benchmark configuration ----
+ *
+ * spkx_session_set_halation(session, n, weights, sigmas_px, strength)
+ *   replace the session's halation with a Gaussian mixture given in pixels:
+ *     H(x) = sum_k weight[k][c] G_{sigma[k][c]}(x);  raw := raw / (1 + A_c) + A_c H(raw) / (1 + A_c)
+ *   weights and sigmas_px hold n x 3 doubles, strength 3; n = 0 restores the film's own halation
+ *   (its preset through the scatter and bounce models). The scatter stage is dropped while set.
+ *   drops every cached negative. SPK_ERR_INVALID_ARG for n > 8 or a NULL array with n > 0.
+ *   The halation configurations of the benchmark workloads (two components of given sigma in pixels)
+ *   cannot be expressed through the reference's parameters, so tests and bench set them here, and
+ *   set the same mixture on the reference oracle.
+ */
+SPK_API spk_status spkx_session_set_halation(spk_session* session, uint32_t n, const double* weights,
+                                             const double* sigmas_px, const double* strength);
+
+/* spkx_session_profile(session, tier, reprint, steps, out_json)
+ *   render (reprint = 0) or reprint (reprint = 1) `steps` times on the device, with no host copy of the
+ *   result, and report per-stage device times from CUDA events on the session's stream:
+ *     {"steps": K, "total_ms": [..K], "stages": {"expose": [...], ...}, "pixels": P}
+ *   before every step the L2 cache is flushed by writing a 256 MiB buffer (untimed).
+ *   a render step develops afresh each time; a reprint step prints the cached negative.
+ */
+SPK_API spk_status spkx_session_profile(spk_session* session, const char* tier, int32_t reprint, uint32_t steps,
+                                        char** out_json);
+
+/* spkx_session_negative(session, tier, out, capacity_floats)
+ *   copy the tier's cached negative (3 floats per pixel) to host memory; SPK_ERR_USER when none is cached.
+ */
+SPK_API spk_status spkx_session_negative(spk_session* session, const char* tier, float* out, size_t capacity_floats);
+
+/* spkx_session_develop_debug(session, tier, film_seed, negative, counts)
+ *   develop the tier's frame once more with the given film seed, without touching the cache:
+ *   negative receives 3 floats per pixel, counts (may be NULL) the grain's Poisson counts, 9 floats per
+ *   pixel [channel][sub-layer]. The first render of a session uses the seed sequence's first draw,
+ *   0x4abea221, so this reproduces its negative and tells which counts it drew.
+ */
+SPK_API spk_status spkx_session_develop_debug(spk_session* session, const char* tier, uint32_t film_seed,
+                                              float* negative, float* counts);
+
+/* spkx_session_setup_json(session, out_json)
+ *   the narrowed kernel constants of the session's pipeline, for set-up parity checks:
+ *   input matrix, curve tables, grain tables and constants at a given pitch, enlarger and scan
+ *   tables of the current live parameters, paper curve, CAM16 arguments and the C_max table.
+ */
+SPK_API spk_status spkx_session_setup_json(spk_session* session, double pitch_um, char** out_json);
+
+/* spkx_setup_json(resources_dir, params_delta_json, pitch_um, out_json)
+ *   the same constants for the parameters an spk_open with this delta would use, built on the host
+ *   alone (no device, no engine): the binary64 set-up can be checked on a machine without a GPU.
+ */
+SPK_API spk_status spkx_setup_json(const char* resources_dir, const char* params_delta_json, double pitch_um,
+                                   char** out_json);
+
+/* ---- stage-level test entry points (host arrays in and out; run on the current device) ---- */
+
+/* Poisson counts (as floats) of the grain sampler for pixel index i = 0..n-1 on one stream and seed */
+SPK_API spk_status spkx_sampler_poisson(const float* lam, float* counts, uint32_t n, uint32_t stream,
+                                        uint32_t seed);
+/* the Box-Muller lognormal value for pixel index i = 0..n-1 */
+SPK_API spk_status spkx_sampler_lognormal(float* out, uint32_t n, float mean, float stddev, uint32_t stream,
+                                          uint32_t seed);
+/* Philox4x32-10 of n (counter[4], key[2]) pairs into out[4n] */
+SPK_API spk_status spkx_philox(const uint32_t* counters, const uint32_t* keys, uint32_t* out, uint32_t n);
+
+/* the Gaussian blur of a w x h RGB float plane (3 floats per pixel) with per-channel sigma in pixels,
+ * by the engine's FIR / recursive branch rule */
+SPK_API spk_status spkx_gaussian(const float* in, float* out, uint32_t w, uint32_t h, const double* sigma3);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SPEKTRALAB_B200_H */

@@ -1,0 +1,239 @@
+"""Test infrastructure: ctypes front of the float64 oracle (liboracle.so, spk_oracle.c).
+
+Only tests, the smoke check and the benchmark's CPU-baseline leg use this module. It fills the
+oracle's OracleSetup from the binary64 set-up that the engine reports (spkx_setup_json, the "f64"
+section), which the set-up parity tests pin bit for bit (after narrowing) against the reference
+engine's own set-up.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "liboracle.so")
+MAXC = 8
+
+D = ctypes.c_double
+I32 = ctypes.c_int32
+PD = ctypes.POINTER(ctypes.c_double)
+
+
+class OracleSetup(ctypes.Structure):
+    _fields_ = [
+        ("A", D * 9), ("gain", D), ("L", I32), ("table", PD),
+        ("n_scatter", I32), ("n_bounce", I32),
+        ("scatter_w", (D * 3) * MAXC), ("scatter_s", (D * 3) * MAXC), ("scatter_a", D * 3), ("scatter_b", D * 3),
+        ("bounce_w", (D * 3) * MAXC), ("bounce_s", (D * 3) * MAXC), ("mix_a", D * 3), ("mix_b", D * 3),
+        ("lens_blur_px", D),
+        ("K", I32), ("cx", PD), ("cinv", PD), ("cy", PD),
+        ("grain", I32), ("positive", I32), ("gK", I32), ("gaxis", PD), ("ginv", PD), ("glayers", PD),
+        ("count", D * 9), ("sat_d", D * 9), ("dmin_l", D * 9), ("uniformity", D * 3), ("dmin_c", D * 3),
+        ("final_blur", D), ("amount", D), ("seed", ctypes.c_uint32),
+        ("printed", I32), ("enl_eps", D * 243), ("enl_beta", D * 81), ("enl_wt", D * 243), ("g", D * 3),
+        ("o", D * 3), ("k_gain", D),
+        ("pK", I32), ("px", PD), ("pr", PD), ("py", PD),
+        ("scan_eps", D * 243), ("scan_beta", D * 81), ("scan_wt", D * 243), ("to_rgb", D * 9),
+        ("cam_k", D * 22), ("m_to_xyz", D * 9), ("m_to_rgb", D * 9), ("m16", D * 9), ("m16_inv", D * 9),
+        ("cmax", PD), ("lc_active", I32),
+        ("scanner_lens_blur", D), ("unsharp_sigma", D), ("unsharp_amount", D),
+        ("cctf_active", I32), ("cctf_mode", I32), ("m_nid", D * 9),
+    ]
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            raise FileNotFoundError(f"{LIB} is not built (make -C oracle)")
+        L = ctypes.CDLL(LIB)
+        FP = ctypes.POINTER(ctypes.c_float)
+        U16 = ctypes.POINTER(ctypes.c_uint16)
+        U32P = ctypes.POINTER(ctypes.c_uint32)
+        L.orc_render.argtypes = [ctypes.POINTER(OracleSetup), FP, I32, I32, FP, U16, PD]
+        L.orc_develop.argtypes = [ctypes.POINTER(OracleSetup), FP, I32, I32, FP, PD]
+        L.orc_print.argtypes = [ctypes.POINTER(OracleSetup), PD, I32, I32, U16, PD]
+        L.orc_gaussian.argtypes = [PD, PD, I32, I32, PD]
+        L.orc_gaussian.restype = None
+        L.orc_poisson.argtypes = [FP, FP, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32]
+        L.orc_poisson.restype = None
+        L.orc_lognormal.argtypes = [FP, ctypes.c_uint32, ctypes.c_float, ctypes.c_float, ctypes.c_uint32,
+                                    ctypes.c_uint32]
+        L.orc_lognormal.restype = None
+        L.orc_philox.argtypes = [U32P, U32P, U32P, ctypes.c_uint32]
+        L.orc_philox.restype = None
+        for f in ("orc_logf", "orc_expf", "orc_cosf"):
+            getattr(L, f).argtypes = [ctypes.c_float]
+            getattr(L, f).restype = ctypes.c_float
+        L.orc_splitmix_next.argtypes = [ctypes.POINTER(ctypes.c_uint64)]
+        L.orc_splitmix_next.restype = ctypes.c_uint32
+        _lib = L
+    return _lib
+
+
+class Oracle:
+    """An OracleSetup plus the arrays it points into (kept alive here)."""
+
+    def __init__(self, f64, seed=0, halation=None, print_exposure=None):
+        s = OracleSetup()
+        self.keep = []
+
+        def buf(values):
+            a = np.ascontiguousarray(np.asarray(values, dtype=np.float64))
+            self.keep.append(a)
+            return a.ctypes.data_as(PD)
+
+        def put(field, values):
+            arr = getattr(s, field)
+            for i, v in enumerate(values):
+                arr[i] = float(v)
+
+        put("A", f64["input_matrix"])
+        s.gain = f64["gain"]
+        s.L = int(round(len(f64["table"]) / 3) ** 0.5 + 0.5)
+        s.table = buf(f64["table"])
+        hal = f64["halation"]
+        sc = hal["scatter"]
+        s.n_scatter = len(sc)
+        for k, (w, sg) in enumerate(sc):
+            for c in range(3):
+                s.scatter_w[k][c] = w[c]
+                s.scatter_s[k][c] = sg[c]
+        put("scatter_a", hal["scatter_a"])
+        put("scatter_b", hal["scatter_b"])
+        if halation is not None:  # the test override: (comps, strength); the scatter stage is dropped
+            comps, strength = halation
+            s.n_scatter = 0
+            s.n_bounce = len(comps)
+            for k, (w, sg) in enumerate(comps):
+                for c in range(3):
+                    s.bounce_w[k][c] = w[c]
+                    s.bounce_s[k][c] = sg[c]
+            put("mix_a", [1.0 / (1.0 + a) for a in strength])
+            put("mix_b", [a / (1.0 + a) for a in strength])
+        else:
+            bo = hal["bounce"]
+            s.n_bounce = len(bo)
+            for k, (w, sg) in enumerate(bo):
+                for c in range(3):
+                    s.bounce_w[k][c] = w[c]
+                    s.bounce_s[k][c] = sg[c]
+            put("mix_a", hal["mix_a"])
+            put("mix_b", hal["mix_b"])
+        s.lens_blur_px = f64["lens_blur_px"]
+        s.K = len(f64["curve_x"])
+        s.cx = buf(f64["curve_x"])
+        s.cinv = buf(f64["curve_inv"])
+        s.cy = buf(f64["curve_y"])
+        s.grain = 1 if f64.get("grain_active") else 0
+        s.positive = 1 if f64.get("positive") else 0
+        if s.grain:
+            s.gK = len(f64["grain_axis"]) // 3
+            s.gaxis = buf(f64["grain_axis"])
+            s.ginv = buf(f64["grain_inv"])
+            s.glayers = buf(f64["grain_layers"])
+            put("count", f64["grain_count"])
+            put("sat_d", f64["grain_sat_d"])
+            put("dmin_l", f64["grain_dmin_l"])
+            put("uniformity", [0.97, 0.99, 0.97])
+            put("dmin_c", [0.03, 0.03, 0.03])
+            s.final_blur = f64["grain_final_blur"]
+            s.amount = f64["grain_amount"]
+        s.seed = seed
+        s.printed = 1 if f64["printed"] else 0
+        put("enl_eps", f64["enl_eps"])
+        put("enl_beta", f64["enl_beta"])
+        put("enl_wt", f64["enl_wt"])
+        put("g", f64["enl_g"])
+        put("o", f64["enl_o"])
+        s.k_gain = f64["k_gain"] if print_exposure is None else print_exposure
+        if "paper_x" in f64:
+            s.pK = len(f64["paper_x"])
+            s.px = buf(f64["paper_x"])
+            s.pr = buf(f64["paper_r"])
+            s.py = buf(f64["paper_y"])
+        put("scan_eps", f64["scan_eps"])
+        put("scan_beta", f64["scan_beta"])
+        put("scan_wt", f64["scan_wt"])
+        put("to_rgb", f64["to_rgb"])
+        put("cam_k", f64["cam_k"])
+        put("m_to_xyz", f64["cam_m_to_xyz"])
+        put("m_to_rgb", f64["cam_m_to_rgb"])
+        put("m16", f64["cam_m16"])
+        put("m16_inv", f64["cam_m16_inv"])
+        s.cmax = buf(f64["cmax"])
+        s.lc_active = 1
+        s.scanner_lens_blur = f64["scanner_lens_blur"]
+        s.unsharp_sigma = f64["unsharp_sigma"]
+        s.unsharp_amount = f64["unsharp_amount"]
+        s.cctf_active = 1 if f64["cctf_active"] else 0
+        s.cctf_mode = int(f64["cctf_mode"])
+        put("m_nid", f64["m_nid"])
+        self.s = s
+
+    def render(self, rgb, counts=None):
+        rgb = np.ascontiguousarray(rgb, np.float32)
+        h, w, _ = rgb.shape
+        out = np.zeros((h, w, 4), np.uint16)
+        neg = np.zeros((h, w, 3), np.float64)
+        cp = None
+        if counts is not None:
+            counts = np.ascontiguousarray(counts, np.float32)
+            cp = counts.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+        lib().orc_render(ctypes.byref(self.s), rgb.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), w, h, cp,
+                         out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint16)), neg.ctypes.data_as(PD))
+        return out, neg
+
+    def print(self, negative, print_exposure=None):
+        if print_exposure is not None:
+            self.s.k_gain = print_exposure
+        neg = np.ascontiguousarray(negative, np.float64)
+        h, w, _ = neg.shape
+        out = np.zeros((h, w, 4), np.uint16)
+        lin = np.zeros((h, w, 3), np.float64)
+        lib().orc_print(ctypes.byref(self.s), neg.ctypes.data_as(PD), w, h,
+                        out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint16)), lin.ctypes.data_as(PD))
+        return out, lin
+
+
+def gaussian(plane, sigma3):
+    x = np.ascontiguousarray(plane, np.float64)
+    h, w, _ = x.shape
+    out = np.zeros_like(x)
+    sg = (ctypes.c_double * 3)(*[float(v) for v in sigma3])
+    lib().orc_gaussian(x.ctypes.data_as(PD), out.ctypes.data_as(PD), w, h, sg)
+    return out
+
+
+def poisson(lam, stream, seed):
+    lam = np.ascontiguousarray(lam, np.float32)
+    out = np.zeros_like(lam)
+    FP = ctypes.POINTER(ctypes.c_float)
+    lib().orc_poisson(lam.ctypes.data_as(FP), out.ctypes.data_as(FP), lam.size, stream, seed)
+    return out
+
+
+def lognormal(n, mean, sd, stream, seed):
+    out = np.zeros(n, np.float32)
+    lib().orc_lognormal(out.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), n, mean, sd, stream, seed)
+    return out
+
+
+def philox(ctr, key):
+    ctr = np.ascontiguousarray(ctr, np.uint32).reshape(-1, 4)
+    key = np.ascontiguousarray(key, np.uint32).reshape(-1, 2)
+    out = np.zeros_like(ctr)
+    U = ctypes.POINTER(ctypes.c_uint32)
+    lib().orc_philox(ctr.ctypes.data_as(U), key.ctypes.data_as(U), out.ctypes.data_as(U), ctr.shape[0])
+    return out
+
+
+def splitmix(n, state=0x243F6A8885A308D3):
+    st = ctypes.c_uint64(state)
+    return [lib().orc_splitmix_next(ctypes.byref(st)) for _ in range(n)]

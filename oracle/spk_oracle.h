@@ -1,0 +1,89 @@
+/* Test infrastructure: the float64 oracle of the spektralab render path.
+ *
+ * A CPU restatement, in binary64, of the reference engine's per-pixel render path: every stage of
+ * the film side (src/film/develop.cpp:101-236) and the print side (src/print/run.cpp:118-188) with
+ * the reference kernels' formulas (kernels/*.metal) evaluated in double, fed from the unrounded
+ * binary64 set-up. Only the tests, the smoke check and the benchmark's CPU baseline load it; the
+ * product never does. Its own correctness is pinned against the reference engine run on this CPU
+ * (oracle/_ref) and the golden vectors in tests/golden.
+ *
+ * Grain: the Poisson counts are either drawn here with the binary32 sampler shared with the device
+ * code (grain_sampler.h) from lambda rounded to binary32, or taken from the caller ("fixed noise"),
+ * so that a device render can be compared with the float64 arithmetic of every other stage.
+ */
+#ifndef SPK_ORACLE_H
+#define SPK_ORACLE_H
+
+#include <stdint.h>
+
+#define ORC_MAX_COMP 8
+
+typedef struct {
+    /* expose */
+    double A[9];
+    double gain;
+    int32_t L;
+    const double* table; /* L*L*3 */
+    /* halation: scatter mixture then bounce mixture, each raw := a raw + b M(raw) */
+    int32_t n_scatter, n_bounce;
+    double scatter_w[ORC_MAX_COMP][3], scatter_s[ORC_MAX_COMP][3], scatter_a[3], scatter_b[3];
+    double bounce_w[ORC_MAX_COMP][3], bounce_s[ORC_MAX_COMP][3], mix_a[3], mix_b[3];
+    double lens_blur_px;
+    /* curves */
+    int32_t K;
+    const double* cx;
+    const double* cinv;
+    const double* cy; /* 3K, channel-major */
+    /* grain */
+    int32_t grain, positive, gK;
+    const double* gaxis;   /* K*3 */
+    const double* ginv;    /* K*3 */
+    const double* glayers; /* K*3*3 */
+    double count[9], sat_d[9], dmin_l[9], uniformity[3], dmin_c[3];
+    double final_blur, amount;
+    uint32_t seed;
+    /* print */
+    int32_t printed;
+    double enl_eps[243], enl_beta[81], enl_wt[243], g[3], o[3], k_gain;
+    int32_t pK;
+    const double* px;
+    const double* pr;
+    const double* py; /* pK*3 */
+    double scan_eps[243], scan_beta[81], scan_wt[243];
+    double to_rgb[9];
+    /* CAM16 gamut */
+    double cam_k[22]; /* F_L N_bb N_cb n z A_w c N_c Jfirst Jlast hfirst hstep knee0..2 lc0..2 Jwhite D_R D_G D_B */
+    double m_to_xyz[9], m_to_rgb[9], m16[9], m16_inv[9];
+    const double* cmax; /* 64 x 720 */
+    int32_t lc_active;
+    /* scanner + encode */
+    double scanner_lens_blur, unsharp_sigma, unsharp_amount;
+    int32_t cctf_active, cctf_mode;
+    double m_nid[9];
+} OracleSetup;
+
+/* The whole render of a w x h frame; rgb is 3 floats per pixel (already non-finite-cleaned),
+ * counts NULL or 9 floats per pixel [c][l]; out_rgba receives w*h*4 uint16 (packed rows),
+ * out_negative (may be NULL) w*h*3 doubles. Returns 0. */
+int orc_render(const OracleSetup* s, const float* rgb, int32_t w, int32_t h, const float* counts,
+               uint16_t* out_rgba, double* out_negative);
+
+/* Film side only / print side only (the print side of a given negative, for reprints). */
+int orc_develop(const OracleSetup* s, const float* rgb, int32_t w, int32_t h, const float* counts, double* negative);
+int orc_print(const OracleSetup* s, const double* negative, int32_t w, int32_t h, uint16_t* out_rgba,
+              double* out_linear_rgb);
+
+/* The Gaussian of a w x h x 3 plane, per-channel sigma in pixels, in binary64 with the engine's
+ * branch rule (FIR below 3, Young-van Vliet above) */
+void orc_gaussian(const double* in, double* out, int32_t w, int32_t h, const double sigma[3]);
+
+/* The shared binary32 sampler (grain_sampler.h), for the bit-exactness tests. */
+void orc_poisson(const float* lam, float* counts, uint32_t n, uint32_t stream, uint32_t seed);
+void orc_lognormal(float* out, uint32_t n, float mean, float sd, uint32_t stream, uint32_t seed);
+void orc_philox(const uint32_t* ctr, const uint32_t* key, uint32_t* out, uint32_t n);
+float orc_logf(float x);
+float orc_expf(float x);
+float orc_cosf(float x);
+uint32_t orc_splitmix_next(uint64_t* state);
+
+#endif

@@ -1,0 +1,706 @@
+// sm_100a kernels of the render path (first generation: one pass per stage, fused where the reference
+// stores and reloads an intermediate plane with no change of value).
+//
+// Numerics follow the reference kernels (kernels/film.metal, print.metal, fx_blur.metal,
+// fx_grain.metal): binary32 arithmetic in the same bracketing; recursive-filter state in binary64
+// (the reference keeps it in double-float on its GPU and in double on its host copy); the grain
+// sampler from grain_sampler.h, which the host checker compiles too.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+#include "../grain_sampler.h"
+#include "../kernel_args.h"
+#include "launch.hpp"
+
+namespace spkb::dev {
+
+namespace {
+
+constexpr float kLog2Of10 = 3.321928094887362f;
+constexpr float kTiny = 1e-10f;
+
+__host__ __device__ inline uint32_t div_up(uint32_t a, uint32_t b) { return (a + b - 1) / b; }
+
+// ---------------------------------------------------------------------------------------------------
+// expose: reference kernels/film.metal:50-99 (Mitchell-Netravali B = C = 1/3) and :189-227.
+
+__device__ __forceinline__ float mitchell(float u) {
+    const float a = fabsf(u);
+    if (a < 1.0f) return (1.0f / 6.0f) * (7.0f * a * a * a - 12.0f * a * a + 16.0f / 3.0f);
+    if (a < 2.0f) return (1.0f / 6.0f) * ((-7.0f / 3.0f) * a * a * a + 12.0f * a * a - 20.0f * a + 32.0f / 3.0f);
+    return 0.0f;
+}
+
+__device__ __forceinline__ void mitchell_axis(float t, uint32_t L, int* idx, float* w) {
+    const float last = float(L - 1);
+    float u = t * last;
+    int base;
+    float frac;
+    if (u <= 0.0f) u = 0.0f;
+    if (u >= last) {
+        base = int(L) - 2;
+        frac = 1.0f;
+    } else {
+        base = int(floorf(u));
+        frac = u - float(base);
+    }
+    const int n = int(L);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        int i = base - 1 + k;
+        if (i < 0) i = -i;
+        if (i >= n) i = 2 * (n - 1) - i;
+        idx[k] = i;
+    }
+    w[0] = mitchell(frac + 1.0f);
+    w[1] = mitchell(frac);
+    w[2] = mitchell(frac - 1.0f);
+    w[3] = mitchell(frac - 2.0f);
+}
+
+__global__ void k_expose(const float* __restrict__ rgb, float* __restrict__ hout, const float* __restrict__ table,
+                         const __grid_constant__ ExposeArgs q) {
+    const uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gid >= q.n) return;
+    const float r = rgb[3 * size_t(gid)], g = rgb[3 * size_t(gid) + 1], b = rgb[3 * size_t(gid) + 2];
+    const float X = (q.a[0] * r + q.a[1] * g) + q.a[2] * b;
+    const float Y = (q.a[3] * r + q.a[4] * g) + q.a[5] * b;
+    const float Z = (q.a[6] * r + q.a[7] * g) + q.a[8] * b;
+    const float bs = (X + Y) + Z;
+    const float d = bs > 1e-10f ? bs : 1e-10f;
+    const float x = X / d, y = Y / d, o = 1.0f - x;
+    const float t0 = fminf(fmaxf(o * o, 0.0f), 1.0f);
+    const float t1 = fminf(fmaxf(y / (o > 1e-10f ? o : 1e-10f), 0.0f), 1.0f);
+    const float bp = isnan(bs) ? 0.0f : bs;
+    int ia[4], ib[4];
+    float wa[4], wb[4];
+    mitchell_axis(t0, q.L, ia, wa);
+    mitchell_axis(t1, q.L, ib, wb);
+    float s = 0.0f, a0 = 0.0f, a1 = 0.0f, a2 = 0.0f;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const float w = wa[i] * wb[j];
+            const float* t = table + 3 * (size_t(ia[i]) * q.L + size_t(ib[j]));
+            s += w;
+            a0 += w * __ldg(t);
+            a1 += w * __ldg(t + 1);
+            a2 += w * __ldg(t + 2);
+        }
+    }
+    if (s != 0.0f) {
+        a0 = a0 / s;
+        a1 = a1 / s;
+        a2 = a2 / s;
+    }
+    float h0 = bp * a0, h1 = bp * a1, h2 = bp * a2;
+    if (q.apply_gain) {
+        h0 = h0 * q.gain;
+        h1 = h1 * q.gain;
+        h2 = h2 * q.gain;
+    }
+    hout[3 * size_t(gid)] = h0;
+    hout[3 * size_t(gid) + 1] = h1;
+    hout[3 * size_t(gid) + 2] = h2;
+}
+
+// ---------------------------------------------------------------------------------------------------
+// FIR: reference kernels/fx_blur.metal:20-78: taps -r..r ascending, float accumulator from 0,
+// half-sample symmetric reflection at the edges.
+
+__device__ __forceinline__ int reflect_index(int i, int n) {
+    if (n <= 1) return 0;
+    const int period = 2 * n;
+    int m = i % period;
+    if (m < 0) m += period;
+    return m < n ? m : period - 1 - m;
+}
+
+__global__ void k_fir_v(const float* __restrict__ in, float* __restrict__ out, uint32_t w, uint32_t h,
+                        const __grid_constant__ FirTaps t) {
+    const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= w || y >= h) return;
+    const int r = t.r;
+    float a0 = 0.0f, a1 = 0.0f, a2 = 0.0f;
+    for (int i = -r; i <= r; ++i) {
+        const int yy = reflect_index(int(y) + i, int(h));
+        const float* p = in + 3 * (size_t(yy) * w + x);
+        const int k = i + r;
+        a0 += t.taps[0][k] * p[0];
+        a1 += t.taps[1][k] * p[1];
+        a2 += t.taps[2][k] * p[2];
+    }
+    float* o = out + 3 * (size_t(y) * w + x);
+    o[0] = a0;
+    o[1] = a1;
+    o[2] = a2;
+}
+
+__global__ void k_fir_h(const float* __restrict__ in, float* out, const float* acc, uint32_t w, uint32_t h,
+                        const __grid_constant__ FirTaps t, int mode, float w0, float w1, float w2) {
+    const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= w || y >= h) return;
+    const int r = t.r;
+    const float* row = in + 3 * size_t(y) * w;
+    float a0 = 0.0f, a1 = 0.0f, a2 = 0.0f;
+    for (int i = -r; i <= r; ++i) {
+        const int xx = reflect_index(int(x) + i, int(w));
+        const float* p = row + 3 * xx;
+        const int k = i + r;
+        a0 += t.taps[0][k] * p[0];
+        a1 += t.taps[1][k] * p[1];
+        a2 += t.taps[2][k] * p[2];
+    }
+    const size_t o = 3 * (size_t(y) * w + x);
+    if (mode == ACC_NONE) {
+        out[o] = a0;
+        out[o + 1] = a1;
+        out[o + 2] = a2;
+    } else if (mode == ACC_ZERO) {
+        out[o] = 0.0f + w0 * a0;
+        out[o + 1] = 0.0f + w1 * a1;
+        out[o + 2] = 0.0f + w2 * a2;
+    } else {
+        const float c0 = acc[o], c1 = acc[o + 1], c2 = acc[o + 2];
+        out[o] = c0 + w0 * a0;
+        out[o + 1] = c1 + w1 * a1;
+        out[o + 2] = c2 + w2 * a2;
+    }
+}
+
+// ---------------------------------------------------------------------------------------------------
+// Recursive Gaussian (Young-van Vliet, third order): reference kernels/fx_blur.metal:125-204.
+//   forward:  w[-1..-3] = x[0];  w[i] = B x[i] + B1 w[i-1] + B2 w[i-2] + B3 w[i-3];  u[i] = float(w[i])
+//   backward: y[n..n+2] = u[n-1]; y[i] = B u[i] + B1 y[i+1] + B2 y[i+2] + B3 y[i+3]
+// State in binary64; x, u and y stored as binary32.
+
+__device__ __forceinline__ void iir_line(const float* src, float* work, float* dst, const float* acc, size_t base,
+                                         size_t stride, uint32_t n, const IirCoefs& q, int c, int mode,
+                                         float wgt) {
+    const double B = q.B[c], B1 = q.B1[c], B2 = q.B2[c], B3 = q.B3[c];
+    double w1 = double(src[base]), w2 = w1, w3 = w1;
+    for (uint32_t i = 0; i < n; ++i) {
+        const size_t o = base + i * stride;
+        const double t = ((B * double(src[o]) + B1 * w1) + B2 * w2) + B3 * w3;
+        w3 = w2;
+        w2 = w1;
+        w1 = t;
+        work[o] = float(t);
+    }
+    double y1 = double(work[base + size_t(n - 1) * stride]), y2 = y1, y3 = y1;
+    for (uint32_t k = n; k-- > 0;) {
+        const size_t o = base + k * stride;
+        const double t = ((B * double(work[o]) + B1 * y1) + B2 * y2) + B3 * y3;
+        y3 = y2;
+        y2 = y1;
+        y1 = t;
+        const float y = float(t);
+        if (mode == ACC_NONE) dst[o] = y;
+        else if (mode == ACC_ZERO) dst[o] = 0.0f + wgt * y;
+        else dst[o] = acc[o] + wgt * y;
+    }
+}
+
+__global__ void k_iir_h(const float* __restrict__ in, float* out, uint32_t w, uint32_t h,
+                        const __grid_constant__ IirCoefs q) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 3u * h) return;
+    const uint32_t y = t / 3u, c = t % 3u;
+    const size_t base = 3 * size_t(y) * w + c;
+    if (((q.mask >> c) & 1u) == 0u) {
+        for (uint32_t x = 0; x < w; ++x) out[base + 3 * size_t(x)] = in[base + 3 * size_t(x)];
+        return;
+    }
+    iir_line(in, out, out, out, base, 3, w, q, int(c), ACC_NONE, 1.0f);
+}
+
+__global__ void k_iir_v(float* work, float* out, const float* acc, uint32_t w, uint32_t h,
+                        const __grid_constant__ IirCoefs q, int mode, float w0, float w1, float w2) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 3u * w) return;
+    const uint32_t c = t % 3u;
+    const size_t stride = 3 * size_t(w);
+    if (((q.mask >> c) & 1u) == 0u) {
+        for (uint32_t y = 0; y < h; ++y) out[t + y * stride] = work[t + y * stride];
+        return;
+    }
+    const float wgt = c == 0 ? w0 : (c == 1 ? w1 : w2);
+    iir_line(work, work, out, acc, t, stride, h, q, int(c), mode, wgt);
+}
+
+__global__ void k_lincomb(const float* x, const float* y, float* out, size_t n, float a0, float a1, float a2,
+                          float b0, float b1, float b2) {
+    const size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float a[3] = {a0, a1, a2}, b[3] = {b0, b1, b2};
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        const size_t o = 3 * i + c;
+        const float yv = y ? y[o] : 0.0f;
+        out[o] = a[c] * x[o] + b[c] * yv;
+    }
+}
+
+__global__ void k_copy(const float* __restrict__ x, float* __restrict__ out, size_t n) {
+    const size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    out[i] = x[i];
+}
+
+// ---------------------------------------------------------------------------------------------------
+// develop: log10 exposure (film.metal:242-246), density curves (:84-101, :249-261), grain draw
+// (fx_grain.metal:39-97, SUM and SIMPLE modes).
+
+__device__ __forceinline__ float curve_lookup(const float* __restrict__ x, const float* __restrict__ inv,
+                                              const float* __restrict__ y, uint32_t K, float v) {
+    if (v <= __ldg(x)) return __ldg(y);
+    if (v >= __ldg(x + K - 1)) return __ldg(y + K - 1);
+    uint32_t lo = 0, hi = K;
+    while (lo < hi) {
+        const uint32_t mid = lo + (hi - lo) / 2;
+        if (__ldg(x + mid) <= v) lo = mid + 1;
+        else hi = mid;
+    }
+    const uint32_t l = lo == 0 ? 0 : lo - 1;
+    const float t = (v - __ldg(x + l)) * __ldg(inv + l);
+    const float y0 = __ldg(y + l);
+    return y0 + t * (__ldg(y + l + 1) - y0);
+}
+
+// spk_sublayer_draw (grain_sampler.h) with the count kept for the test hook: the same operations.
+__device__ __forceinline__ float grain_draw(float d, float D, float n, float u, uint32_t pixel, uint32_t stream,
+                                            uint32_t seed, float* count_slot) {
+    float sat;
+    const float lam = spk_sublayer_lambda(d, D, n, u, &sat);
+    const float k = spk_poisson(lam, pixel, stream, seed);
+    if (count_slot) *count_slot = k;
+    return SPK_MUL(k, SPK_MUL(SPK_DIV(D, n), sat));
+}
+
+__global__ void k_develop(const float* __restrict__ exposure, float* __restrict__ out, uint32_t w, uint32_t h,
+                          const __grid_constant__ DevelopArgs q) {
+    const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= w || y >= h) return;
+    const uint32_t pixel = y * q.width + x;
+    const size_t o = 3 * (size_t(y) * w + x);
+    for (uint32_t c = 0; c < 3; ++c) {
+        const float L = log10f(fmaxf(exposure[o + c], 0.0f) + 1e-10f);
+        const float D = curve_lookup(q.cx, q.cinv, q.cy + size_t(c) * q.K, q.K, L);
+        if (!q.grain) {
+            out[o + c] = D;
+            continue;
+        }
+        if (q.mode == 2) {  // SIMPLE
+            const float d = D + q.dmin_c[c];
+            float G = 0.0f;
+            for (uint32_t l = 0; l < q.n_sub; ++l)
+                G = G + grain_draw(d, q.sat_d[c], q.count[c], q.uniformity[c], pixel, SPK_STREAM_GRAIN(c, l), q.seed,
+                                   q.counts_out && l < 3 ? q.counts_out + size_t(pixel) * 9 + c * 3 + l : nullptr);
+            out[o + c] = G * q.inv_n_sub + (-q.dmin_c[c]);
+            continue;
+        }
+        const float v = q.positive ? -D : D;
+        const uint32_t K = q.gK;
+        float dl[3];
+        if (v <= __ldg(q.axis + c)) {
+            for (uint32_t l = 0; l < 3u; ++l) dl[l] = __ldg(q.layers + l * 3u + c);
+        } else if (v >= __ldg(q.axis + 3u * (K - 1u) + c)) {
+            for (uint32_t l = 0; l < 3u; ++l) dl[l] = __ldg(q.layers + ((K - 1u) * 3u + l) * 3u + c);
+        } else {
+            uint32_t lo = 0, hi = K;
+            while (lo < hi) {
+                const uint32_t mid = lo + (hi - lo) / 2u;
+                if (__ldg(q.axis + 3u * mid + c) <= v) lo = mid + 1u;
+                else hi = mid;
+            }
+            // a finite v above axis[0] gives lo >= 1; lo == 0 (a NaN v) stays in bounds and yields NaN
+            const uint32_t j = lo == 0u ? 0u : lo - 1u;
+            const float t = (v - __ldg(q.axis + 3u * j + c)) * __ldg(q.ginv + 3u * j + c);
+            for (uint32_t l = 0; l < 3u; ++l) {
+                const float y0 = __ldg(q.layers + (j * 3u + l) * 3u + c);
+                const float y1 = __ldg(q.layers + ((j + 1u) * 3u + l) * 3u + c);
+                dl[l] = y0 + t * (y1 - y0);
+            }
+        }
+        float val[3];
+        for (uint32_t l = 0; l < 3u; ++l) {
+            const uint32_t lc = l * 3u + c;
+            val[l] = grain_draw(dl[l] + q.dmin_l[lc], q.sat_d[lc], q.count[lc], q.uniformity[c], pixel,
+                                SPK_STREAM_GRAIN(c, l), q.seed,
+                                q.counts_out ? q.counts_out + size_t(pixel) * 9 + c * 3 + l : nullptr);
+        }
+        float G = ((0.0f + val[0]) + val[1]) + val[2];
+        if (q.shift) G = G * 1.0f + (-q.dmin_c[c]);
+        out[o + c] = G;
+    }
+}
+
+// ---------------------------------------------------------------------------------------------------
+// print: reference kernels/print.metal:29-127 (helpers) and :165-317 (enlarger, gain, paper, scan,
+// matrix, gamut), one pixel per thread, the intermediate planes kept in registers.
+
+__device__ __forceinline__ float sgnf(float v) { return v > 0.0f ? 1.0f : (v < 0.0f ? -1.0f : 0.0f); }
+
+__device__ __forceinline__ float knee(float d, float tau, float lim, float p) {
+    if (d <= tau) return d;
+    const float x = (d - tau) / (lim - tau);
+    return tau + (lim - tau) * (x / powf(1.0f + powf(x, p), 1.0f / p));
+}
+
+__device__ __forceinline__ float post_adapt(float v, float f_l) {
+    const float f = powf((f_l * fabsf(v)) / 100.0f, 0.42f);
+    return ((400.0f * sgnf(v)) * f) / (27.13f + f) + 0.1f;
+}
+
+__device__ __forceinline__ void mat_apply(const float* m, float x, float y, float z, float& a, float& b, float& c) {
+    a = (m[0] * x + m[1] * y) + m[2] * z;
+    b = (m[3] * x + m[4] * y) + m[5] * z;
+    c = (m[6] * x + m[7] * y) + m[8] * z;
+}
+
+__device__ __forceinline__ void spectral(const SpectralTables& a, float d0, float d1, float d2, float& r0, float& r1,
+                                         float& r2) {
+    r0 = r1 = r2 = 0.0f;
+#pragma unroll 9
+    for (int l = 0; l < SPKB_NL; ++l) {
+        const float D = ((d0 * a.eps[3 * l] + d1 * a.eps[3 * l + 1]) + d2 * a.eps[3 * l + 2]) + a.beta[l];
+        const float T = exp2f(-D * kLog2Of10);
+        r0 += T * a.wt[3 * l];
+        r1 += T * a.wt[3 * l + 1];
+        r2 += T * a.wt[3 * l + 2];
+    }
+}
+
+__device__ __forceinline__ float paper_lookup(const float* __restrict__ tab, uint32_t K, uint32_t c, float v) {
+    if (isnan(v)) return v;
+    const float* x = tab;
+    const float* r = tab + K;
+    const float* y = tab + 2 * K;
+    if (v <= __ldg(x)) return __ldg(y + c);
+    if (v >= __ldg(x + K - 1)) return __ldg(y + 3 * (K - 1) + c);
+    uint32_t lo = 0, hi = K;
+    while (lo < hi) {
+        const uint32_t mid = lo + (hi - lo) / 2;
+        if (__ldg(x + mid) <= v) lo = mid + 1;
+        else hi = mid;
+    }
+    const uint32_t j = lo - 1;
+    const float y0 = __ldg(y + 3 * j + c);
+    return y0 + ((v - __ldg(x + j)) * __ldg(r + j)) * (__ldg(y + 3 * (j + 1) + c) - y0);
+}
+
+__device__ void gamut(const PrintArgs& pa, float& r, float& g, float& b) {
+    const Cam16Args& q = pa.cam;
+    // per-pixel constants from the k numbers (print.metal:53-64)
+    const float cz = q.c * q.z;
+    const float inv_cz = 1.0f / cz;
+    const float f_l_qrt = powf(q.f_l, 0.25f);
+    const float chroma_k = powf(1.64f - powf(0.29f, q.n), 0.73f);
+    const float hundred_over_f_l = 100.0f / q.f_l;
+    float X, Y, Z;
+    mat_apply(q.m_to_xyz, r, g, b, X, Y, Z);
+    // forward (print.metal:66-86)
+    float R16, G16, B16;
+    mat_apply(q.m16, 100.0f * X, 100.0f * Y, 100.0f * Z, R16, G16, B16);
+    const float ra = post_adapt(q.d_rgb[0] * R16, q.f_l);
+    const float ga = post_adapt(q.d_rgb[1] * G16, q.f_l);
+    const float ba = post_adapt(q.d_rgb[2] * B16, q.f_l);
+    const float a = (ra - (12.0f * ga) / 11.0f) + ba / 11.0f;
+    const float bb = ((ra + ga) - 2.0f * ba) / 9.0f;
+    const float h = atan2f(bb, a);
+    const float et = 0.25f * (cosf(h + 2.0f) + 3.8f);
+    const float A = (((2.0f * ra + ga) + ba / 20.0f) - 0.305f) * q.n_bb;
+    const float ratio = A / q.a_w;
+    const float J = (100.0f * sgnf(ratio)) * powf(fabsf(ratio), cz);
+    const float den = (ra + ga) + (21.0f * ba) / 20.0f;
+    const float t = den != 0.0f ? (((((50000.0f / 13.0f) * q.n_c) * q.n_cb) * et) * sqrtf(a * a + bb * bb)) / den : 0.0f;
+    const float C = t > 0.0f ? (powf(t, 0.9f) * sqrtf(fabsf(J) / 100.0f)) * chroma_k : 0.0f;
+    const float M = C * f_l_qrt;
+    const float Mp = logf(1.0f + 0.0228f * M) / 0.0228f;
+    float Jp = (1.7f * J) / (1.0f + 0.007f * J);
+    // lightness knee
+    if (q.lc_active != 0u) {
+        float Ln = Jp / q.j_white;
+        if (Ln > q.lc[0]) {
+            Ln = knee(Ln, q.lc[0], q.lc[1], q.lc[2]);
+            Jp = Ln * q.j_white;
+        }
+    }
+    // C_max(J', h), bilinear with hue wrap
+    const float Jc = fminf(fmaxf(Jp, q.j_first), q.j_last);
+    const float u = ((Jc - q.j_first) / (q.j_last - q.j_first)) * float(q.rows - 1);
+    int l0 = int(floorf(u));
+    l0 = l0 < 0 ? 0 : (l0 > int(q.rows) - 2 ? int(q.rows) - 2 : l0);
+    const float fl = u - float(l0);
+    const float v = (h - q.h_first) / q.h_step;
+    const float vf = floorf(v);
+    const int cols = int(q.cols);
+    int h0 = int(vf) % cols;
+    if (h0 < 0) h0 += cols;
+    const int h1 = h0 == cols - 1 ? 0 : h0 + 1;
+    const float fh = v - vf;
+    const float t00 = __ldg(pa.cmax + l0 * cols + h0), t01 = __ldg(pa.cmax + l0 * cols + h1);
+    const float t10 = __ldg(pa.cmax + (l0 + 1) * cols + h0), t11 = __ldg(pa.cmax + (l0 + 1) * cols + h1);
+    const float cm = (1.0f - fl) * ((1.0f - fh) * t00 + fh * t01) + fl * ((1.0f - fh) * t10 + fh * t11);
+    const float cs = fmaxf(cm, 1e-9f);
+    float dch = Mp / cs;
+    if (dch > 0.0f) dch = knee(dch, q.knee[0], q.knee[1], q.knee[2]);
+    const float Mn = dch * cs;
+    // guarded inverse (print.metal:88-127)
+    const float Mi = (expf(0.0228f * Mn) - 1.0f) / 0.0228f;
+    const float Ji = Jp / (1.7f - 0.007f * Jp);
+    const float Ci = Mi / f_l_qrt;
+    const float Ai = (q.a_w * sgnf(Ji)) * powf(fabsf(Ji / 100.0f), inv_cz);
+    const float sq = sqrtf(fabsf(Ji) / 100.0f);
+    const float ti = (sq > 0.0f && Ci > 0.0f) ? powf(Ci / (sq * chroma_k), 1.0f / 0.9f) : 0.0f;
+    const float eti = 0.25f * (cosf(h + 2.0f) + 3.8f);
+    const float p2 = Ai / q.n_bb + 0.305f;
+    const float p3 = 21.0f / 20.0f;
+    float ai = 0.0f, bi = 0.0f;
+    if (ti != 0.0f) {
+        const float p1 = ((((50000.0f / 13.0f) * q.n_c) * q.n_cb) * eti) / ti;
+        const float sh = sinf(h), ch = cosf(h);
+        if (fabsf(sh) >= fabsf(ch)) {
+            const float p4 = p1 / sh;
+            bi = ((p2 * (2.0f + p3)) * (460.0f / 1403.0f)) /
+                 (((p4 + ((2.0f + p3) * (220.0f / 1403.0f)) * (ch / sh)) - 27.0f / 1403.0f) + p3 * (6300.0f / 1403.0f));
+            ai = (bi * ch) / sh;
+        } else {
+            const float p5 = p1 / ch;
+            ai = ((p2 * (2.0f + p3)) * (460.0f / 1403.0f)) /
+                 ((p5 + (2.0f + p3) * (220.0f / 1403.0f)) - (27.0f / 1403.0f - p3 * (6300.0f / 1403.0f)) * (sh / ch));
+            bi = (ai * sh) / ch;
+        }
+    }
+    const float xa[3] = {((460.0f * p2 + 451.0f * ai) + 288.0f * bi) / 1403.0f,
+                         ((460.0f * p2 - 891.0f * ai) - 261.0f * bi) / 1403.0f,
+                         ((460.0f * p2 - 220.0f * ai) - 6300.0f * bi) / 1403.0f};
+    float rc[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        const float vv = xa[i] - 0.1f;
+        const float av = fabsf(vv);
+        const float beta = av >= 400.0f ? 0.0f : (27.13f * av) / (400.0f - av);
+        rc[i] = ((hundred_over_f_l * sgnf(vv)) * powf(beta, 1.0f / 0.42f)) / q.d_rgb[i];
+    }
+    float x100, y100, z100;
+    mat_apply(q.m16_inv, rc[0], rc[1], rc[2], x100, y100, z100);
+    mat_apply(q.m_to_rgb, x100 / 100.0f, y100 / 100.0f, z100 / 100.0f, r, g, b);
+}
+
+__global__ void k_print(const float* __restrict__ neg, float* __restrict__ rgb, const __grid_constant__ PrintArgs a) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    const size_t o = 3 * size_t(i);
+    float d0 = neg[o], d1 = neg[o + 1], d2 = neg[o + 2];
+    if (a.printed) {
+        float r0, r1, r2;
+        spectral(a.enl, d0, d1, d2, r0, r1, r2);
+        float l0 = log10f(fmaxf(r0 * a.g[0] + a.o[0], 0.0f) + kTiny);
+        float l1 = log10f(fmaxf(r1 * a.g[1] + a.o[1], 0.0f) + kTiny);
+        float l2 = log10f(fmaxf(r2 * a.g[2] + a.o[2], 0.0f) + kTiny);
+        l0 = log10f(fmaxf(exp2f(l0 * kLog2Of10) * a.k_gain, 0.0f) + kTiny);
+        l1 = log10f(fmaxf(exp2f(l1 * kLog2Of10) * a.k_gain, 0.0f) + kTiny);
+        l2 = log10f(fmaxf(exp2f(l2 * kLog2Of10) * a.k_gain, 0.0f) + kTiny);
+        d0 = paper_lookup(a.paper, a.paper_K, 0, l0);
+        d1 = paper_lookup(a.paper, a.paper_K, 1, l1);
+        d2 = paper_lookup(a.paper, a.paper_K, 2, l2);
+    }
+    float X, Y, Z;
+    spectral(a.scan, d0, d1, d2, X, Y, Z);
+    X = fmaxf(X, 0.0f) + kTiny;
+    Y = fmaxf(Y, 0.0f) + kTiny;
+    Z = fmaxf(Z, 0.0f) + kTiny;
+    float r, g, b;
+    mat_apply(a.to_rgb, X, Y, Z, r, g, b);
+    gamut(a, r, g, b);
+    rgb[o] = r;
+    rgb[o + 1] = g;
+    rgb[o + 2] = b;
+}
+
+// ---------------------------------------------------------------------------------------------------
+// encode: reference kernels/print.metal:129-156 and :350-366.
+
+__device__ __forceinline__ float spowf(float v, float p) { return sgnf(v) * powf(fabsf(v), p); }
+
+__device__ __forceinline__ float cctf_encode(float v, uint32_t mode) {
+    switch (mode) {
+        case 0: return v <= 0.0031308f ? 12.92f * v : 1.055f * spowf(v, 0.41666666666666669f) - 0.055f;
+        case 1: return v < 0.001953125f ? 16.0f * v : powf(v, 0.55555555555555558f);
+        case 2: return powf(v, 0.45470692717584371f);
+        case 3: return v < 0.018f ? 4.5f * v : 1.099f * spowf(v, 0.45f) - 0.099f;
+        default: return v;
+    }
+}
+
+__device__ __forceinline__ uint16_t encode16(float v) {
+    if (isnan(v)) return 0;
+    const float c = fminf(fmaxf(v, 0.0f), 1.0f);
+    return uint16_t(floorf(c * 65535.0f + 0.5f));
+}
+
+__global__ void k_encode(const float* __restrict__ rgb, const float* __restrict__ gpl, uint16_t* __restrict__ out,
+                         uint32_t w, uint32_t h, const __grid_constant__ EncodeArgs e) {
+    const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= w || y >= h) return;
+    const size_t i = 3 * (size_t(y) * w + x);
+    float v0 = rgb[i], v1 = rgb[i + 1], v2 = rgb[i + 2];
+    if (e.unsharp) {
+        v0 = e.lincomb_a * v0 + e.lincomb_b * gpl[i];
+        v1 = e.lincomb_a * v1 + e.lincomb_b * gpl[i + 1];
+        v2 = e.lincomb_a * v2 + e.lincomb_b * gpl[i + 2];
+    }
+    if (e.cctf_active) {
+        float m0, m1, m2;
+        mat_apply(e.m_nid, v0, v1, v2, m0, m1, m2);
+        v0 = cctf_encode(m0, e.cctf_mode);
+        v1 = cctf_encode(m1, e.cctf_mode);
+        v2 = cctf_encode(m2, e.cctf_mode);
+    }
+    ushort4 p;
+    p.x = encode16(v0);
+    p.y = encode16(v1);
+    p.z = encode16(v2);
+    p.w = 65535;
+    reinterpret_cast<ushort4*>(out)[size_t(y) * e.stride + x] = p;
+}
+
+// ---------------------------------------------------------------------------------------------------
+// source copy: channels 3 or 4 -> interleaved RGB, non-finite -> 0 (reference src/session/session.cpp:164-168)
+
+__global__ void k_source(const float* __restrict__ raw, float* __restrict__ out, size_t n, uint32_t channels) {
+    const size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        const float v = raw[i * channels + c];
+        out[3 * i + c] = isfinite(v) ? v : 0.0f;
+    }
+}
+
+// L2 flush: write a buffer larger than the L2 cache
+__global__ void k_fill(uint4* p, size_t n, uint32_t v) {
+    for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x)
+        p[i] = make_uint4(v, v, v, v);
+}
+
+// ---------------------------------------------------------------------------------------------------
+// test kernels
+
+__global__ void k_sampler_poisson(const float* lam, float* out, uint32_t n, uint32_t stream, uint32_t seed) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    out[i] = spk_poisson(lam[i], i, stream, seed);
+}
+
+__global__ void k_sampler_lognormal(float* out, uint32_t n, float mean, float sd, uint32_t stream, uint32_t seed) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    out[i] = spk_lognormal(mean, sd, i, stream, seed);
+}
+
+__global__ void k_philox(const uint32_t* ctr, const uint32_t* key, uint32_t* out, uint32_t n) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    spk_u4 c;
+    c.x = ctr[4 * i];
+    c.y = ctr[4 * i + 1];
+    c.z = ctr[4 * i + 2];
+    c.w = ctr[4 * i + 3];
+    const spk_u4 r = spk_philox(c, key[2 * i], key[2 * i + 1]);
+    out[4 * i] = r.x;
+    out[4 * i + 1] = r.y;
+    out[4 * i + 2] = r.z;
+    out[4 * i + 3] = r.w;
+}
+
+}  // namespace
+
+// ---- launchers ------------------------------------------------------------------------------------
+
+void expose(const float* rgb, float* h, const float* table, const ExposeArgs& a, cudaStream_t s) {
+    if (a.n == 0) return;
+    k_expose<<<div_up(a.n, 256), 256, 0, s>>>(rgb, h, table, a);
+}
+
+void fir_v(const float* in, float* out, uint32_t w, uint32_t h, const FirTaps& t, cudaStream_t s) {
+    const dim3 b(32, 8), g(div_up(w, 32), div_up(h, 8));
+    k_fir_v<<<g, b, 0, s>>>(in, out, w, h, t);
+}
+
+void fir_h(const float* in, float* out, const float* acc, uint32_t w, uint32_t h, const FirTaps& t, int mode,
+           const float weight[3], cudaStream_t s) {
+    const dim3 b(32, 8), g(div_up(w, 32), div_up(h, 8));
+    k_fir_h<<<g, b, 0, s>>>(in, out, acc, w, h, t, mode, weight[0], weight[1], weight[2]);
+}
+
+void iir_h(const float* in, float* out, uint32_t w, uint32_t h, const IirCoefs& c, cudaStream_t s) {
+    k_iir_h<<<div_up(3 * h, 64), 64, 0, s>>>(in, out, w, h, c);
+}
+
+void iir_v(float* work, float* out, const float* acc, uint32_t w, uint32_t h, const IirCoefs& c, int mode,
+           const float weight[3], cudaStream_t s) {
+    k_iir_v<<<div_up(3 * w, 64), 64, 0, s>>>(work, out, acc, w, h, c, mode, weight[0], weight[1], weight[2]);
+}
+
+void lincomb(const float* x, const float* y, float* out, size_t pixels, const float a[3], const float b[3],
+             cudaStream_t s) {
+    if (pixels == 0) return;
+    k_lincomb<<<unsigned((pixels + 255) / 256), 256, 0, s>>>(x, y, out, pixels, a[0], a[1], a[2], b[0], b[1], b[2]);
+}
+
+void copy(const float* x, float* out, size_t pixels, cudaStream_t s) {
+    const size_t n = 3 * pixels;
+    if (n == 0) return;
+    k_copy<<<unsigned((n + 255) / 256), 256, 0, s>>>(x, out, n);
+}
+
+void develop(const float* exposure, float* out, const DevelopArgs& a, uint32_t w, uint32_t h, cudaStream_t s) {
+    const dim3 b(32, 4), g(div_up(w, 32), div_up(h, 4));
+    k_develop<<<g, b, 0, s>>>(exposure, out, w, h, a);
+}
+
+void print(const float* neg, float* rgb, const PrintArgs& a, cudaStream_t s) {
+    if (a.n == 0) return;
+    k_print<<<div_up(a.n, 128), 128, 0, s>>>(neg, rgb, a);
+}
+
+void encode(const float* rgb, const float* g, uint16_t* out, uint32_t w, uint32_t h, const EncodeArgs& e,
+            cudaStream_t s) {
+    const dim3 b(32, 8), gr(div_up(w, 32), div_up(h, 8));
+    k_encode<<<gr, b, 0, s>>>(rgb, g, out, w, h, e);
+}
+
+void source_copy(const float* raw, float* out, size_t pixels, uint32_t channels, cudaStream_t s) {
+    if (pixels == 0) return;
+    k_source<<<unsigned((pixels + 255) / 256), 256, 0, s>>>(raw, out, pixels, channels);
+}
+
+void fill(void* p, size_t bytes, uint32_t v, cudaStream_t s) {
+    k_fill<<<148 * 8, 256, 0, s>>>(static_cast<uint4*>(p), bytes / 16, v);
+}
+
+void sampler_poisson(const float* lam, float* out, uint32_t n, uint32_t stream, uint32_t seed, cudaStream_t s) {
+    if (n == 0) return;
+    k_sampler_poisson<<<div_up(n, 128), 128, 0, s>>>(lam, out, n, stream, seed);
+}
+
+void sampler_lognormal(float* out, uint32_t n, float mean, float stddev, uint32_t stream, uint32_t seed,
+                       cudaStream_t s) {
+    if (n == 0) return;
+    k_sampler_lognormal<<<div_up(n, 128), 128, 0, s>>>(out, n, mean, stddev, stream, seed);
+}
+
+void philox_blocks(const uint32_t* ctr, const uint32_t* key, uint32_t* out, uint32_t n, cudaStream_t s) {
+    if (n == 0) return;
+    k_philox<<<div_up(n, 128), 128, 0, s>>>(ctr, key, out, n);
+}
+
+}  // namespace spkb::dev

@@ -1,0 +1,53 @@
+// Host-callable launchers of the sm_100a render kernels. Planes are interleaved binary32 RGB
+// (12 bytes per pixel, row-major, top row first) in device memory; every launcher enqueues on the
+// given stream and returns without synchronising.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../kernel_args.h"
+
+namespace spkb::dev {
+
+// RGB -> film exposure H (Mitchell bicubic of the spectral table), times the compensation gain.
+void expose(const float* rgb, float* h, const float* table, const ExposeArgs& a, cudaStream_t s);
+
+// Separable FIR: vertical pass in -> out (no accumulation).
+void fir_v(const float* in, float* out, uint32_t w, uint32_t h, const FirTaps& t, cudaStream_t s);
+// Horizontal pass with the accumulation of the last pass (ACC_NONE / ZERO / PLANE with weights).
+void fir_h(const float* in, float* out, const float* acc, uint32_t w, uint32_t h, const FirTaps& t, int mode,
+           const float weight[3], cudaStream_t s);
+// Recursive Gaussian, horizontal: in -> out (forward then backward along each row).
+void iir_h(const float* in, float* out, uint32_t w, uint32_t h, const IirCoefs& c, cudaStream_t s);
+// Recursive Gaussian, vertical: work holds the horizontal result and is overwritten with the forward
+// pass; out := y, 0 + w y or acc + w y.
+void iir_v(float* work, float* out, const float* acc, uint32_t w, uint32_t h, const IirCoefs& c, int mode,
+           const float weight[3], cudaStream_t s);
+// out = a x + b y per channel (y reads as 0 when y == nullptr).
+void lincomb(const float* x, const float* y, float* out, size_t pixels, const float a[3], const float b[3],
+             cudaStream_t s);
+void copy(const float* x, float* out, size_t pixels, cudaStream_t s);
+
+// log10 exposure -> density curves -> grain draw (grain mode) or density (no grain).
+void develop(const float* exposure, float* out, const DevelopArgs& a, uint32_t w, uint32_t h, cudaStream_t s);
+
+// negative density -> linear output RGB (enlarger, gain, paper, scan, XYZ -> RGB, CAM16 gamut).
+void print(const float* neg, float* rgb, const PrintArgs& a, cudaStream_t s);
+
+// (optional unsharp combine with g) -> transfer function -> RGBA16 with row pitch e.stride.
+void encode(const float* rgb, const float* g, uint16_t* out, uint32_t w, uint32_t h, const EncodeArgs& e,
+            cudaStream_t s);
+
+// host frame (channels 3 or 4, already on the device) -> interleaved RGB plane, non-finite -> 0
+void source_copy(const float* raw, float* out, size_t pixels, uint32_t channels, cudaStream_t s);
+// write `bytes` (a multiple of 16) with a constant word (the L2 flush between timed steps)
+void fill(void* p, size_t bytes, uint32_t v, cudaStream_t s);
+
+// Test entry points: the sampler over an array of lambdas (counts as floats) and raw Philox blocks.
+void sampler_poisson(const float* lam, float* out, uint32_t n, uint32_t stream, uint32_t seed, cudaStream_t s);
+void sampler_lognormal(float* out, uint32_t n, float mean, float stddev, uint32_t stream, uint32_t seed,
+                       cudaStream_t s);
+void philox_blocks(const uint32_t* ctr, const uint32_t* key, uint32_t* out, uint32_t n, cudaStream_t s);
+
+}  // namespace spkb::dev

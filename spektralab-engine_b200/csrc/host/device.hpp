@@ -1,0 +1,93 @@
+// Device memory and streams of the B200 engine.
+//
+//   Pool        per engine: device scratch buffers reused by the rule "smallest free buffer of size in
+//               [b, 2b]" (the reference's scratch pool rule, src/gpu/gpu.mm:125-161). A render returns its
+//               scratch only after its stream has completed, so reuse never races with a kernel.
+//   DevBuffer   a handle; dropping the last copy returns the memory to its pool (or frees it).
+//   Plane       interleaved binary32 RGB in device memory.
+//   OutputImage a rendered RGBA16 image: a device copy and a pinned host copy, drawn from a process-wide
+//               cache so that a result outlives its session and engine and pinning is paid once.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+
+namespace spkb {
+
+void cuda_check(cudaError_t e, const char* what);  // throws SPK_ERR_GPU
+
+struct PoolState;
+
+class DevBuffer {
+public:
+    DevBuffer() = default;
+    explicit operator bool() const { return p_ != nullptr; }
+    void* ptr() const;
+    size_t size() const;
+    template <class T>
+    T* as() const { return static_cast<T*>(ptr()); }
+
+private:
+    friend class Pool;
+    struct Impl;
+    std::shared_ptr<Impl> p_;
+};
+
+class Pool {
+public:
+    Pool();
+    DevBuffer acquire(size_t bytes);          // device memory, contents undefined
+    DevBuffer persistent(size_t bytes);       // never pooled: freed when the last handle drops
+    size_t trim();                            // frees every idle buffer; returns bytes freed
+    size_t live_bytes() const;
+    size_t free_bytes() const;
+
+private:
+    std::shared_ptr<PoolState> s_;
+};
+
+struct Plane {
+    DevBuffer buf;
+    uint32_t w = 0, h = 0;
+    explicit operator bool() const { return static_cast<bool>(buf); }
+    float* data() const { return buf.as<float>(); }
+    size_t pixels() const { return size_t(w) * h; }
+    size_t bytes() const { return pixels() * 3 * sizeof(float); }
+};
+
+inline Plane make_plane(Pool& pool, uint32_t w, uint32_t h) {
+    Plane p;
+    p.w = w;
+    p.h = h;
+    p.buf = pool.acquire(size_t(w) * h * 3 * sizeof(float));
+    return p;
+}
+
+// The result image behind spk_result.texture.
+struct OutputImage {
+    uint16_t* dev = nullptr;   // RGBA16, row pitch stride_px pixels
+    uint16_t* host = nullptr;  // pinned
+    size_t bytes = 0;
+    uint32_t width = 0, height = 0, stride_px = 0;
+    int device = 0;
+};
+constexpr uint32_t kOutputRowAlignPx = 32;  // 256-byte rows
+OutputImage* output_acquire(int device, uint32_t w, uint32_t h);
+void output_release(OutputImage* img);
+size_t output_trim();
+
+// Pinned host staging for host inputs (spk_open's frame upload), process-wide and reused.
+struct PinnedBuffer {
+    void* p = nullptr;
+    size_t bytes = 0;
+};
+PinnedBuffer pinned_acquire(size_t bytes);
+void pinned_release(PinnedBuffer b);
+
+}  // namespace spkb

@@ -1,0 +1,1138 @@
+// Engine, session and every exported entry point of the B200 build.
+//
+// Behaviour mirrors the reference's session layer where the render path needs it
+// (src/session/session.cpp: open :121-197, set_params :216-259, render/reprint :405-450, seeds
+// :327-345; src/abi/abi.cpp: status mapping :40-65, result zeroing and scrubbing :84-92, :293-308).
+// The device work is this build's own: one CUDA stream and one scratch pool per session, the source
+// frame and the per-tier negatives resident in device memory, the result copied once to pinned host
+// memory.
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <set>
+
+#include "../cuda/launch.hpp"
+#include "device.hpp"
+#include "render.hpp"
+#include "spektralab.h"
+#include "spektralab_b200.h"
+#include "status.hpp"
+
+namespace spkb {
+
+// ---- last error ----------------------------------------------------------------------------------
+namespace last_error {
+namespace {
+thread_local std::string slot;
+}
+void set(const std::string& m) { slot = m; }
+void clear() { slot.clear(); }
+const char* get() { return slot.c_str(); }
+}  // namespace last_error
+
+namespace {
+
+std::atomic<uint64_t> g_next_id{1};
+constexpr uint64_t kMaxPixels = 151301008ull;
+
+// splitmix64 seed sequence (reference src/fx/rng.hpp:17-41): one per pipeline, reset at every build.
+struct SeedSequence {
+    uint64_t state = 0x243F6A8885A308D3ull;
+    uint32_t next() {
+        state += 0x9E3779B97F4A7C15ull;
+        uint64_t z = state;
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        z = z ^ (z >> 31);
+        return uint32_t(z);
+    }
+};
+constexpr uint32_t kNoGrainFilmSeed = 0x5EEDu;
+
+enum class Tier { Live = 0, Preview = 1, Full = 2 };
+std::optional<Tier> parse_tier(const char* s) {
+    if (!s) return std::nullopt;
+    const std::string t(s);
+    if (t == "live") return Tier::Live;
+    if (t == "preview") return Tier::Preview;
+    if (t == "full") return Tier::Full;
+    return std::nullopt;
+}
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        cudaGetDevice(&prev);
+        if (prev != dev) cuda_check(cudaSetDevice(dev), "cudaSetDevice");
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        cudaGetDevice(&cur);
+        if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+}  // namespace
+
+class Session;
+
+class Engine {
+public:
+    int device = 0;
+    std::shared_ptr<Resources> res;
+    Cam16Cache cam16;
+    std::mutex m;
+    std::set<Session*> sessions;
+    std::string capabilities, memory_report;
+};
+
+struct TierState {
+    Plane negative;
+    double pitch_um = 0.0;
+};
+
+class Session {
+public:
+    Engine* engine = nullptr;
+    std::string id;
+    std::mutex m;
+    cudaStream_t stream = nullptr;
+    Pool pool;
+    bool product_defaults = false;
+    Plane source;
+    ParamSet params;
+    std::shared_ptr<const Profile> film, print;
+    Pipeline pipe;
+    LiveParams live;
+    SeedSequence seeds;
+    TierState tiers[3];
+    std::optional<HalationOverride> hal;
+    std::atomic<bool> cancel{false};
+    std::string progress_id;
+    std::atomic<uint32_t> nodes_done{0};
+    uint32_t nodes_total = 0;
+    bool done = false;
+
+    ~Session() {
+        if (stream) cudaStreamDestroy(stream);
+    }
+
+    void digest(ParamSet& p, const Profile& f) const {
+        if (auto pack = engine->res->neutral_filters(p.s(P::print_stock), p.s(P::enlarger_illuminant), f)) {
+            p.set(P::c_filter_neutral, (*pack)[0]);
+            p.set(P::m_filter_neutral, (*pack)[1]);
+            p.set(P::y_filter_neutral, (*pack)[2]);
+        }
+    }
+
+    Pipeline build(const ParamSet& p, std::shared_ptr<const Profile> f, std::shared_ptr<const Profile> pr) {
+        check_supported(p);
+        Pipeline pl;
+        auto fs = build_film_setup(p, f, *engine->res);
+        pl.print = build_print_setup(p, *fs, pr, *engine->res, engine->cam16, !product_defaults);
+        pl.film = fs;
+        upload_tables(pool, stream, pl);
+        return pl;
+    }
+
+    // tier source: the frame itself when its long edge fits the tier (reference src/session/tiers.cpp:55-64)
+    void check_tier(Tier t) const {
+        const uint32_t M = std::max(source.w, source.h);
+        uint32_t L = 0;
+        if (t == Tier::Live) L = uint32_t(params.i(P::preview_long_edge));
+        if (t == Tier::Preview) L = 3400;
+        if (L != 0 && M > L)
+            fail_user("tier '" + std::string(t == Tier::Live ? "live" : "preview") +
+                      "' needs a downscale of this frame, which is outside this B200 build's render path; "
+                      "render the 'full' tier");
+    }
+
+    double pitch_um() const {
+        return 1000.0 * params.f(P::film_format_mm) / double(std::max(source.w, source.h));
+    }
+
+    void node() {
+        if (cancel.load(std::memory_order_relaxed)) fail_cancelled();
+        nodes_done.fetch_add(1, std::memory_order_relaxed);
+    }
+};
+
+namespace {
+
+Engine* E(spk_engine* e) { return reinterpret_cast<Engine*>(e); }
+Session* S(spk_session* s) { return reinterpret_cast<Session*>(s); }
+
+int32_t map_exception() noexcept {
+    try {
+        throw;
+    } catch (const Error& e) {
+        last_error::set(e.what());
+        return e.status();
+    } catch (const std::bad_alloc&) {
+        last_error::set("out of memory");
+        return SPK_ERR_GPU;
+    } catch (const std::exception& e) {
+        last_error::set(std::string("internal error: ") + e.what());
+        return SPK_ERR_INTERNAL;
+    } catch (...) {
+        last_error::set("internal error: unknown exception");
+        return SPK_ERR_INTERNAL;
+    }
+}
+
+template <class F>
+int32_t guarded(F&& f) noexcept {
+    try {
+        return f();
+    } catch (...) {
+        return map_exception();
+    }
+}
+
+int32_t invalid(const char* msg) noexcept {
+    last_error::set(msg);
+    return SPK_ERR_INVALID_ARG;
+}
+
+void put_json(char** out, const std::string& s) {
+    if (!out) return;
+    char* p = static_cast<char*>(std::malloc(s.size() + 1));
+    if (!p) throw std::bad_alloc();
+    std::memcpy(p, s.data(), s.size() + 1);
+    *out = p;
+}
+
+void release_result(spk_result* r) {
+    if (r->texture) output_release(static_cast<OutputImage*>(r->texture));
+    std::memset(r, 0, sizeof *r);
+}
+
+std::string build_info_string() {
+    return std::string("spektralab-native ") + SPK_VERSION_STRING + " (b200 sm_100a, math=safe)";
+}
+
+spk_engine* create(const char* dir, void* device, int32_t type) noexcept {
+    last_error::clear();
+    try {
+        if (!dir) fail_invalid("resources_dir is NULL");
+        if (type != SPK_DEVICE_DESKTOP)
+            fail_user("device types PHONE and TABLET select mobile effect variants, which this B200 build does not have");
+        int n = 0;
+        if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+            (void)cudaGetLastError();
+            fail_gpu("no CUDA device");
+        }
+        int dev = 0;
+        if (device) dev = *static_cast<const int*>(device);
+        else cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+        if (dev < 0 || dev >= n) fail_gpu("CUDA device ordinal out of range");
+        DeviceGuard g(dev);
+        auto e = std::make_unique<Engine>();
+        e->device = dev;
+        e->res = Resources::load(dir);
+        return reinterpret_cast<spk_engine*>(e.release());
+    } catch (...) {
+        map_exception();
+        return nullptr;
+    }
+}
+
+Session* open_session(Engine& e, const void* data, bool device_ptr, uint32_t w, uint32_t h, uint32_t ch,
+                      const char* delta_text, std::string* reply) {
+    if (ch != 3 && ch != 4) fail_user("input has " + std::to_string(ch) + " channels; expected 3 or 4");
+    if (w == 0 || h == 0) fail_user("input has a zero width or height");
+    const uint64_t npx = uint64_t(w) * h;
+    if (npx > kMaxPixels)
+        fail_user("input of " + std::to_string(w) + " x " + std::to_string(h) + " = " + std::to_string(npx) +
+                  " pixels exceeds the cap of 151301008 pixels (14204 x 10652)");
+    if (!data) fail_invalid(device_ptr ? "input->buffer is NULL" : "input->data is NULL");
+    const Delta d = validate_delta(delta_text ? delta_text : "", DeltaContext::Open);
+    DeviceGuard dg(e.device);
+    auto s = std::make_unique<Session>();
+    s->engine = &e;
+    s->product_defaults = d.product_defaults.value_or(false);
+    cuda_check(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    ParamSet p;
+    for (const auto& [fid, v] : d.fields)
+        if (fid == size_t(P::film_stock) || fid == size_t(P::print_stock)) p.set(fid, v);
+    auto film = e.res->profile(p.s(P::film_stock));
+    auto print = e.res->profile(p.s(P::print_stock));
+    s->digest(p, *film);
+    p.set(P::output_color_space, "ProPhoto RGB");
+    p.set(P::output_cctf_encoding, true);
+    apply_delta(p, d);
+    s->digest(p, *film);
+
+    // the frame: raw upload, then channels and non-finite values fixed on the device
+    s->source = Plane{s->pool.persistent(size_t(npx) * 12), w, h};
+    const size_t raw_bytes = size_t(npx) * ch * sizeof(float);
+    DevBuffer raw = s->pool.acquire(raw_bytes);
+    cuda_check(cudaMemcpyAsync(raw.ptr(), data, raw_bytes, device_ptr ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                               s->stream),
+               "frame upload");
+    dev::source_copy(raw.as<float>(), s->source.data(), size_t(npx), ch, s->stream);
+    cuda_check(cudaGetLastError(), "source copy");
+
+    s->pipe = s->build(p, film, print);
+    s->params = p;
+    s->live = LiveParams::from(p);
+    s->film = film;
+    s->print = print;
+    s->id = "s" + std::to_string(g_next_id++);
+    cuda_check(cudaStreamSynchronize(s->stream), "open");
+    if (reply) {
+        json::Value r;
+        json::Value meta;
+        meta["width"] = w;
+        meta["height"] = h;
+        meta["megapixels"] = std::round(double(npx) / 1e4) / 100.0;
+        meta["source"] = "<in-process>";
+        r["meta"] = std::move(meta);
+        json::Value di;
+        di["input_cctf_decoding"] = s->params.b(P::input_cctf_decoding);
+        di["input_color_space"] = s->params.s(P::input_color_space);
+        di["input_color_space_source"] = "caller";
+        r["detected_input"] = std::move(di);
+        r["params"] = s->params.to_json();
+        r["session_id"] = s->id;
+        *reply = json::write(r);
+    }
+    Session* out = s.release();
+    std::lock_guard<std::mutex> g(e.m);
+    e.sessions.insert(out);
+    return out;
+}
+
+// develop the tier (reference src/session/session.cpp:327-340): drop its negative, draw the film seed
+void develop_tier(Session& s, Tier t, RenderCtx& ctx) {
+    TierState& ts = s.tiers[int(t)];
+    ts.negative = Plane{};
+    const uint32_t seed = s.params.b(P::grain_active) ? s.seeds.next() : kNoGrainFilmSeed;
+    ctx.pitch_um = s.pitch_um();
+    s.node();
+    ts.negative = develop(ctx, s.pipe, s.source, seed, s.hal);
+    ts.pitch_um = ctx.pitch_um;
+}
+
+void render(Session& s, const char* tier_name, bool reprint, spk_result* out) {
+    std::lock_guard<std::mutex> lock(s.m);
+    const auto t0 = std::chrono::steady_clock::now();
+    const std::optional<Tier> t = parse_tier(tier_name);
+    if (!t) fail_invalid(std::string("unknown tier '") + (tier_name ? tier_name : "") + "'");
+    s.check_tier(*t);
+    DeviceGuard dg(s.engine->device);
+    TierState& ts = s.tiers[int(*t)];
+    const bool reuse = reprint && static_cast<bool>(ts.negative);
+    s.progress_id = "p" + std::to_string(g_next_id++);
+    s.cancel.store(false);
+    s.nodes_done.store(0);
+    s.nodes_total = reuse ? 1 : 2;
+    s.done = false;
+    bool developed = false;
+    OutputImage* img = nullptr;
+    try {
+        RenderCtx ctx{s.pool, s.stream};
+        ctx.rho_tier = 1.0;
+        if (!reuse) {
+            developed = true;
+            develop_tier(s, *t, ctx);
+        }
+        ctx.pitch_um = ts.pitch_um;
+        s.node();
+        img = output_acquire(s.engine->device, s.source.w, s.source.h);
+        print_scan_encode(ctx, s.pipe, s.live, ts.negative, img);
+        cuda_check(cudaMemcpyAsync(img->host, img->dev, img->bytes, cudaMemcpyDeviceToHost, s.stream), "result copy");
+        cuda_check(cudaStreamSynchronize(s.stream), "render");
+        cuda_check(cudaGetLastError(), "render");
+    } catch (...) {
+        if (img) output_release(img);
+        if (developed) ts.negative = Plane{};
+        (void)cudaStreamSynchronize(s.stream);
+        try {
+            throw;
+        } catch (const Error& e) {
+            if (e.status() == SPK_ERR_CANCELLED || e.status() == SPK_ERR_INVALID_ARG) throw;
+            fail_gpu(e.what());
+        } catch (const std::bad_alloc&) {
+            fail_gpu("out of memory");
+        }
+    }
+    s.done = true;
+    out->rgba16 = img->host;
+    out->texture = img;
+    out->width = img->width;
+    out->height = img->height;
+    out->row_stride_px = img->stride_px;
+    out->elapsed_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    out->reprint = reuse ? 1 : 0;
+    out->negative_was_cached = reuse ? 1 : 0;
+    std::memset(out->progress_id, 0, sizeof out->progress_id);
+    std::strncpy(out->progress_id, s.progress_id.c_str(), sizeof out->progress_id - 1);
+}
+
+spk_status render_common(spk_session* session, const char* tier, spk_result* out, bool reprint) {
+    last_error::clear();
+    if (!session) return invalid("session is NULL");
+    if (!out) return invalid("out is NULL");
+    if (!parse_tier(tier)) {
+        last_error::set(std::string("unknown tier '") + (tier ? tier : "") + "'; expected live, preview or full");
+        return SPK_ERR_INVALID_ARG;
+    }
+    std::memset(out, 0, sizeof *out);
+    const int32_t st = guarded([&] {
+        render(*S(session), tier, reprint, out);
+        return SPK_OK;
+    });
+    if (st != SPK_OK) release_result(out);
+    return st;
+}
+
+}  // namespace
+
+// ---- internal entry points used by the extension functions ---------------------------------------
+
+std::string session_profile(Session& s, const char* tier_name, bool reprint, uint32_t steps) {
+    std::lock_guard<std::mutex> lock(s.m);
+    const std::optional<Tier> t = parse_tier(tier_name);
+    if (!t) fail_invalid("unknown tier");
+    s.check_tier(*t);
+    DeviceGuard dg(s.engine->device);
+    TierState& ts = s.tiers[int(*t)];
+    DevBuffer flush = s.pool.acquire(size_t(256) << 20);
+    OutputImage* img = output_acquire(s.engine->device, s.source.w, s.source.h);
+    json::Value stages = json::Object{};
+    json::Array totals;
+    Timer timer;
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    try {
+        for (uint32_t k = 0; k < steps; ++k) {
+            dev::fill(flush.ptr(), flush.size() / 16 * 16, k, s.stream);
+            RenderCtx ctx{s.pool, s.stream};
+            ctx.timer = &timer;
+            cudaEventRecord(a, s.stream);
+            if (!reprint || !ts.negative) {
+                ctx.pitch_um = s.pitch_um();
+                const uint32_t seed = s.params.b(P::grain_active) ? s.seeds.next() : kNoGrainFilmSeed;
+                ts.negative = develop(ctx, s.pipe, s.source, seed, s.hal);
+                ts.pitch_um = ctx.pitch_um;
+            }
+            ctx.pitch_um = ts.pitch_um;
+            print_scan_encode(ctx, s.pipe, s.live, ts.negative, img);
+            cudaEventRecord(b, s.stream);
+            cuda_check(cudaStreamSynchronize(s.stream), "profile step");
+            float ms = 0;
+            cudaEventElapsedTime(&ms, a, b);
+            totals.push_back(json::Value(double(ms)));
+            for (const Timer::Mark& m : timer.marks) {
+                float sm = 0;
+                cudaEventElapsedTime(&sm, m.a, m.b);
+                json::Value& arr = stages[m.name];
+                if (arr.is_null()) arr = json::Array{};
+                arr.as_array().push_back(json::Value(double(sm)));
+            }
+            timer.reset();
+        }
+    } catch (...) {
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+        output_release(img);
+        throw;
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    output_release(img);
+    json::Value r;
+    r["steps"] = steps;
+    r["total_ms"] = std::move(totals);
+    r["stages"] = std::move(stages);
+    r["pixels"] = double(s.source.pixels());
+    return json::write(r);
+}
+
+}  // namespace spkb
+
+using namespace spkb;
+
+extern "C" {
+
+SPK_API spk_engine* spk_engine_create(const char* resources_dir, void* device) {
+    return create(resources_dir, device, SPK_DEVICE_DESKTOP);
+}
+
+SPK_API spk_engine* spk_engine_create_for_device(const char* resources_dir, void* device, int32_t device_type) {
+    return create(resources_dir, device, device_type);
+}
+
+SPK_API void spk_engine_destroy(spk_engine* engine) {
+    last_error::clear();
+    if (!engine) return;
+    Engine* e = E(engine);
+    std::set<Session*> ss;
+    {
+        std::lock_guard<std::mutex> g(e->m);
+        ss.swap(e->sessions);
+    }
+    DeviceGuard dg(e->device);
+    for (Session* s : ss) delete s;
+    delete e;
+}
+
+SPK_API size_t spk_engine_trim(spk_engine* engine) {
+    last_error::clear();
+    if (!engine) return 0;
+    size_t freed = 0;
+    try {
+        Engine* e = E(engine);
+        DeviceGuard dg(e->device);
+        std::lock_guard<std::mutex> g(e->m);
+        for (Session* s : e->sessions) freed += s->pool.trim();
+        freed += output_trim();
+    } catch (...) {
+        map_exception();
+    }
+    return freed;
+}
+
+SPK_API const char* spk_build_info(void) {
+    static const std::string s = build_info_string();
+    return s.c_str();
+}
+
+SPK_API const char* spk_capabilities(spk_engine* engine) {
+    if (!engine) return "";
+    Engine* e = E(engine);
+    std::lock_guard<std::mutex> g(e->m);
+    json::Value c;
+    c["engine"] = SPK_ENGINE_NAME;
+    c["version"] = SPK_VERSION_STRING;
+    c["transport_version"] = SPK_TRANSPORT_VERSION;
+    c["schema_version"] = SPK_SCHEMA_VERSION;
+    c["backend"] = "cuda sm_100a";
+    c["device"] = e->device;
+    c["effect_versions"] =
+        "halation=reference;grain=reference;glare=absent;print_spatial=reference;dir_couplers=absent";
+    e->capabilities = json::write(c);
+    return e->capabilities.c_str();
+}
+
+SPK_API const char* spk_params_schema(spk_engine* engine) { return engine ? schema_json().c_str() : ""; }
+
+SPK_API const char* spk_memory_report(spk_engine* engine) {
+    if (!engine) return "";
+    Engine* e = E(engine);
+    std::lock_guard<std::mutex> g(e->m);
+    size_t live = 0, idle = 0, negs = 0;
+    for (Session* s : e->sessions) {
+        live += s->pool.live_bytes();
+        idle += s->pool.free_bytes();
+        for (const TierState& t : s->tiers) negs += t.negative ? t.negative.bytes() : 0;
+    }
+    json::Value r;
+    r["pool_live_bytes"] = double(live);
+    r["pool_free_bytes"] = double(idle);
+    r["cached_negative_bytes"] = double(negs);
+    r["sessions"] = unsigned(e->sessions.size());
+    e->memory_report = json::write(r);
+    return e->memory_report.c_str();
+}
+
+SPK_API spk_status spk_warm_up(spk_engine* engine, const char*, const char*, char**) {
+    last_error::clear();
+    if (!engine) return invalid("engine is NULL");
+    last_error::set("spk_warm_up is outside this B200 build's render path");
+    return SPK_ERR_UNSUPPORTED;
+}
+
+SPK_API spk_session* spk_open(spk_engine* engine, const spk_image* input, const char* delta, char** out_json) {
+    last_error::clear();
+    if (!engine) {
+        invalid("engine is NULL");
+        return nullptr;
+    }
+    if (!input) {
+        invalid("input is NULL");
+        return nullptr;
+    }
+    try {
+        std::string reply;
+        Session* s = open_session(*E(engine), input->data, false, input->width, input->height, input->channels, delta,
+                                  out_json ? &reply : nullptr);
+        put_json(out_json, reply);
+        return reinterpret_cast<spk_session*>(s);
+    } catch (...) {
+        map_exception();
+        return nullptr;
+    }
+}
+
+SPK_API spk_session* spk_open_device(spk_engine* engine, const spk_device_image* input, const char* delta,
+                                     char** out_json) {
+    last_error::clear();
+    if (!engine) {
+        invalid("engine is NULL");
+        return nullptr;
+    }
+    if (!input) {
+        invalid("input is NULL");
+        return nullptr;
+    }
+    try {
+        std::string reply;
+        Session* s = open_session(*E(engine), input->buffer, true, input->width, input->height, input->channels, delta,
+                                  out_json ? &reply : nullptr);
+        put_json(out_json, reply);
+        return reinterpret_cast<spk_session*>(s);
+    } catch (...) {
+        map_exception();
+        return nullptr;
+    }
+}
+
+SPK_API spk_status spk_set_params(spk_session* session, const char* delta_text, char** out_json) {
+    last_error::clear();
+    if (!session) return invalid("session is NULL");
+    return guarded([&] {
+        Session& s = *S(session);
+        const Delta d = validate_delta(delta_text ? delta_text : "", DeltaContext::SetParams);
+        std::lock_guard<std::mutex> lock(s.m);
+        DeviceGuard dg(s.engine->device);
+        ParamSet cand = s.params;
+        apply_delta(cand, d);
+        auto film = s.film, print = s.print;
+        if (d.has_stock) {
+            film = s.engine->res->profile(cand.s(P::film_stock));
+            print = s.engine->res->profile(cand.s(P::print_stock));
+            s.digest(cand, *film);
+        }
+        if (d.any_rebuild) {
+            Pipeline pl = s.build(cand, film, print);
+            s.pipe = std::move(pl);
+            s.seeds = SeedSequence{};
+        }
+        s.live = LiveParams::from(cand);
+        s.params = cand;
+        s.film = film;
+        s.print = print;
+        if (d.any_shoot)
+            for (TierState& t : s.tiers) t.negative = Plane{};
+        json::Value r;
+        r["invalidated"] = d.any_shoot ? "shoot" : "print";
+        r["params"] = s.params.to_json();
+        put_json(out_json, json::write(r));
+        return SPK_OK;
+    });
+}
+
+SPK_API spk_status spk_get_params(spk_session* session, char** out_json) {
+    if (!session) return invalid("session is NULL");
+    return guarded([&] {
+        Session& s = *S(session);
+        std::lock_guard<std::mutex> lock(s.m);
+        put_json(out_json, json::write(s.params.to_json()));
+        return SPK_OK;
+    });
+}
+
+SPK_API void spk_session_release(spk_session* session) {
+    last_error::clear();
+    if (!session) return;
+    Session* s = S(session);
+    Engine* e = s->engine;
+    {
+        std::lock_guard<std::mutex> g(e->m);
+        e->sessions.erase(s);
+    }
+    DeviceGuard dg(e->device);
+    cudaStreamSynchronize(s->stream);
+    delete s;
+}
+
+SPK_API spk_status spk_render(spk_session* session, const char* tier, spk_result* out) {
+    return render_common(session, tier, out, false);
+}
+
+SPK_API spk_status spk_reprint(spk_session* session, const char* tier, spk_result* out) {
+    return render_common(session, tier, out, true);
+}
+
+SPK_API void spk_result_free(spk_result* result) {
+    last_error::clear();
+    if (!result || !result->texture) return;
+    output_release(static_cast<OutputImage*>(result->texture));
+    result->texture = nullptr;
+    result->rgba16 = nullptr;
+}
+
+SPK_API spk_status spk_solve(spk_session* session, const char*, char**) {
+    last_error::clear();
+    if (!session) return invalid("session is NULL");
+    last_error::set("spk_solve is outside this B200 build's render path");
+    return SPK_ERR_UNSUPPORTED;
+}
+
+SPK_API const char* spk_print_lut_catalog(spk_engine*) { return "{}"; }
+
+SPK_API spk_status spk_print_lut_table(spk_engine* engine, const char* print_stock, const float** out_table,
+                                       uint32_t* out_size) {
+    last_error::clear();
+    if (!engine || !print_stock || !out_table || !out_size) return invalid("a required pointer is NULL");
+    last_error::set("print-preview tables are outside this B200 build's render path");
+    return SPK_ERR_UNSUPPORTED;
+}
+
+SPK_API spk_status spk_preview_stock_lut(spk_session* session, const char*, const char*, spk_result* out, char**) {
+    last_error::clear();
+    if (!session || !out) return invalid("a required pointer is NULL");
+    std::memset(out, 0, sizeof *out);
+    last_error::set("spk_preview_stock_lut is outside this B200 build's render path");
+    return SPK_ERR_UNSUPPORTED;
+}
+
+SPK_API spk_status spk_output_transform(spk_engine* engine, const char* src, const char* dst, const char*,
+                                        char**, const float**, uint32_t*) {
+    last_error::clear();
+    if (!engine || !src || !dst) return invalid("a required pointer is NULL");
+    last_error::set("spk_output_transform is outside this B200 build's render path");
+    return SPK_ERR_UNSUPPORTED;
+}
+
+SPK_API void spk_cancel(spk_session* session, const char* progress_id) {
+    if (!session) return;
+    Session* s = S(session);
+    (void)progress_id;
+    s->cancel.store(true);
+}
+
+SPK_API spk_status spk_progress(spk_session* session, const char* progress_id, char** out_json) {
+    if (!session) return invalid("session is NULL");
+    return guarded([&] {
+        Session& s = *S(session);
+        json::Value r;
+        r["progress_id"] = s.progress_id;
+        r["nodes_done"] = unsigned(s.nodes_done.load());
+        r["nodes_total"] = s.nodes_total;
+        r["done"] = s.done;
+        if (progress_id && *progress_id && s.progress_id != progress_id) fail_user("unknown progress id");
+        put_json(out_json, json::write(r));
+        return SPK_OK;
+    });
+}
+
+SPK_API void spk_string_free(char* s) { std::free(s); }
+
+SPK_API const char* spk_last_error(spk_engine*) { return last_error::get(); }
+
+// ---- extensions -----------------------------------------------------------------------------------
+
+SPK_API spk_status spkx_session_set_halation(spk_session* session, uint32_t n, const double* weights,
+                                             const double* sigmas, const double* strength) {
+    last_error::clear();
+    if (!session) return invalid("session is NULL");
+    if (n > SPKB_MAX_COMPONENTS) return invalid("at most 8 halation components");
+    if (n > 0 && (!weights || !sigmas || !strength)) return invalid("a required array is NULL");
+    return guarded([&] {
+        Session& s = *S(session);
+        std::lock_guard<std::mutex> lock(s.m);
+        if (n == 0) {
+            s.hal.reset();
+        } else {
+            HalationOverride o;
+            for (uint32_t k = 0; k < n; ++k) {
+                MixtureComponent m;
+                for (int c = 0; c < 3; ++c) {
+                    m.weight[c] = weights[3 * k + c];
+                    m.sigma[c] = sigmas[3 * k + c];
+                }
+                o.comps.push_back(m);
+            }
+            for (int c = 0; c < 3; ++c) o.strength[c] = strength[c];
+            s.hal = o;
+        }
+        for (TierState& t : s.tiers) t.negative = Plane{};
+        return SPK_OK;
+    });
+}
+
+SPK_API spk_status spkx_session_profile(spk_session* session, const char* tier, int32_t reprint, uint32_t steps,
+                                        char** out_json) {
+    last_error::clear();
+    if (!session) return invalid("session is NULL");
+    return guarded([&] {
+        put_json(out_json, session_profile(*S(session), tier, reprint != 0, steps));
+        return SPK_OK;
+    });
+}
+
+SPK_API spk_status spkx_session_negative(spk_session* session, const char* tier, float* out, size_t capacity) {
+    last_error::clear();
+    if (!session || !out) return invalid("a required pointer is NULL");
+    return guarded([&] {
+        Session& s = *S(session);
+        std::lock_guard<std::mutex> lock(s.m);
+        auto t = parse_tier(tier);
+        if (!t) fail_invalid("unknown tier");
+        const TierState& ts = s.tiers[int(*t)];
+        if (!ts.negative) fail_user("no cached negative for this tier");
+        if (capacity < 3 * ts.negative.pixels()) fail_invalid("output capacity too small");
+        DeviceGuard dg(s.engine->device);
+        cuda_check(cudaMemcpyAsync(out, ts.negative.data(), ts.negative.bytes(), cudaMemcpyDeviceToHost, s.stream),
+                   "negative copy");
+        cuda_check(cudaStreamSynchronize(s.stream), "negative copy");
+        return SPK_OK;
+    });
+}
+
+}  // extern "C"
+
+namespace spkb {
+
+// The same constants before narrowing (binary64), which feed the float64 oracle.
+json::Value setup_f64(const FilmSetup& f, const PrintSetup& p, const PrintRun& run, const LiveParams& live,
+                      double pitch_um) {
+    auto arr = [](const double* v, size_t n) {
+        json::Array a;
+        for (size_t i = 0; i < n; ++i) a.push_back(json::Value(v[i]));
+        return json::Value(std::move(a));
+    };
+    const Profile& film = *f.profile;
+    const size_t K = film.K();
+    const double gamma = f.params.f(P::density_curve_gamma);
+    std::vector<double> cx(K), cinv(K, 0.0), cy(3 * K);
+    for (size_t k = 0; k < K; ++k) {
+        cx[k] = film.log_exposure[k] / gamma;
+        if (k + 1 < K) {
+            const double d = film.log_exposure[k + 1] / gamma - film.log_exposure[k] / gamma;
+            cinv[k] = d == 0.0 ? 0.0 : 1.0 / d;
+        }
+        for (size_t c = 0; c < 3; ++c) cy[c * K + k] = film.normalized(k, c);
+    }
+    json::Value r;
+    r["input_matrix"] = arr(f.input_matrix.data(), 9);
+    r["gain"] = std::pow(2.0, f.params.f(P::exposure_compensation_ev));
+    r["table"] = arr(f.table64.data(), f.table64.size());
+    r["curve_x"] = arr(cx.data(), K);
+    r["curve_inv"] = arr(cinv.data(), K);
+    r["curve_y"] = arr(cy.data(), 3 * K);
+    if (f.grain && f.grain->K) {
+        const GrainSetup& g = *f.grain;
+        const GrainConstants kc = grain_constants(g, pitch_um);
+        double cnt[9], sat[9], dml[9];
+        for (int l = 0; l < 3; ++l)
+            for (int c = 0; c < 3; ++c) {
+                cnt[3 * l + c] = kc.count[l][c];
+                sat[3 * l + c] = kc.sat_d[l][c];
+                dml[3 * l + c] = kc.dmin_l[l][c];
+            }
+        r["grain_count"] = arr(cnt, 9);
+        r["grain_sat_d"] = arr(sat, 9);
+        r["grain_dmin_l"] = arr(dml, 9);
+        r["grain_final_blur"] = kc.final_blur;
+        std::vector<double> ax(K * 3), gi(K * 3, 0.0);
+        for (size_t k = 0; k < K; ++k)
+            for (size_t c = 0; c < 3; ++c) ax[k * 3 + c] = g.positive ? -film.normalized(k, c) : film.normalized(k, c);
+        for (size_t k = 0; k + 1 < K; ++k)
+            for (size_t c = 0; c < 3; ++c) {
+                const double st = ax[(k + 1) * 3 + c] - ax[k * 3 + c];
+                gi[k * 3 + c] = st == 0.0 ? 0.0 : 1.0 / st;
+            }
+        r["grain_axis"] = arr(ax.data(), ax.size());
+        r["grain_inv"] = arr(gi.data(), gi.size());
+        r["grain_layers"] = arr(film.layers.data(), film.layers.size());
+    }
+    {
+        const HalationPlan pl = halation_plan(f.halation, pitch_um);
+        auto comps = [&](const std::vector<MixtureComponent>& v) {
+            json::Array a;
+            for (const MixtureComponent& m : v)
+                a.push_back(json::Array{arr(m.weight.data(), 3), arr(m.sigma.data(), 3)});
+            return json::Value(std::move(a));
+        };
+        json::Value hv;
+        hv["scatter"] = comps(pl.scatter ? pl.scatter_comps : std::vector<MixtureComponent>{});
+        hv["scatter_a"] = arr(pl.scatter_a.data(), 3);
+        hv["scatter_b"] = arr(pl.scatter_b.data(), 3);
+        hv["bounce"] = comps(pl.bounce ? pl.bounce_comps : std::vector<MixtureComponent>{});
+        hv["mix_a"] = arr(pl.mix_a.data(), 3);
+        hv["mix_b"] = arr(pl.mix_b.data(), 3);
+        r["halation"] = std::move(hv);
+        r["lens_blur_px"] = f.params.f(P::lens_blur_um) / pitch_um;
+        r["grain_active"] = f.grain && f.grain->active && f.grain->amount > 0.0;
+        r["grain_amount"] = f.grain ? f.grain->amount : 0.0;
+        r["positive"] = f.positive;
+    }
+    r["enl_eps"] = arr(run.eps_n.data(), 243);
+    r["enl_beta"] = arr(run.beta_n.data(), 81);
+    r["enl_wt"] = arr(run.w_n.data(), 243);
+    r["enl_g"] = arr(run.g.data(), 3);
+    r["enl_o"] = arr(run.o.data(), 3);
+    r["k_gain"] = live.print_exposure;
+    r["scan_eps"] = arr(p.scan_eps.data(), 243);
+    r["scan_beta"] = arr(p.scan_beta.data(), 81);
+    r["scan_wt"] = arr(p.scan_wt.data(), 243);
+    if (p.paper) {
+        const Profile& paper = *p.paper;
+        const size_t pk = paper.K();
+        std::vector<double> pr(pk, 0.0);
+        for (size_t i = 0; i + 1 < pk; ++i) {
+            const double d = paper.log_exposure[i + 1] - paper.log_exposure[i];
+            pr[i] = d == 0.0 ? 0.0 : 1.0 / d;
+        }
+        r["paper_x"] = arr(paper.log_exposure.data(), pk);
+        r["paper_r"] = arr(pr.data(), pk);
+        r["paper_y"] = arr(p.paper_y64.data(), p.paper_y64.size());
+    }
+    r["to_rgb"] = arr(p.to_rgb64.data(), 9);
+    r["m_nid"] = arr(p.m_nid64.data(), 9);
+    const Cam16Constants& k = p.cam->k;
+    const double cam[] = {k.F_L, k.N_bb, k.N_cb, k.n, k.z, k.A_w, k.c, k.N_c, 1.0, 110.0, -M_PI, 2.0 * M_PI / 720.0,
+                          0.0, 1.0, 6.0, 0.7, 1.0, 2.2, k.J_white, k.D_rgb[0], k.D_rgb[1], k.D_rgb[2]};
+    r["cam_k"] = arr(cam, 22);
+    r["cam_m_to_xyz"] = arr(p.cam->m_to_xyz.data(), 9);
+    r["cam_m_to_rgb"] = arr(p.cam->m_to_rgb.data(), 9);
+    r["cam_m16"] = arr(k.m16.data(), 9);
+    static constexpr double kInvPublished[9] = {1.86206786,  -1.01125463, 0.14918677,  0.38752654, 0.62144744,
+                                                -0.00897398, -0.01584150, -0.03412294, 1.04996444};
+    r["cam_m16_inv"] = arr(kInvPublished, 9);
+    r["cmax"] = arr(p.cam->cmax64.data(), p.cam->cmax64.size());
+    r["scanner_lens_blur"] = p.scanner_lens_blur_px;
+    r["unsharp_sigma"] = p.unsharp_sigma_full;
+    r["unsharp_amount"] = p.unsharp_amount;
+    r["cctf_active"] = p.cctf;
+    r["cctf_mode"] = p.cctf_mode;
+    r["printed"] = !p.scanned;
+    return r;
+}
+
+// The narrowed kernel constants of a pipeline, for set-up parity checks against the reference.
+std::string setup_json(const FilmSetup& f, const PrintSetup& p, const LiveParams& live, double pitch_um) {
+        auto arr = [](const float* v, size_t n) {
+            json::Array a;
+            for (size_t i = 0; i < n; ++i) a.push_back(json::Value(double(v[i])));
+            return json::Value(std::move(a));
+        };
+        json::Value r;
+        r["input_matrix"] = arr(f.input_matrix_f32.data(), 9);
+        r["L"] = f.L;
+        r["table"] = arr(f.table32.data(), f.table32.size());
+        r["curve_x"] = arr(f.cx.data(), f.cx.size());
+        r["curve_inv"] = arr(f.cinv.data(), f.cinv.size());
+        r["curve_y"] = arr(f.cy.data(), f.cy.size());
+        if (f.grain) {
+            const GrainConstants kc = grain_constants(*f.grain, pitch_um);
+            float cnt[9], sat[9], dml[9];
+            for (int l = 0; l < 3; ++l)
+                for (int c = 0; c < 3; ++c) {
+                    cnt[3 * l + c] = f32(kc.count[l][c]);
+                    sat[3 * l + c] = f32(kc.sat_d[l][c]);
+                    dml[3 * l + c] = f32(kc.dmin_l[l][c]);
+                }
+            r["grain_count"] = arr(cnt, 9);
+            r["grain_sat_d"] = arr(sat, 9);
+            r["grain_dmin_l"] = arr(dml, 9);
+            r["grain_axis"] = arr(f.grain->axis.data(), f.grain->axis.size());
+            r["grain_inv"] = arr(f.grain->inv.data(), f.grain->inv.size());
+            r["grain_layers"] = arr(f.grain->layers.data(), f.grain->layers.size());
+        }
+        const PrintRun run = compute_run(p, live);
+        r["enl_eps"] = arr(run.enl32.eps, 243);
+        r["enl_beta"] = arr(run.enl32.beta, 81);
+        r["enl_wt"] = arr(run.enl32.wt, 243);
+        float g[3], o[3];
+        for (int c = 0; c < 3; ++c) {
+            g[c] = f32(run.g[c]);
+            o[c] = f32(run.o[c]);
+        }
+        r["enl_g"] = arr(g, 3);
+        r["enl_o"] = arr(o, 3);
+        r["k_gain"] = double(run.k_gain);
+        r["scan_eps"] = arr(p.scan32.eps, 243);
+        r["scan_beta"] = arr(p.scan32.beta, 81);
+        r["scan_wt"] = arr(p.scan32.wt, 243);
+        r["paper"] = arr(p.paper_tab.data(), p.paper_tab.size());
+        r["to_rgb"] = arr(p.to_rgb, 9);
+        r["m_nid"] = arr(p.m_nid, 9);
+        const Cam16Args& q = p.cam_args;
+        const float cam[] = {q.f_l, q.n_bb, q.n_cb, q.n, q.z, q.a_w, q.c, q.n_c, q.j_first, q.j_last, q.h_first,
+                             q.h_step, q.knee[0], q.knee[1], q.knee[2], q.lc[0], q.lc[1], q.lc[2], q.j_white,
+                             q.d_rgb[0], q.d_rgb[1], q.d_rgb[2]};
+        r["cam_k"] = arr(cam, 22);
+        r["cam_m_to_xyz"] = arr(q.m_to_xyz, 9);
+        r["cam_m_to_rgb"] = arr(q.m_to_rgb, 9);
+        r["cmax"] = arr(p.cam->cmax32.data(), p.cam->cmax32.size());
+    r["f64"] = setup_f64(f, p, run, live, pitch_um);
+    return json::write(r);
+}
+
+// Parameters of an open (reference src/session/session.cpp:142-152): defaults, the delta's stocks,
+// the digest, the forced working output space, the delta, the digest again.
+ParamSet open_params(const Resources& res, const Delta& d, std::shared_ptr<const Profile>& film,
+                     std::shared_ptr<const Profile>& print) {
+    ParamSet p;
+    for (const auto& [fid, v] : d.fields)
+        if (fid == size_t(P::film_stock) || fid == size_t(P::print_stock)) p.set(fid, v);
+    film = res.profile(p.s(P::film_stock));
+    print = res.profile(p.s(P::print_stock));
+    auto digest = [&] {
+        if (auto pack = res.neutral_filters(p.s(P::print_stock), p.s(P::enlarger_illuminant), *film)) {
+            p.set(P::c_filter_neutral, (*pack)[0]);
+            p.set(P::m_filter_neutral, (*pack)[1]);
+            p.set(P::y_filter_neutral, (*pack)[2]);
+        }
+    };
+    digest();
+    p.set(P::output_color_space, "ProPhoto RGB");
+    p.set(P::output_cctf_encoding, true);
+    apply_delta(p, d);
+    digest();
+    return p;
+}
+
+}  // namespace spkb
+
+extern "C" {
+
+SPK_API spk_status spkx_session_develop_debug(spk_session* session, const char* tier, uint32_t seed, float* negative,
+                                              float* counts) {
+    last_error::clear();
+    if (!session || !negative) return invalid("a required pointer is NULL");
+    return guarded([&] {
+        Session& s = *S(session);
+        std::lock_guard<std::mutex> lock(s.m);
+        auto t = parse_tier(tier);
+        if (!t) fail_invalid("unknown tier");
+        s.check_tier(*t);
+        DeviceGuard dg(s.engine->device);
+        RenderCtx ctx{s.pool, s.stream};
+        ctx.pitch_um = s.pitch_um();
+        DevBuffer dc;
+        if (counts) {
+            dc = s.pool.acquire(s.source.pixels() * 9 * sizeof(float));
+            cuda_check(cudaMemsetAsync(dc.ptr(), 0, s.source.pixels() * 9 * sizeof(float), s.stream), "memset");
+        }
+        Plane neg = develop(ctx, s.pipe, s.source, seed, s.hal, counts ? dc.as<float>() : nullptr);
+        cuda_check(cudaMemcpyAsync(negative, neg.data(), neg.bytes(), cudaMemcpyDeviceToHost, s.stream), "copy");
+        if (counts)
+            cuda_check(cudaMemcpyAsync(counts, dc.ptr(), s.source.pixels() * 9 * sizeof(float), cudaMemcpyDeviceToHost,
+                                       s.stream),
+                       "copy");
+        cuda_check(cudaStreamSynchronize(s.stream), "develop");
+        return SPK_OK;
+    });
+}
+
+SPK_API spk_status spkx_session_setup_json(spk_session* session, double pitch_um, char** out_json) {
+    last_error::clear();
+    if (!session) return invalid("session is NULL");
+    return guarded([&] {
+        Session& s = *S(session);
+        std::lock_guard<std::mutex> lock(s.m);
+        put_json(out_json, setup_json(*s.pipe.film, *s.pipe.print, s.live, pitch_um));
+        return SPK_OK;
+    });
+}
+
+SPK_API spk_status spkx_setup_json(const char* resources_dir, const char* delta, double pitch_um, char** out_json) {
+    last_error::clear();
+    if (!resources_dir) return invalid("resources_dir is NULL");
+    return guarded([&] {
+        auto res = Resources::load(resources_dir);
+        const Delta d = validate_delta(delta ? delta : "", DeltaContext::Open);
+        std::shared_ptr<const Profile> film, print;
+        const ParamSet p = open_params(*res, d, film, print);
+        Cam16Cache cache;
+        auto fs = build_film_setup(p, film, *res);
+        auto ps = build_print_setup(p, *fs, print, *res, cache, !d.product_defaults.value_or(false));
+        put_json(out_json, setup_json(*fs, *ps, LiveParams::from(p), pitch_um));
+        return SPK_OK;
+    });
+}
+
+}  // extern "C"
+
+namespace {
+template <class F>
+spk_status with_scratch_stream(F&& f) {
+    return guarded([&] {
+        cudaStream_t s = nullptr;
+        cuda_check(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "cudaStreamCreate");
+        try {
+            f(s);
+            cuda_check(cudaStreamSynchronize(s), "test kernel");
+            cuda_check(cudaGetLastError(), "test kernel");
+        } catch (...) {
+            cudaStreamDestroy(s);
+            throw;
+        }
+        cudaStreamDestroy(s);
+        return SPK_OK;
+    });
+}
+
+struct DevArray {
+    void* p = nullptr;
+    explicit DevArray(size_t bytes) { cuda_check(cudaMalloc(&p, std::max<size_t>(bytes, 16)), "cudaMalloc"); }
+    ~DevArray() { cudaFree(p); }
+};
+}  // namespace
+
+extern "C" {
+
+SPK_API spk_status spkx_sampler_poisson(const float* lam, float* counts, uint32_t n, uint32_t stream, uint32_t seed) {
+    last_error::clear();
+    if ((!lam || !counts) && n) return invalid("a required pointer is NULL");
+    return with_scratch_stream([&](cudaStream_t s) {
+        DevArray dl(n * 4ull), dc(n * 4ull);
+        cuda_check(cudaMemcpyAsync(dl.p, lam, n * 4ull, cudaMemcpyHostToDevice, s), "copy");
+        dev::sampler_poisson(static_cast<float*>(dl.p), static_cast<float*>(dc.p), n, stream, seed, s);
+        cuda_check(cudaMemcpyAsync(counts, dc.p, n * 4ull, cudaMemcpyDeviceToHost, s), "copy");
+        cuda_check(cudaStreamSynchronize(s), "sampler");
+    });
+}
+
+SPK_API spk_status spkx_sampler_lognormal(float* out, uint32_t n, float mean, float stddev, uint32_t stream,
+                                          uint32_t seed) {
+    last_error::clear();
+    if (!out && n) return invalid("out is NULL");
+    return with_scratch_stream([&](cudaStream_t s) {
+        DevArray d(n * 4ull);
+        dev::sampler_lognormal(static_cast<float*>(d.p), n, mean, stddev, stream, seed, s);
+        cuda_check(cudaMemcpyAsync(out, d.p, n * 4ull, cudaMemcpyDeviceToHost, s), "copy");
+        cuda_check(cudaStreamSynchronize(s), "sampler");
+    });
+}
+
+SPK_API spk_status spkx_philox(const uint32_t* counters, const uint32_t* keys, uint32_t* out, uint32_t n) {
+    last_error::clear();
+    if ((!counters || !keys || !out) && n) return invalid("a required pointer is NULL");
+    return with_scratch_stream([&](cudaStream_t s) {
+        DevArray dc(n * 16ull), dk(n * 8ull), dout(n * 16ull);
+        cuda_check(cudaMemcpyAsync(dc.p, counters, n * 16ull, cudaMemcpyHostToDevice, s), "copy");
+        cuda_check(cudaMemcpyAsync(dk.p, keys, n * 8ull, cudaMemcpyHostToDevice, s), "copy");
+        dev::philox_blocks(static_cast<uint32_t*>(dc.p), static_cast<uint32_t*>(dk.p), static_cast<uint32_t*>(dout.p),
+                           n, s);
+        cuda_check(cudaMemcpyAsync(out, dout.p, n * 16ull, cudaMemcpyDeviceToHost, s), "copy");
+        cuda_check(cudaStreamSynchronize(s), "philox");
+    });
+}
+
+SPK_API spk_status spkx_gaussian(const float* in, float* out, uint32_t w, uint32_t h, const double* sigma3) {
+    last_error::clear();
+    if (!in || !out || !sigma3) return invalid("a required pointer is NULL");
+    if (w == 0 || h == 0) return invalid("empty plane");
+    return with_scratch_stream([&](cudaStream_t s) {
+        Pool pool;
+        RenderCtx ctx{pool, s};
+        Plane a = make_plane(pool, w, h), b = make_plane(pool, w, h);
+        cuda_check(cudaMemcpyAsync(a.data(), in, a.bytes(), cudaMemcpyHostToDevice, s), "copy");
+        gaussian(ctx, a, b, Vec3{sigma3[0], sigma3[1], sigma3[2]});
+        cuda_check(cudaMemcpyAsync(out, b.data(), b.bytes(), cudaMemcpyDeviceToHost, s), "copy");
+        cuda_check(cudaStreamSynchronize(s), "gaussian");
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,390 @@
+#include "render.hpp"
+
+#include <cmath>
+#include <cstring>
+
+#include "../cuda/launch.hpp"
+#include "status.hpp"
+
+namespace spkb {
+
+namespace {
+
+void upload(Pool& pool, cudaStream_t s, DevBuffer& dst, const void* src, size_t bytes) {
+    dst = pool.persistent(bytes);
+    cuda_check(cudaMemcpyAsync(dst.ptr(), src, bytes, cudaMemcpyHostToDevice, s), "table upload");
+}
+
+}  // namespace
+
+void upload_tables(Pool& pool, cudaStream_t s, Pipeline& p) {
+    const FilmSetup& f = *p.film;
+    upload(pool, s, p.dev.table, f.table32.data(), f.table32.size() * sizeof(float));
+    std::vector<float> c(5 * size_t(f.K));
+    std::memcpy(c.data(), f.cx.data(), f.K * sizeof(float));
+    std::memcpy(c.data() + f.K, f.cinv.data(), f.K * sizeof(float));
+    std::memcpy(c.data() + 2 * f.K, f.cy.data(), 3 * f.K * sizeof(float));
+    upload(pool, s, p.dev.curves, c.data(), c.size() * sizeof(float));
+    if (f.grain && f.grain->K) {
+        upload(pool, s, p.dev.gaxis, f.grain->axis.data(), f.grain->axis.size() * sizeof(float));
+        upload(pool, s, p.dev.ginv, f.grain->inv.data(), f.grain->inv.size() * sizeof(float));
+        upload(pool, s, p.dev.glayers, f.grain->layers.data(), f.grain->layers.size() * sizeof(float));
+    }
+    const PrintSetup& pr = *p.print;
+    if (!pr.paper_tab.empty()) upload(pool, s, p.dev.paper, pr.paper_tab.data(), pr.paper_tab.size() * sizeof(float));
+    upload(pool, s, p.dev.cmax, pr.cam->cmax32.data(), pr.cam->cmax32.size() * sizeof(float));
+    cuda_check(cudaStreamSynchronize(s), "table upload");
+}
+
+// ---- timing -------------------------------------------------------------------------------------
+
+void Timer::begin(const char* name, cudaStream_t s) {
+    Mark m{name, nullptr, nullptr};
+    cudaEventCreate(&m.a);
+    cudaEventCreate(&m.b);
+    cudaEventRecord(m.a, s);
+    marks.push_back(m);
+}
+void Timer::end(cudaStream_t s) { cudaEventRecord(marks.back().b, s); }
+void Timer::reset() {
+    for (Mark& m : marks) {
+        cudaEventDestroy(m.a);
+        cudaEventDestroy(m.b);
+    }
+    marks.clear();
+}
+Timer::~Timer() { reset(); }
+
+namespace {
+struct Stage {
+    RenderCtx& ctx;
+    Stage(RenderCtx& c, const char* name) : ctx(c) {
+        if (ctx.timer) ctx.timer->begin(name, ctx.stream);
+    }
+    ~Stage() {
+        if (ctx.timer) ctx.timer->end(ctx.stream);
+    }
+};
+
+// ---- the blur machinery (reference src/fx/gaussian.cpp:167-273) ----------------------------------
+
+struct Fuse {
+    int mode = ACC_NONE;
+    const Plane* acc = nullptr;
+    Vec3 weight{1.0, 1.0, 1.0};
+};
+
+bool same(const Plane& a, const Plane& b) { return a.data() == b.data(); }
+
+FirTaps fir_taps(const Vec3& sigma, const bool iir[3]) {
+    FirTaps t{};
+    int r = 0;
+    for (int c = 0; c < 3; ++c)
+        if (!iir[c] && sigma[c] > 0.0) r = std::max(r, fir_radius(sigma[c]));
+    t.r = r;
+    for (int c = 0; c < 3; ++c) {
+        if (iir[c] || !(sigma[c] > 0.0)) {
+            t.taps[c][r] = 1.0f;
+            continue;
+        }
+        const std::vector<double> k = gaussian_kernel(sigma[c], 3.0);
+        const int rc = int(k.size() / 2);
+        for (int i = -rc; i <= rc; ++i) t.taps[c][r + i] = f32(k[size_t(i + rc)]);
+    }
+    return t;
+}
+
+IirCoefs iir_coefs(const Vec3& sigma, const bool iir[3]) {
+    IirCoefs a{};
+    for (int c = 0; c < 3; ++c) {
+        if (!iir[c]) continue;
+        a.mask |= 1u << c;
+        const IirCoefficients k = iir_coefficients(sigma[c]);
+        a.B[c] = k.B;
+        a.B1[c] = k.B1;
+        a.B2[c] = k.B2;
+        a.B3[c] = k.B3;
+    }
+    return a;
+}
+
+void weights(const Vec3& w, float out[3]) {
+    for (int c = 0; c < 3; ++c) out[c] = f32(w[c]);
+}
+
+void encode_fir(RenderCtx& ctx, const Plane& in, const Plane& dst, const FirTaps& t, const Fuse& fuse) {
+    Plane tmp = make_plane(ctx.pool, in.w, in.h);
+    dev::fir_v(in.data(), tmp.data(), in.w, in.h, t, ctx.stream);
+    float w[3];
+    weights(fuse.weight, w);
+    const Plane& acc = (fuse.mode == ACC_PLANE && fuse.acc) ? *fuse.acc : dst;
+    dev::fir_h(tmp.data(), dst.data(), acc.data(), in.w, in.h, t, fuse.mode, w, ctx.stream);
+}
+
+void encode_iir(RenderCtx& ctx, const Plane& in, const Plane& dst, const IirCoefs& c, const Fuse& fuse) {
+    Plane tmp = make_plane(ctx.pool, in.w, in.h);
+    dev::iir_h(in.data(), tmp.data(), in.w, in.h, c, ctx.stream);
+    float w[3];
+    weights(fuse.weight, w);
+    const Plane& acc = (fuse.mode == ACC_PLANE && fuse.acc) ? *fuse.acc : dst;
+    dev::iir_v(tmp.data(), dst.data(), acc.data(), in.w, in.h, c, fuse.mode, w, ctx.stream);
+}
+
+void lincomb(RenderCtx& ctx, const Vec3& a, const Plane& x, const Vec3& b, const Plane* y, const Plane& out) {
+    float fa[3], fb[3];
+    weights(a, fa);
+    weights(b, fb);
+    dev::lincomb(x.data(), y ? y->data() : nullptr, out.data(), x.pixels(), fa, fb, ctx.stream);
+}
+
+void encode_blur(RenderCtx& ctx, const Plane& in, const Plane& dst, const Vec3& sigma, const Fuse& fuse) {
+    bool iir[3];
+    int n_iir = 0;
+    for (int c = 0; c < 3; ++c) {
+        iir[c] = blur_branch(sigma[c]) == Branch::Iir;
+        n_iir += iir[c];
+    }
+    const FirTaps fa = fir_taps(sigma, iir);
+    if (n_iir == 0) {
+        if (fuse.mode == ACC_NONE && fa.r == 0) {
+            if (!same(in, dst)) dev::copy(in.data(), dst.data(), in.pixels(), ctx.stream);
+            return;
+        }
+        encode_fir(ctx, in, dst, fa, fuse);
+        return;
+    }
+    const IirCoefs ia = iir_coefs(sigma, iir);
+    if (n_iir == 3) {
+        encode_iir(ctx, in, dst, ia, fuse);
+        return;
+    }
+    if (fuse.mode != ACC_NONE) {
+        Plane t = make_plane(ctx.pool, in.w, in.h);
+        encode_blur(ctx, in, t, sigma, Fuse{});
+        if (fuse.mode == ACC_ZERO) lincomb(ctx, fuse.weight, t, Vec3{1.0, 1.0, 1.0}, nullptr, dst);
+        else lincomb(ctx, Vec3{1.0, 1.0, 1.0}, *fuse.acc, fuse.weight, &t, dst);
+        return;
+    }
+    if (fa.r > 0) {
+        Plane t = make_plane(ctx.pool, in.w, in.h);
+        encode_fir(ctx, in, t, fa, Fuse{});
+        encode_iir(ctx, t, dst, ia, Fuse{});
+    } else {
+        encode_iir(ctx, in, dst, ia, Fuse{});
+    }
+}
+
+}  // namespace
+
+void gaussian(RenderCtx& ctx, const Plane& in, const Plane& dst, const Vec3& sigma) {
+    encode_blur(ctx, in, dst, sigma, Fuse{});
+}
+
+void gaussian_mixture(RenderCtx& ctx, const Plane& in, const Plane& out, const std::vector<MixtureComponent>& comps) {
+    if (comps.empty()) fail_internal("empty mixture");
+    Plane acc = same(in, out) ? make_plane(ctx.pool, in.w, in.h) : out;
+    for (size_t k = 0; k < comps.size(); ++k) {
+        const MixtureComponent& m = comps[k];
+        const bool ident = !(m.sigma[0] > 0.0) && !(m.sigma[1] > 0.0) && !(m.sigma[2] > 0.0);
+        if (k == 0 && ident) {
+            lincomb(ctx, Vec3{0.0, 0.0, 0.0}, in, m.weight, &in, acc);
+            continue;
+        }
+        Fuse f;
+        f.mode = k == 0 ? ACC_ZERO : ACC_PLANE;
+        f.acc = &acc;
+        f.weight = m.weight;
+        encode_blur(ctx, in, acc, m.sigma, f);
+    }
+    if (!same(acc, out)) dev::copy(acc.data(), out.data(), acc.pixels(), ctx.stream);
+}
+
+void check_supported(const ParamSet& p) {
+    auto refuse = [](const std::string& what) {
+        fail_user(what + " is outside this B200 build's render path");
+    };
+    if (p.b(P::auto_exposure)) refuse("auto_exposure=true (the meter)");
+    if (p.b(P::dir_couplers_active)) refuse("dir_couplers_active=true (DIR couplers)");
+    if (p.b(P::glare_active) && p.f(P::glare_amount) > 0.0) refuse("glare_active=true (print glare)");
+    if (p.b(P::input_cctf_decoding)) refuse("input_cctf_decoding=true (input transfer decode)");
+    if (p.f(P::halation_boost_ev) != 0.0) refuse("halation_boost_ev != 0 (highlight boost)");
+    if (p.b(P::scanner_white_correction) || p.b(P::scanner_black_correction))
+        refuse("scanner white/black correction (levels)");
+    if (p.b(P::extended_dynamic_range)) refuse("extended_dynamic_range=true (EDR tone map)");
+    const bool geometry_identity = p.f(P::geometry_crop_x) == 0.0 && p.f(P::geometry_crop_y) == 0.0 &&
+                                   p.f(P::geometry_crop_w) == 1.0 && p.f(P::geometry_crop_h) == 1.0 &&
+                                   p.f(P::geometry_rotation_deg) == 0.0 && p.i(P::geometry_quarter_turns) % 4 == 0 &&
+                                   !p.b(P::geometry_flip_h) && !p.b(P::geometry_flip_v);
+    if (!geometry_identity) refuse("a crop, rotation, quarter turn or flip (geometry)");
+}
+
+Plane develop(RenderCtx& ctx, const Pipeline& p, const Plane& source, uint32_t film_seed,
+              const std::optional<HalationOverride>& hov, float* counts_out) {
+    const FilmSetup& f = *p.film;
+    const ParamSet& b = f.params;
+    const uint32_t w = source.w, h = source.h;
+    Plane H = make_plane(ctx.pool, w, h);
+    {
+        Stage st(ctx, "expose");
+        ExposeArgs a{};
+        for (int i = 0; i < 9; ++i) a.a[i] = f.input_matrix_f32[size_t(i)];
+        a.gain = f32(std::pow(2.0, b.f(P::exposure_compensation_ev)));
+        a.apply_gain = a.gain != 1.0f;
+        a.L = f.L;
+        a.n = uint32_t(source.pixels());
+        dev::expose(source.data(), H.data(), p.dev.table.as<float>(), a, ctx.stream);
+    }
+    if (b.f(P::lens_blur_um) > 0.0) {
+        Stage st(ctx, "lens_blur");
+        const double s = b.f(P::lens_blur_um) / ctx.pitch_um;
+        if (s > 0.0) gaussian(ctx, H, H, Vec3{s, s, s});
+    }
+    {
+        HalationPlan pl;
+        if (hov) {
+            pl.bounce = !hov->comps.empty();
+            pl.bounce_comps = hov->comps;
+            for (size_t c = 0; c < 3; ++c) {
+                const double A = hov->strength[c];
+                pl.mix_a[c] = 1.0 / (1.0 + A);
+                pl.mix_b[c] = A / (1.0 + A);
+            }
+        } else {
+            if (f.halation.back_reflection && f.halation.active && f.halation.headroom_ev > 0.0 && f.halation.amount > 0.0)
+                fail_user("the back-reflection halation preset (highlight headroom) is outside this B200 build's render path");
+            pl = halation_plan(f.halation, ctx.pitch_um);
+        }
+        if (pl.scatter || pl.bounce) {
+            Stage st(ctx, "halation");
+            if (pl.scatter) {
+                Plane m = make_plane(ctx.pool, w, h);
+                gaussian_mixture(ctx, H, m, pl.scatter_comps);
+                lincomb(ctx, pl.scatter_a, H, pl.scatter_b, &m, H);
+            }
+            if (pl.bounce) {
+                Plane Hh = make_plane(ctx.pool, w, h);
+                gaussian_mixture(ctx, H, Hh, pl.bounce_comps);
+                lincomb(ctx, pl.mix_a, H, pl.mix_b, &Hh, H);
+            }
+        }
+    }
+    DevelopArgs da{};
+    da.cx = p.dev.curves.as<float>();
+    da.cinv = da.cx + f.K;
+    da.cy = da.cx + 2 * size_t(f.K);
+    da.K = f.K;
+    da.width = w;
+    da.counts_out = counts_out;
+    Plane neg = make_plane(ctx.pool, w, h);
+    const GrainSetup* g = f.grain.get();
+    const bool grain = g && g->active && g->amount > 0.0;
+    if (!grain) {
+        Stage st(ctx, "develop");
+        dev::develop(H.data(), neg.data(), da, w, h, ctx.stream);
+        return neg;
+    }
+    const GrainConstants kc = grain_constants(*g, ctx.pitch_um);
+    if (kc.sublayers && (kc.dye || kc.micro))
+        fail_user("grain dye clouds or micro-structure (pixel pitch below about 2 um) are outside this B200 build's render path");
+    da.grain = 1;
+    da.seed = film_seed;
+    da.positive = g->positive ? 1u : 0u;
+    da.n_sub = 1;
+    da.inv_n_sub = f32(1.0);
+    for (size_t c = 0; c < 3; ++c) {
+        da.uniformity[c] = f32(c == 1 ? 0.99 : 0.97);
+        da.dmin_c[c] = f32(kGrainDmin[c]);
+    }
+    for (size_t l = 0; l < 3; ++l)
+        for (size_t c = 0; c < 3; ++c) {
+            da.dmin_l[l * 3 + c] = f32(kc.dmin_l[l][c]);
+            da.sat_d[l * 3 + c] = f32(kc.sat_d[l][c]);
+            da.count[l * 3 + c] = f32(kc.count[l][c]);
+        }
+    if (g->sublayers) {
+        da.mode = 0;  // SUM
+        da.shift = 1;
+        da.gK = g->K;
+        da.axis = p.dev.gaxis.as<float>();
+        da.ginv = p.dev.ginv.as<float>();
+        da.layers = p.dev.glayers.as<float>();
+    } else {
+        da.mode = 2;  // SIMPLE
+    }
+    Plane G = make_plane(ctx.pool, w, h);
+    {
+        Stage st(ctx, "develop");
+        dev::develop(H.data(), G.data(), da, w, h, ctx.stream);
+    }
+    if (kc.final_blur > 0.0) {
+        Stage st(ctx, "grain_blur");
+        const double s = kc.final_blur;
+        gaussian(ctx, G, G, Vec3{s, s, s});
+    }
+    {
+        Stage st(ctx, "grain_mix");
+        if (g->amount == 1.0) {
+            dev::copy(G.data(), neg.data(), G.pixels(), ctx.stream);
+        } else {
+            DevelopArgs dd = da;
+            dd.grain = 0;
+            dev::develop(H.data(), neg.data(), dd, w, h, ctx.stream);
+            const double k = g->amount;
+            lincomb(ctx, Vec3{1.0 - k, 1.0 - k, 1.0 - k}, neg, Vec3{k, k, k}, &G, neg);
+        }
+    }
+    return neg;
+}
+
+void print_scan_encode(RenderCtx& ctx, const Pipeline& p, const LiveParams& live, const Plane& negative,
+                       OutputImage* img) {
+    const PrintSetup& s = *p.print;
+    const uint32_t w = negative.w, h = negative.h;
+    const PrintRun r = compute_run(s, live);
+    PrintArgs a{};
+    a.enl = r.enl32;
+    a.scan = s.scan32;
+    for (int c = 0; c < 3; ++c) {
+        a.g[c] = f32(r.g[c]);
+        a.o[c] = f32(r.o[c]);
+    }
+    a.k_gain = r.k_gain;
+    a.printed = s.scanned ? 0 : 1;
+    a.paper = p.dev.paper.as<float>();
+    a.paper_K = s.paper_K;
+    std::memcpy(a.to_rgb, s.to_rgb, sizeof a.to_rgb);
+    a.cam = s.cam_args;
+    a.cmax = p.dev.cmax.as<float>();
+    a.n = uint32_t(negative.pixels());
+    Plane rgb = make_plane(ctx.pool, w, h);
+    {
+        Stage st(ctx, "print");
+        dev::print(negative.data(), rgb.data(), a, ctx.stream);
+    }
+    EncodeArgs e{};
+    std::memcpy(e.m_nid, s.m_nid, sizeof e.m_nid);
+    e.cctf_active = s.cctf ? 1 : 0;
+    e.cctf_mode = s.cctf_mode;
+    e.stride = img->stride_px;
+    Plane gpl;
+    {
+        Stage st(ctx, "scanner");
+        const double sb = s.scanner_lens_blur_px;
+        const double su = s.unsharp_sigma_full * ctx.rho_tier;
+        const double am = s.unsharp_amount;
+        if (sb > 0.0) gaussian(ctx, rgb, rgb, Vec3{sb, sb, sb});
+        if (su > 0.0 && am > 0.0) {
+            gpl = make_plane(ctx.pool, w, h);
+            gaussian(ctx, rgb, gpl, Vec3{su, su, su});
+            e.unsharp = 1;
+            e.lincomb_a = f32(1.0 + am);
+            e.lincomb_b = f32(-am);
+        }
+    }
+    {
+        Stage st(ctx, "encode");
+        dev::encode(rgb.data(), gpl ? gpl.data() : nullptr, img->dev, w, h, e, ctx.stream);
+    }
+}
+
+}  // namespace spkb

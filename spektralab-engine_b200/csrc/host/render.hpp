@@ -1,0 +1,74 @@
+// The render path on the device: film side (develop) and print side (print, scan, encode), driven
+// from the binary64 set-up. Stage order and the rules of every blur follow the reference
+// (src/film/develop.cpp:101-236, src/print/run.cpp:118-188, src/fx/gaussian.cpp:167-273,
+// src/fx/halation.cpp:307-329, src/fx/grain.cpp:167-267, src/fx/scanner.cpp:16-31); the kernels are
+// this build's own (csrc/cuda).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <optional>
+#include <vector>
+
+#include "device.hpp"
+#include "setup.hpp"
+
+namespace spkb {
+
+// A film/print set-up pair with its device tables, built once per pipeline.
+struct DeviceTables {
+    DevBuffer table;              // L x L x 3 spectral table
+    DevBuffer curves;             // x[K] | inv[K] | y[3K]
+    DevBuffer gaxis, ginv, glayers;
+    DevBuffer paper;              // x[K] | r[K] | y[K][3]
+    DevBuffer cmax;               // 64 x 720
+};
+
+struct Pipeline {
+    std::shared_ptr<const FilmSetup> film;
+    std::shared_ptr<const PrintSetup> print;
+    DeviceTables dev;
+};
+
+// Upload a pipeline's tables (stream-ordered, then synchronised).
+void upload_tables(Pool& pool, cudaStream_t s, Pipeline& p);
+
+struct RenderCtx {
+    Pool& pool;
+    cudaStream_t stream;
+    double pitch_um = 0.0;
+    double rho_tier = 1.0;
+    // optional per-stage timing: events recorded around each stage when set
+    struct Timer* timer = nullptr;
+};
+
+// Stage timing with CUDA events on the render stream (bench and profile entry points).
+struct Timer {
+    struct Mark {
+        const char* name;
+        cudaEvent_t a, b;
+    };
+    std::vector<Mark> marks;
+    void begin(const char* name, cudaStream_t s);
+    void end(cudaStream_t s);
+    void reset();
+    ~Timer();
+};
+
+// film side: raw source plane -> developed negative density plane (a fresh persistent plane)
+// counts_out: nullptr, or device memory for 9 floats per pixel receiving the grain's Poisson counts
+Plane develop(RenderCtx& ctx, const Pipeline& p, const Plane& source, uint32_t film_seed,
+              const std::optional<HalationOverride>& hov, float* counts_out = nullptr);
+
+// print side: negative -> RGBA16 into img->dev (row pitch img->stride_px); no host copy
+void print_scan_encode(RenderCtx& ctx, const Pipeline& p, const LiveParams& live, const Plane& negative,
+                       OutputImage* img);
+
+// The blur machinery on device planes (exposed for the tests' stage entry points).
+void gaussian(RenderCtx& ctx, const Plane& in, const Plane& dst, const Vec3& sigma);
+void gaussian_mixture(RenderCtx& ctx, const Plane& in, const Plane& out, const std::vector<MixtureComponent>& comps);
+
+// Checks that a parameter set stays inside this build's render path; SPK_ERR_USER with the reason.
+void check_supported(const ParamSet& p);
+
+}  // namespace spkb

@@ -1,0 +1,305 @@
+"""ctypes binding of the spektralab C ABI (include/spektralab.h) and of the B200 extensions
+(include/spektralab_b200.h).
+
+The same binding loads the B200 library (libspektralab.so beside this file) and the CPU build of the
+reference engine used as the oracle (oracle/_ref/libspektralab_ref.so); both export the reference's
+26 entry points with identical signatures. Mirrors the role of the reference's tests/spk_ctypes.py:
+signatures bound once, RGBA16 results read through row_stride_px.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import json
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(HERE)
+LIB_PATH = os.path.join(HERE, "libspektralab.so")
+REF_PATH = os.path.join(REPO, "oracle", "_ref", "libspektralab_ref.so")
+RESOURCES = os.path.join(REPO, "_build", "resources")
+
+SPK_OK = 0
+SPK_ERR_INVALID_ARG = -1
+SPK_ERR_USER = -2
+SPK_ERR_UNSUPPORTED = -4
+SPK_ERR_GPU = -5
+SPK_ERR_IO = -6
+SPK_ERR_CANCELLED = -7
+
+
+class SpkImage(ctypes.Structure):
+    _fields_ = [("data", ctypes.POINTER(ctypes.c_float)), ("width", ctypes.c_uint32),
+                ("height", ctypes.c_uint32), ("channels", ctypes.c_uint32)]
+
+
+class SpkDeviceImage(ctypes.Structure):
+    _fields_ = [("buffer", ctypes.c_void_p), ("width", ctypes.c_uint32),
+                ("height", ctypes.c_uint32), ("channels", ctypes.c_uint32)]
+
+
+class SpkResult(ctypes.Structure):
+    _fields_ = [("rgba16", ctypes.POINTER(ctypes.c_uint16)), ("texture", ctypes.c_void_p),
+                ("width", ctypes.c_uint32), ("height", ctypes.c_uint32), ("row_stride_px", ctypes.c_uint32),
+                ("elapsed_ms", ctypes.c_double), ("reprint", ctypes.c_int32),
+                ("negative_was_cached", ctypes.c_int32), ("progress_id", ctypes.c_char * 40)]
+
+
+assert ctypes.sizeof(SpkImage) == 24 and ctypes.sizeof(SpkResult) == 88
+
+P = ctypes.c_void_p
+C = ctypes.c_char_p
+PS = ctypes.POINTER(ctypes.c_char_p)
+I32 = ctypes.c_int32
+U32 = ctypes.c_uint32
+
+# name -> (restype, argtypes); the 26 entry points of the reference ABI
+ABI = {
+    "spk_engine_create": (P, [C, P]),
+    "spk_engine_create_for_device": (P, [C, P, I32]),
+    "spk_engine_destroy": (None, [P]),
+    "spk_engine_trim": (ctypes.c_size_t, [P]),
+    "spk_build_info": (C, []),
+    "spk_capabilities": (C, [P]),
+    "spk_params_schema": (C, [P]),
+    "spk_memory_report": (C, [P]),
+    "spk_warm_up": (I32, [P, C, C, PS]),
+    "spk_open": (P, [P, ctypes.POINTER(SpkImage), C, PS]),
+    "spk_open_device": (P, [P, ctypes.POINTER(SpkDeviceImage), C, PS]),
+    "spk_set_params": (I32, [P, C, PS]),
+    "spk_get_params": (I32, [P, PS]),
+    "spk_session_release": (None, [P]),
+    "spk_render": (I32, [P, C, ctypes.POINTER(SpkResult)]),
+    "spk_reprint": (I32, [P, C, ctypes.POINTER(SpkResult)]),
+    "spk_result_free": (None, [ctypes.POINTER(SpkResult)]),
+    "spk_solve": (I32, [P, C, PS]),
+    "spk_print_lut_catalog": (C, [P]),
+    "spk_print_lut_table": (I32, [P, C, ctypes.POINTER(ctypes.POINTER(ctypes.c_float)), ctypes.POINTER(U32)]),
+    "spk_preview_stock_lut": (I32, [P, C, C, ctypes.POINTER(SpkResult), PS]),
+    "spk_output_transform": (I32, [P, C, C, C, PS, ctypes.POINTER(ctypes.POINTER(ctypes.c_float)),
+                                   ctypes.POINTER(U32)]),
+    "spk_cancel": (None, [P, C]),
+    "spk_progress": (I32, [P, C, PS]),
+    "spk_string_free": (None, [ctypes.c_void_p]),
+    "spk_last_error": (C, [P]),
+}
+
+FP = ctypes.POINTER(ctypes.c_float)
+DP = ctypes.POINTER(ctypes.c_double)
+UP = ctypes.POINTER(ctypes.c_uint32)
+EXT = {
+    "spkx_session_set_halation": (I32, [P, U32, DP, DP, DP]),
+    "spkx_session_profile": (I32, [P, C, I32, U32, PS]),
+    "spkx_session_negative": (I32, [P, C, FP, ctypes.c_size_t]),
+    "spkx_session_setup_json": (I32, [P, ctypes.c_double, PS]),
+    "spkx_sampler_poisson": (I32, [FP, FP, U32, U32, U32]),
+    "spkx_sampler_lognormal": (I32, [FP, U32, ctypes.c_float, ctypes.c_float, U32, U32]),
+    "spkx_philox": (I32, [UP, UP, UP, U32]),
+    "spkx_gaussian": (I32, [FP, FP, U32, U32, DP]),
+    "spkx_setup_json": (I32, [C, C, ctypes.c_double, PS]),
+    "spkx_session_develop_debug": (I32, [P, C, U32, FP, FP]),
+}
+
+REF_EXT = {
+    "spkref_render": (I32, [P, FP, U32, U32, C, U32, DP, DP, DP, DP, U32, ctypes.POINTER(ctypes.c_uint16), FP]),
+    "spkref_setup_json": (I32, [P, C, ctypes.c_double, PS]),
+    "spkref_sampler": (I32, [P, FP, FP, FP, U32, U32, U32, ctypes.c_float, ctypes.c_float]),
+    "spkref_gaussian": (I32, [P, FP, FP, U32, U32, DP, I32]),
+}
+
+
+class SpkError(RuntimeError):
+    def __init__(self, status, message):
+        super().__init__(f"status {status}: {message}")
+        self.status = status
+
+
+def _bind(lib, table):
+    for name, (res, args) in table.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+
+
+class Library:
+    """One loaded library (the B200 engine or the reference oracle)."""
+
+    def __init__(self, path, extensions=True):
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} is not built")
+        self.path = path
+        self.lib = ctypes.CDLL(path, mode=ctypes.RTLD_LOCAL)
+        _bind(self.lib, ABI)
+        self.has_ext = extensions
+        if extensions:
+            _bind(self.lib, EXT)
+
+    def last_error(self):
+        return (self.lib.spk_last_error(None) or b"").decode()
+
+    def check(self, status):
+        if status != SPK_OK:
+            raise SpkError(status, self.last_error())
+
+    def take_json(self, out):
+        if not out.value:
+            return None
+        text = out.value.decode()
+        self.lib.spk_string_free(ctypes.cast(out, ctypes.c_void_p))
+        return json.loads(text)
+
+    def engine(self, resources=RESOURCES, device=None):
+        dev = ctypes.c_int(device) if device is not None else None
+        e = self.lib.spk_engine_create(resources.encode(), ctypes.byref(dev) if dev is not None else None)
+        if not e:
+            raise SpkError(-1, self.last_error())
+        return Engine(self, e)
+
+
+class Engine:
+    def __init__(self, lib, handle):
+        self.L = lib
+        self.h = handle
+
+    def close(self):
+        if self.h:
+            self.L.lib.spk_engine_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def open(self, image, delta=None):
+        img = np.ascontiguousarray(image, dtype=np.float32)
+        h, w, c = img.shape
+        si = SpkImage(img.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), w, h, c)
+        out = ctypes.c_char_p()
+        d = json.dumps(delta).encode() if isinstance(delta, dict) else (delta.encode() if delta else None)
+        s = self.L.lib.spk_open(self.h, ctypes.byref(si), d, ctypes.byref(out))
+        if not s:
+            raise SpkError(-2, self.L.last_error())
+        return Session(self, s, self.L.take_json(out))
+
+
+class Session:
+    def __init__(self, engine, handle, reply):
+        self.E = engine
+        self.L = engine.L
+        self.h = handle
+        self.reply = reply
+
+    def close(self):
+        if self.h:
+            self.L.lib.spk_session_release(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def set_params(self, delta):
+        out = ctypes.c_char_p()
+        self.L.check(self.L.lib.spk_set_params(self.h, json.dumps(delta).encode(), ctypes.byref(out)))
+        return self.L.take_json(out)
+
+    def _render(self, fn, tier):
+        r = SpkResult()
+        self.L.check(fn(self.h, tier.encode(), ctypes.byref(r)))
+        try:
+            a = np.ctypeslib.as_array(r.rgba16, shape=(r.height, r.row_stride_px, 4))[:, : r.width].copy()
+            meta = {"reprint": r.reprint, "negative_was_cached": r.negative_was_cached,
+                    "elapsed_ms": r.elapsed_ms, "row_stride_px": r.row_stride_px,
+                    "progress_id": r.progress_id.decode()}
+        finally:
+            self.L.lib.spk_result_free(ctypes.byref(r))
+        return a, meta
+
+    def render(self, tier="full"):
+        return self._render(self.L.lib.spk_render, tier)
+
+    def reprint(self, tier="full"):
+        return self._render(self.L.lib.spk_reprint, tier)
+
+    # ---- extensions ----
+    def set_halation(self, comps, strength):
+        """comps: list of (weight3, sigma3_px); strength: A per channel."""
+        n = len(comps)
+        w = (ctypes.c_double * max(3 * n, 1))(*[float(v) for c in comps for v in c[0]])
+        s = (ctypes.c_double * max(3 * n, 1))(*[float(v) for c in comps for v in c[1]])
+        a = (ctypes.c_double * 3)(*[float(v) for v in strength])
+        self.L.check(self.L.lib.spkx_session_set_halation(self.h, n, w, s, a))
+
+    def profile(self, tier="full", reprint=False, steps=3):
+        out = ctypes.c_char_p()
+        self.L.check(self.L.lib.spkx_session_profile(self.h, tier.encode(), int(reprint), steps, ctypes.byref(out)))
+        return self.L.take_json(out)
+
+    def negative(self, tier, w, h):
+        buf = np.empty((h, w, 3), np.float32)
+        self.L.check(self.L.lib.spkx_session_negative(self.h, tier.encode(), buf.ctypes.data_as(FP), buf.size))
+        return buf
+
+    def develop_debug(self, tier, seed, w, h, counts=True):
+        neg = np.empty((h, w, 3), np.float32)
+        cnt = np.zeros((h, w, 9), np.float32) if counts else None
+        self.L.check(self.L.lib.spkx_session_develop_debug(self.h, tier.encode(), seed, neg.ctypes.data_as(FP),
+                                                           cnt.ctypes.data_as(FP) if counts else None))
+        return neg, cnt
+
+    def setup_json(self, pitch_um):
+        out = ctypes.c_char_p()
+        self.L.check(self.L.lib.spkx_session_setup_json(self.h, float(pitch_um), ctypes.byref(out)))
+        return self.L.take_json(out)
+
+
+def load(path=LIB_PATH):
+    return Library(path)
+
+
+def load_reference(path=REF_PATH):
+    """The reference engine built for the CPU (oracle); its driver adds the spkref_* entry points."""
+    lib = Library(path, extensions=False)
+    _bind(lib.lib, REF_EXT)
+    return lib
+
+
+def synthetic_image(w, h, seed=0):
+    """Linear ProPhoto RGB, per pixel and channel v = 2^(-8 + 10 u), u from Philox4x32-10 with
+    counter (pixel, channel, 0, 0) and key (seed, 0): the same numbers in C++ and Python."""
+    n = w * h
+    pix = np.arange(n, dtype=np.uint64)
+    out = np.empty((n, 3), np.float32)
+    for c in range(3):
+        words = philox_np(pix, np.full(n, c, np.uint64), seed)
+        u = ((words >> np.uint64(8)).astype(np.float32) + np.float32(0.5)) * np.float32(2.0 ** -24)
+        out[:, c] = np.exp2(np.float32(-8.0) + np.float32(10.0) * u).astype(np.float32)
+    return out.reshape(h, w, 3)
+
+
+M0, M1, W0, W1 = 0xD2511F53, 0xCD9E8D57, 0x9E3779B9, 0xBB67AE85
+
+
+def philox_np(c0, c1, k0, c2=None, c3=None, k1=0):
+    """Philox4x32-10 (Salmon et al. 2011) vectorised in numpy; returns the x word of the block."""
+    mask = np.uint64(0xFFFFFFFF)
+    n = len(c0)
+    x = np.asarray(c0, np.uint64) & mask
+    y = np.asarray(c1, np.uint64) & mask
+    z = np.zeros(n, np.uint64) if c2 is None else np.asarray(c2, np.uint64)
+    w = np.zeros(n, np.uint64) if c3 is None else np.asarray(c3, np.uint64)
+    ka = np.full(n, k0, np.uint64)
+    kb = np.full(n, k1, np.uint64)
+    for _ in range(10):
+        p0 = np.uint64(M0) * x
+        p1 = np.uint64(M1) * z
+        x, y, z, w = ((p1 >> np.uint64(32)) ^ y ^ ka) & mask, p1 & mask, ((p0 >> np.uint64(32)) ^ w ^ kb) & mask, p0 & mask
+        ka = (ka + np.uint64(W0)) & mask
+        kb = (kb + np.uint64(W1)) & mask
+    return x
