@@ -1,0 +1,336 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 spektralab render path: the 4K full render plus reprint workload.
+
+Workload (one step): a 3840 x 2160 float32 linear ProPhoto RGB frame (synthetic, log-uniform in
+[2^-8, 2^2], seed 0), synthetic 3-layer negative and paper stocks, halation as a 2-Gaussian mixture of
+sigma 20 and 120 px (weight 0.03), scanner lens blur 1.5 px, grain on at a pixel pitch giving a mean
+of 600 grains per pixel and sub-layer; one full render (develop + print at print_exposure 1.0), then a
+reprint of the device-resident negative at print_exposure 1.2.
+
+  value         steps / device time, one GPU or the whole job (replicas: every rank renders its own
+                frames, no collective), time = CUDA events on the session stream, L2 flushed (256 MiB
+                written) before every render and reprint, max over ranks
+  e2e           the same workload through the C ABI with host buffers: spk_open from pinned host memory
+                (host->device copy), spk_render, spk_set_params, spk_reprint, each result copied to
+                pinned host memory, wall clock
+  roofline      the dominant kernel: algorithmic bytes per launch / its mean CUDA-event duration
+  cpu_baseline  the reference engine's own code (oracle/_ref) on this host's cores, one quarter-frame
+                render + reprint at the same pixel pitch, scaled to 4K frames/s
+  --impl reference  the reference engine alone on the host cores, same workload and metric
+"""
+
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(REPO, "spektralab-engine_b200"))
+
+import numpy as np  # noqa: E402
+
+import spk_ctypes as sc  # noqa: E402
+import synth_resources  # noqa: E402
+
+METRIC = "4K render/reprint frames/s"
+UNIT = "frames/s"
+W, H = 3840, 2160
+BASE = {"film_stock": "synthetic_negative_400", "print_stock": "synthetic_paper", "auto_exposure": False,
+        "dir_couplers_active": False, "glare_active": False, "scanner_lens_blur": 1.5}
+HALATION = ([((1, 1, 1), (20, 20, 20)), ((1, 1, 1), (120, 120, 120))], (0.03, 0.03, 0.03))
+TARGET_GRAINS = 600.0
+MEASURED_PEAKS = os.path.join(REPO, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+
+# Compulsory HBM bytes per pixel of each kernel in this workload (read + write of its planes; tables
+# that stay in L2 are not counted): 12 bytes per RGB float32 plane pass, 8 per RGBA16 pixel.
+KERNEL_BYTES_PER_PX = {
+    "expose": 24, "iir_h": 24, "iir_v": 36, "fir_v": 24, "fir_h": 24, "lincomb": 36, "copy": 24,
+    "develop": 24, "print": 24, "encode": 32, "halation_h": 36, "halation_v": 60, "scan_blur": 44,
+}
+# ncu DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) per launch of the kernels captured so far,
+# from the summaries under profiles/ (scaled to a 3840 x 2160 launch); None until captured.
+NCU_TRAFFIC_PER_LAUNCH = {}
+
+
+def film_format_for_grains(lib, resources, long_edge):
+    """film_format_mm giving a mean of TARGET_GRAINS grains per sub-layer and pixel (counts scale with
+    the square of the pixel pitch)."""
+    p0 = 10.0
+    out = ctypes.c_char_p()
+    lib.check(lib.lib.spkx_setup_json(resources.encode(), json.dumps(BASE).encode(), p0, ctypes.byref(out)))
+    counts = lib.take_json(out)["f64"]["grain_count"]
+    p = p0 * (TARGET_GRAINS / float(np.mean(counts))) ** 0.5
+    return p * long_edge / 1000.0
+
+
+def hbm_peak():
+    try:
+        with open(MEASURED_PEAKS) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class Clocks:
+    """nvidia-smi samples every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.device)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_init(gpus):
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        pg = dist
+    return rank, local, world, pg
+
+
+def reduce_max(pg, local, value):
+    if pg is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=f"cuda:{local}")
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(pg, local):
+    if pg is None:
+        return
+    import torch
+    pg.barrier(device_ids=[local])
+    torch.cuda.synchronize(local)
+
+
+def cpu_reference_sample(resources, film_format_mm, steps=1):
+    """The reference engine on this host's cores: a 1920 x 1080 quadrant of the workload at the same
+    pixel pitch (film format halved), render + reprint; returns (4K frames/s, seconds, cores)."""
+    ref = sc.load_reference()
+    eng = ref.engine(resources)
+    w, h = W // 2, H // 2
+    img = np.ascontiguousarray(sc.synthetic_image(W, H, 0)[:h, :w])
+    delta = dict(BASE, film_format_mm=film_format_mm / 2.0)
+    comps, strength = HALATION
+    wts = (ctypes.c_double * 6)(*[float(v) for c in comps for v in c[0]])
+    sig = (ctypes.c_double * 6)(*[float(v) for c in comps for v in c[1]])
+    st = (ctypes.c_double * 3)(*strength)
+    s = ref.lib.spkref_open(eng.h, img.ctypes.data_as(sc.FP), w, h, json.dumps(delta).encode(), 2, wts, sig, st)
+    if not s:
+        raise RuntimeError(ref.last_error())
+    out = np.zeros((h, w, 4), np.uint16)
+    times = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        ref.check(ref.lib.spkref_develop(s))
+        ref.check(ref.lib.spkref_print(s, 1.0, out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint16))))
+        ref.check(ref.lib.spkref_print(s, 1.2, out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint16))))
+        times.append(time.perf_counter() - t0)
+    ref.lib.spkref_close(s)
+    eng.close()
+    t = sum(times) / len(times)
+    return 1.0 / (4.0 * t), times, os.cpu_count()
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    resources = synth_resources.ensure(sc.RESOURCES)
+    lib = sc.load()
+    ff = film_format_for_grains(lib, resources, W)
+    if args.warmup > 0:
+        cpu_reference_sample(resources, ff, steps=1)  # warm-up: set-up caches, page faults
+    fps, times, cores = cpu_reference_sample(resources, ff, steps=max(args.steps, 1))
+    sample = f"{args.steps} x (1920x1080 quadrant render + reprint at the 4K pitch), scaled x4 to 3840x2160"
+    line = {"impl": "reference", "metric": METRIC, "value": fps, "unit": UNIT, "n_gpus": 0, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000.0 * 4.0 * sum(times) / len(times), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "4K full render + reprint", "width": W, "height": H},
+            "cpu_baseline": {"value": fps, "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample},
+            "e2e": {"value": fps, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    args.warmup = max(args.warmup, 3)
+
+    rank, local, world, pg = dist_init(args.gpus)
+    resources = synth_resources.ensure(sc.RESOURCES)
+    lib = sc.load()
+    ff = film_format_for_grains(lib, resources, W)
+    delta = dict(BASE, film_format_mm=ff)
+    eng = lib.engine(resources, device=local)
+    img = sc.synthetic_image(W, H, rank)
+
+    # ---- device throughput ----
+    sess = eng.open(img, delta)
+    sess.set_halation(*HALATION)
+    sess.set_params({"print_exposure": 1.0})
+    sess.profile("full", False, args.warmup)
+    sess.set_params({"print_exposure": 1.2})
+    sess.profile("full", True, args.warmup)
+    sess.set_params({"print_exposure": 1.0})
+    barrier(pg, local)
+    with Clocks(local) as clk:
+        t0 = time.perf_counter()
+        pr = sess.profile("full", False, args.steps)
+        sess.set_params({"print_exposure": 1.2})
+        pp = sess.profile("full", True, args.steps)
+        wall = time.perf_counter() - t0
+    barrier(pg, local)
+    dev_ms = sum(pr["total_ms"]) + sum(pp["total_ms"])
+    dev_ms_max = reduce_max(pg, local, dev_ms)
+    value = world * args.steps / (dev_ms_max / 1000.0)
+    render_ms = sum(pr["total_ms"]) / args.steps
+    reprint_ms = sum(pp["total_ms"]) / args.steps
+    launches = int(pr["launches"] + pp["launches"])
+
+    # per-kernel times and the roofline of the dominant kernel
+    kern = {}
+    for prof in (pr, pp):
+        for name, ms in prof["kernels"].items():
+            k = kern.setdefault(name, [])
+            k.extend(ms)
+    table = {n: {"launches": len(v), "total_ms": sum(v), "mean_ms": sum(v) / len(v)} for n, v in kern.items()}
+    dom = max(table, key=lambda n: table[n]["total_ms"])
+    peak, peak_kind = hbm_peak()
+    bytes_launch = KERNEL_BYTES_PER_PX.get(dom, 24) * W * H
+    achieved = bytes_launch / (table[dom]["mean_ms"] / 1000.0) / 1e9
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": NCU_TRAFFIC_PER_LAUNCH.get(dom), "kernel": dom,
+                "algorithmic_bytes_per_launch": bytes_launch, "peak_source": peak_kind}
+    stage_ms = {}
+    for prof in (pr, pp):
+        for name, ms in prof["stages"].items():
+            stage_ms[name] = stage_ms.get(name, 0.0) + sum(ms) / args.steps
+    sess.close()
+
+    # ---- end to end through the C ABI with host buffers ----
+    import torch
+    pinned = torch.empty((H, W, 3), dtype=torch.float32, pin_memory=True).numpy()
+    pinned[...] = img
+    for _ in range(args.warmup):
+        with eng.open(pinned, delta) as s:
+            s.set_halation(*HALATION)
+            s.render("full")
+            s.set_params({"print_exposure": 1.2})
+            s.reprint("full")
+    barrier(pg, local)
+    t0 = time.perf_counter()
+    stride = 0
+    for _ in range(args.steps):
+        with eng.open(pinned, delta) as s:
+            s.set_halation(*HALATION)
+            a, meta = s.render("full")
+            s.set_params({"print_exposure": 1.2})
+            b, _ = s.reprint("full")
+            stride = meta["row_stride_px"]
+    e2e_s = reduce_max(pg, local, time.perf_counter() - t0)
+    barrier(pg, local)
+    e2e = {"value": world * args.steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": W * H * 3 * 4,
+           "d2h_bytes_per_step": 2 * stride * H * 8}
+    eng.close()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and os.path.exists(sc.REF_PATH):
+        fps, times, cores = cpu_reference_sample(resources, ff, steps=1)
+        cpu = {"value": fps, "unit": UNIT, "cores": cores, "kind": "reference",
+               "sample": "one 1920x1080 quadrant render + reprint at the 4K pixel pitch, scaled x4 "
+                         f"({times[0]:.2f} s on {cores} host threads)"}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": dev_ms_max / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": "4K full render + reprint", "width": W, "height": H,
+                           "halation_sigma_px": [20, 120], "halation_weight": 0.03, "scanner_lens_blur_px": 1.5,
+                           "grains_per_px": TARGET_GRAINS, "film_format_mm": round(ff, 4),
+                           "parallelism": f"replicas{world}", "l2": "flushed (256 MiB write) before each step"},
+                "render_ms": render_ms, "reprint_ms": reprint_ms,
+                "render_fps": 1000.0 / render_ms, "reprint_fps": 1000.0 / reprint_ms,
+                "wall_s_timed": wall, "stage_ms": stage_ms, "kernels": table,
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+                "clocks": clk.summary()}
+        print(json.dumps(line), flush=True)
+    if pg is not None:
+        pg.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -71,6 +71,8 @@ def lib():
         for f in ("orc_logf", "orc_expf", "orc_cosf"):
             getattr(L, f).argtypes = [ctypes.c_float]
             getattr(L, f).restype = ctypes.c_float
+        L.orc_uniform.argtypes = [ctypes.c_uint32]
+        L.orc_uniform.restype = ctypes.c_float
         L.orc_splitmix_next.argtypes = [ctypes.POINTER(ctypes.c_uint64)]
         L.orc_splitmix_next.restype = ctypes.c_uint32
         _lib = L

@@ -186,6 +186,76 @@ __attribute__((visibility("default"))) int32_t spkref_render(spk_engine* eng, co
     }
 }
 
+/* A session-like handle for timing: spkref_open builds the set-up and copies the frame (what the
+ * reference's spk_open does), spkref_develop and spkref_print are the render and the reprint. */
+struct RefSession {
+    Engine* e = nullptr;
+    Built b;
+    gpu::Plane src, neg;
+    std::vector<double> weights, sigmas;
+    double strength[3] = {0, 0, 0};
+    uint32_t n = 0;
+    fx::SeedSequence seeds;
+};
+
+__attribute__((visibility("default"))) void* spkref_open(spk_engine* eng, const float* rgb, uint32_t w, uint32_t h,
+                                                         const char* delta, uint32_t n, const double* weights,
+                                                         const double* sigmas, const double* strength) {
+    try {
+        auto* s = new RefSession();
+        s->e = reinterpret_cast<Engine*>(eng);
+        s->b = build(*s->e, delta);
+        s->src = s->e->gpu().persistent_plane(w, h, gpu::MemTag::Source);
+        float* o = s->src.data();
+        for (size_t i = 0; i < size_t(w) * h * 3; ++i) o[i] = std::isfinite(rgb[i]) ? rgb[i] : 0.0f;
+        s->n = n;
+        s->weights.assign(weights, weights + 3 * n);
+        s->sigmas.assign(sigmas, sigmas + 3 * n);
+        for (int c = 0; c < 3; ++c) s->strength[c] = strength ? strength[c] : 0.0;
+        return s;
+    } catch (const std::exception& ex) {
+        fail_status(ex);
+        return nullptr;
+    }
+}
+
+__attribute__((visibility("default"))) int32_t spkref_develop(void* handle) {
+    try {
+        auto* s = static_cast<RefSession*>(handle);
+        using params::P;
+        core::RenderContext ctx{.gpu = s->e->gpu(), .device = s->e->device(), .variants = s->e->variants()};
+        ctx.pitch_um = film::pitch_um(s->b.p->f(P::film_format_mm), std::max(s->src.w, s->src.h));
+        const uint32_t seed = s->b.p->b(P::grain_active) ? s->seeds.next() : fx::kNoGrainFilmSeed;
+        s->neg = gpu::Plane{};
+        s->neg = develop_override(ctx, *s->b.film, s->src, seed, s->n, s->weights.data(), s->sigmas.data(), s->strength);
+        return SPK_OK;
+    } catch (const std::exception& ex) {
+        return fail_status(ex);
+    }
+}
+
+__attribute__((visibility("default"))) int32_t spkref_print(void* handle, double print_exposure, uint16_t* out_rgba) {
+    try {
+        auto* s = static_cast<RefSession*>(handle);
+        core::RenderContext ctx{.gpu = s->e->gpu(), .device = s->e->device(), .variants = s->e->variants()};
+        ctx.pitch_um = film::pitch_um(s->b.p->f(params::P::film_format_mm), std::max(s->src.w, s->src.h));
+        ctx.rho_tier = 1.0;
+        print::LiveParams live = print::LiveParams::from(*s->b.p);
+        live.print_exposure = print_exposure;
+        gpu::OutputImage img = print::print_scan_encode(ctx, *s->b.print, {s->neg, live, 0u});
+        if (out_rgba)
+            for (uint32_t y = 0; y < s->neg.h; ++y)
+                std::memcpy(out_rgba + size_t(y) * s->neg.w * 4, img.rgba16 + size_t(y) * img.row_stride_px * 4,
+                            size_t(s->neg.w) * 8);
+        gpu::Context::release_texture(img.texture);
+        return SPK_OK;
+    } catch (const std::exception& ex) {
+        return fail_status(ex);
+    }
+}
+
+__attribute__((visibility("default"))) void spkref_close(void* handle) { delete static_cast<RefSession*>(handle); }
+
 /* spkref_setup_json(engine, delta, pitch_um, out_json): the reference's narrowed kernel constants under the
  * same keys as the B200 build's spkx_session_setup_json */
 __attribute__((visibility("default"))) int32_t spkref_setup_json(spk_engine* eng, const char* delta, double pitch_um,

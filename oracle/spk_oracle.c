@@ -508,6 +508,7 @@ void orc_philox(const uint32_t* ctr, const uint32_t* key, uint32_t* out, uint32_
     }
 }
 
+float orc_uniform(uint32_t word) { return spk_uniform(word); }
 float orc_logf(float x) { return spk_logf(x); }
 float orc_expf(float x) { return spk_expf(x); }
 float orc_cosf(float x) { return spk_cosf(x); }

@@ -81,6 +81,7 @@ void orc_gaussian(const double* in, double* out, int32_t w, int32_t h, const dou
 void orc_poisson(const float* lam, float* counts, uint32_t n, uint32_t stream, uint32_t seed);
 void orc_lognormal(float* out, uint32_t n, float mean, float sd, uint32_t stream, uint32_t seed);
 void orc_philox(const uint32_t* ctr, const uint32_t* key, uint32_t* out, uint32_t n);
+float orc_uniform(uint32_t word);
 float orc_logf(float x);
 float orc_expf(float x);
 float orc_cosf(float x);

@@ -9,6 +9,8 @@
 #include <math.h>
 #include <stdint.h>
 
+#include <atomic>
+
 #include "../grain_sampler.h"
 #include "../kernel_args.h"
 #include "launch.hpp"
@@ -625,81 +627,116 @@ __global__ void k_philox(const uint32_t* ctr, const uint32_t* key, uint32_t* out
 
 // ---- launchers ------------------------------------------------------------------------------------
 
+namespace {
+thread_local LaunchHook* t_hook = nullptr;
+std::atomic<uint64_t> g_launches{0};
+
+// Counts a launch and lets the thread's hook bracket it with events.
+struct Probe {
+    cudaStream_t s;
+    Probe(const char* name, cudaStream_t st) : s(st) {
+        g_launches.fetch_add(1, std::memory_order_relaxed);
+        if (t_hook) t_hook->before(name, s);
+    }
+    ~Probe() {
+        if (t_hook) t_hook->after(s);
+    }
+};
+}  // namespace
+
+void set_launch_hook(LaunchHook* hook) { t_hook = hook; }
+uint64_t launch_count() { return g_launches.load(); }
+
 void expose(const float* rgb, float* h, const float* table, const ExposeArgs& a, cudaStream_t s) {
     if (a.n == 0) return;
+    Probe p("expose", s);
     k_expose<<<div_up(a.n, 256), 256, 0, s>>>(rgb, h, table, a);
 }
 
 void fir_v(const float* in, float* out, uint32_t w, uint32_t h, const FirTaps& t, cudaStream_t s) {
     const dim3 b(32, 8), g(div_up(w, 32), div_up(h, 8));
+    Probe p("fir_v", s);
     k_fir_v<<<g, b, 0, s>>>(in, out, w, h, t);
 }
 
 void fir_h(const float* in, float* out, const float* acc, uint32_t w, uint32_t h, const FirTaps& t, int mode,
            const float weight[3], cudaStream_t s) {
     const dim3 b(32, 8), g(div_up(w, 32), div_up(h, 8));
+    Probe p("fir_h", s);
     k_fir_h<<<g, b, 0, s>>>(in, out, acc, w, h, t, mode, weight[0], weight[1], weight[2]);
 }
 
 void iir_h(const float* in, float* out, uint32_t w, uint32_t h, const IirCoefs& c, cudaStream_t s) {
+    Probe p("iir_h", s);
     k_iir_h<<<div_up(3 * h, 64), 64, 0, s>>>(in, out, w, h, c);
 }
 
 void iir_v(float* work, float* out, const float* acc, uint32_t w, uint32_t h, const IirCoefs& c, int mode,
            const float weight[3], cudaStream_t s) {
+    Probe p("iir_v", s);
     k_iir_v<<<div_up(3 * w, 64), 64, 0, s>>>(work, out, acc, w, h, c, mode, weight[0], weight[1], weight[2]);
 }
 
 void lincomb(const float* x, const float* y, float* out, size_t pixels, const float a[3], const float b[3],
              cudaStream_t s) {
     if (pixels == 0) return;
+    Probe p("lincomb", s);
     k_lincomb<<<unsigned((pixels + 255) / 256), 256, 0, s>>>(x, y, out, pixels, a[0], a[1], a[2], b[0], b[1], b[2]);
 }
 
 void copy(const float* x, float* out, size_t pixels, cudaStream_t s) {
     const size_t n = 3 * pixels;
     if (n == 0) return;
+    Probe p("copy", s);
     k_copy<<<unsigned((n + 255) / 256), 256, 0, s>>>(x, out, n);
 }
 
 void develop(const float* exposure, float* out, const DevelopArgs& a, uint32_t w, uint32_t h, cudaStream_t s) {
     const dim3 b(32, 4), g(div_up(w, 32), div_up(h, 4));
+    Probe p("develop", s);
     k_develop<<<g, b, 0, s>>>(exposure, out, w, h, a);
 }
 
 void print(const float* neg, float* rgb, const PrintArgs& a, cudaStream_t s) {
     if (a.n == 0) return;
+    Probe p("print", s);
     k_print<<<div_up(a.n, 128), 128, 0, s>>>(neg, rgb, a);
 }
 
 void encode(const float* rgb, const float* g, uint16_t* out, uint32_t w, uint32_t h, const EncodeArgs& e,
             cudaStream_t s) {
     const dim3 b(32, 8), gr(div_up(w, 32), div_up(h, 8));
+    Probe p("encode", s);
     k_encode<<<gr, b, 0, s>>>(rgb, g, out, w, h, e);
 }
 
 void source_copy(const float* raw, float* out, size_t pixels, uint32_t channels, cudaStream_t s) {
     if (pixels == 0) return;
+    Probe p("source_copy", s);
     k_source<<<unsigned((pixels + 255) / 256), 256, 0, s>>>(raw, out, pixels, channels);
 }
 
 void fill(void* p, size_t bytes, uint32_t v, cudaStream_t s) {
+    Probe pr("fill", s);
     k_fill<<<148 * 8, 256, 0, s>>>(static_cast<uint4*>(p), bytes / 16, v);
 }
 
 void sampler_poisson(const float* lam, float* out, uint32_t n, uint32_t stream, uint32_t seed, cudaStream_t s) {
     if (n == 0) return;
+    Probe p("sampler_poisson", s);
     k_sampler_poisson<<<div_up(n, 128), 128, 0, s>>>(lam, out, n, stream, seed);
 }
 
 void sampler_lognormal(float* out, uint32_t n, float mean, float stddev, uint32_t stream, uint32_t seed,
                        cudaStream_t s) {
     if (n == 0) return;
+    Probe p("sampler_lognormal", s);
     k_sampler_lognormal<<<div_up(n, 128), 128, 0, s>>>(out, n, mean, stddev, stream, seed);
 }
 
 void philox_blocks(const uint32_t* ctr, const uint32_t* key, uint32_t* out, uint32_t n, cudaStream_t s) {
     if (n == 0) return;
+    Probe p("philox", s);
     k_philox<<<div_up(n, 128), 128, 0, s>>>(ctr, key, out, n);
 }
 

@@ -10,6 +10,16 @@
 
 namespace spkb::dev {
 
+// Observation of kernel launches: every launcher below counts itself, and when the calling thread has
+// a hook set, brackets its launch with before/after (the hook records CUDA events on the stream).
+struct LaunchHook {
+    virtual void before(const char* kernel, cudaStream_t s) = 0;
+    virtual void after(cudaStream_t s) = 0;
+    virtual ~LaunchHook() = default;
+};
+void set_launch_hook(LaunchHook* hook);  // per thread; nullptr clears
+uint64_t launch_count();                 // kernels launched by this library since load
+
 // RGB -> film exposure H (Mitchell bicubic of the spectral table), times the compensation gain.
 void expose(const float* rgb, float* h, const float* table, const ExposeArgs& a, cudaStream_t s);
 

@@ -87,6 +87,11 @@ public:
     std::mutex m;
     std::set<Session*> sessions;
     std::string capabilities, memory_report;
+    // Built pipelines by parameter set: the binary64 set-up and its device tables depend only on the
+    // parameters and the resources, so a later open or rebuild with the same parameters reuses them.
+    std::mutex pipelines_m;
+    std::vector<std::pair<std::string, Pipeline>> pipelines;  // most recent last
+    static constexpr size_t kPipelineCache = 8;
 };
 
 struct TierState {
@@ -130,11 +135,20 @@ public:
 
     Pipeline build(const ParamSet& p, std::shared_ptr<const Profile> f, std::shared_ptr<const Profile> pr) {
         check_supported(p);
+        const std::string key = json::write(p.to_json()) + (product_defaults ? "|pd" : "|");
+        {
+            std::lock_guard<std::mutex> g(engine->pipelines_m);
+            for (auto& [k, pl] : engine->pipelines)
+                if (k == key) return pl;
+        }
         Pipeline pl;
         auto fs = build_film_setup(p, f, *engine->res);
         pl.print = build_print_setup(p, *fs, pr, *engine->res, engine->cam16, !product_defaults);
         pl.film = fs;
         upload_tables(pool, stream, pl);
+        std::lock_guard<std::mutex> g(engine->pipelines_m);
+        engine->pipelines.emplace_back(key, pl);
+        if (engine->pipelines.size() > Engine::kPipelineCache) engine->pipelines.erase(engine->pipelines.begin());
         return pl;
     }
 
@@ -322,7 +336,6 @@ void render(Session& s, const char* tier_name, bool reprint, spk_result* out) {
     const auto t0 = std::chrono::steady_clock::now();
     const std::optional<Tier> t = parse_tier(tier_name);
     if (!t) fail_invalid(std::string("unknown tier '") + (tier_name ? tier_name : "") + "'");
-    s.check_tier(*t);
     DeviceGuard dg(s.engine->device);
     TierState& ts = s.tiers[int(*t)];
     const bool reuse = reprint && static_cast<bool>(ts.negative);
@@ -334,6 +347,7 @@ void render(Session& s, const char* tier_name, bool reprint, spk_result* out) {
     bool developed = false;
     OutputImage* img = nullptr;
     try {
+        s.check_tier(*t);  // a tier this build cannot make is a render failure (SPK_ERR_GPU), as in the reference
         RenderCtx ctx{s.pool, s.stream};
         ctx.rho_tier = 1.0;
         if (!reuse) {
@@ -404,14 +418,23 @@ std::string session_profile(Session& s, const char* tier_name, bool reprint, uin
     DevBuffer flush = s.pool.acquire(size_t(256) << 20);
     OutputImage* img = output_acquire(s.engine->device, s.source.w, s.source.h);
     json::Value stages = json::Object{};
+    json::Value kernels = json::Object{};
     json::Array totals;
     Timer timer;
     cudaEvent_t a, b;
     cudaEventCreate(&a);
     cudaEventCreate(&b);
+    const uint64_t launches0 = dev::launch_count();
+    uint64_t flushes = 0;
+    struct HookGuard {
+        ~HookGuard() { dev::set_launch_hook(nullptr); }
+    } hook_guard;
     try {
         for (uint32_t k = 0; k < steps; ++k) {
+            dev::set_launch_hook(nullptr);
             dev::fill(flush.ptr(), flush.size() / 16 * 16, k, s.stream);
+            ++flushes;
+            dev::set_launch_hook(&timer);
             RenderCtx ctx{s.pool, s.stream};
             ctx.timer = &timer;
             cudaEventRecord(a, s.stream);
@@ -435,6 +458,13 @@ std::string session_profile(Session& s, const char* tier_name, bool reprint, uin
                 if (arr.is_null()) arr = json::Array{};
                 arr.as_array().push_back(json::Value(double(sm)));
             }
+            for (const Timer::Mark& m : timer.kernels) {
+                float sm = 0;
+                cudaEventElapsedTime(&sm, m.a, m.b);
+                json::Value& arr = kernels[m.name];
+                if (arr.is_null()) arr = json::Array{};
+                arr.as_array().push_back(json::Value(double(sm)));
+            }
             timer.reset();
         }
     } catch (...) {
@@ -450,6 +480,8 @@ std::string session_profile(Session& s, const char* tier_name, bool reprint, uin
     r["steps"] = steps;
     r["total_ms"] = std::move(totals);
     r["stages"] = std::move(stages);
+    r["kernels"] = std::move(kernels);  // per kernel name: the duration of every launch, all steps
+    r["launches"] = double(dev::launch_count() - launches0 - flushes);
     r["pixels"] = double(s.source.pixels());
     return json::write(r);
 }

@@ -46,12 +46,22 @@ void Timer::begin(const char* name, cudaStream_t s) {
     marks.push_back(m);
 }
 void Timer::end(cudaStream_t s) { cudaEventRecord(marks.back().b, s); }
+void Timer::before(const char* kernel, cudaStream_t s) {
+    Mark m{kernel, nullptr, nullptr};
+    cudaEventCreate(&m.a);
+    cudaEventCreate(&m.b);
+    cudaEventRecord(m.a, s);
+    kernels.push_back(m);
+}
+void Timer::after(cudaStream_t s) { cudaEventRecord(kernels.back().b, s); }
 void Timer::reset() {
-    for (Mark& m : marks) {
-        cudaEventDestroy(m.a);
-        cudaEventDestroy(m.b);
+    for (std::vector<Mark>* v : {&marks, &kernels}) {
+        for (Mark& m : *v) {
+            cudaEventDestroy(m.a);
+            cudaEventDestroy(m.b);
+        }
+        v->clear();
     }
-    marks.clear();
 }
 Timer::~Timer() { reset(); }
 

@@ -10,6 +10,7 @@
 #include <optional>
 #include <vector>
 
+#include "../cuda/launch.hpp"
 #include "device.hpp"
 #include "setup.hpp"
 
@@ -43,16 +44,19 @@ struct RenderCtx {
 };
 
 // Stage timing with CUDA events on the render stream (bench and profile entry points).
-struct Timer {
+struct Timer : dev::LaunchHook {
     struct Mark {
         const char* name;
         cudaEvent_t a, b;
     };
-    std::vector<Mark> marks;
+    std::vector<Mark> marks;    // stages
+    std::vector<Mark> kernels;  // every kernel launch inside them
     void begin(const char* name, cudaStream_t s);
     void end(cudaStream_t s);
+    void before(const char* kernel, cudaStream_t s) override;
+    void after(cudaStream_t s) override;
     void reset();
-    ~Timer();
+    ~Timer() override;
 };
 
 // film side: raw source plane -> developed negative density plane (a fresh persistent plane)

@@ -107,6 +107,10 @@ REF_EXT = {
     "spkref_setup_json": (I32, [P, C, ctypes.c_double, PS]),
     "spkref_sampler": (I32, [P, FP, FP, FP, U32, U32, U32, ctypes.c_float, ctypes.c_float]),
     "spkref_gaussian": (I32, [P, FP, FP, U32, U32, DP, I32]),
+    "spkref_open": (P, [P, FP, U32, U32, C, U32, DP, DP, DP]),
+    "spkref_develop": (I32, [P]),
+    "spkref_print": (I32, [P, ctypes.c_double, ctypes.POINTER(ctypes.c_uint16)]),
+    "spkref_close": (None, [P]),
 }
 
 

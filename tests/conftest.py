@@ -1,0 +1,75 @@
+"""Shared fixtures. Tests marked `gpu` need a CUDA device (they run on a B200 box); all others run
+on any CPU machine. The checkers (the float64 oracle and the CPU build of the reference engine) are
+loaded only here and in the tests."""
+
+import json
+import os
+import sys
+
+import numpy as np
+import pytest
+
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+PKG = os.path.join(REPO, "spektralab-engine_b200")
+ORACLE = os.path.join(REPO, "oracle")
+GOLDEN = os.path.join(REPO, "tests", "golden")
+for p in (PKG, ORACLE):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+import spk_ctypes as sc  # noqa: E402
+import synth_resources  # noqa: E402
+
+BASE = {"film_stock": "synthetic_negative_400", "print_stock": "synthetic_paper", "auto_exposure": False,
+        "dir_couplers_active": False, "glare_active": False}
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA device (B200)")
+
+
+@pytest.fixture(scope="session")
+def resources():
+    return synth_resources.ensure(sc.RESOURCES)
+
+
+@pytest.fixture(scope="session")
+def lib():
+    return sc.load()
+
+
+@pytest.fixture(scope="session")
+def ref(resources):
+    if not os.path.exists(sc.REF_PATH):
+        pytest.skip("the CPU build of the reference engine (oracle/_ref) is not built here")
+    return sc.load_reference()
+
+
+@pytest.fixture(scope="session")
+def ref_engine(ref, resources):
+    e = ref.engine(resources)
+    yield e
+    e.close()
+
+
+@pytest.fixture(scope="session")
+def engine(lib, resources):
+    e = lib.engine(resources)
+    yield e
+    e.close()
+
+
+def setup_f64(lib, resources, delta, pitch):
+    import ctypes
+    out = ctypes.c_char_p()
+    lib.check(lib.lib.spkx_setup_json(resources.encode(), json.dumps(delta).encode(), float(pitch), ctypes.byref(out)))
+    return lib.take_json(out)
+
+
+def lsb_stats(a, b):
+    d = np.abs(a.astype(np.int64) - b.astype(np.int64))[..., :3]
+    return {"max": int(d.max()), "mean": float(d.mean()), "frac_gt1": float((d > 1).mean())}
+
+
+def golden(name):
+    return np.load(os.path.join(GOLDEN, name))
