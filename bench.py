@@ -94,7 +94,7 @@ class Clocks:
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                                          "-lms", "200", "-i", str(self.device)], stdout=subprocess.PIPE,
+                                          "-lms", "100", "-i", str(self.device)], stdout=subprocess.PIPE,
                                          stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
@@ -246,7 +246,12 @@ def main():
     sess.profile("full", True, args.warmup)
     sess.set_params({"print_exposure": 1.0})
     barrier(pg, local)
+    # clocks are sampled every 100 ms from one second of untimed load before the timed steps to their end
     with Clocks(local) as clk:
+        t_heat = time.perf_counter()
+        while time.perf_counter() - t_heat < 1.0:
+            sess.profile("full", False, 1)
+        barrier(pg, local)
         t0 = time.perf_counter()
         pr = sess.profile("full", False, args.steps)
         sess.set_params({"print_exposure": 1.2})

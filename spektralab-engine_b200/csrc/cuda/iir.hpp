@@ -1,0 +1,49 @@
+// The block-parallel recursive Gaussian mixture (iir.cu): arguments and launchers.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../kernel_args.h"
+#include "launch.hpp"
+
+namespace spkb::dev {
+
+// One channel of one component: Young-van Vliet coefficients and M, the map of a segment's entry
+// state (w[i-1], w[i-2], w[i-3]) through seg_len steps of the homogeneous recurrence.
+struct IirChannel {
+    double B, B1, B2, B3;
+    double M[3][3];
+    int32_t active;  // 0: the channel passes through (its sigma is on the FIR or identity branch)
+    int32_t pad;
+};
+
+struct IirLaunch {
+    int32_t seg_len;
+    int32_t pad;
+    IirChannel ch[3 * SPKB_MAX_COMPONENTS];  // [component * 3 + channel]
+};
+
+struct IirMixture {
+    uint32_t ncomp;
+    float weight[SPKB_MAX_COMPONENTS][3];
+    float mix_a[3], mix_b[3];  // raw := mix_a raw + mix_b sum_k weight_k G_k(raw)
+    IirLaunch rows, cols;
+};
+
+struct IirPlanes {
+    float* p[SPKB_MAX_COMPONENTS];
+};
+
+size_t iir_rows_smem(uint32_t w);
+size_t iir_cols_smem(uint32_t h);
+int iir_row_segments();
+int iir_col_segments();
+bool iir_mixture_fits(uint32_t w, uint32_t h);  // both kernels' lines fit in shared memory
+
+// raw := mix_a raw + mix_b sum_k weight_k G_k(raw), every component recursive on every channel.
+// tmp: ncomp planes for the row results; acc: one plane for the running sum (unused for one component).
+void iir_mixture(float* raw, float* const* tmp, float* acc, uint32_t w, uint32_t h, const IirMixture& m,
+                 cudaStream_t s);
+
+}  // namespace spkb::dev

@@ -630,19 +630,15 @@ __global__ void k_philox(const uint32_t* ctr, const uint32_t* key, uint32_t* out
 namespace {
 thread_local LaunchHook* t_hook = nullptr;
 std::atomic<uint64_t> g_launches{0};
-
-// Counts a launch and lets the thread's hook bracket it with events.
-struct Probe {
-    cudaStream_t s;
-    Probe(const char* name, cudaStream_t st) : s(st) {
-        g_launches.fetch_add(1, std::memory_order_relaxed);
-        if (t_hook) t_hook->before(name, s);
-    }
-    ~Probe() {
-        if (t_hook) t_hook->after(s);
-    }
-};
 }  // namespace
+
+Probe::Probe(const char* name, cudaStream_t st) : s(st) {
+    g_launches.fetch_add(1, std::memory_order_relaxed);
+    if (t_hook) t_hook->before(name, s);
+}
+Probe::~Probe() {
+    if (t_hook) t_hook->after(s);
+}
 
 void set_launch_hook(LaunchHook* hook) { t_hook = hook; }
 uint64_t launch_count() { return g_launches.load(); }

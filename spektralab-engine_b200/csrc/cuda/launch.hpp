@@ -20,6 +20,13 @@ struct LaunchHook {
 void set_launch_hook(LaunchHook* hook);  // per thread; nullptr clears
 uint64_t launch_count();                 // kernels launched by this library since load
 
+// Brackets one launch: counts it and calls the thread's hook.
+struct Probe {
+    cudaStream_t s;
+    Probe(const char* kernel, cudaStream_t stream);
+    ~Probe();
+};
+
 // RGB -> film exposure H (Mitchell bicubic of the spectral table), times the compensation gain.
 void expose(const float* rgb, float* h, const float* table, const ExposeArgs& a, cudaStream_t s);
 

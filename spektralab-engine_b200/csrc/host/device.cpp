@@ -1,5 +1,6 @@
 #include "device.hpp"
 
+#include <cstdint>
 #include <vector>
 
 #include "status.hpp"
@@ -11,25 +12,21 @@ void cuda_check(cudaError_t e, const char* what) {
 }
 
 struct PoolState {
-    mutable std::mutex m;
-    std::multimap<size_t, void*> free;
-    size_t live = 0, idle = 0;
-    ~PoolState() {
-        for (auto& [sz, p] : free) cudaFree(p);
-    }
+    std::mutex m;
+    cudaStream_t stream = nullptr;
+    size_t live = 0;
 };
 
 struct DevBuffer::Impl {
     void* p = nullptr;
     size_t size = 0;
-    std::shared_ptr<PoolState> pool;  // null: persistent
+    std::shared_ptr<PoolState> pool;  // null: persistent (cudaMalloc)
     ~Impl() {
         if (!p) return;
         if (pool) {
             std::lock_guard<std::mutex> g(pool->m);
-            pool->free.emplace(size, p);
+            cudaFreeAsync(p, pool->stream);
             pool->live -= size;
-            pool->idle += size;
         } else {
             cudaFree(p);
         }
@@ -39,38 +36,34 @@ struct DevBuffer::Impl {
 void* DevBuffer::ptr() const { return p_ ? p_->p : nullptr; }
 size_t DevBuffer::size() const { return p_ ? p_->size : 0; }
 
-Pool::Pool() : s_(std::make_shared<PoolState>()) {}
+Pool::Pool(cudaStream_t stream) : s_(std::make_shared<PoolState>()) { s_->stream = stream; }
+
+void Pool::set_stream(cudaStream_t s) {
+    std::lock_guard<std::mutex> g(s_->m);
+    s_->stream = s;
+}
+
+cudaStream_t Pool::stream() const { return s_->stream; }
 
 DevBuffer Pool::acquire(size_t bytes) {
     bytes = std::max<size_t>((bytes + 255) / 256 * 256, 256);
     void* p = nullptr;
-    size_t size = 0;
-    {
-        std::lock_guard<std::mutex> g(s_->m);
-        auto it = s_->free.lower_bound(bytes);
-        if (it != s_->free.end() && it->first <= 2 * bytes) {
-            size = it->first;
-            p = it->second;
-            s_->free.erase(it);
-            s_->idle -= size;
-        }
-    }
-    if (!p) {
-        cudaError_t e = cudaMalloc(&p, bytes);
-        if (e != cudaSuccess) {
-            (void)cudaGetLastError();
-            trim();
-            cuda_check(cudaMalloc(&p, bytes), "cudaMalloc (scratch)");
-        }
-        size = bytes;
+    cudaError_t e = cudaMallocAsync(&p, bytes, s_->stream);
+    if (e != cudaSuccess) {
+        (void)cudaGetLastError();
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaStreamSynchronize(s_->stream);
+        device_pool_trim(dev);
+        cuda_check(cudaMallocAsync(&p, bytes, s_->stream), "cudaMallocAsync (scratch)");
     }
     {
         std::lock_guard<std::mutex> g(s_->m);
-        s_->live += size;
+        s_->live += bytes;
     }
     auto impl = std::make_shared<DevBuffer::Impl>();
     impl->p = p;
-    impl->size = size;
+    impl->size = bytes;
     impl->pool = s_;
     DevBuffer b;
     b.p_ = std::move(impl);
@@ -83,7 +76,9 @@ DevBuffer Pool::persistent(size_t bytes) {
     cudaError_t e = cudaMalloc(&p, bytes);
     if (e != cudaSuccess) {
         (void)cudaGetLastError();
-        trim();
+        int dev = 0;
+        cudaGetDevice(&dev);
+        device_pool_trim(dev);
         cuda_check(cudaMalloc(&p, bytes), "cudaMalloc (persistent)");
     }
     auto impl = std::make_shared<DevBuffer::Impl>();
@@ -94,25 +89,33 @@ DevBuffer Pool::persistent(size_t bytes) {
     return b;
 }
 
-size_t Pool::trim() {
-    std::lock_guard<std::mutex> g(s_->m);
-    size_t freed = 0;
-    for (auto& [sz, p] : s_->free) {
-        cudaFree(p);
-        freed += sz;
-    }
-    s_->free.clear();
-    s_->idle = 0;
-    return freed;
-}
-
 size_t Pool::live_bytes() const {
     std::lock_guard<std::mutex> g(s_->m);
     return s_->live;
 }
-size_t Pool::free_bytes() const {
-    std::lock_guard<std::mutex> g(s_->m);
-    return s_->idle;
+
+void configure_device_pool(int device) {
+    cudaMemPool_t mp = nullptr;
+    cuda_check(cudaDeviceGetDefaultMemPool(&mp, device), "cudaDeviceGetDefaultMemPool");
+    uint64_t threshold = UINT64_MAX;
+    cuda_check(cudaMemPoolSetAttribute(mp, cudaMemPoolAttrReleaseThreshold, &threshold), "cudaMemPoolSetAttribute");
+}
+
+size_t device_pool_reserved(int device) {
+    cudaMemPool_t mp = nullptr;
+    if (cudaDeviceGetDefaultMemPool(&mp, device) != cudaSuccess) return 0;
+    uint64_t v = 0;
+    cudaMemPoolGetAttribute(mp, cudaMemPoolAttrReservedMemCurrent, &v);
+    return size_t(v);
+}
+
+size_t device_pool_trim(int device) {
+    cudaMemPool_t mp = nullptr;
+    if (cudaDeviceGetDefaultMemPool(&mp, device) != cudaSuccess) return 0;
+    const size_t before = device_pool_reserved(device);
+    cudaMemPoolTrimTo(mp, 0);
+    const size_t after = device_pool_reserved(device);
+    return before > after ? before - after : 0;
 }
 
 // ---- result images -------------------------------------------------------------------------------

@@ -1,9 +1,11 @@
 // Device memory and streams of the B200 engine.
 //
-//   Pool        per engine: device scratch buffers reused by the rule "smallest free buffer of size in
-//               [b, 2b]" (the reference's scratch pool rule, src/gpu/gpu.mm:125-161). A render returns its
-//               scratch only after its stream has completed, so reuse never races with a kernel.
-//   DevBuffer   a handle; dropping the last copy returns the memory to its pool (or frees it).
+//   Pool        per session: scratch buffers from CUDA's stream-ordered allocator (cudaMallocAsync on the
+//               session's stream, from the device's memory pool, which keeps freed memory cached), so a
+//               plane freed by one stage is reused by the next on the same stream with no
+//               synchronisation and a new session allocates from the cache.
+//   persistent  tables that can outlive a session (cached pipelines): plain cudaMalloc / cudaFree.
+//   DevBuffer   a handle; dropping the last copy frees the memory (stream-ordered for scratch).
 //   Plane       interleaved binary32 RGB in device memory.
 //   OutputImage a rendered RGBA16 image: a device copy and a pinned host copy, drawn from a process-wide
 //               cache so that a result outlives its session and engine and pinning is paid once.
@@ -41,16 +43,21 @@ private:
 
 class Pool {
 public:
-    Pool();
-    DevBuffer acquire(size_t bytes);          // device memory, contents undefined
-    DevBuffer persistent(size_t bytes);       // never pooled: freed when the last handle drops
-    size_t trim();                            // frees every idle buffer; returns bytes freed
-    size_t live_bytes() const;
-    size_t free_bytes() const;
+    explicit Pool(cudaStream_t stream = nullptr);
+    void set_stream(cudaStream_t s);
+    cudaStream_t stream() const;
+    DevBuffer acquire(size_t bytes);          // stream-ordered device memory, contents undefined
+    DevBuffer persistent(size_t bytes);       // cudaMalloc'd: may outlive the stream
+    size_t live_bytes() const;                // bytes of this pool's live scratch buffers
 
 private:
     std::shared_ptr<PoolState> s_;
 };
+
+// The device memory pool behind every Pool: keep all freed memory cached (release threshold max).
+void configure_device_pool(int device);
+size_t device_pool_trim(int device);          // returns the cached bytes released to the driver
+size_t device_pool_reserved(int device);
 
 struct Plane {
     DevBuffer buf;

@@ -122,7 +122,14 @@ public:
     bool done = false;
 
     ~Session() {
-        if (stream) cudaStreamDestroy(stream);
+        // stream-ordered buffers are freed on the stream, so they go before it does
+        for (TierState& t : tiers) t.negative = Plane{};
+        source = Plane{};
+        pipe = Pipeline{};
+        if (stream) {
+            cudaStreamSynchronize(stream);
+            cudaStreamDestroy(stream);
+        }
     }
 
     void digest(ParamSet& p, const Profile& f) const {
@@ -244,6 +251,7 @@ spk_engine* create(const char* dir, void* device, int32_t type) noexcept {
         else cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
         if (dev < 0 || dev >= n) fail_gpu("CUDA device ordinal out of range");
         DeviceGuard g(dev);
+        configure_device_pool(dev);
         auto e = std::make_unique<Engine>();
         e->device = dev;
         e->res = Resources::load(dir);
@@ -269,6 +277,7 @@ Session* open_session(Engine& e, const void* data, bool device_ptr, uint32_t w, 
     s->engine = &e;
     s->product_defaults = d.product_defaults.value_or(false);
     cuda_check(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    s->pool.set_stream(s->stream);
     ParamSet p;
     for (const auto& [fid, v] : d.fields)
         if (fid == size_t(P::film_stock) || fid == size_t(P::print_stock)) p.set(fid, v);
@@ -281,7 +290,7 @@ Session* open_session(Engine& e, const void* data, bool device_ptr, uint32_t w, 
     s->digest(p, *film);
 
     // the frame: raw upload, then channels and non-finite values fixed on the device
-    s->source = Plane{s->pool.persistent(size_t(npx) * 12), w, h};
+    s->source = Plane{s->pool.acquire(size_t(npx) * 12), w, h};
     const size_t raw_bytes = size_t(npx) * ch * sizeof(float);
     DevBuffer raw = s->pool.acquire(raw_bytes);
     cuda_check(cudaMemcpyAsync(raw.ptr(), data, raw_bytes, device_ptr ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
@@ -522,7 +531,8 @@ SPK_API size_t spk_engine_trim(spk_engine* engine) {
         Engine* e = E(engine);
         DeviceGuard dg(e->device);
         std::lock_guard<std::mutex> g(e->m);
-        for (Session* s : e->sessions) freed += s->pool.trim();
+        for (Session* s : e->sessions) cudaStreamSynchronize(s->stream);
+        freed += device_pool_trim(e->device);
         freed += output_trim();
     } catch (...) {
         map_exception();
@@ -558,15 +568,14 @@ SPK_API const char* spk_memory_report(spk_engine* engine) {
     if (!engine) return "";
     Engine* e = E(engine);
     std::lock_guard<std::mutex> g(e->m);
-    size_t live = 0, idle = 0, negs = 0;
+    size_t live = 0, negs = 0;
     for (Session* s : e->sessions) {
         live += s->pool.live_bytes();
-        idle += s->pool.free_bytes();
         for (const TierState& t : s->tiers) negs += t.negative ? t.negative.bytes() : 0;
     }
     json::Value r;
     r["pool_live_bytes"] = double(live);
-    r["pool_free_bytes"] = double(idle);
+    r["pool_reserved_bytes"] = double(device_pool_reserved(e->device));
     r["cached_negative_bytes"] = double(negs);
     r["sessions"] = unsigned(e->sessions.size());
     e->memory_report = json::write(r);
@@ -1157,7 +1166,7 @@ SPK_API spk_status spkx_gaussian(const float* in, float* out, uint32_t w, uint32
     if (!in || !out || !sigma3) return invalid("a required pointer is NULL");
     if (w == 0 || h == 0) return invalid("empty plane");
     return with_scratch_stream([&](cudaStream_t s) {
-        Pool pool;
+        Pool pool(s);
         RenderCtx ctx{pool, s};
         Plane a = make_plane(pool, w, h), b = make_plane(pool, w, h);
         cuda_check(cudaMemcpyAsync(a.data(), in, a.bytes(), cudaMemcpyHostToDevice, s), "copy");

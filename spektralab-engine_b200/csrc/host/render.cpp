@@ -3,6 +3,7 @@
 #include <cmath>
 #include <cstring>
 
+#include "../cuda/iir.hpp"
 #include "../cuda/launch.hpp"
 #include "status.hpp"
 
@@ -209,6 +210,69 @@ void gaussian_mixture(RenderCtx& ctx, const Plane& in, const Plane& out, const s
     if (!same(acc, out)) dev::copy(acc.data(), out.data(), acc.pixels(), ctx.stream);
 }
 
+namespace {
+
+// M: the map of an entry state (s1, s2, s3) through L steps of the homogeneous recurrence.
+void entry_map(const IirCoefficients& k, int L, double M[3][3]) {
+    for (int j = 0; j < 3; ++j) {
+        double s[3] = {0.0, 0.0, 0.0};
+        s[j] = 1.0;
+        for (int i = 0; i < L; ++i) {
+            const double t = (k.B1 * s[0] + k.B2 * s[1]) + k.B3 * s[2];
+            s[2] = s[1];
+            s[1] = s[0];
+            s[0] = t;
+        }
+        for (int r = 0; r < 3; ++r) M[r][j] = s[r];
+    }
+}
+
+void fill_launch(dev::IirLaunch& q, const std::vector<MixtureComponent>& comps, int L) {
+    q.seg_len = L;
+    for (size_t c = 0; c < comps.size(); ++c)
+        for (int ch = 0; ch < 3; ++ch) {
+            dev::IirChannel& d = q.ch[3 * c + ch];
+            const IirCoefficients k = iir_coefficients(comps[c].sigma[ch]);
+            d.B = k.B;
+            d.B1 = k.B1;
+            d.B2 = k.B2;
+            d.B3 = k.B3;
+            entry_map(k, L, d.M);
+            d.active = 1;
+        }
+}
+
+// raw := a raw + b M(raw) with the block-parallel recursive kernels, when every channel of every
+// component is on the recursive branch and the lines fit in shared memory; false otherwise.
+bool iir_mixture_mix(RenderCtx& ctx, const Plane& raw, const std::vector<MixtureComponent>& comps, const Vec3& a,
+                     const Vec3& b) {
+    if (comps.empty() || comps.size() > SPKB_MAX_COMPONENTS) return false;
+    for (const MixtureComponent& m : comps)
+        for (int c = 0; c < 3; ++c)
+            if (blur_branch(m.sigma[c]) != Branch::Iir) return false;
+    if (!dev::iir_mixture_fits(raw.w, raw.h)) return false;
+    dev::IirMixture q{};
+    q.ncomp = uint32_t(comps.size());
+    for (size_t c = 0; c < comps.size(); ++c) weights(comps[c].weight, q.weight[c]);
+    weights(a, q.mix_a);
+    weights(b, q.mix_b);
+    const int Lr = int((raw.w + dev::iir_row_segments() - 1) / dev::iir_row_segments());
+    const int Lc = int((raw.h + dev::iir_col_segments() - 1) / dev::iir_col_segments());
+    fill_launch(q.rows, comps, Lr);
+    fill_launch(q.cols, comps, Lc);
+    std::vector<Plane> tmp;
+    float* tp[SPKB_MAX_COMPONENTS] = {};
+    for (size_t c = 0; c < comps.size(); ++c) {
+        tmp.push_back(make_plane(ctx.pool, raw.w, raw.h));
+        tp[c] = tmp.back().data();
+    }
+    Plane acc = comps.size() > 1 ? make_plane(ctx.pool, raw.w, raw.h) : Plane{};
+    dev::iir_mixture(raw.data(), tp, acc ? acc.data() : nullptr, raw.w, raw.h, q, ctx.stream);
+    return true;
+}
+
+}  // namespace
+
 void check_supported(const ParamSet& p) {
     auto refuse = [](const std::string& what) {
         fail_user(what + " is outside this B200 build's render path");
@@ -266,12 +330,12 @@ Plane develop(RenderCtx& ctx, const Pipeline& p, const Plane& source, uint32_t f
         }
         if (pl.scatter || pl.bounce) {
             Stage st(ctx, "halation");
-            if (pl.scatter) {
+            if (pl.scatter && !iir_mixture_mix(ctx, H, pl.scatter_comps, pl.scatter_a, pl.scatter_b)) {
                 Plane m = make_plane(ctx.pool, w, h);
                 gaussian_mixture(ctx, H, m, pl.scatter_comps);
                 lincomb(ctx, pl.scatter_a, H, pl.scatter_b, &m, H);
             }
-            if (pl.bounce) {
+            if (pl.bounce && !iir_mixture_mix(ctx, H, pl.bounce_comps, pl.mix_a, pl.mix_b)) {
                 Plane Hh = make_plane(ctx.pool, w, h);
                 gaussian_mixture(ctx, H, Hh, pl.bounce_comps);
                 lincomb(ctx, pl.mix_a, H, pl.mix_b, &Hh, H);
