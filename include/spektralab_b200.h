@@ -80,6 +80,25 @@ SPK_API spk_status spkx_philox(const uint32_t* counters, const uint32_t* keys, u
  * by the engine's FIR / recursive branch rule */
 SPK_API spk_status spkx_gaussian(const float* in, float* out, uint32_t w, uint32_t h, const double* sigma3);
 
+/* ---- allocation-free entry point (no counterpart in the reference engine) ----
+ *
+ * spkx_gaussian_noalloc(in, out, w, h, sigma3, stream)
+ *   The Gaussian blur of spkx_gaussian for callers that cannot have device memory allocated on their
+ *   behalf: a host application that owns all device memory through its own allocator and calls its
+ *   plug-ins inside a per-frame render callback, or a real-time pipeline in which cudaMalloc's latency and
+ *   implicit synchronisation are not allowed. The caller passes device buffers (w x h x 3 floats each;
+ *   out may equal in) and a cudaStream_t (NULL: the legacy default stream); the work is enqueued on that
+ *   stream and the call returns without waiting. It allocates nothing: the intermediate planes live in a
+ *   fixed 16 MiB array compiled into the library, so w * h must not exceed 699,050 pixels (2^21 floats
+ *   per plane); larger frames are refused with SPK_ERR_INVALID_ARG. Every GPU that loads the library
+ *   keeps the array until the process exits. The first call on each device (with that device current)
+ *   looks up the array's device address; make it before any stream capture. All calls on a device share
+ *   the one array and leave their data in it, so calls whose work overlaps on the GPU race: order them on
+ *   one stream, or wait for one before starting the next on another.
+ */
+SPK_API spk_status spkx_gaussian_noalloc(const float* in, float* out, uint32_t w, uint32_t h, const double* sigma3,
+                                         void* stream);
+
 #ifdef __cplusplus
 }
 #endif

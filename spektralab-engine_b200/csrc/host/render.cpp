@@ -5,6 +5,7 @@
 
 #include "../cuda/iir.hpp"
 #include "../cuda/launch.hpp"
+#include "blur_plan.h"
 #include "status.hpp"
 
 namespace spkb {
@@ -186,6 +187,22 @@ void encode_blur(RenderCtx& ctx, const Plane& in, const Plane& dst, const Vec3& 
 }
 
 }  // namespace
+
+int blur_branch_code(double sigma) {
+    switch (blur_branch(sigma)) {
+        case Branch::Identity: return BLUR_IDENTITY;
+        case Branch::Fir: return BLUR_FIR;
+        default: return BLUR_IIR;
+    }
+}
+
+FirTaps blur_fir_taps(const double sigma[3], const bool iir[3]) {
+    return fir_taps(Vec3{sigma[0], sigma[1], sigma[2]}, iir);
+}
+
+IirCoefs blur_iir_coefs(const double sigma[3], const bool iir[3]) {
+    return iir_coefs(Vec3{sigma[0], sigma[1], sigma[2]}, iir);
+}
 
 void gaussian(RenderCtx& ctx, const Plane& in, const Plane& dst, const Vec3& sigma) {
     encode_blur(ctx, in, dst, sigma, Fuse{});
