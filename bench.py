@@ -51,9 +51,11 @@ FALLBACK_HBM_GBS = 6650.0
 
 # Compulsory HBM bytes per pixel of each kernel in this workload (read + write of its planes; tables
 # that stay in L2 are not counted): 12 bytes per RGB float32 plane pass, 8 per RGBA16 pixel.
+N_HALATION = len(HALATION[0])
 KERNEL_BYTES_PER_PX = {
     "expose": 24, "iir_h": 24, "iir_v": 36, "fir_v": 24, "fir_h": 24, "lincomb": 36, "copy": 24,
-    "develop": 24, "print": 24, "encode": 32, "halation_h": 36, "halation_v": 60, "scan_blur": 44,
+    "develop": 24, "develop_layers": 24, "print": 24, "encode": 32, "fir_tile": 24, "scan_encode": 20,
+    "iir_rows": 12 + 12 * N_HALATION, "iir_cols": 12 * N_HALATION + 24,
 }
 # ncu DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) per launch of the kernels captured so far,
 # from the summaries under profiles/ (scaled to a 3840 x 2160 launch); None until captured.

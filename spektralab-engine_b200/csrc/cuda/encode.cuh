@@ -1,0 +1,53 @@
+// Device helpers shared by the print and scanner kernels: a 3x3 matrix in the reference's bracketing,
+// the output transfer functions and the 16-bit quantiser (reference kernels/print.metal:129-156,
+// :350-366, print_shared.h).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+namespace spkb::dev {
+namespace {
+
+__device__ __forceinline__ float sgnf(float v) { return v > 0.0f ? 1.0f : (v < 0.0f ? -1.0f : 0.0f); }
+
+__device__ __forceinline__ void mat_apply(const float* m, float x, float y, float z, float& a, float& b, float& c) {
+    a = (m[0] * x + m[1] * y) + m[2] * z;
+    b = (m[3] * x + m[4] * y) + m[5] * z;
+    c = (m[6] * x + m[7] * y) + m[8] * z;
+}
+
+// x^y for x >= 0 (NaN for x < 0, 0 for x = 0, y > 0) as 2^(y log2 x) on the special-function unit
+// (PTX lg2.approx and ex2.approx, subnormals kept): relative error within about 2^-22 (1 + |y log2 x|),
+// against 2 ulp for powf. Every use feeds a 16-bit output, whose 1 LSB is 2^-16 of full scale; the
+// render tests hold the output to the binary64 oracle and to the reference's precise-math build.
+__device__ __forceinline__ float powm(float x, float y) {
+    float l, r;
+    asm("lg2.approx.f32 %0, %1;" : "=f"(l) : "f"(x));
+    asm("ex2.approx.f32 %0, %1;" : "=f"(r) : "f"(y * l));
+    return r;
+}
+
+__device__ __forceinline__ float spowm(float v, float p) { return sgnf(v) * powm(fabsf(v), p); }
+
+// mode 0 sRGB, 1 ProPhoto (ROMM), 2 Adobe RGB, 3 BT.709, otherwise identity
+__device__ __forceinline__ float cctf_encode(float v, uint32_t mode) {
+    switch (mode) {
+        case 0: return v <= 0.0031308f ? 12.92f * v : 1.055f * spowm(v, 0.41666666666666669f) - 0.055f;
+        case 1: return v < 0.001953125f ? 16.0f * v : powm(v, 0.55555555555555558f);
+        case 2: return powm(v, 0.45470692717584371f);
+        case 3: return v < 0.018f ? 4.5f * v : 1.099f * spowm(v, 0.45f) - 0.099f;
+        default: return v;
+    }
+}
+
+// floor(clamp(v, 0, 1) 65535 + 0.5); NaN -> 0
+__device__ __forceinline__ uint16_t encode16(float v) {
+    if (isnan(v)) return 0;
+    const float c = fminf(fmaxf(v, 0.0f), 1.0f);
+    return uint16_t(floorf(c * 65535.0f + 0.5f));
+}
+
+}  // namespace
+}  // namespace spkb::dev

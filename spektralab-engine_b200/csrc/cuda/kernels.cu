@@ -13,14 +13,13 @@
 
 #include "../grain_sampler.h"
 #include "../kernel_args.h"
+#include "encode.cuh"
 #include "launch.hpp"
+#include "lookup.cuh"
 
 namespace spkb::dev {
 
 namespace {
-
-constexpr float kLog2Of10 = 3.321928094887362f;
-constexpr float kTiny = 1e-10f;
 
 __host__ __device__ inline uint32_t div_up(uint32_t a, uint32_t b) { return (a + b - 1) / b; }
 
@@ -61,7 +60,7 @@ __device__ __forceinline__ void mitchell_axis(float t, uint32_t L, int* idx, flo
     w[3] = mitchell(frac - 2.0f);
 }
 
-__global__ void k_expose(const float* __restrict__ rgb, float* __restrict__ hout, const float* __restrict__ table,
+__global__ void k_expose(const float* __restrict__ rgb, float* __restrict__ hout, const float4* __restrict__ table,
                          const __grid_constant__ ExposeArgs q) {
     const uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
     if (gid >= q.n) return;
@@ -85,11 +84,11 @@ __global__ void k_expose(const float* __restrict__ rgb, float* __restrict__ hout
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
             const float w = wa[i] * wb[j];
-            const float* t = table + 3 * (size_t(ia[i]) * q.L + size_t(ib[j]));
+            const float4 t = __ldg(table + (size_t(ia[i]) * q.L + size_t(ib[j])));
             s += w;
-            a0 += w * __ldg(t);
-            a1 += w * __ldg(t + 1);
-            a2 += w * __ldg(t + 2);
+            a0 += w * t.x;
+            a1 += w * t.y;
+            a2 += w * t.z;
         }
     }
     if (s != 0.0f) {
@@ -258,19 +257,32 @@ __global__ void k_copy(const float* __restrict__ x, float* __restrict__ out, siz
 // (fx_grain.metal:39-97, SUM and SIMPLE modes).
 
 __device__ __forceinline__ float curve_lookup(const float* __restrict__ x, const float* __restrict__ inv,
-                                              const float* __restrict__ y, uint32_t K, float v) {
+                                              const float* __restrict__ y, uint32_t K, const AxisGrid& g, float v) {
     if (v <= __ldg(x)) return __ldg(y);
     if (v >= __ldg(x + K - 1)) return __ldg(y + K - 1);
-    uint32_t lo = 0, hi = K;
-    while (lo < hi) {
-        const uint32_t mid = lo + (hi - lo) / 2;
-        if (__ldg(x + mid) <= v) lo = mid + 1;
-        else hi = mid;
-    }
-    const uint32_t l = lo == 0 ? 0 : lo - 1;
+    const uint32_t l = axis_index(x, 1, K, g, v);
     const float t = (v - __ldg(x + l)) * __ldg(inv + l);
     const float y0 = __ldg(y + l);
     return y0 + t * (__ldg(y + l + 1) - y0);
+}
+
+// the three sub-layer densities of channel c at density v (reference fx_grain.metal:60-75)
+__device__ __forceinline__ void layer_densities(const DevelopArgs& q, uint32_t c, float v, float dl[3]) {
+    const uint32_t K = q.gK;
+    if (v <= __ldg(q.axis + c)) {
+        for (uint32_t l = 0; l < 3u; ++l) dl[l] = __ldg(q.layers + l * 3u + c);
+    } else if (v >= __ldg(q.axis + 3u * (K - 1u) + c)) {
+        for (uint32_t l = 0; l < 3u; ++l) dl[l] = __ldg(q.layers + ((K - 1u) * 3u + l) * 3u + c);
+    } else {
+        // a NaN v gives j = 0, in bounds, and NaN densities
+        const uint32_t j = axis_index(q.axis + c, 3u, K, q.ggrid[c], v);
+        const float t = (v - __ldg(q.axis + 3u * j + c)) * __ldg(q.ginv + 3u * j + c);
+        for (uint32_t l = 0; l < 3u; ++l) {
+            const float y0 = __ldg(q.layers + (j * 3u + l) * 3u + c);
+            const float y1 = __ldg(q.layers + ((j + 1u) * 3u + l) * 3u + c);
+            dl[l] = y0 + t * (y1 - y0);
+        }
+    }
 }
 
 // spk_sublayer_draw (grain_sampler.h) with the count kept for the test hook: the same operations.
@@ -292,7 +304,7 @@ __global__ void k_develop(const float* __restrict__ exposure, float* __restrict_
     const size_t o = 3 * (size_t(y) * w + x);
     for (uint32_t c = 0; c < 3; ++c) {
         const float L = log10f(fmaxf(exposure[o + c], 0.0f) + 1e-10f);
-        const float D = curve_lookup(q.cx, q.cinv, q.cy + size_t(c) * q.K, q.K, L);
+        const float D = curve_lookup(q.cx, q.cinv, q.cy + size_t(c) * q.K, q.K, q.cgrid, L);
         if (!q.grain) {
             out[o + c] = D;
             continue;
@@ -307,28 +319,8 @@ __global__ void k_develop(const float* __restrict__ exposure, float* __restrict_
             continue;
         }
         const float v = q.positive ? -D : D;
-        const uint32_t K = q.gK;
         float dl[3];
-        if (v <= __ldg(q.axis + c)) {
-            for (uint32_t l = 0; l < 3u; ++l) dl[l] = __ldg(q.layers + l * 3u + c);
-        } else if (v >= __ldg(q.axis + 3u * (K - 1u) + c)) {
-            for (uint32_t l = 0; l < 3u; ++l) dl[l] = __ldg(q.layers + ((K - 1u) * 3u + l) * 3u + c);
-        } else {
-            uint32_t lo = 0, hi = K;
-            while (lo < hi) {
-                const uint32_t mid = lo + (hi - lo) / 2u;
-                if (__ldg(q.axis + 3u * mid + c) <= v) lo = mid + 1u;
-                else hi = mid;
-            }
-            // a finite v above axis[0] gives lo >= 1; lo == 0 (a NaN v) stays in bounds and yields NaN
-            const uint32_t j = lo == 0u ? 0u : lo - 1u;
-            const float t = (v - __ldg(q.axis + 3u * j + c)) * __ldg(q.ginv + 3u * j + c);
-            for (uint32_t l = 0; l < 3u; ++l) {
-                const float y0 = __ldg(q.layers + (j * 3u + l) * 3u + c);
-                const float y1 = __ldg(q.layers + ((j + 1u) * 3u + l) * 3u + c);
-                dl[l] = y0 + t * (y1 - y0);
-            }
-        }
+        layer_densities(q, c, v, dl);
         float val[3];
         for (uint32_t l = 0; l < 3u; ++l) {
             const uint32_t lc = l * 3u + c;
@@ -343,209 +335,171 @@ __global__ void k_develop(const float* __restrict__ exposure, float* __restrict_
 }
 
 // ---------------------------------------------------------------------------------------------------
-// print: reference kernels/print.metal:29-127 (helpers) and :165-317 (enlarger, gain, paper, scan,
-// matrix, gamut), one pixel per thread, the intermediate planes kept in registers.
+// develop with sub-layer grain (SUM mode), the draws compacted per warp.
+//
+// A pixel's nine Poisson draws take data-dependent paths: most PTRS draws end at the first attempt's
+// squeeze, the rest need the logarithm test, further attempts or (lam < 10) the product method. Run
+// per lane, a warp would wait on its slowest lane at every draw. Here each lane makes every draw's
+// first attempt in lockstep; a draw the squeeze does not settle goes to a ring of deferred draws in the
+// warp's shared memory, and whenever 32 are queued the whole warp finishes them, one per lane. Every
+// draw consumes the same uniforms in the same order and with the same arithmetic as spk_poisson, so the
+// counts are those of the per-lane sampler.
 
-__device__ __forceinline__ float sgnf(float v) { return v > 0.0f ? 1.0f : (v < 0.0f ? -1.0f : 0.0f); }
+constexpr uint32_t kDrawWarps = 4;
+constexpr uint32_t kDrawRing = 64;  // holds the < 32 left over plus one draw's 32
 
-__device__ __forceinline__ float knee(float d, float tau, float lim, float p) {
-    if (d <= tau) return d;
-    const float x = (d - tau) / (lim - tau);
-    return tau + (lim - tau) * (x / powf(1.0f + powf(x, p), 1.0f / p));
-}
+struct DeferredDraw {
+    spk_ptrs p;          // PTRS constants (kind 1, 2); p.lam alone for kind 0
+    float V, k, us;      // attempt 0's full test, pending (kind 1)
+    uint32_t w2, w3;     // words z, w of Philox block 0: attempt 1's uniforms (kinds 1, 2)
+    uint32_t pixel;
+    uint32_t tag;        // kind | stream << 2 | (draw * 32 + lane) << 10
+};
+// kinds: 0 product method (lam < 10 or NaN); 1 attempt 0 needs the full test; 2 attempt 0 rejected
 
-__device__ __forceinline__ float post_adapt(float v, float f_l) {
-    const float f = powf((f_l * fabsf(v)) / 100.0f, 0.42f);
-    return ((400.0f * sgnf(v)) * f) / (27.13f + f) + 0.1f;
-}
-
-__device__ __forceinline__ void mat_apply(const float* m, float x, float y, float z, float& a, float& b, float& c) {
-    a = (m[0] * x + m[1] * y) + m[2] * z;
-    b = (m[3] * x + m[4] * y) + m[5] * z;
-    c = (m[6] * x + m[7] * y) + m[8] * z;
-}
-
-__device__ __forceinline__ void spectral(const SpectralTables& a, float d0, float d1, float d2, float& r0, float& r1,
-                                         float& r2) {
-    r0 = r1 = r2 = 0.0f;
-#pragma unroll 9
-    for (int l = 0; l < SPKB_NL; ++l) {
-        const float D = ((d0 * a.eps[3 * l] + d1 * a.eps[3 * l + 1]) + d2 * a.eps[3 * l + 2]) + a.beta[l];
-        const float T = exp2f(-D * kLog2Of10);
-        r0 += T * a.wt[3 * l];
-        r1 += T * a.wt[3 * l + 1];
-        r2 += T * a.wt[3 * l + 2];
-    }
-}
-
-__device__ __forceinline__ float paper_lookup(const float* __restrict__ tab, uint32_t K, uint32_t c, float v) {
-    if (isnan(v)) return v;
-    const float* x = tab;
-    const float* r = tab + K;
-    const float* y = tab + 2 * K;
-    if (v <= __ldg(x)) return __ldg(y + c);
-    if (v >= __ldg(x + K - 1)) return __ldg(y + 3 * (K - 1) + c);
-    uint32_t lo = 0, hi = K;
-    while (lo < hi) {
-        const uint32_t mid = lo + (hi - lo) / 2;
-        if (__ldg(x + mid) <= v) lo = mid + 1;
-        else hi = mid;
-    }
-    const uint32_t j = lo - 1;
-    const float y0 = __ldg(y + 3 * j + c);
-    return y0 + ((v - __ldg(x + j)) * __ldg(r + j)) * (__ldg(y + 3 * (j + 1) + c) - y0);
-}
-
-__device__ void gamut(const PrintArgs& pa, float& r, float& g, float& b) {
-    const Cam16Args& q = pa.cam;
-    // per-pixel constants from the k numbers (print.metal:53-64)
-    const float cz = q.c * q.z;
-    const float inv_cz = 1.0f / cz;
-    const float f_l_qrt = powf(q.f_l, 0.25f);
-    const float chroma_k = powf(1.64f - powf(0.29f, q.n), 0.73f);
-    const float hundred_over_f_l = 100.0f / q.f_l;
-    float X, Y, Z;
-    mat_apply(q.m_to_xyz, r, g, b, X, Y, Z);
-    // forward (print.metal:66-86)
-    float R16, G16, B16;
-    mat_apply(q.m16, 100.0f * X, 100.0f * Y, 100.0f * Z, R16, G16, B16);
-    const float ra = post_adapt(q.d_rgb[0] * R16, q.f_l);
-    const float ga = post_adapt(q.d_rgb[1] * G16, q.f_l);
-    const float ba = post_adapt(q.d_rgb[2] * B16, q.f_l);
-    const float a = (ra - (12.0f * ga) / 11.0f) + ba / 11.0f;
-    const float bb = ((ra + ga) - 2.0f * ba) / 9.0f;
-    const float h = atan2f(bb, a);
-    const float et = 0.25f * (cosf(h + 2.0f) + 3.8f);
-    const float A = (((2.0f * ra + ga) + ba / 20.0f) - 0.305f) * q.n_bb;
-    const float ratio = A / q.a_w;
-    const float J = (100.0f * sgnf(ratio)) * powf(fabsf(ratio), cz);
-    const float den = (ra + ga) + (21.0f * ba) / 20.0f;
-    const float t = den != 0.0f ? (((((50000.0f / 13.0f) * q.n_c) * q.n_cb) * et) * sqrtf(a * a + bb * bb)) / den : 0.0f;
-    const float C = t > 0.0f ? (powf(t, 0.9f) * sqrtf(fabsf(J) / 100.0f)) * chroma_k : 0.0f;
-    const float M = C * f_l_qrt;
-    const float Mp = logf(1.0f + 0.0228f * M) / 0.0228f;
-    float Jp = (1.7f * J) / (1.0f + 0.007f * J);
-    // lightness knee
-    if (q.lc_active != 0u) {
-        float Ln = Jp / q.j_white;
-        if (Ln > q.lc[0]) {
-            Ln = knee(Ln, q.lc[0], q.lc[1], q.lc[2]);
-            Jp = Ln * q.j_white;
+// The rest of a deferred draw: attempt 0's pending full test (kind 1), then attempts 1..63 exactly as
+// spk_ptrs_from runs them, with one copy of the test, the squeeze and the generator in the loop.
+__device__ __forceinline__ void finish_draw(const DeferredDraw& d, uint32_t seed, float* res) {
+    const uint32_t kind = d.tag & 3u, stream = (d.tag >> 2) & 0xFFu, slot = d.tag >> 10;
+    spk_stream g;
+    spk_stream_init(&g, d.pixel, stream, seed);
+    float value;
+    if (kind == 0u) {
+        value = spk_poisson_product(d.p.lam, &g);
+    } else {
+        g.block.z = d.w2;
+        g.block.w = d.w3;
+        g.used = 2;
+        g.j = 1;
+        float k = d.k, us = d.us, V = d.V;
+        int state = kind == 1u ? SPK_PTRS_TEST : SPK_PTRS_REJECT;
+        for (int it = 1;; ++it) {
+            // state: the outcome of attempt it - 1's squeeze
+            if (state == SPK_PTRS_ACCEPT || (state == SPK_PTRS_TEST && spk_ptrs_test(&d.p, V, k, us))) {
+                value = k;
+                break;
+            }
+            if (it == 64) {
+                value = SPK_FLOOR(d.p.lam);
+                break;
+            }
+            const float u = spk_stream_uniform(&g);
+            V = spk_stream_uniform(&g);
+            state = spk_ptrs_squeeze(&d.p, u, V, &k, &us);
         }
     }
-    // C_max(J', h), bilinear with hue wrap
-    const float Jc = fminf(fmaxf(Jp, q.j_first), q.j_last);
-    const float u = ((Jc - q.j_first) / (q.j_last - q.j_first)) * float(q.rows - 1);
-    int l0 = int(floorf(u));
-    l0 = l0 < 0 ? 0 : (l0 > int(q.rows) - 2 ? int(q.rows) - 2 : l0);
-    const float fl = u - float(l0);
-    const float v = (h - q.h_first) / q.h_step;
-    const float vf = floorf(v);
-    const int cols = int(q.cols);
-    int h0 = int(vf) % cols;
-    if (h0 < 0) h0 += cols;
-    const int h1 = h0 == cols - 1 ? 0 : h0 + 1;
-    const float fh = v - vf;
-    const float t00 = __ldg(pa.cmax + l0 * cols + h0), t01 = __ldg(pa.cmax + l0 * cols + h1);
-    const float t10 = __ldg(pa.cmax + (l0 + 1) * cols + h0), t11 = __ldg(pa.cmax + (l0 + 1) * cols + h1);
-    const float cm = (1.0f - fl) * ((1.0f - fh) * t00 + fh * t01) + fl * ((1.0f - fh) * t10 + fh * t11);
-    const float cs = fmaxf(cm, 1e-9f);
-    float dch = Mp / cs;
-    if (dch > 0.0f) dch = knee(dch, q.knee[0], q.knee[1], q.knee[2]);
-    const float Mn = dch * cs;
-    // guarded inverse (print.metal:88-127)
-    const float Mi = (expf(0.0228f * Mn) - 1.0f) / 0.0228f;
-    const float Ji = Jp / (1.7f - 0.007f * Jp);
-    const float Ci = Mi / f_l_qrt;
-    const float Ai = (q.a_w * sgnf(Ji)) * powf(fabsf(Ji / 100.0f), inv_cz);
-    const float sq = sqrtf(fabsf(Ji) / 100.0f);
-    const float ti = (sq > 0.0f && Ci > 0.0f) ? powf(Ci / (sq * chroma_k), 1.0f / 0.9f) : 0.0f;
-    const float eti = 0.25f * (cosf(h + 2.0f) + 3.8f);
-    const float p2 = Ai / q.n_bb + 0.305f;
-    const float p3 = 21.0f / 20.0f;
-    float ai = 0.0f, bi = 0.0f;
-    if (ti != 0.0f) {
-        const float p1 = ((((50000.0f / 13.0f) * q.n_c) * q.n_cb) * eti) / ti;
-        const float sh = sinf(h), ch = cosf(h);
-        if (fabsf(sh) >= fabsf(ch)) {
-            const float p4 = p1 / sh;
-            bi = ((p2 * (2.0f + p3)) * (460.0f / 1403.0f)) /
-                 (((p4 + ((2.0f + p3) * (220.0f / 1403.0f)) * (ch / sh)) - 27.0f / 1403.0f) + p3 * (6300.0f / 1403.0f));
-            ai = (bi * ch) / sh;
-        } else {
-            const float p5 = p1 / ch;
-            ai = ((p2 * (2.0f + p3)) * (460.0f / 1403.0f)) /
-                 ((p5 + (2.0f + p3) * (220.0f / 1403.0f)) - (27.0f / 1403.0f - p3 * (6300.0f / 1403.0f)) * (sh / ch));
-            bi = (ai * sh) / ch;
-        }
-    }
-    const float xa[3] = {((460.0f * p2 + 451.0f * ai) + 288.0f * bi) / 1403.0f,
-                         ((460.0f * p2 - 891.0f * ai) - 261.0f * bi) / 1403.0f,
-                         ((460.0f * p2 - 220.0f * ai) - 6300.0f * bi) / 1403.0f};
-    float rc[3];
+    res[slot] = value;
+}
+
+__global__ void __launch_bounds__(kDrawWarps * 32) k_develop_layers(const float* __restrict__ exposure,
+                                                                    float* __restrict__ out, uint32_t w,
+                                                                    uint32_t blocks_per_row,
+                                                                    const __grid_constant__ DevelopArgs q) {
+    __shared__ DeferredDraw ring[kDrawWarps][kDrawRing];
+    __shared__ float res[kDrawWarps][9 * 32];
+    __shared__ float lam[9][kDrawWarps * 32], scale[9][kDrawWarps * 32];  // [c * 3 + l][thread]
+    const uint32_t lane = threadIdx.x & 31u, wi = threadIdx.x >> 5, tid = threadIdx.x;
+    const uint32_t y = blockIdx.x / blocks_per_row;
+    const uint32_t x = (blockIdx.x - y * blocks_per_row) * (kDrawWarps * 32) + threadIdx.x;
+    const bool live = x < w;
+    const uint32_t pixel = y * q.width + x;
+    const size_t o = 3 * (size_t(y) * w + x);
+
+    // lambda and the count's scale of the nine draws, [c][l], kept in shared memory
 #pragma unroll
-    for (int i = 0; i < 3; ++i) {
-        const float vv = xa[i] - 0.1f;
-        const float av = fabsf(vv);
-        const float beta = av >= 400.0f ? 0.0f : (27.13f * av) / (400.0f - av);
-        rc[i] = ((hundred_over_f_l * sgnf(vv)) * powf(beta, 1.0f / 0.42f)) / q.d_rgb[i];
+    for (int c = 0; c < 3; ++c) {
+        float dl[3] = {0.0f, 0.0f, 0.0f};
+        if (live) {
+            const float L = log10f(fmaxf(exposure[o + c], 0.0f) + 1e-10f);
+            const float D = curve_lookup(q.cx, q.cinv, q.cy + size_t(c) * q.K, q.K, q.cgrid, L);
+            layer_densities(q, uint32_t(c), q.positive ? -D : D, dl);
+        }
+#pragma unroll
+        for (int l = 0; l < 3; ++l) {
+            const int lc = l * 3 + c;
+            float sat = 1.0f;
+            lam[c * 3 + l][tid] =
+                live ? spk_sublayer_lambda(dl[l] + q.dmin_l[lc], q.sat_d[lc], q.count[lc], q.uniformity[c], &sat)
+                     : 0.0f;
+            scale[c * 3 + l][tid] = SPK_MUL(SPK_DIV(q.sat_d[lc], q.count[lc]), sat);
+        }
     }
-    float x100, y100, z100;
-    mat_apply(q.m16_inv, rc[0], rc[1], rc[2], x100, y100, z100);
-    mat_apply(q.m_to_rgb, x100 / 100.0f, y100 / 100.0f, z100 / 100.0f, r, g, b);
-}
 
-__global__ void k_print(const float* __restrict__ neg, float* __restrict__ rgb, const __grid_constant__ PrintArgs a) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= a.n) return;
-    const size_t o = 3 * size_t(i);
-    float d0 = neg[o], d1 = neg[o + 1], d2 = neg[o + 2];
-    if (a.printed) {
-        float r0, r1, r2;
-        spectral(a.enl, d0, d1, d2, r0, r1, r2);
-        float l0 = log10f(fmaxf(r0 * a.g[0] + a.o[0], 0.0f) + kTiny);
-        float l1 = log10f(fmaxf(r1 * a.g[1] + a.o[1], 0.0f) + kTiny);
-        float l2 = log10f(fmaxf(r2 * a.g[2] + a.o[2], 0.0f) + kTiny);
-        l0 = log10f(fmaxf(exp2f(l0 * kLog2Of10) * a.k_gain, 0.0f) + kTiny);
-        l1 = log10f(fmaxf(exp2f(l1 * kLog2Of10) * a.k_gain, 0.0f) + kTiny);
-        l2 = log10f(fmaxf(exp2f(l2 * kLog2Of10) * a.k_gain, 0.0f) + kTiny);
-        d0 = paper_lookup(a.paper, a.paper_K, 0, l0);
-        d1 = paper_lookup(a.paper, a.paper_K, 1, l1);
-        d2 = paper_lookup(a.paper, a.paper_K, 2, l2);
+    DeferredDraw* ringw = ring[wi];
+    float* resw = res[wi];
+    uint32_t head = 0, tail = 0;
+#pragma unroll 1
+    for (uint32_t k = 0; k < 9u; ++k) {
+        const uint32_t stream = SPK_STREAM_GRAIN(k / 3u, k % 3u);
+        bool defer = false;
+        float value = 0.0f;
+        DeferredDraw d{};
+        d.pixel = pixel;
+        uint32_t kind = 0u;
+        const float lm = lam[k][tid];
+        if (live) {
+            if (lm >= 10.0f) {
+                spk_ptrs_init(&d.p, lm);
+                spk_u4 c4;
+                c4.x = pixel;
+                c4.y = stream;
+                c4.z = 0u;
+                c4.w = 0u;
+                const spk_u4 b0 = spk_philox(c4, q.seed, 0u);
+                float kk, us;
+                const int r = spk_ptrs_squeeze(&d.p, spk_uniform(b0.x), spk_uniform(b0.y), &kk, &us);
+                if (r == SPK_PTRS_ACCEPT) {
+                    value = kk;
+                } else {
+                    defer = true;
+                    kind = r == SPK_PTRS_TEST ? 1u : 2u;
+                    d.V = spk_uniform(b0.y);
+                    d.k = kk;
+                    d.us = us;
+                    d.w2 = b0.z;
+                    d.w3 = b0.w;
+                }
+            } else {
+                defer = true;
+                d.p.lam = lm;
+            }
+        }
+        const uint32_t mask = __ballot_sync(0xFFFFFFFFu, defer);
+        if (defer) {
+            d.tag = kind | (stream << 2) | ((k * 32u + lane) << 10);
+            ringw[(tail + __popc(mask & ((1u << lane) - 1u))) & (kDrawRing - 1u)] = d;
+        } else {
+            resw[k * 32u + lane] = value;
+        }
+        tail += __popc(mask);
+        if (tail - head >= 32u) {
+            __syncwarp();
+            finish_draw(ringw[(head + lane) & (kDrawRing - 1u)], q.seed, resw);
+            head += 32u;
+            __syncwarp();
+        }
     }
-    float X, Y, Z;
-    spectral(a.scan, d0, d1, d2, X, Y, Z);
-    X = fmaxf(X, 0.0f) + kTiny;
-    Y = fmaxf(Y, 0.0f) + kTiny;
-    Z = fmaxf(Z, 0.0f) + kTiny;
-    float r, g, b;
-    mat_apply(a.to_rgb, X, Y, Z, r, g, b);
-    gamut(a, r, g, b);
-    rgb[o] = r;
-    rgb[o + 1] = g;
-    rgb[o + 2] = b;
+    __syncwarp();
+    if (lane < tail - head) finish_draw(ringw[(head + lane) & (kDrawRing - 1u)], q.seed, resw);
+    __syncwarp();
+    if (!live) return;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        float val[3];
+#pragma unroll
+        for (int l = 0; l < 3; ++l) {
+            const float cnt = resw[(c * 3 + l) * 32 + lane];
+            if (q.counts_out) q.counts_out[size_t(pixel) * 9 + c * 3 + l] = cnt;
+            val[l] = SPK_MUL(cnt, scale[c * 3 + l][tid]);
+        }
+        float G = ((0.0f + val[0]) + val[1]) + val[2];
+        if (q.shift) G = G * 1.0f + (-q.dmin_c[c]);
+        out[o + c] = G;
+    }
 }
 
 // ---------------------------------------------------------------------------------------------------
-// encode: reference kernels/print.metal:129-156 and :350-366.
-
-__device__ __forceinline__ float spowf(float v, float p) { return sgnf(v) * powf(fabsf(v), p); }
-
-__device__ __forceinline__ float cctf_encode(float v, uint32_t mode) {
-    switch (mode) {
-        case 0: return v <= 0.0031308f ? 12.92f * v : 1.055f * spowf(v, 0.41666666666666669f) - 0.055f;
-        case 1: return v < 0.001953125f ? 16.0f * v : powf(v, 0.55555555555555558f);
-        case 2: return powf(v, 0.45470692717584371f);
-        case 3: return v < 0.018f ? 4.5f * v : 1.099f * spowf(v, 0.45f) - 0.099f;
-        default: return v;
-    }
-}
-
-__device__ __forceinline__ uint16_t encode16(float v) {
-    if (isnan(v)) return 0;
-    const float c = fminf(fmaxf(v, 0.0f), 1.0f);
-    return uint16_t(floorf(c * 65535.0f + 0.5f));
-}
+// encode: reference kernels/print.metal:129-156 and :350-366 (helpers in encode.cuh).
 
 __global__ void k_encode(const float* __restrict__ rgb, const float* __restrict__ gpl, uint16_t* __restrict__ out,
                          uint32_t w, uint32_t h, const __grid_constant__ EncodeArgs e) {
@@ -643,10 +597,10 @@ Probe::~Probe() {
 void set_launch_hook(LaunchHook* hook) { t_hook = hook; }
 uint64_t launch_count() { return g_launches.load(); }
 
-void expose(const float* rgb, float* h, const float* table, const ExposeArgs& a, cudaStream_t s) {
+void expose(const float* rgb, float* h, const float* table4, const ExposeArgs& a, cudaStream_t s) {
     if (a.n == 0) return;
     Probe p("expose", s);
-    k_expose<<<div_up(a.n, 256), 256, 0, s>>>(rgb, h, table, a);
+    k_expose<<<div_up(a.n, 256), 256, 0, s>>>(rgb, h, reinterpret_cast<const float4*>(table4), a);
 }
 
 void fir_v(const float* in, float* out, uint32_t w, uint32_t h, const FirTaps& t, cudaStream_t s) {
@@ -688,15 +642,16 @@ void copy(const float* x, float* out, size_t pixels, cudaStream_t s) {
 }
 
 void develop(const float* exposure, float* out, const DevelopArgs& a, uint32_t w, uint32_t h, cudaStream_t s) {
+    if (uint64_t(w) * h == 0) return;
+    if (a.grain && a.mode == 0) {
+        const uint32_t bx = div_up(w, kDrawWarps * 32);
+        Probe p("develop_layers", s);
+        k_develop_layers<<<bx * h, kDrawWarps * 32, 0, s>>>(exposure, out, w, bx, a);
+        return;
+    }
     const dim3 b(32, 4), g(div_up(w, 32), div_up(h, 4));
     Probe p("develop", s);
     k_develop<<<g, b, 0, s>>>(exposure, out, w, h, a);
-}
-
-void print(const float* neg, float* rgb, const PrintArgs& a, cudaStream_t s) {
-    if (a.n == 0) return;
-    Probe p("print", s);
-    k_print<<<div_up(a.n, 128), 128, 0, s>>>(neg, rgb, a);
 }
 
 void encode(const float* rgb, const float* g, uint16_t* out, uint32_t w, uint32_t h, const EncodeArgs& e,

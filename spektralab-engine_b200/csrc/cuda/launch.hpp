@@ -27,8 +27,9 @@ struct Probe {
     ~Probe();
 };
 
-// RGB -> film exposure H (Mitchell bicubic of the spectral table), times the compensation gain.
-void expose(const float* rgb, float* h, const float* table, const ExposeArgs& a, cudaStream_t s);
+// RGB -> film exposure H (Mitchell bicubic of the spectral table, L x L float4 texels), times the
+// compensation gain.
+void expose(const float* rgb, float* h, const float* table4, const ExposeArgs& a, cudaStream_t s);
 
 // Separable FIR: vertical pass in -> out (no accumulation).
 void fir_v(const float* in, float* out, uint32_t w, uint32_t h, const FirTaps& t, cudaStream_t s);
@@ -55,6 +56,16 @@ void print(const float* neg, float* rgb, const PrintArgs& a, cudaStream_t s);
 // (optional unsharp combine with g) -> transfer function -> RGBA16 with row pitch e.stride.
 void encode(const float* rgb, const float* g, uint16_t* out, uint32_t w, uint32_t h, const EncodeArgs& e,
             cudaStream_t s);
+
+// The scanner stage in one tiled pass: lens blur (radius a.r1), unsharp (a.r2, when a.e.unsharp), matrix,
+// transfer function, RGBA16. scan_encode_fits tells whether the tiled kernel takes this frame and these radii.
+bool scan_encode_fits(uint32_t w, uint32_t h, int r1, int r2);
+void scan_encode(const float* rgb, uint16_t* out, uint32_t w, uint32_t h, const ScanArgs& a, cudaStream_t s);
+
+// A separable FIR (taps[0..2r], the same for the three channels) with both passes in one tiled kernel;
+// out must not alias in. fir_tile_fits tells whether the tiled kernel takes this frame and radius.
+bool fir_tile_fits(uint32_t w, uint32_t h, int r);
+void fir_tile(const float* in, float* out, uint32_t w, uint32_t h, int r, const float* taps, cudaStream_t s);
 
 // host frame (channels 3 or 4, already on the device) -> interleaved RGB plane, non-finite -> 0
 void source_copy(const float* raw, float* out, size_t pixels, uint32_t channels, cudaStream_t s);

@@ -1,0 +1,261 @@
+// The scanner stage in one pass: lens blur (FIR), unsharp mask (FIR + combine), output matrix, transfer
+// function and RGBA16 encode, over 32 x 32 pixel tiles staged in shared memory.
+//
+// Reference: src/fx/scanner.cpp:16-31 (blur, then (1 + a) x - a G(x)), kernels/fx_blur.metal:20-78
+// (FIR: taps -r..r ascending, binary32 accumulator from 0, half-sample symmetric reflection at the
+// edges, a vertical pass then a horizontal pass) and kernels/print.metal:350-366 (encode).
+//
+// Every intermediate value is the one the separate passes compute: each pass is evaluated only at
+// pixels inside the image, in the same tap order, and where a pass reads past an edge it reads the
+// value at the reflected pixel. The vertical passes do not mix columns, so a column loaded from the
+// reflected source column already carries the reflected result; after the lens blur's horizontal pass
+// the tile copies the reflected values into the (at most r2 wide) border that the unsharp pass reads.
+//
+// Shared memory (floats, interleaved RGB rows), R = r1 + r2:
+//   A: the print output with an R halo (TH + 2R rows x 3 (TW + 2R)), later the lens-blurred tile with an
+//      r2 halo (TH + 2 r2 rows x 3 (TW + 2 r2))
+//   B: the lens blur's vertical pass (TH + 2 r2 rows x 3 (TW + 2R)), later the unsharp vertical pass
+//      (TH rows x 3 (TW + 2 r2))
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../kernel_args.h"
+#include "encode.cuh"
+#include "launch.hpp"
+
+namespace spkb::dev {
+
+namespace {
+
+constexpr int kTW = 32, kTH = 32, kThreads = 256, kWarps = kThreads / 32;
+
+// half-sample symmetric reflection, exact for p in [-n, 2n)
+__device__ __forceinline__ int reflect_near(int p, int n) { return p < 0 ? -1 - p : (p >= n ? 2 * n - 1 - p : p); }
+
+template <int R1, int R2>
+__global__ void __launch_bounds__(kThreads) k_scan_encode(const float* __restrict__ rgb, uint16_t* __restrict__ out,
+                                                          int w, int h, const __grid_constant__ ScanArgs a) {
+    extern __shared__ float smem[];
+    const int r1 = R1 >= 0 ? R1 : a.r1, r2 = R2 >= 0 ? R2 : a.r2, R = r1 + r2;
+    const int PC = 3 * (kTW + 2 * R);  // floats per row of the print tile and the first vertical pass
+    const int PR = kTH + 2 * R;
+    const int BR = kTH + 2 * r2;       // rows of the lens-blurred tile
+    const int BC = 3 * (kTW + 2 * r2);
+    float* A = smem;
+    float* B = smem + PR * PC;
+    const int x0 = blockIdx.x * kTW, y0 = blockIdx.y * kTH;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+    // 1. the print output at (y0 - R + i, x0 - R + j), reflected; pixels more than R past an edge are
+    //    never read and load a clamped pixel
+    for (int i = warp; i < PR; i += kWarps) {
+        const int yy = min(max(reflect_near(y0 - R + i, h), 0), h - 1);
+        const float* row = rgb + size_t(yy) * size_t(w) * 3;
+        for (int f = lane; f < PC; f += 32) {
+            const int j = f / 3, c = f - 3 * j;
+            const int xx = min(max(reflect_near(x0 - R + j, w), 0), w - 1);
+            A[i * PC + f] = __ldg(row + 3 * xx + c);
+        }
+    }
+    __syncthreads();
+
+    // 2. lens blur, vertical: rows y0 - r2 + i inside the image, every column of the tile
+    for (int i = warp; i < BR; i += kWarps) {
+        const int yy = y0 - r2 + i;
+        if (yy < 0 || yy >= h) continue;
+        for (int f = lane; f < PC; f += 32) {
+            float acc = 0.0f;
+#pragma unroll
+            for (int k = 0; k <= 2 * r1; ++k) acc += a.t1[k] * A[(i + k) * PC + f];
+            B[i * PC + f] = acc;
+        }
+    }
+    __syncthreads();
+
+    // 3. lens blur, horizontal: pixels (y0 - r2 + i, x0 - r2 + jb) inside the image, into A
+    for (int i = warp; i < BR; i += kWarps) {
+        const int yy = y0 - r2 + i;
+        if (yy < 0 || yy >= h) continue;
+        for (int fb = lane; fb < BC; fb += 32) {
+            const int xx = x0 - r2 + fb / 3;
+            if (xx < 0 || xx >= w) continue;
+            float acc = 0.0f;
+#pragma unroll
+            for (int k = 0; k <= 2 * r1; ++k) acc += a.t1[k] * B[i * PC + fb + 3 * k];
+            A[i * BC + fb] = acc;
+        }
+    }
+    __syncthreads();
+
+    if (r2 > 0) {
+        // 4. the border up to r2 past an edge takes the lens-blurred value of the reflected pixel
+        if (x0 - r2 < 0 || x0 + kTW + r2 > w || y0 - r2 < 0 || y0 + kTH + r2 > h) {
+            for (int i = warp; i < BR; i += kWarps) {
+                const int yy = y0 - r2 + i;
+                if (yy < -r2 || yy >= h + r2) continue;
+                const bool row_out = yy < 0 || yy >= h;
+                const int is = reflect_near(yy, h) - (y0 - r2);
+                for (int fb = lane; fb < BC; fb += 32) {
+                    const int jb = fb / 3, c = fb - 3 * jb;
+                    const int xx = x0 - r2 + jb;
+                    if (xx < -r2 || xx >= w + r2) continue;
+                    if (!row_out && xx >= 0 && xx < w) continue;
+                    const int js = reflect_near(xx, w) - (x0 - r2);
+                    A[i * BC + fb] = A[is * BC + 3 * js + c];
+                }
+            }
+            __syncthreads();
+        }
+        // 5. unsharp blur, vertical: the tile's rows inside the image, every column of the blurred tile
+        for (int i = warp; i < kTH; i += kWarps) {
+            if (y0 + i >= h) break;
+            for (int fb = lane; fb < BC; fb += 32) {
+                float acc = 0.0f;
+#pragma unroll
+                for (int k = 0; k <= 2 * r2; ++k) acc += a.t2[k] * A[(i + k) * BC + fb];
+                B[i * BC + fb] = acc;
+            }
+        }
+        __syncthreads();
+    }
+
+    // 6. unsharp horizontal pass and combine, matrix, transfer function, RGBA16: a pixel per lane
+    const EncodeArgs& e = a.e;
+    for (int i = warp; i < kTH; i += kWarps) {
+        const int yy = y0 + i, xx = x0 + lane;
+        if (yy >= h) break;
+        if (xx >= w) continue;
+        const float* bc = A + (i + r2) * BC + 3 * (lane + r2);
+        float v0 = bc[0], v1 = bc[1], v2 = bc[2];
+        if (e.unsharp) {
+            const float* vr = B + i * BC + 3 * lane;
+            float g0 = 0.0f, g1 = 0.0f, g2 = 0.0f;
+#pragma unroll
+            for (int k = 0; k <= 2 * r2; ++k) {
+                g0 += a.t2[k] * vr[3 * k];
+                g1 += a.t2[k] * vr[3 * k + 1];
+                g2 += a.t2[k] * vr[3 * k + 2];
+            }
+            v0 = e.lincomb_a * v0 + e.lincomb_b * g0;
+            v1 = e.lincomb_a * v1 + e.lincomb_b * g1;
+            v2 = e.lincomb_a * v2 + e.lincomb_b * g2;
+        }
+        if (e.cctf_active) {
+            float m0, m1, m2;
+            mat_apply(e.m_nid, v0, v1, v2, m0, m1, m2);
+            v0 = cctf_encode(m0, e.cctf_mode);
+            v1 = cctf_encode(m1, e.cctf_mode);
+            v2 = cctf_encode(m2, e.cctf_mode);
+        }
+        ushort4 p;
+        p.x = encode16(v0);
+        p.y = encode16(v1);
+        p.z = encode16(v2);
+        p.w = 65535;
+        reinterpret_cast<ushort4*>(out)[size_t(yy) * e.stride + xx] = p;
+    }
+}
+
+// A separable FIR Gaussian with one tap vector for the three channels, both passes in one tiled kernel:
+// the vertical pass at the tile's rows (every column of the haloed tile; a halo column holds the
+// reflected source column, so its vertical result is that of the reflected column), then the horizontal
+// pass. out must not alias in (neighbouring tiles read in's halo).
+template <int R>
+__global__ void __launch_bounds__(kThreads) k_fir_tile(const float* __restrict__ in, float* __restrict__ out, int w,
+                                                       int h, const __grid_constant__ ScanArgs a) {
+    extern __shared__ float smem[];
+    const int r = R >= 0 ? R : a.r1;
+    const int PC = 3 * (kTW + 2 * r), PR = kTH + 2 * r;
+    float* A = smem;
+    float* B = smem + PR * PC;
+    const int x0 = blockIdx.x * kTW, y0 = blockIdx.y * kTH;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int i = warp; i < PR; i += kWarps) {
+        const int yy = min(max(reflect_near(y0 - r + i, h), 0), h - 1);
+        const float* row = in + size_t(yy) * size_t(w) * 3;
+        for (int f = lane; f < PC; f += 32) {
+            const int j = f / 3, c = f - 3 * j;
+            const int xx = min(max(reflect_near(x0 - r + j, w), 0), w - 1);
+            A[i * PC + f] = __ldg(row + 3 * xx + c);
+        }
+    }
+    __syncthreads();
+    for (int i = warp; i < kTH; i += kWarps) {
+        if (y0 + i >= h) break;
+        for (int f = lane; f < PC; f += 32) {
+            float acc = 0.0f;
+#pragma unroll
+            for (int k = 0; k <= 2 * r; ++k) acc += a.t1[k] * A[(i + k) * PC + f];
+            B[i * PC + f] = acc;
+        }
+    }
+    __syncthreads();
+    const int OC = 3 * kTW;
+    for (int i = warp; i < kTH; i += kWarps) {
+        const int yy = y0 + i;
+        if (yy >= h) break;
+        float* orow = out + size_t(yy) * size_t(w) * 3 + size_t(x0) * 3;
+        const int lim = 3 * min(kTW, w - x0);
+        for (int f = lane; f < OC; f += 32) {
+            if (f >= lim) break;
+            float acc = 0.0f;
+#pragma unroll
+            for (int k = 0; k <= 2 * r; ++k) acc += a.t1[k] * B[i * PC + f + 3 * k];
+            orow[f] = acc;
+        }
+    }
+}
+
+size_t scan_smem_bytes(int r1, int r2) {
+    const int R = r1 + r2;
+    return size_t((kTH + 2 * R) + (kTH + 2 * r2)) * size_t(3 * (kTW + 2 * R)) * sizeof(float);
+}
+
+template <int R1, int R2>
+void launch_scan(const float* rgb, uint16_t* out, uint32_t w, uint32_t h, const ScanArgs& a, cudaStream_t s) {
+    const size_t smem = scan_smem_bytes(a.r1, a.r2);  // at most 96 KB (r1 = r2 = 9)
+    cudaFuncSetAttribute(k_scan_encode<R1, R2>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    const dim3 g((w + kTW - 1) / kTW, (h + kTH - 1) / kTH);
+    k_scan_encode<R1, R2><<<g, kThreads, smem, s>>>(rgb, out, int(w), int(h), a);
+}
+
+}  // namespace
+
+bool scan_encode_fits(uint32_t w, uint32_t h, int r1, int r2) {
+    const int R = r1 + r2;
+    return r1 >= 0 && r2 >= 0 && r1 <= SPKB_FIR_MAX_R && r2 <= SPKB_FIR_MAX_R && w >= uint32_t(R) + 1 &&
+           h >= uint32_t(R) + 1 && (uint64_t(h) + kTH - 1) / kTH <= 65535u;
+}
+
+void scan_encode(const float* rgb, uint16_t* out, uint32_t w, uint32_t h, const ScanArgs& a, cudaStream_t s) {
+    if (uint64_t(w) * h == 0) return;
+    Probe p("scan_encode", s);
+    if (a.r1 == 5 && a.r2 == 2) launch_scan<5, 2>(rgb, out, w, h, a, s);
+    else if (a.r1 == 0 && a.r2 == 2) launch_scan<0, 2>(rgb, out, w, h, a, s);
+    else launch_scan<-1, -1>(rgb, out, w, h, a, s);
+}
+
+namespace {
+template <int R>
+void launch_fir_tile(const float* in, float* out, uint32_t w, uint32_t h, const ScanArgs& a, cudaStream_t s) {
+    const size_t smem = size_t(2 * kTH + 2 * a.r1) * size_t(3 * (kTW + 2 * a.r1)) * sizeof(float);
+    cudaFuncSetAttribute(k_fir_tile<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    const dim3 g((w + kTW - 1) / kTW, (h + kTH - 1) / kTH);
+    k_fir_tile<R><<<g, kThreads, smem, s>>>(in, out, int(w), int(h), a);
+}
+}  // namespace
+
+bool fir_tile_fits(uint32_t w, uint32_t h, int r) { return scan_encode_fits(w, h, r, 0); }
+
+void fir_tile(const float* in, float* out, uint32_t w, uint32_t h, int r, const float* taps, cudaStream_t s) {
+    if (uint64_t(w) * h == 0) return;
+    ScanArgs a{};
+    a.r1 = r;
+    for (int k = 0; k <= 2 * r; ++k) a.t1[k] = taps[k];
+    Probe p("fir_tile", s);
+    if (r == 2) launch_fir_tile<2>(in, out, w, h, a, s);
+    else if (r == 5) launch_fir_tile<5>(in, out, w, h, a, s);
+    else launch_fir_tile<-1>(in, out, w, h, a, s);
+}
+
+}  // namespace spkb::dev

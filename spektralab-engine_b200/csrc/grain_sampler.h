@@ -265,36 +265,68 @@ SPK_HD float spk_lgamma_k(float x) {
     return gl;
 }
 
-SPK_HD float spk_poisson(float lam, uint32_t pixel, uint32_t stream, uint32_t seed) {
-    spk_stream g;
-    spk_stream_init(&g, pixel, stream, seed);
-    if (lam >= 10.0f) {
-        const float slam = SPK_SQRT(lam);
-        const float loglam = spk_logf(lam);
-        const float b = SPK_ADD(0.931f, SPK_MUL(2.53f, slam));
-        const float a = SPK_ADD(-0.059f, SPK_MUL(0.02483f, b));
-        const float invalpha = SPK_ADD(1.1239f, SPK_DIV(1.1328f, SPK_SUB(b, 3.4f)));
-        const float vr = SPK_SUB(0.9277f, SPK_DIV(3.6224f, SPK_SUB(b, 2.0f)));
-        for (int it = 0; it < 64; ++it) {
-            const float U = SPK_SUB(spk_stream_uniform(&g), 0.5f);
-            const float V = spk_stream_uniform(&g);
-            const float us = SPK_SUB(0.5f, fabsf(U));
-            const float k = SPK_FLOOR(
-                SPK_ADD(SPK_ADD(SPK_MUL(SPK_ADD(SPK_DIV(SPK_MUL(2.0f, a), us), b), U), lam), 0.43f));
-            if (us >= 0.07f && V <= vr) return k;
-            if (k < 0.0f || (us < 0.013f && V > us)) continue;
-            const float L = SPK_SUB(SPK_ADD(spk_logf(V), spk_logf(invalpha)),
-                                    spk_logf(SPK_ADD(SPK_DIV(a, SPK_MUL(us, us)), b)));
-            const float Rt = SPK_SUB(SPK_ADD(-lam, SPK_MUL(k, loglam)), spk_lgamma_k(SPK_ADD(k, 1.0f)));
-            if (L <= Rt) return k;
-        }
-        return SPK_FLOOR(lam);
+/* PTRS in pieces, so that a caller can run every draw's first attempt in lockstep and finish the
+ * rest apart. Attempt `it` of a draw takes uniforms 2 it (U) and 2 it + 1 (V) of its stream. */
+typedef struct {
+    float lam, loglam, b, a, invalpha, vr;
+} spk_ptrs;
+
+#define SPK_PTRS_REJECT 0
+#define SPK_PTRS_ACCEPT 1
+#define SPK_PTRS_TEST 2 /* neither squeeze decides: the full test follows */
+
+SPK_HD void spk_ptrs_init(spk_ptrs* p, float lam) {
+    const float slam = SPK_SQRT(lam);
+    p->lam = lam;
+    p->loglam = spk_logf(lam);
+    p->b = SPK_ADD(0.931f, SPK_MUL(2.53f, slam));
+    p->a = SPK_ADD(-0.059f, SPK_MUL(0.02483f, p->b));
+    p->invalpha = SPK_ADD(1.1239f, SPK_DIV(1.1328f, SPK_SUB(p->b, 3.4f)));
+    p->vr = SPK_SUB(0.9277f, SPK_DIV(3.6224f, SPK_SUB(p->b, 2.0f)));
+}
+
+/* the candidate k of an attempt and its two squeezes */
+SPK_HD int spk_ptrs_squeeze(const spk_ptrs* p, float u, float V, float* k_out, float* us_out) {
+    const float U = SPK_SUB(u, 0.5f);
+    const float us = SPK_SUB(0.5f, fabsf(U));
+    const float k =
+        SPK_FLOOR(SPK_ADD(SPK_ADD(SPK_MUL(SPK_ADD(SPK_DIV(SPK_MUL(2.0f, p->a), us), p->b), U), p->lam), 0.43f));
+    *k_out = k;
+    *us_out = us;
+    if (us >= 0.07f && V <= p->vr) return SPK_PTRS_ACCEPT;
+    if (k < 0.0f || (us < 0.013f && V > us)) return SPK_PTRS_REJECT;
+    return SPK_PTRS_TEST;
+}
+
+/* the full acceptance test: log V + log(1/alpha) - log(a / us^2 + b) <= -lam + k log lam - log k! */
+SPK_HD int spk_ptrs_test(const spk_ptrs* p, float V, float k, float us) {
+    const float L = SPK_SUB(SPK_ADD(spk_logf(V), spk_logf(p->invalpha)),
+                            spk_logf(SPK_ADD(SPK_DIV(p->a, SPK_MUL(us, us)), p->b)));
+    const float Rt = SPK_SUB(SPK_ADD(-p->lam, SPK_MUL(k, p->loglam)), spk_lgamma_k(SPK_ADD(k, 1.0f)));
+    return L <= Rt;
+}
+
+/* attempts it0..63 on a generator positioned at attempt it0's first uniform; floor(lam) after 64 */
+SPK_HD float spk_ptrs_from(const spk_ptrs* p, spk_stream* g, int it0) {
+    for (int it = it0; it < 64; ++it) {
+        const float u = spk_stream_uniform(g);
+        const float V = spk_stream_uniform(g);
+        float k, us;
+        const int r = spk_ptrs_squeeze(p, u, V, &k, &us);
+        if (r == SPK_PTRS_ACCEPT) return k;
+        if (r == SPK_PTRS_REJECT) continue;
+        if (spk_ptrs_test(p, V, k, us)) return k;
     }
+    return SPK_FLOOR(p->lam);
+}
+
+/* lam < 10 (and NaN): multiply uniforms until the product falls to exp(-lam) */
+SPK_HD float spk_poisson_product(float lam, spk_stream* g) {
     const float E = spk_expf(-lam);
     float X = 0.0f;
     float prod = 1.0f;
     for (int it = 0; it < 512; ++it) {
-        prod = SPK_MUL(prod, spk_stream_uniform(&g));
+        prod = SPK_MUL(prod, spk_stream_uniform(g));
         if (prod > E) {
             X = SPK_ADD(X, 1.0f);
         } else {
@@ -302,6 +334,17 @@ SPK_HD float spk_poisson(float lam, uint32_t pixel, uint32_t stream, uint32_t se
         }
     }
     return X;
+}
+
+SPK_HD float spk_poisson(float lam, uint32_t pixel, uint32_t stream, uint32_t seed) {
+    spk_stream g;
+    spk_stream_init(&g, pixel, stream, seed);
+    if (lam >= 10.0f) {
+        spk_ptrs p;
+        spk_ptrs_init(&p, lam);
+        return spk_ptrs_from(&p, &g, 0);
+    }
+    return spk_poisson_product(lam, &g);
 }
 
 /* lam for a sub-layer draw; a NaN density gives NaN (and then no draws) */

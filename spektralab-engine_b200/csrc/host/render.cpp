@@ -21,7 +21,14 @@ void upload(Pool& pool, cudaStream_t s, DevBuffer& dst, const void* src, size_t 
 
 void upload_tables(Pool& pool, cudaStream_t s, Pipeline& p) {
     const FilmSetup& f = *p.film;
-    upload(pool, s, p.dev.table, f.table32.data(), f.table32.size() * sizeof(float));
+    {
+        // the spectral table as 16-byte texels (R, G, B, 0): one vector load per bicubic tap
+        const size_t texels = f.table32.size() / 3;
+        std::vector<float> t4(4 * texels, 0.0f);
+        for (size_t i = 0; i < texels; ++i)
+            for (size_t c = 0; c < 3; ++c) t4[4 * i + c] = f.table32[3 * i + c];
+        upload(pool, s, p.dev.table, t4.data(), t4.size() * sizeof(float));
+    }
     std::vector<float> c(5 * size_t(f.K));
     std::memcpy(c.data(), f.cx.data(), f.K * sizeof(float));
     std::memcpy(c.data() + f.K, f.cinv.data(), f.K * sizeof(float));
@@ -88,6 +95,50 @@ struct Fuse {
 
 bool same(const Plane& a, const Plane& b) { return a.data() == b.data(); }
 
+// The kernels' direct index into an ascending axis (AxisGrid): g(v) = clamp(int((v - x0) s), 0, K - 2),
+// the same binary32 operations as on the device. The grid is switched on only when, for every interval
+// [x[j], x[j+1]), g stays within one of j at both ends (g rises with v, so then everywhere in between).
+int grid_guess(float v, float x0, float s, uint32_t K) {
+    const float t = (v - x0) * s;
+    const int g = t >= float(K) ? int(K) : (t > 0.0f ? int(t) : 0);
+    return std::min(std::max(g, 0), int(K) - 2);
+}
+
+AxisGrid axis_grid(const float* x, uint32_t K, uint32_t stride) {
+    AxisGrid a{};
+    if (K < 3) return a;
+    for (uint32_t j = 0; j + 1 < K; ++j)
+        if (!(x[size_t(j + 1) * stride] > x[size_t(j) * stride])) return a;
+    const float x0 = x[0], xl = x[size_t(K - 1) * stride];
+    const float s = f32(double(K - 1) / (double(xl) - double(x0)));
+    if (!std::isfinite(s) || !(s > 0.0f)) return a;
+    for (uint32_t j = 0; j + 1 < K; ++j) {
+        const float lo = x[size_t(j) * stride];
+        const float hi = std::nextafter(x[size_t(j + 1) * stride], -INFINITY);
+        if (grid_guess(lo, x0, s, K) < int(j) - 1 || grid_guess(hi, x0, s, K) > int(j) + 1) return a;
+    }
+    a.x0 = x0;
+    a.s = s;
+    a.active = 1;
+    return a;
+}
+
+// The print kernel's form of a spectral integral R_k = sum_l 10^-D(l) wt_k(l), D(l) = sum_c d_c eps_c(l)
+// + beta(l) (reference kernels/print.metal:165-189): R_k = sum_l 2^(sum_c d_c e_c(l)) w_k(l) with
+// e = -log2(10) eps and w_k = wt_k 10^-beta, each formed in binary64 from the binary32 tables and rounded
+// once, and held twice for the packed two-pixel arithmetic.
+SpectralPairs spectral_pairs(const SpectralTables& t) {
+    constexpr double kNegLog2Of10 = -3.32192809488736234787;
+    SpectralPairs o{};
+    for (int i = 0; i < 3 * SPKB_NL; ++i) {
+        const float e = f32(double(t.eps[i]) * kNegLog2Of10);
+        const float w = f32(double(t.wt[i]) * std::pow(10.0, -double(t.beta[i / 3])));
+        o.e[i] = F32Pair{e, e};
+        o.w[i] = F32Pair{w, w};
+    }
+    return o;
+}
+
 FirTaps fir_taps(const Vec3& sigma, const bool iir[3]) {
     FirTaps t{};
     int r = 0;
@@ -124,7 +175,24 @@ void weights(const Vec3& w, float out[3]) {
     for (int c = 0; c < 3; ++c) out[c] = f32(w[c]);
 }
 
+bool uniform_taps(const FirTaps& t) {
+    for (int k = 0; k <= 2 * t.r; ++k)
+        if (t.taps[1][k] != t.taps[0][k] || t.taps[2][k] != t.taps[0][k]) return false;
+    return true;
+}
+
 void encode_fir(RenderCtx& ctx, const Plane& in, const Plane& dst, const FirTaps& t, const Fuse& fuse) {
+    if (fuse.mode == ACC_NONE && uniform_taps(t) && dev::fir_tile_fits(in.w, in.h, t.r)) {
+        // both passes in one tiled kernel (out of place; an in-place blur goes through a fresh plane)
+        if (!same(in, dst)) {
+            dev::fir_tile(in.data(), dst.data(), in.w, in.h, t.r, t.taps[0], ctx.stream);
+            return;
+        }
+        Plane tmp = make_plane(ctx.pool, in.w, in.h);
+        dev::fir_tile(in.data(), tmp.data(), in.w, in.h, t.r, t.taps[0], ctx.stream);
+        dev::copy(tmp.data(), dst.data(), dst.pixels(), ctx.stream);
+        return;
+    }
     Plane tmp = make_plane(ctx.pool, in.w, in.h);
     dev::fir_v(in.data(), tmp.data(), in.w, in.h, t, ctx.stream);
     float w[3];
@@ -328,7 +396,11 @@ Plane develop(RenderCtx& ctx, const Pipeline& p, const Plane& source, uint32_t f
     if (b.f(P::lens_blur_um) > 0.0) {
         Stage st(ctx, "lens_blur");
         const double s = b.f(P::lens_blur_um) / ctx.pitch_um;
-        if (s > 0.0) gaussian(ctx, H, H, Vec3{s, s, s});
+        if (s > 0.0) {
+            Plane Hb = make_plane(ctx.pool, w, h);
+            gaussian(ctx, H, Hb, Vec3{s, s, s});
+            H = std::move(Hb);
+        }
     }
     {
         HalationPlan pl;
@@ -364,6 +436,7 @@ Plane develop(RenderCtx& ctx, const Pipeline& p, const Plane& source, uint32_t f
     da.cinv = da.cx + f.K;
     da.cy = da.cx + 2 * size_t(f.K);
     da.K = f.K;
+    da.cgrid = axis_grid(f.cx.data(), f.K, 1);
     da.width = w;
     da.counts_out = counts_out;
     Plane neg = make_plane(ctx.pool, w, h);
@@ -399,6 +472,7 @@ Plane develop(RenderCtx& ctx, const Pipeline& p, const Plane& source, uint32_t f
         da.axis = p.dev.gaxis.as<float>();
         da.ginv = p.dev.ginv.as<float>();
         da.layers = p.dev.glayers.as<float>();
+        for (uint32_t c = 0; c < 3; ++c) da.ggrid[c] = axis_grid(g->axis.data() + c, g->K, 3);
     } else {
         da.mode = 2;  // SIMPLE
     }
@@ -410,7 +484,13 @@ Plane develop(RenderCtx& ctx, const Pipeline& p, const Plane& source, uint32_t f
     if (kc.final_blur > 0.0) {
         Stage st(ctx, "grain_blur");
         const double s = kc.final_blur;
-        gaussian(ctx, G, G, Vec3{s, s, s});
+        if (g->amount == 1.0) {  // the blurred grain is the negative
+            gaussian(ctx, G, neg, Vec3{s, s, s});
+            return neg;
+        }
+        Plane Gb = make_plane(ctx.pool, w, h);
+        gaussian(ctx, G, Gb, Vec3{s, s, s});
+        G = std::move(Gb);
     }
     {
         Stage st(ctx, "grain_mix");
@@ -433,8 +513,8 @@ void print_scan_encode(RenderCtx& ctx, const Pipeline& p, const LiveParams& live
     const uint32_t w = negative.w, h = negative.h;
     const PrintRun r = compute_run(s, live);
     PrintArgs a{};
-    a.enl = r.enl32;
-    a.scan = s.scan32;
+    a.enl = spectral_pairs(r.enl32);
+    a.scan = spectral_pairs(s.scan32);
     for (int c = 0; c < 3; ++c) {
         a.g[c] = f32(r.g[c]);
         a.o[c] = f32(r.o[c]);
@@ -443,6 +523,7 @@ void print_scan_encode(RenderCtx& ctx, const Pipeline& p, const LiveParams& live
     a.printed = s.scanned ? 0 : 1;
     a.paper = p.dev.paper.as<float>();
     a.paper_K = s.paper_K;
+    if (!s.paper_tab.empty()) a.paper_grid = axis_grid(s.paper_tab.data(), s.paper_K, 1);
     std::memcpy(a.to_rgb, s.to_rgb, sizeof a.to_rgb);
     a.cam = s.cam_args;
     a.cmax = p.dev.cmax.as<float>();
@@ -457,6 +538,35 @@ void print_scan_encode(RenderCtx& ctx, const Pipeline& p, const LiveParams& live
     e.cctf_active = s.cctf ? 1 : 0;
     e.cctf_mode = s.cctf_mode;
     e.stride = img->stride_px;
+    {
+        // the scanner's blurs on the FIR branch: one tiled pass from the print output to RGBA16
+        const double sb = s.scanner_lens_blur_px;
+        const double su = s.unsharp_sigma_full * ctx.rho_tier;
+        const double am = s.unsharp_amount;
+        const bool unsharp = su > 0.0 && am > 0.0;
+        const Branch bb = blur_branch(sb), bu = unsharp ? blur_branch(su) : Branch::Identity;
+        const bool no_iir[3] = {false, false, false};
+        ScanArgs sa{};
+        if (bb != Branch::Iir && bu != Branch::Iir) {
+            const FirTaps t1 = fir_taps(Vec3{sb, sb, sb}, no_iir);
+            const FirTaps t2 = fir_taps(Vec3{su, su, su}, no_iir);
+            sa.r1 = t1.r;
+            std::memcpy(sa.t1, t1.taps[0], sizeof sa.t1);
+            sa.r2 = unsharp ? t2.r : 0;
+            if (unsharp) std::memcpy(sa.t2, t2.taps[0], sizeof sa.t2);
+            if (sa.r1 == 0) sa.t1[0] = 1.0f;
+            if (sa.r2 == 0) sa.t2[0] = 1.0f;
+        }
+        if (bb != Branch::Iir && bu != Branch::Iir && dev::scan_encode_fits(w, h, sa.r1, sa.r2)) {
+            sa.e = e;
+            sa.e.unsharp = unsharp ? 1 : 0;
+            sa.e.lincomb_a = f32(1.0 + am);
+            sa.e.lincomb_b = f32(-am);
+            Stage st(ctx, "scanner");
+            dev::scan_encode(rgb.data(), img->dev, w, h, sa, ctx.stream);
+            return;
+        }
+    }
     Plane gpl;
     {
         Stage st(ctx, "scanner");

@@ -18,7 +18,7 @@ namespace spkb {
 
 // A film/print set-up pair with its device tables, built once per pipeline.
 struct DeviceTables {
-    DevBuffer table;              // L x L x 3 spectral table
+    DevBuffer table;              // L x L spectral table, float4 texels (R, G, B, 0)
     DevBuffer curves;             // x[K] | inv[K] | y[3K]
     DevBuffer gaxis, ginv, glayers;
     DevBuffer paper;              // x[K] | r[K] | y[K][3]

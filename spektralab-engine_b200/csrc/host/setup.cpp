@@ -933,6 +933,12 @@ std::shared_ptr<PrintSetup> build_print_setup(const ParamSet& p, const FilmSetup
         }
         q.lc_active = 1;
         q.j_white = f32(c.J_white);
+        // the kernel's per-pixel constants in binary32, the operations of print.metal:53-64
+        q.cz = q.c * q.z;
+        q.inv_cz = 1.0f / q.cz;
+        q.f_l_qrt = std::pow(q.f_l, 0.25f);
+        q.chroma_k = std::pow(1.64f - std::pow(0.29f, q.n), 0.73f);
+        q.hundred_over_f_l = 100.0f / q.f_l;
     }
     s->cctf = p.b(P::output_cctf_encoding);
     s->cctf_mode = uint32_t(s->out_cs.cctf);

@@ -16,7 +16,7 @@ struct ExposeArgs {
     float a[9];        // input matrix A, row-major
     float gain;        // f32(2^exposure_compensation_ev)
     int32_t apply_gain;
-    uint32_t L;        // table size; the table is L x L x 3, [i][j][c]
+    uint32_t L;        // table size; the table is L x L float4 texels, [i][j] = (R, G, B, 0)
     uint32_t n;        // pixels
 };
 
@@ -37,12 +37,22 @@ struct IirCoefs {
 enum AccMode { ACC_NONE = 0, ACC_ZERO = 1, ACC_PLANE = 2 };
 
 // Film-side point work after halation: log10 exposure, density curves, grain draw.
+// Direct index into an ascending binary32 axis x[0..K-1]: g(v) = clamp(int((v - x0) s), 0, K - 2). The
+// host sets `active` only after checking that g is within one of the bisection's interval for every v
+// in (x[0], x[K-1]); the kernel then corrects g by one comparison on each side. Inactive: bisection.
+struct AxisGrid {
+    float x0, s;
+    int32_t active;
+};
+
 struct DevelopArgs {
     // curves: x[K], inv[K], y[3K] (channel-major)
     const float* cx;
     const float* cinv;
     const float* cy;
     uint32_t K;
+    AxisGrid cgrid;       // the curves' log-exposure axis
+    AxisGrid ggrid[3];    // the grain layers' density axis of each channel
     // grain (reference fx_grain.metal:39-97 modes)
     int32_t grain;        // 0: no grain, write the density
     uint32_t mode;        // 0 SUM (sub-layers, no dye clouds), 1 PLANES, 2 SIMPLE
@@ -69,6 +79,17 @@ struct SpectralTables {
     float wt[SPKB_NL * 3];   // [l][k]
 };
 
+// One spectral integral in the print kernel's form, for packed f32x2 arithmetic over a pair of pixels:
+// e_c(l) = -log2(10) eps_c(l) and w_k(l) = wt_k(l) 10^-beta(l), each value held twice (both halves of a
+// packed operand), so that sum_l 2^(sum_c d_c e_c(l)) w_k(l) = sum_l 10^-D(l) wt_k(l).
+struct alignas(8) F32Pair {
+    float x, y;
+};
+struct SpectralPairs {
+    F32Pair e[SPKB_NL * 3];  // [l][c]
+    F32Pair w[SPKB_NL * 3];  // [l][k]
+};
+
 // CAM16-UCS gamut compression constants (reference kernels/print_shared.h:74-100 field meanings).
 struct Cam16Args {
     uint32_t rows, cols;
@@ -79,17 +100,21 @@ struct Cam16Args {
     float knee[3], lc[3];
     uint32_t lc_active;
     float j_white;
+    // per-frame constants of the reference's per-pixel set-up (kernels/print.metal:53-64), formed on the
+    // host in binary32 by the same operations: c z, 1 / (c z), F_L^0.25, (1.64 - 0.29^n)^0.73, 100 / F_L
+    float cz, inv_cz, f_l_qrt, chroma_k, hundred_over_f_l;
 };
 
 // The print kernel: negative density -> linear output RGB.
 struct PrintArgs {
-    SpectralTables enl;
-    SpectralTables scan;
+    SpectralPairs enl;
+    SpectralPairs scan;
     float g[3], o[3];
     float k_gain;
     int32_t printed;            // 0: scan_film (the negative is scanned directly)
     const float* paper;         // x[K], r[K], y[K][3]
     uint32_t paper_K;
+    AxisGrid paper_grid;
     float to_rgb[9];
     Cam16Args cam;
     const float* cmax;
@@ -104,4 +129,15 @@ struct EncodeArgs {
     uint32_t stride;      // output row pitch in pixels
     float lincomb_a, lincomb_b;  // out = a x + b g (unsharp), applied when unsharp != 0
     int32_t unsharp;
+};
+
+// The scanner's two FIR blurs, the unsharp combine and the encode in one tiled pass
+// (reference src/fx/scanner.cpp:16-31 and kernels/print.metal:350-366). Both blurs have one sigma for
+// all three channels, so one tap vector each; r = 0 with taps {1} is the identity.
+struct ScanArgs {
+    int32_t r1;                              // lens blur radius
+    float t1[2 * SPKB_FIR_MAX_R + 1];
+    int32_t r2;                              // unsharp blur radius (0 when unsharp is off)
+    float t2[2 * SPKB_FIR_MAX_R + 1];
+    EncodeArgs e;
 };

@@ -119,4 +119,4 @@ def test_4k_properties(engine):
         c, _ = s.reprint("full")
         assert np.array_equal(a, c)
         prof = s.profile("full", True, 2)
-        assert set(prof["stages"]) >= {"print", "encode"}
+        assert set(prof["stages"]) >= {"print", "scanner"}
