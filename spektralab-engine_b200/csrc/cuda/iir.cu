@@ -10,13 +10,13 @@
 //   1. every segment runs the recurrence from a zero state (the first segment from the true edge
 //      state) and keeps its last three values e_s;
 //   2. the true state entering segment s+1 is S_s = e_s + M S_{s-1}, with M the 3 x 3 map of an
-//      entry state through L steps of the homogeneous recurrence (a short serial pass per line);
+//      entry state through L steps of the homogeneous recurrence (a parallel scan over the segments);
 //   3. every segment recomputes from its true entry state and stores its values.
 // State and the carries are binary64 (the reference keeps double-float state on its GPU and double
 // state on its host copy); x, u and y are stored as binary32 exactly as there.
 //
-// k_iir_rows: one CTA per image row; the row (3 w floats) in shared memory; every mixture component
-//             blurred in turn from the same row and written to its own plane.
+// k_iir_rows: one CTA per image row, 3 lines x 128 segments; the row (3 w floats) in shared memory,
+//             loaded afresh for every mixture component, blurred and written to the component's plane.
 // k_iir_cols: one CTA per strip of 4 pixel columns (12 lines); every component's row result blurred
 //             down the columns in turn; the mixture accumulated as the reference's fused passes do
 //             (acc = 0 + w0 y0, acc = acc + w_k y_k) and the halation mix raw := a raw + b acc written
@@ -31,7 +31,7 @@ namespace spkb::dev {
 
 namespace {
 
-constexpr int kSegRows = 64;       // segments per channel line in a row
+constexpr int kSegRows = 128;      // segments per channel line in a row
 constexpr int kRowThreads = 3 * kSegRows;
 constexpr int kColPixels = 4;       // pixels per column strip
 constexpr int kColLines = 3 * kColPixels;
@@ -43,14 +43,16 @@ struct Coef {
 };
 
 __device__ __forceinline__ double step(const Coef& k, double x, double s1, double s2, double s3) {
-    // the product with the newest state last, so that only one multiply-add waits on it
-    return fma(k.B1, s1, fma(k.B3, s3, fma(k.B2, s2, k.B * x)));
+    // the oldest state first and the newest last: each state is j steps old when it enters the j-th
+    // multiply-add from the end, so the chain costs one multiply-add latency per sample
+    return fma(k.B1, s1, fma(k.B2, s2, fma(k.B3, s3, k.B * x)));
 }
 
 // Forward pass over one segment [a, b) of a line in shared memory (element i at base[i * stride]).
 // Zero-state run: returns the end state. Writing run: from `in` state, stores float(w) back.
 __device__ __forceinline__ void seg_forward(const Coef& k, float* base, int stride, int a, int b, double& s1,
                                             double& s2, double& s3, bool write) {
+#pragma unroll 4
     for (int i = a; i < b; ++i) {
         const double t = step(k, double(base[i * stride]), s1, s2, s3);
         s3 = s2;
@@ -62,6 +64,7 @@ __device__ __forceinline__ void seg_forward(const Coef& k, float* base, int stri
 
 __device__ __forceinline__ void seg_backward(const Coef& k, float* base, int stride, int a, int b, double& s1,
                                              double& s2, double& s3, bool write) {
+#pragma unroll 4
     for (int i = b - 1; i >= a; --i) {
         const double t = step(k, double(base[i * stride]), s1, s2, s3);
         s3 = s2;
@@ -71,22 +74,58 @@ __device__ __forceinline__ void seg_backward(const Coef& k, float* base, int str
     }
 }
 
+// The true entry states of the segments, by a Kogge-Stone scan of the zero-state end states e_s held in
+// carry (log2 of the segment count in steps rather than one serial pass per line):
+//   forward   S_s = e_s + M S_{s-1}, s = 1 .. last-1; S_0 = e_0 is already true (the edge state)
+//   backward  S_s = e_s + M S_{s+1}, s = last-1 .. 0; S_last = e_last is already true
+// Step p adds M^(2^p) times the carry 2^p segments away. The segments whose maps are composed are full
+// length, so M is the same for each. Every thread of the block runs the loop (it has barriers).
+__device__ void carry_scan(double* carry, int nt, int cstep, int seg, int last, const IirChannel& ch, bool active,
+                           bool forward) {
+    // component i of thread t's carry at carry[i * nt + t]; the neighbouring segment's is cstep away
+    double* cs = carry + threadIdx.x;
+    for (int p = 0, k = 1; k <= last; ++p, k <<= 1) {
+        const int src = forward ? seg - k : seg + k;
+        const bool upd = active && (forward ? (src >= 0 && seg <= last - 1) : src <= last);
+        double n0 = 0.0, n1 = 0.0, n2 = 0.0;
+        if (upd) {
+            const double* ps = cs + (forward ? -k : k) * cstep;
+            const double p0 = ps[0], p1 = ps[nt], p2 = ps[2 * nt];
+            const double(&M)[3][3] = ch.Mp[p];
+            n0 = cs[0] + (M[0][0] * p0 + M[0][1] * p1 + M[0][2] * p2);
+            n1 = cs[nt] + (M[1][0] * p0 + M[1][1] * p1 + M[1][2] * p2);
+            n2 = cs[2 * nt] + (M[2][0] * p0 + M[2][1] * p1 + M[2][2] * p2);
+        }
+        __syncthreads();
+        if (upd) {
+            cs[0] = n0;
+            cs[nt] = n1;
+            cs[2 * nt] = n2;
+        }
+        __syncthreads();
+    }
+}
+
 // One full forward + backward blur of `nlines` interleaved lines of length n held in shared memory
-// (line j, element i at buf[i * pitch + j]); nseg segments per line; threads = nlines * nseg, thread
-// t handles line t % nlines, segment t / nlines. carry: shared scratch of nlines * nseg * 3 doubles.
-__device__ void blur_lines(float* buf, int pitch, int nlines, int n, int nseg, const IirLaunch& q, const int* comp_line,
-                           double* carry) {
+// (line j, element i at buf[i * pitch + j]), nseg segments per line, threads = nlines * nseg. Thread t
+// handles line t / nseg, segment t % nseg when seg_major, else line t % nlines, segment t / nlines; the
+// channel of line j is 3 comp + j % 3. carry: shared scratch of 3 * nlines * nseg doubles, component i of
+// thread t's segment at carry[i * nlines * nseg + t].
+__device__ void blur_lines(float* buf, int pitch, int nlines, int n, int nseg, const IirLaunch& q, int comp,
+                           double* carry, bool seg_major) {
     const int t = threadIdx.x;
-    const int line = t % nlines;
-    const int seg = t / nlines;
+    const int line = seg_major ? t / nseg : t % nlines;
+    const int seg = seg_major ? t % nseg : t / nlines;
+    const int cstep = seg_major ? 1 : nlines;  // carry distance between neighbouring segments of a line
     const int L = q.seg_len;
     const int a = seg * L;
     const int b = min(n, a + L);
-    const IirChannel& ch = q.ch[comp_line[line]];
-    const bool active = ch.active != 0;
+    const IirChannel& ch = q.ch[3 * comp + line % 3];
+    const bool active = ch.active != 0 && line < nlines;
     const Coef k{ch.B, ch.B1, ch.B2, ch.B3};
     float* base = buf + line;
-    double* cs = carry + (size_t(seg) * nlines + line) * 3;
+    const int nt = nlines * nseg;
+    double* cs = carry + t;
 
     // ---- forward ----
     if (active && a < n) {
@@ -94,32 +133,22 @@ __device__ void blur_lines(float* buf, int pitch, int nlines, int n, int nseg, c
         if (seg == 0) s1 = s2 = s3 = double(base[0]);
         seg_forward(k, base, pitch, a, b, s1, s2, s3, false);
         cs[0] = s1;
-        cs[1] = s2;
-        cs[2] = s3;
+        cs[nt] = s2;
+        cs[2 * nt] = s3;
     }
     __syncthreads();
     const int nseg_used = (n + L - 1) / L;
     const int last = nseg_used - 1;
-    if (active && seg == 0) {  // serial carry: true end state of every segment that has a successor
-        for (int s = 1; s < last; ++s) {  // segments 1 .. last-1 are full length L
-            const double* prev = carry + (size_t(s - 1) * nlines + line) * 3;
-            double* cur = carry + (size_t(s) * nlines + line) * 3;
-            const double p0 = prev[0], p1 = prev[1], p2 = prev[2];
-            cur[0] = cur[0] + (ch.M[0][0] * p0 + ch.M[0][1] * p1 + ch.M[0][2] * p2);
-            cur[1] = cur[1] + (ch.M[1][0] * p0 + ch.M[1][1] * p1 + ch.M[1][2] * p2);
-            cur[2] = cur[2] + (ch.M[2][0] * p0 + ch.M[2][1] * p1 + ch.M[2][2] * p2);
-        }
-    }
-    __syncthreads();
+    carry_scan(carry, nt, cstep, seg, last, ch, active, true);
     if (active && a < n) {
         double s1, s2, s3;
         if (seg == 0) {
             s1 = s2 = s3 = double(base[0]);
         } else {
-            const double* prev = carry + (size_t(seg - 1) * nlines + line) * 3;
+            const double* prev = cs - cstep;
             s1 = prev[0];
-            s2 = prev[1];
-            s3 = prev[2];
+            s2 = prev[nt];
+            s3 = prev[2 * nt];
         }
         seg_forward(k, base, pitch, a, b, s1, s2, s3, true);
     }
@@ -130,35 +159,33 @@ __device__ void blur_lines(float* buf, int pitch, int nlines, int n, int nseg, c
         if (seg == last) s1 = s2 = s3 = double(base[(n - 1) * pitch]);
         seg_backward(k, base, pitch, a, b, s1, s2, s3, false);
         cs[0] = s1;
-        cs[1] = s2;
-        cs[2] = s3;
+        cs[nt] = s2;
+        cs[2 * nt] = s3;
     }
     __syncthreads();
-    if (active && seg == 0) {  // serial carry from the right end leftwards; full segments only
-        for (int s = last - 1; s >= 0; --s) {
-            const double* prev = carry + (size_t(s + 1) * nlines + line) * 3;
-            double* cur = carry + (size_t(s) * nlines + line) * 3;
-            const double p0 = prev[0], p1 = prev[1], p2 = prev[2];
-            cur[0] = cur[0] + (ch.M[0][0] * p0 + ch.M[0][1] * p1 + ch.M[0][2] * p2);
-            cur[1] = cur[1] + (ch.M[1][0] * p0 + ch.M[1][1] * p1 + ch.M[1][2] * p2);
-            cur[2] = cur[2] + (ch.M[2][0] * p0 + ch.M[2][1] * p1 + ch.M[2][2] * p2);
-        }
-    }
-    __syncthreads();
+    carry_scan(carry, nt, cstep, seg, last, ch, active, false);
     if (active && a < n) {
         double s1, s2, s3;
         if (seg == last) {
             s1 = s2 = s3 = double(base[(n - 1) * pitch]);
         } else {
-            const double* prev = carry + (size_t(seg + 1) * nlines + line) * 3;
+            const double* prev = cs + cstep;
             s1 = prev[0];
-            s2 = prev[1];
-            s3 = prev[2];
+            s2 = prev[nt];
+            s3 = prev[2 * nt];
         }
         seg_backward(k, base, pitch, a, b, s1, s2, s3, true);
     }
     __syncthreads();
 }
+
+// 16-byte asynchronous copy global -> shared (both addresses 16-byte aligned), and the wait for all of
+// this thread's copies
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+    const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 __global__ void __launch_bounds__(kRowThreads) k_iir_rows(const float* __restrict__ in, IirPlanes outs, uint32_t w,
                                                           uint32_t h, const __grid_constant__ IirMixture mix) {
@@ -166,20 +193,28 @@ __global__ void __launch_bounds__(kRowThreads) k_iir_rows(const float* __restric
     const uint32_t y = blockIdx.x;
     if (y >= h) return;
     const int n3 = int(3 * w);
-    const int n3r = (n3 + 3) & ~3;  // keeps work and carry 16-byte aligned
-    float* row = reinterpret_cast<float*>(smem);
-    float* work = row + n3r;
+    const int n3r = (n3 + 3) & ~3;  // keeps carry 16-byte aligned
+    float* work = reinterpret_cast<float*>(smem);
     double* carry = reinterpret_cast<double*>(work + n3r);
     const float* src = in + size_t(y) * n3;
-    for (int i = threadIdx.x; i < n3; i += blockDim.x) row[i] = src[i];
-    __syncthreads();
+    const bool vec = (n3 & 3) == 0;  // rows start on 16-byte boundaries
     for (int c = 0; c < int(mix.ncomp); ++c) {
-        for (int i = threadIdx.x; i < n3; i += blockDim.x) work[i] = row[i];
+        // each component blurs the row afresh: the source row is read again (from L2 after the first)
+        if (vec) {
+            for (int i = threadIdx.x; i < n3 / 4; i += blockDim.x) cp_async16(work + 4 * i, src + 4 * i);
+            cp_async_wait_all();
+        } else {
+            for (int i = threadIdx.x; i < n3; i += blockDim.x) work[i] = src[i];
+        }
         __syncthreads();
-        const int comp_line[3] = {3 * c + 0, 3 * c + 1, 3 * c + 2};
-        blur_lines(work, 3, 3, int(w), kSegRows, mix.rows, comp_line, carry);
+        blur_lines(work, 3, 3, int(w), kSegRows, mix.rows, c, carry, true);
         float* dst = outs.p[c] + size_t(y) * n3;
-        for (int i = threadIdx.x; i < n3; i += blockDim.x) dst[i] = work[i];
+        if (vec) {
+            for (int i = threadIdx.x; i < n3 / 4; i += blockDim.x)
+                reinterpret_cast<float4*>(dst)[i] = reinterpret_cast<const float4*>(work)[i];
+        } else {
+            for (int i = threadIdx.x; i < n3; i += blockDim.x) dst[i] = work[i];
+        }
         __syncthreads();
     }
 }
@@ -195,31 +230,67 @@ __global__ void __launch_bounds__(kColThreads) k_iir_cols(float* raw, IirPlanes 
     double* carry = reinterpret_cast<double*>(strip + size_t(n) * kColLines);
     const size_t pitch = 3 * size_t(w);
     const size_t off = 3 * size_t(x0);
+    // a full strip of a frame whose width is a multiple of 4: every strip row is three aligned float4
+    const bool vec = px == kColPixels && (w & 3u) == 0;
+    constexpr int kQuads = kColLines / 4;
     for (int c = 0; c < int(mix.ncomp); ++c) {
         const float* src = hs.p[c];
-        for (int i = threadIdx.x; i < n * kColLines; i += blockDim.x) {
-            const int r = i / kColLines, j = i % kColLines;
-            strip[i] = j < nl ? src[size_t(r) * pitch + off + j] : 0.0f;
+        if (vec) {
+            for (int i = threadIdx.x; i < n * kQuads; i += blockDim.x) {
+                const int r = i / kQuads, qd = i - r * kQuads;
+                cp_async16(strip + size_t(r) * kColLines + 4 * qd, src + size_t(r) * pitch + off + 4 * qd);
+            }
+            cp_async_wait_all();
+        } else {
+            for (int i = threadIdx.x; i < n * kColLines; i += blockDim.x) {
+                const int r = i / kColLines, j = i % kColLines;
+                strip[i] = j < nl ? src[size_t(r) * pitch + off + j] : 0.0f;
+            }
         }
         __syncthreads();
-        int comp_line[kColLines];
+        blur_lines(strip, kColLines, kColLines, n, kSegCols, mix.cols, c, carry, false);
+        const bool first = c == 0, last = c + 1 == int(mix.ncomp);
+        if (vec) {
+            for (int i = threadIdx.x; i < n * kQuads; i += blockDim.x) {
+                const int r = i / kQuads, qd = i - r * kQuads;
+                const size_t o = size_t(r) * pitch + off + 4 * qd;
+                const float4 v = *reinterpret_cast<const float4*>(strip + size_t(r) * kColLines + 4 * qd);
+                const float vv[4] = {v.x, v.y, v.z, v.w};
+                float av[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+                if (!first) {
+                    const float4 p = *reinterpret_cast<const float4*>(acc + o);
+                    av[0] = p.x;
+                    av[1] = p.y;
+                    av[2] = p.z;
+                    av[3] = p.w;
+                }
+                float4 rw = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                if (last) rw = *reinterpret_cast<const float4*>(raw + o);
+                float rr[4] = {rw.x, rw.y, rw.z, rw.w};
 #pragma unroll
-        for (int j = 0; j < kColLines; ++j) comp_line[j] = 3 * c + j % 3;
-        blur_lines(strip, kColLines, kColLines, n, kSegCols, mix.cols, comp_line, carry);
-        const float wgt[3] = {mix.weight[c][0], mix.weight[c][1], mix.weight[c][2]};
-        const bool last = c + 1 == int(mix.ncomp);
-        for (int i = threadIdx.x; i < n * kColLines; i += blockDim.x) {
-            const int r = i / kColLines, j = i % kColLines;
-            if (j >= nl) continue;
-            const size_t o = size_t(r) * pitch + off + j;
-            const float v = strip[i];
-            const float wc = wgt[j % 3];
-            const float a = c == 0 ? 0.0f + wc * v : acc[o] + wc * v;
-            if (last) {
-                const float m0 = mix.mix_a[j % 3], m1 = mix.mix_b[j % 3];
-                raw[o] = m0 * raw[o] + m1 * a;
-            } else {
-                acc[o] = a;
+                for (int e = 0; e < 4; ++e) {
+                    const int ch3 = (4 * qd + e) % 3;
+                    const float wc = mix.weight[c][ch3];
+                    av[e] = first ? 0.0f + wc * vv[e] : av[e] + wc * vv[e];
+                    if (last) rr[e] = mix.mix_a[ch3] * rr[e] + mix.mix_b[ch3] * av[e];
+                }
+                if (last) *reinterpret_cast<float4*>(raw + o) = make_float4(rr[0], rr[1], rr[2], rr[3]);
+                else *reinterpret_cast<float4*>(acc + o) = make_float4(av[0], av[1], av[2], av[3]);
+            }
+        } else {
+            for (int i = threadIdx.x; i < n * kColLines; i += blockDim.x) {
+                const int r = i / kColLines, j = i % kColLines;
+                if (j >= nl) continue;
+                const size_t o = size_t(r) * pitch + off + j;
+                const float v = strip[i];
+                const float wc = mix.weight[c][j % 3];
+                const float a = first ? 0.0f + wc * v : acc[o] + wc * v;
+                if (last) {
+                    const float m0 = mix.mix_a[j % 3], m1 = mix.mix_b[j % 3];
+                    raw[o] = m0 * raw[o] + m1 * a;
+                } else {
+                    acc[o] = a;
+                }
             }
         }
         __syncthreads();
@@ -230,15 +301,33 @@ __global__ void __launch_bounds__(kColThreads) k_iir_cols(float* raw, IirPlanes 
 
 size_t iir_rows_smem(uint32_t w) {
     const size_t n3r = (3 * size_t(w) + 3) & ~size_t(3);
-    return 2 * n3r * sizeof(float) + size_t(3) * kSegRows * 3 * sizeof(double);
+    return n3r * sizeof(float) + size_t(3) * kSegRows * 3 * sizeof(double);
 }
 
 size_t iir_cols_smem(uint32_t h) {
     return size_t(h) * kColLines * sizeof(float) + size_t(kColLines) * kSegCols * 3 * sizeof(double);
 }
 
-int iir_row_segments() { return kSegRows; }
-int iir_col_segments() { return kSegCols; }
+// The column segment length: at least n / nseg, and with nlines L = nlines (mod 32), so that a warp's
+// lanes (line t % nlines, segment t / nlines, sample i) address floats equal to t + nlines i modulo 32
+// and never share a shared-memory bank (L = 1 (mod 8) for twelve lines).
+namespace {
+int seg_len(uint32_t n, int nseg, int nlines) {
+    int g = 32;
+    while (nlines % g != 0) g /= 2;  // gcd(nlines, 32)
+    const int m = 32 / g;
+    const int L0 = int((n + uint32_t(nseg) - 1) / uint32_t(nseg));
+    return L0 + ((1 - L0) % m + m) % m;
+}
+}  // namespace
+
+// rows run segment-major (a warp's lanes: one line, 32 consecutive segments, addresses 3 L t + const):
+// any odd L keeps them in distinct banks
+int iir_row_seg_len(uint32_t w) {
+    const int L0 = int((w + uint32_t(kSegRows) - 1) / uint32_t(kSegRows));
+    return L0 | 1;
+}
+int iir_col_seg_len(uint32_t h) { return seg_len(h, kSegCols, kColLines); }
 
 bool iir_mixture_fits(uint32_t w, uint32_t h) {
     int dev = 0, optin = 0;

@@ -9,11 +9,14 @@
 
 namespace spkb::dev {
 
-// One channel of one component: Young-van Vliet coefficients and M, the map of a segment's entry
-// state (w[i-1], w[i-2], w[i-3]) through seg_len steps of the homogeneous recurrence.
+constexpr int kIirScanSteps = 7;  // carries of up to 2^7 segments per line
+
+// One channel of one component: Young-van Vliet coefficients and the powers M^(2^p), p = 0..6, of M,
+// the map of a segment's entry state (w[i-1], w[i-2], w[i-3]) through seg_len steps of the homogeneous
+// recurrence (the parallel scan of the segment carries applies M^(2^p) at step p).
 struct IirChannel {
     double B, B1, B2, B3;
-    double M[3][3];
+    double Mp[kIirScanSteps][3][3];
     int32_t active;  // 0: the channel passes through (its sigma is on the FIR or identity branch)
     int32_t pad;
 };
@@ -37,8 +40,8 @@ struct IirPlanes {
 
 size_t iir_rows_smem(uint32_t w);
 size_t iir_cols_smem(uint32_t h);
-int iir_row_segments();
-int iir_col_segments();
+int iir_row_seg_len(uint32_t w);  // segment length of the row and column passes for this frame
+int iir_col_seg_len(uint32_t h);
 bool iir_mixture_fits(uint32_t w, uint32_t h);  // both kernels' lines fit in shared memory
 
 // raw := mix_a raw + mix_b sum_k weight_k G_k(raw), every component recursive on every channel.

@@ -349,7 +349,7 @@ constexpr uint32_t kDrawWarps = 4;
 constexpr uint32_t kDrawRing = 64;  // holds the < 32 left over plus one draw's 32
 
 struct DeferredDraw {
-    spk_ptrs p;          // PTRS constants (kind 1, 2); p.lam alone for kind 0
+    float lam, b, a, vr; // the squeeze's PTRS constants (kinds 1, 2); lam alone for kind 0
     float V, k, us;      // attempt 0's full test, pending (kind 1)
     uint32_t w2, w3;     // words z, w of Philox block 0: attempt 1's uniforms (kinds 1, 2)
     uint32_t pixel;
@@ -358,15 +358,22 @@ struct DeferredDraw {
 // kinds: 0 product method (lam < 10 or NaN); 1 attempt 0 needs the full test; 2 attempt 0 rejected
 
 // The rest of a deferred draw: attempt 0's pending full test (kind 1), then attempts 1..63 exactly as
-// spk_ptrs_from runs them, with one copy of the test, the squeeze and the generator in the loop.
+// spk_ptrs_from runs them, with one copy of the test, the squeeze and the generator in the loop. The
+// test's own constants (log lam, 1 / alpha) are formed here, for the draws that reach it.
 __device__ __forceinline__ void finish_draw(const DeferredDraw& d, uint32_t seed, float* res) {
     const uint32_t kind = d.tag & 3u, stream = (d.tag >> 2) & 0xFFu, slot = d.tag >> 10;
     spk_stream g;
     spk_stream_init(&g, d.pixel, stream, seed);
     float value;
     if (kind == 0u) {
-        value = spk_poisson_product(d.p.lam, &g);
+        value = spk_poisson_product(d.lam, &g);
     } else {
+        spk_ptrs p;
+        p.lam = d.lam;
+        p.b = d.b;
+        p.a = d.a;
+        p.vr = d.vr;
+        spk_ptrs_init_test(&p);
         g.block.z = d.w2;
         g.block.w = d.w3;
         g.used = 2;
@@ -375,17 +382,17 @@ __device__ __forceinline__ void finish_draw(const DeferredDraw& d, uint32_t seed
         int state = kind == 1u ? SPK_PTRS_TEST : SPK_PTRS_REJECT;
         for (int it = 1;; ++it) {
             // state: the outcome of attempt it - 1's squeeze
-            if (state == SPK_PTRS_ACCEPT || (state == SPK_PTRS_TEST && spk_ptrs_test(&d.p, V, k, us))) {
+            if (state == SPK_PTRS_ACCEPT || (state == SPK_PTRS_TEST && spk_ptrs_test(&p, V, k, us))) {
                 value = k;
                 break;
             }
             if (it == 64) {
-                value = SPK_FLOOR(d.p.lam);
+                value = SPK_FLOOR(p.lam);
                 break;
             }
             const float u = spk_stream_uniform(&g);
             V = spk_stream_uniform(&g);
-            state = spk_ptrs_squeeze(&d.p, u, V, &k, &us);
+            state = spk_ptrs_squeeze(&p, u, V, &k, &us);
         }
     }
     res[slot] = value;
@@ -437,9 +444,11 @@ __global__ void __launch_bounds__(kDrawWarps * 32) k_develop_layers(const float*
         d.pixel = pixel;
         uint32_t kind = 0u;
         const float lm = lam[k][tid];
+        d.lam = lm;
         if (live) {
             if (lm >= 10.0f) {
-                spk_ptrs_init(&d.p, lm);
+                spk_ptrs p;
+                spk_ptrs_init(&p, lm);
                 spk_u4 c4;
                 c4.x = pixel;
                 c4.y = stream;
@@ -447,12 +456,15 @@ __global__ void __launch_bounds__(kDrawWarps * 32) k_develop_layers(const float*
                 c4.w = 0u;
                 const spk_u4 b0 = spk_philox(c4, q.seed, 0u);
                 float kk, us;
-                const int r = spk_ptrs_squeeze(&d.p, spk_uniform(b0.x), spk_uniform(b0.y), &kk, &us);
+                const int r = spk_ptrs_squeeze(&p, spk_uniform(b0.x), spk_uniform(b0.y), &kk, &us);
                 if (r == SPK_PTRS_ACCEPT) {
                     value = kk;
                 } else {
                     defer = true;
                     kind = r == SPK_PTRS_TEST ? 1u : 2u;
+                    d.b = p.b;
+                    d.a = p.a;
+                    d.vr = p.vr;
                     d.V = spk_uniform(b0.y);
                     d.k = kk;
                     d.us = us;
@@ -461,7 +473,6 @@ __global__ void __launch_bounds__(kDrawWarps * 32) k_develop_layers(const float*
                 }
             } else {
                 defer = true;
-                d.p.lam = lm;
             }
         }
         const uint32_t mask = __ballot_sync(0xFFFFFFFFu, defer);
@@ -472,16 +483,14 @@ __global__ void __launch_bounds__(kDrawWarps * 32) k_develop_layers(const float*
             resw[k * 32u + lane] = value;
         }
         tail += __popc(mask);
-        if (tail - head >= 32u) {
+        // finish 32 deferred draws at a time; after the last draw, whatever is left (at most 63)
+        while (tail - head >= 32u || (k == 8u && tail != head)) {
             __syncwarp();
-            finish_draw(ringw[(head + lane) & (kDrawRing - 1u)], q.seed, resw);
-            head += 32u;
+            if (lane < tail - head) finish_draw(ringw[(head + lane) & (kDrawRing - 1u)], q.seed, resw);
+            head += min(tail - head, 32u);
             __syncwarp();
         }
     }
-    __syncwarp();
-    if (lane < tail - head) finish_draw(ringw[(head + lane) & (kDrawRing - 1u)], q.seed, resw);
-    __syncwarp();
     if (!live) return;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {

@@ -82,14 +82,18 @@ __device__ __forceinline__ float paper_lookup(const float* __restrict__ tab, uin
     return y0 + ((v - __ldg(x + j)) * __ldg(r + j)) * (__ldg(y + 3 * (j + 1) + c) - y0);
 }
 
-__device__ __forceinline__ float knee(float d, float tau, float lim, float p) {
+// A division by a per-frame or literal constant is a product with its binary32 reciprocal (formed on the
+// host, or folded by the compiler): as accurate as the approximate divide and no special-function op.
+#define RCP(x) (1.0f / (x))
+
+__device__ __forceinline__ float knee(float d, float tau, float lim, float p, float inv_span, float inv_p) {
     if (d <= tau) return d;
-    const float x = fdiv(d - tau, lim - tau);
-    return tau + (lim - tau) * fdiv(x, powm(1.0f + powm(x, p), fdiv(1.0f, p)));
+    const float x = (d - tau) * inv_span;
+    return tau + (lim - tau) * fdiv(x, powm(1.0f + powm(x, p), inv_p));
 }
 
 __device__ __forceinline__ float post_adapt(float v, float f_l) {
-    const float f = powm(fdiv(f_l * fabsf(v), 100.0f), 0.42f);
+    const float f = powm((f_l * fabsf(v)) * RCP(100.0f), 0.42f);
     return fdiv((400.0f * sgnf(v)) * f, 27.13f + f) + 0.1f;
 }
 
@@ -106,34 +110,34 @@ __device__ __forceinline__ void gamut(const PrintArgs& pa, float& r, float& g, f
     const float ra = post_adapt(q.d_rgb[0] * R16, q.f_l);
     const float ga = post_adapt(q.d_rgb[1] * G16, q.f_l);
     const float ba = post_adapt(q.d_rgb[2] * B16, q.f_l);
-    const float a = (ra - fdiv(12.0f * ga, 11.0f)) + fdiv(ba, 11.0f);
-    const float bb = fdiv((ra + ga) - 2.0f * ba, 9.0f);
+    const float a = (ra - (12.0f * ga) * RCP(11.0f)) + ba * RCP(11.0f);
+    const float bb = ((ra + ga) - 2.0f * ba) * RCP(9.0f);
     const float h = atan2f(bb, a);
     const float et = 0.25f * (cosf(h + 2.0f) + 3.8f);
-    const float A = (((2.0f * ra + ga) + fdiv(ba, 20.0f)) - 0.305f) * q.n_bb;
-    const float ratio = fdiv(A, q.a_w);
+    const float A = (((2.0f * ra + ga) + ba * RCP(20.0f)) - 0.305f) * q.n_bb;
+    const float ratio = A * q.inv_a_w;
     const float J = (100.0f * sgnf(ratio)) * powm(fabsf(ratio), cz);
-    const float den = (ra + ga) + fdiv(21.0f * ba, 20.0f);
+    const float den = (ra + ga) + (21.0f * ba) * RCP(20.0f);
     const float t = den != 0.0f ? fdiv(((((50000.0f / 13.0f) * q.n_c) * q.n_cb) * et) * fsqrt(a * a + bb * bb), den)
                                 : 0.0f;
-    const float C = t > 0.0f ? (powm(t, 0.9f) * fsqrt(fdiv(fabsf(J), 100.0f))) * chroma_k : 0.0f;
+    const float C = t > 0.0f ? (powm(t, 0.9f) * fsqrt(fabsf(J) * RCP(100.0f))) * chroma_k : 0.0f;
     const float M = C * f_l_qrt;
-    const float Mp = fdiv(logf(1.0f + 0.0228f * M), 0.0228f);
+    const float Mp = logf(1.0f + 0.0228f * M) * RCP(0.0228f);
     float Jp = fdiv(1.7f * J, 1.0f + 0.007f * J);
     if (q.lc_active != 0u) {
-        float Ln = fdiv(Jp, q.j_white);
+        float Ln = Jp * q.inv_j_white;
         if (Ln > q.lc[0]) {
-            Ln = knee(Ln, q.lc[0], q.lc[1], q.lc[2]);
+            Ln = knee(Ln, q.lc[0], q.lc[1], q.lc[2], q.lc_inv_span, q.lc_inv_p);
             Jp = Ln * q.j_white;
         }
     }
     // C_max(J', h), bilinear with hue wrap
     const float Jc = fminf(fmaxf(Jp, q.j_first), q.j_last);
-    const float u = fdiv(Jc - q.j_first, q.j_last - q.j_first) * float(q.rows - 1);
+    const float u = ((Jc - q.j_first) * q.inv_j_span) * float(q.rows - 1);
     int l0 = int(floorf(u));
     l0 = l0 < 0 ? 0 : (l0 > int(q.rows) - 2 ? int(q.rows) - 2 : l0);
     const float fl = u - float(l0);
-    const float v = fdiv(h - q.h_first, q.h_step);
+    const float v = (h - q.h_first) * q.inv_h_step;
     const float vf = floorf(v);
     const int cols = int(q.cols);
     int h0 = int(vf) % cols;
@@ -145,16 +149,16 @@ __device__ __forceinline__ void gamut(const PrintArgs& pa, float& r, float& g, f
     const float cm = (1.0f - fl) * ((1.0f - fh) * t00 + fh * t01) + fl * ((1.0f - fh) * t10 + fh * t11);
     const float cs = fmaxf(cm, 1e-9f);
     float dch = fdiv(Mp, cs);
-    if (dch > 0.0f) dch = knee(dch, q.knee[0], q.knee[1], q.knee[2]);
+    if (dch > 0.0f) dch = knee(dch, q.knee[0], q.knee[1], q.knee[2], q.knee_inv_span, q.knee_inv_p);
     const float Mn = dch * cs;
     // guarded inverse
-    const float Mi = fdiv(expf(0.0228f * Mn) - 1.0f, 0.0228f);
+    const float Mi = (expf(0.0228f * Mn) - 1.0f) * RCP(0.0228f);
     const float Ji = fdiv(Jp, 1.7f - 0.007f * Jp);
-    const float Ci = fdiv(Mi, f_l_qrt);
-    const float Ai = (q.a_w * sgnf(Ji)) * powm(fabsf(fdiv(Ji, 100.0f)), inv_cz);
-    const float sq = fsqrt(fdiv(fabsf(Ji), 100.0f));
+    const float Ci = Mi * q.inv_f_l_qrt;
+    const float Ai = (q.a_w * sgnf(Ji)) * powm(fabsf(Ji * RCP(100.0f)), inv_cz);
+    const float sq = fsqrt(fabsf(Ji) * RCP(100.0f));
     const float ti = (sq > 0.0f && Ci > 0.0f) ? powm(fdiv(Ci, sq * chroma_k), 1.0f / 0.9f) : 0.0f;
-    const float p2 = fdiv(Ai, q.n_bb) + 0.305f;
+    const float p2 = Ai * q.inv_n_bb + 0.305f;
     const float p3 = 21.0f / 20.0f;
     float ai = 0.0f, bi = 0.0f;
     if (ti != 0.0f) {
@@ -162,33 +166,34 @@ __device__ __forceinline__ void gamut(const PrintArgs& pa, float& r, float& g, f
         float sh, ch;
         sincosf(h, &sh, &ch);
         if (fabsf(sh) >= fabsf(ch)) {
-            const float p4 = fdiv(p1, sh);
+            const float rs = fdiv(1.0f, sh);
+            const float p4 = p1 * rs;
             bi = fdiv((p2 * (2.0f + p3)) * (460.0f / 1403.0f),
-                      ((p4 + ((2.0f + p3) * (220.0f / 1403.0f)) * fdiv(ch, sh)) - 27.0f / 1403.0f) +
+                      ((p4 + ((2.0f + p3) * (220.0f / 1403.0f)) * (ch * rs)) - 27.0f / 1403.0f) +
                           p3 * (6300.0f / 1403.0f));
-            ai = fdiv(bi * ch, sh);
+            ai = (bi * ch) * rs;
         } else {
-            const float p5 = fdiv(p1, ch);
+            const float rc = fdiv(1.0f, ch);
+            const float p5 = p1 * rc;
             ai = fdiv((p2 * (2.0f + p3)) * (460.0f / 1403.0f),
-                      (p5 + (2.0f + p3) * (220.0f / 1403.0f)) -
-                          (27.0f / 1403.0f - p3 * (6300.0f / 1403.0f)) * fdiv(sh, ch));
-            bi = fdiv(ai * sh, ch);
+                      (p5 + (2.0f + p3) * (220.0f / 1403.0f)) - (27.0f / 1403.0f - p3 * (6300.0f / 1403.0f)) * (sh * rc));
+            bi = (ai * sh) * rc;
         }
     }
-    const float xa[3] = {fdiv((460.0f * p2 + 451.0f * ai) + 288.0f * bi, 1403.0f),
-                         fdiv((460.0f * p2 - 891.0f * ai) - 261.0f * bi, 1403.0f),
-                         fdiv((460.0f * p2 - 220.0f * ai) - 6300.0f * bi, 1403.0f)};
-    float rc[3];
+    const float xa[3] = {((460.0f * p2 + 451.0f * ai) + 288.0f * bi) * RCP(1403.0f),
+                         ((460.0f * p2 - 891.0f * ai) - 261.0f * bi) * RCP(1403.0f),
+                         ((460.0f * p2 - 220.0f * ai) - 6300.0f * bi) * RCP(1403.0f)};
+    float rc3[3];
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
         const float vv = xa[i] - 0.1f;
         const float av = fabsf(vv);
         const float beta = av >= 400.0f ? 0.0f : fdiv(27.13f * av, 400.0f - av);
-        rc[i] = fdiv((hundred_over_f_l * sgnf(vv)) * powm(beta, 1.0f / 0.42f), q.d_rgb[i]);
+        rc3[i] = ((hundred_over_f_l * sgnf(vv)) * powm(beta, 1.0f / 0.42f)) * q.inv_d_rgb[i];
     }
     float x100, y100, z100;
-    mat_apply(q.m16_inv, rc[0], rc[1], rc[2], x100, y100, z100);
-    mat_apply(q.m_to_rgb, fdiv(x100, 100.0f), fdiv(y100, 100.0f), fdiv(z100, 100.0f), r, g, b);
+    mat_apply(q.m16_inv, rc3[0], rc3[1], rc3[2], x100, y100, z100);
+    mat_apply(q.m_to_rgb, x100 * RCP(100.0f), y100 * RCP(100.0f), z100 * RCP(100.0f), r, g, b);
 }
 
 // the print gain and paper curve of one pixel (print.metal:192-232): l := log10(max(R g + o, 0) + 1e-10),

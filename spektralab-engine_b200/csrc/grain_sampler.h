@@ -275,14 +275,19 @@ typedef struct {
 #define SPK_PTRS_ACCEPT 1
 #define SPK_PTRS_TEST 2 /* neither squeeze decides: the full test follows */
 
+/* the constants of the squeeze: lam, b, a, vr */
 SPK_HD void spk_ptrs_init(spk_ptrs* p, float lam) {
     const float slam = SPK_SQRT(lam);
     p->lam = lam;
-    p->loglam = spk_logf(lam);
     p->b = SPK_ADD(0.931f, SPK_MUL(2.53f, slam));
     p->a = SPK_ADD(-0.059f, SPK_MUL(0.02483f, p->b));
-    p->invalpha = SPK_ADD(1.1239f, SPK_DIV(1.1328f, SPK_SUB(p->b, 3.4f)));
     p->vr = SPK_SUB(0.9277f, SPK_DIV(3.6224f, SPK_SUB(p->b, 2.0f)));
+}
+
+/* the constants only the full test reads: log lam and 1 / alpha (after spk_ptrs_init) */
+SPK_HD void spk_ptrs_init_test(spk_ptrs* p) {
+    p->loglam = spk_logf(p->lam);
+    p->invalpha = SPK_ADD(1.1239f, SPK_DIV(1.1328f, SPK_SUB(p->b, 3.4f)));
 }
 
 /* the candidate k of an attempt and its two squeezes */
@@ -342,6 +347,7 @@ SPK_HD float spk_poisson(float lam, uint32_t pixel, uint32_t stream, uint32_t se
     if (lam >= 10.0f) {
         spk_ptrs p;
         spk_ptrs_init(&p, lam);
+        spk_ptrs_init_test(&p);
         return spk_ptrs_from(&p, &g, 0);
     }
     return spk_poisson_product(lam, &g);

@@ -322,7 +322,8 @@ void fill_launch(dev::IirLaunch& q, const std::vector<MixtureComponent>& comps, 
             d.B1 = k.B1;
             d.B2 = k.B2;
             d.B3 = k.B3;
-            entry_map(k, L, d.M);
+            // M^(2^p): the map through L 2^p steps, iterated directly
+            for (int p = 0; p < dev::kIirScanSteps; ++p) entry_map(k, L << p, d.Mp[p]);
             d.active = 1;
         }
 }
@@ -341,8 +342,8 @@ bool iir_mixture_mix(RenderCtx& ctx, const Plane& raw, const std::vector<Mixture
     for (size_t c = 0; c < comps.size(); ++c) weights(comps[c].weight, q.weight[c]);
     weights(a, q.mix_a);
     weights(b, q.mix_b);
-    const int Lr = int((raw.w + dev::iir_row_segments() - 1) / dev::iir_row_segments());
-    const int Lc = int((raw.h + dev::iir_col_segments() - 1) / dev::iir_col_segments());
+    const int Lr = dev::iir_row_seg_len(raw.w);
+    const int Lc = dev::iir_col_seg_len(raw.h);
     fill_launch(q.rows, comps, Lr);
     fill_launch(q.cols, comps, Lc);
     std::vector<Plane> tmp;

@@ -939,6 +939,17 @@ std::shared_ptr<PrintSetup> build_print_setup(const ParamSet& p, const FilmSetup
         q.f_l_qrt = std::pow(q.f_l, 0.25f);
         q.chroma_k = std::pow(1.64f - std::pow(0.29f, q.n), 0.73f);
         q.hundred_over_f_l = 100.0f / q.f_l;
+        q.inv_a_w = 1.0f / q.a_w;
+        q.inv_j_white = 1.0f / q.j_white;
+        q.inv_n_bb = 1.0f / q.n_bb;
+        q.inv_f_l_qrt = 1.0f / q.f_l_qrt;
+        q.inv_h_step = 1.0f / q.h_step;
+        q.inv_j_span = 1.0f / (q.j_last - q.j_first);
+        for (int i = 0; i < 3; ++i) q.inv_d_rgb[i] = 1.0f / q.d_rgb[i];
+        q.knee_inv_span = 1.0f / (q.knee[1] - q.knee[0]);
+        q.knee_inv_p = 1.0f / q.knee[2];
+        q.lc_inv_span = 1.0f / (q.lc[1] - q.lc[0]);
+        q.lc_inv_p = 1.0f / q.lc[2];
     }
     s->cctf = p.b(P::output_cctf_encoding);
     s->cctf_mode = uint32_t(s->out_cs.cctf);

@@ -103,6 +103,9 @@ struct Cam16Args {
     // per-frame constants of the reference's per-pixel set-up (kernels/print.metal:53-64), formed on the
     // host in binary32 by the same operations: c z, 1 / (c z), F_L^0.25, (1.64 - 0.29^n)^0.73, 100 / F_L
     float cz, inv_cz, f_l_qrt, chroma_k, hundred_over_f_l;
+    // binary32 reciprocals of the frame's divisors, for the gamut stage's approximate arithmetic
+    float inv_a_w, inv_j_white, inv_n_bb, inv_f_l_qrt, inv_h_step, inv_j_span, inv_d_rgb[3];
+    float knee_inv_span, knee_inv_p, lc_inv_span, lc_inv_p;  // 1 / (lim - tau), 1 / p of the two knees
 };
 
 // The print kernel: negative density -> linear output RGB.
