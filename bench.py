@@ -57,9 +57,18 @@ KERNEL_BYTES_PER_PX = {
     "develop": 24, "develop_layers": 24, "print": 24, "encode": 32, "fir_tile": 24, "scan_encode": 20,
     "iir_rows": 12 + 12 * N_HALATION, "iir_cols": 12 * N_HALATION + 24,
 }
-# ncu DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) per launch of the kernels captured so far,
-# from the summaries under profiles/ (scaled to a 3840 x 2160 launch); None until captured.
-NCU_TRAFFIC_PER_LAUNCH = {}
+N_SM = 148
+# From the ncu capture summarised in profiles/render_kernels_2048x2048_ncu.md (one 2048 x 2048 render +
+# reprint, --set full): DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) and warp instructions
+# (smsp__inst_executed.sum) per pixel of each kernel's launch. Traffic scales with the pixels launched.
+NCU_TRAFFIC_PER_PX = {"expose": 14.17, "iir_rows": 25.03, "iir_cols": 54.04, "develop_layers": 14.08,
+                      "fir_tile": 14.24, "print": 13.00, "scan_encode": 13.13}
+NCU_WARP_INST_PER_PX = {"expose": 15.07, "iir_rows": 18.28, "iir_cols": 13.01, "develop_layers": 174.92,
+                        "fir_tile": 10.06, "print": 60.29, "scan_encode": 28.16}
+
+
+def workload_name():
+    return "4K full render + reprint" if (W, H) == (3840, 2160) else f"{W}x{H} full render + reprint"
 
 
 def film_format_for_grains(lib, resources, long_edge):
@@ -212,11 +221,44 @@ def run_reference(args):
     line = {"impl": "reference", "metric": METRIC, "value": fps, "unit": UNIT, "n_gpus": 0, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1000.0 * 4.0 * sum(times) / len(times), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "4K full render + reprint", "width": W, "height": H},
+            "config": {"workload": workload_name(), "width": W, "height": H},
             "cpu_baseline": {"value": fps, "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample},
             "e2e": {"value": fps, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
+
+
+def run_e2e(args, eng, img, delta, pg, local, world):
+    """The workload through the C ABI with host buffers: spk_open from pinned host memory, spk_render,
+    spk_set_params, spk_reprint, both results copied to pinned host memory and read in place."""
+    import torch
+
+    pinned = torch.empty((H, W, 3), dtype=torch.float32, pin_memory=True).numpy()
+    pinned[...] = img
+
+    def e2e_step():
+        # spk_open copies the frame from pinned host memory; spk_render / spk_reprint copy each result to
+        # pinned host memory (the pixels are read in place, as a caller of the C ABI reads them)
+        with eng.open(pinned, delta) as s:
+            s.set_halation(*HALATION)
+            with s.render_result("full") as a:
+                s.set_params({"print_exposure": 1.2})
+                with s.render_result("full", reprint=True) as b:
+                    checksum = int(a.pixels[H // 2, W // 2, 1]) + int(b.pixels[H // 2, W // 2, 1])
+                    return a.row_stride_px, checksum
+
+    for _ in range(args.warmup):
+        e2e_step()
+    barrier(pg, local)
+    t0 = time.perf_counter()
+    stride = 0
+    for _ in range(args.steps):
+        stride, _ = e2e_step()
+    e2e_s = reduce_max(pg, local, time.perf_counter() - t0)
+    barrier(pg, local)
+    e2e = {"value": world * args.steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": W * H * 3 * 4,
+           "d2h_bytes_per_step": 2 * stride * H * 8}
+    return e2e
 
 
 def main():
@@ -226,7 +268,12 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
+    ap.add_argument("--width", type=int, default=3840, help="frame width (the benchmark workload is 3840)")
+    ap.add_argument("--height", type=int, default=2160, help="frame height (the benchmark workload is 2160)")
     args = ap.parse_args()
+    global W, H
+    W, H = args.width, args.height
     if args.impl == "reference":
         return run_reference(args)
     args.warmup = max(args.warmup, 3)
@@ -276,11 +323,26 @@ def main():
     table = {n: {"launches": len(v), "total_ms": sum(v), "mean_ms": sum(v) / len(v)} for n, v in kern.items()}
     dom = max(table, key=lambda n: table[n]["total_ms"])
     peak, peak_kind = hbm_peak()
+    clk_sum = clk.summary()
+    sm_ghz = (clk_sum["sm_mhz"] or 1965.0) / 1000.0
+    issue_peak = N_SM * 4 * sm_ghz  # G warp-instructions/s: four schedulers per SM, one issue each per clock
+    for n, t in table.items():
+        t["hbm_gbs"] = KERNEL_BYTES_PER_PX.get(n, 24) * W * H / (t["mean_ms"] / 1000.0) / 1e9
+        t["hbm_frac"] = t["hbm_gbs"] / peak
+        if n in NCU_WARP_INST_PER_PX:
+            t["issue_frac"] = NCU_WARP_INST_PER_PX[n] * W * H / (t["mean_ms"] / 1000.0) / 1e9 / issue_peak
     bytes_launch = KERNEL_BYTES_PER_PX.get(dom, 24) * W * H
     achieved = bytes_launch / (table[dom]["mean_ms"] / 1000.0) / 1e9
+    traffic = NCU_TRAFFIC_PER_PX.get(dom)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": NCU_TRAFFIC_PER_LAUNCH.get(dom), "kernel": dom,
-                "algorithmic_bytes_per_launch": bytes_launch, "peak_source": peak_kind}
+                "traffic": traffic * W * H if traffic else None, "kernel": dom,
+                "algorithmic_bytes_per_launch": bytes_launch, "peak_source": f"{peak_kind} (MEASURED_PEAKS hbm_gbs)",
+                # the render kernels are instruction-bound, not HBM-bound: the fraction of the SMs' issue
+                # rate the kernel sustains (warp instructions per pixel from its ncu capture, the launch time
+                # measured here, peak = 4 warp instructions per SM per clock at the sampled SM clock)
+                "issue_frac": table[dom].get("issue_frac"),
+                "step_hbm_gbs": (sum(KERNEL_BYTES_PER_PX.get(n, 24) * t["launches"] for n, t in table.items())
+                                 * W * H / args.steps) / (dev_ms_max / args.steps / 1000.0) / 1e9}
     stage_ms = {}
     for prof in (pr, pp):
         for name, ms in prof["stages"].items():
@@ -288,29 +350,9 @@ def main():
     sess.close()
 
     # ---- end to end through the C ABI with host buffers ----
-    import torch
-    pinned = torch.empty((H, W, 3), dtype=torch.float32, pin_memory=True).numpy()
-    pinned[...] = img
-    for _ in range(args.warmup):
-        with eng.open(pinned, delta) as s:
-            s.set_halation(*HALATION)
-            s.render("full")
-            s.set_params({"print_exposure": 1.2})
-            s.reprint("full")
-    barrier(pg, local)
-    t0 = time.perf_counter()
-    stride = 0
-    for _ in range(args.steps):
-        with eng.open(pinned, delta) as s:
-            s.set_halation(*HALATION)
-            a, meta = s.render("full")
-            s.set_params({"print_exposure": 1.2})
-            b, _ = s.reprint("full")
-            stride = meta["row_stride_px"]
-    e2e_s = reduce_max(pg, local, time.perf_counter() - t0)
-    barrier(pg, local)
-    e2e = {"value": world * args.steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": W * H * 3 * 4,
-           "d2h_bytes_per_step": 2 * stride * H * 8}
+    e2e = None
+    if not args.no_e2e:
+        e2e = run_e2e(args, eng, img, delta, pg, local, world)
     eng.close()
 
     cpu = None
@@ -324,7 +366,7 @@ def main():
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": dev_ms_max / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": {"workload": "4K full render + reprint", "width": W, "height": H,
+                "config": {"workload": workload_name(), "width": W, "height": H,
                            "halation_sigma_px": [20, 120], "halation_weight": 0.03, "scanner_lens_blur_px": 1.5,
                            "grains_per_px": TARGET_GRAINS, "film_format_mm": round(ff, 4),
                            "parallelism": f"replicas{world}", "l2": "flushed (256 MiB write) before each step"},
@@ -332,7 +374,7 @@ def main():
                 "render_fps": 1000.0 / render_ms, "reprint_fps": 1000.0 / reprint_ms,
                 "wall_s_timed": wall, "stage_ms": stage_ms, "kernels": table,
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
-                "clocks": clk.summary()}
+                "clocks": clk_sum}
         print(json.dumps(line), flush=True)
     if pg is not None:
         pg.destroy_process_group()

@@ -190,6 +190,29 @@ class Engine:
         return Session(self, s, self.L.take_json(out))
 
 
+class Result:
+    """An spk_result held open: .pixels is a (height, width, 4) uint16 view of its pinned host pixels,
+    valid until .free()."""
+
+    def __init__(self, lib, r):
+        self.L = lib
+        self.r = r
+        self.pixels = np.ctypeslib.as_array(r.rgba16, shape=(r.height, r.row_stride_px, 4))[:, : r.width]
+        self.row_stride_px = r.row_stride_px
+
+    def free(self):
+        if self.r is not None:
+            self.pixels = None
+            self.L.lib.spk_result_free(ctypes.byref(self.r))
+            self.r = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.free()
+
+
 class Session:
     def __init__(self, engine, handle, reply):
         self.E = engine
@@ -230,6 +253,14 @@ class Session:
 
     def reprint(self, tier="full"):
         return self._render(self.L.lib.spk_reprint, tier)
+
+    def render_result(self, tier="full", reprint=False):
+        """spk_render / spk_reprint without a copy: a Result that owns the spk_result (its pinned host
+        pixels and device image) until .free()."""
+        r = SpkResult()
+        fn = self.L.lib.spk_reprint if reprint else self.L.lib.spk_render
+        self.L.check(fn(self.h, tier.encode(), ctypes.byref(r)))
+        return Result(self.L, r)
 
     # ---- extensions ----
     def set_halation(self, comps, strength):
