@@ -80,6 +80,26 @@ SPK_API spk_status spkx_philox(const uint32_t* counters, const uint32_t* keys, u
  * by the engine's FIR / recursive branch rule */
 SPK_API spk_status spkx_gaussian(const float* in, float* out, uint32_t w, uint32_t h, const double* sigma3);
 
+/* ---- the render's adjoint (no counterpart in the reference engine) ----
+ *
+ * spk_render_vjp(session, tier, film_seed, grad_output, grad_input, grad_params, n_params, output)
+ *   The differentiated output is the scanned linear RGB of the session's frame: the render up to the
+ *   scanner's lens blur and unsharp mask, before the output transfer function and the 16-bit encode, with
+ *   the grain held as fixed noise (the Poisson counts of film_seed). Host arrays of 3 floats per pixel:
+ *     output       (may be NULL) receives that linear RGB;
+ *     grad_output  (NULL: the output alone is computed) the gradient of a loss with respect to it;
+ *     grad_input   receives the gradient with respect to the session's source frame (RGB).
+ *   grad_params (n_params doubles) receives the gradient with respect to
+ *     [print_exposure, m_filter_shift, y_filter_shift, halation weight 0..K-1, halation sigma 0..K-1],
+ *   K the components set by spkx_session_set_halation (none otherwise; entries past the list are 0). A
+ *   halation weight or sigma is taken as one value for the three channels.
+ *   Blur passes are recomputed, not stored; the recursive blurs run transposed. Refused with
+ *   SPK_ERR_UNSUPPORTED: grain below full strength or without sub-layers, halation components whose
+ *   three channels differ in sigma.
+ */
+SPK_API spk_status spk_render_vjp(spk_session* session, const char* tier, uint32_t film_seed, const float* grad_output,
+                                  float* grad_input, double* grad_params, uint32_t n_params, float* output);
+
 /* ---- allocation-free entry point (no counterpart in the reference engine) ----
  *
  * spkx_gaussian_noalloc(in, out, w, h, sigma3, stream)

@@ -59,6 +59,7 @@ def lib():
         L.orc_render.argtypes = [ctypes.POINTER(OracleSetup), FP, I32, I32, FP, U16, PD]
         L.orc_develop.argtypes = [ctypes.POINTER(OracleSetup), FP, I32, I32, FP, PD]
         L.orc_print.argtypes = [ctypes.POINTER(OracleSetup), PD, I32, I32, U16, PD]
+        L.orc_render_linear.argtypes = [ctypes.POINTER(OracleSetup), PD, I32, I32, FP, PD]
         L.orc_gaussian.argtypes = [PD, PD, I32, I32, PD]
         L.orc_gaussian.restype = None
         L.orc_poisson.argtypes = [FP, FP, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32]
@@ -191,6 +192,16 @@ class Oracle:
         lib().orc_render(ctypes.byref(self.s), rgb.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), w, h, cp,
                          out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint16)), neg.ctypes.data_as(PD))
         return out, neg
+
+    def render_linear(self, rgb64, counts):
+        """The scanned linear RGB of a binary64 frame (the output the render's adjoint differentiates)."""
+        rgb64 = np.ascontiguousarray(rgb64, np.float64)
+        h, w, _ = rgb64.shape
+        counts = np.ascontiguousarray(counts, np.float32)
+        lin = np.zeros((h, w, 3), np.float64)
+        lib().orc_render_linear(ctypes.byref(self.s), rgb64.ctypes.data_as(PD), w, h,
+                                counts.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), lin.ctypes.data_as(PD))
+        return lin
 
     def print(self, negative, print_exposure=None):
         if print_exposure is not None:

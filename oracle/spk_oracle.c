@@ -154,10 +154,13 @@ static void mitchell_axis(double t, int L, int idx[4], double wt[4]) {
     wt[3] = mitchell(frac - 2.0);
 }
 
-static void expose(const OracleSetup* s, const float* rgb, double* H, size_t n) {
+/* rgb (binary32) or rgb64 (binary64, when rgb is NULL) */
+static void expose(const OracleSetup* s, const float* rgb, const double* rgb64, double* H, size_t n) {
 #pragma omp parallel for
     for (size_t p = 0; p < n; ++p) {
-        const double r = rgb[3 * p], g = rgb[3 * p + 1], b = rgb[3 * p + 2];
+        const double r = rgb ? rgb[3 * p] : rgb64[3 * p];
+        const double g = rgb ? rgb[3 * p + 1] : rgb64[3 * p + 1];
+        const double b = rgb ? rgb[3 * p + 2] : rgb64[3 * p + 2];
         const double* A = s->A;
         const double X = A[0] * r + A[1] * g + A[2] * b;
         const double Y = A[3] * r + A[4] * g + A[5] * b;
@@ -241,10 +244,11 @@ static double grain_value(const OracleSetup* s, double D, int c, uint32_t pixel,
     return G - s->dmin_c[c];
 }
 
-int orc_develop(const OracleSetup* s, const float* rgb, int32_t w, int32_t h, const float* counts, double* neg) {
+static int develop_impl(const OracleSetup* s, const float* rgb, const double* rgb64, int32_t w, int32_t h,
+                        const float* counts, double* neg) {
     const size_t n = (size_t)w * h, N = 3 * n;
     double* H = (double*)malloc(N * sizeof(double));
-    expose(s, rgb, H, n);
+    expose(s, rgb, rgb64, H, n);
     if (s->lens_blur_px > 0.0) {
         double* t = (double*)malloc(N * sizeof(double));
         const double sg[3] = {s->lens_blur_px, s->lens_blur_px, s->lens_blur_px};
@@ -274,6 +278,10 @@ int orc_develop(const OracleSetup* s, const float* rgb, int32_t w, int32_t h, co
     free(D);
     free(H);
     return 0;
+}
+
+int orc_develop(const OracleSetup* s, const float* rgb, int32_t w, int32_t h, const float* counts, double* neg) {
+    return develop_impl(s, rgb, NULL, w, h, counts, neg);
 }
 
 /* ---- print (reference kernels/print.metal:29-127, :165-317) -------------------------------------- */
@@ -522,4 +530,16 @@ uint32_t orc_splitmix_next(uint64_t* state) {
     z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
     z = z ^ (z >> 31);
     return (uint32_t)z;
+}
+
+int orc_render_linear(const OracleSetup* s, const double* rgb, int32_t w, int32_t h, const float* counts,
+                      double* out_linear) {
+    const size_t n = (size_t)w * h;
+    double* neg = (double*)malloc(3 * n * sizeof(double));
+    uint16_t* out = (uint16_t*)malloc(4 * n * sizeof(uint16_t));
+    develop_impl(s, NULL, rgb, w, h, counts, neg);
+    orc_print(s, neg, w, h, out, out_linear);
+    free(out);
+    free(neg);
+    return 0;
 }

@@ -73,6 +73,12 @@ int orc_develop(const OracleSetup* s, const float* rgb, int32_t w, int32_t h, co
 int orc_print(const OracleSetup* s, const double* negative, int32_t w, int32_t h, uint16_t* out_rgba,
               double* out_linear_rgb);
 
+/* The scanned linear RGB (print, scanner lens blur and unsharp mask, before the transfer function and
+ * the encode) of a binary64 frame, for the finite-difference checks of the render's adjoint; counts as
+ * for orc_render. Returns 0. */
+int orc_render_linear(const OracleSetup* s, const double* rgb, int32_t w, int32_t h, const float* counts,
+                      double* out_linear);
+
 /* The Gaussian of a w x h x 3 plane, per-channel sigma in pixels, in binary64 with the engine's
  * branch rule (FIR below 3, Young-van Vliet above) */
 void orc_gaussian(const double* in, double* out, int32_t w, int32_t h, const double sigma[3]);

@@ -106,6 +106,16 @@ __device__ void carry_scan(double* carry, int nt, int cstep, int seg, int last, 
     }
 }
 
+// The transpose's edge term: v[e] += ((B1 + B2 + B3) v[e] + (B2 + B3) v[e + step] + B3 v[e + 2 step]) / B,
+// with the samples that exist (a line shorter than three samples folds what it has)
+__device__ __forceinline__ void edge_fold(const Coef& k, float* base, int e, int step, int n, bool doit) {
+    if (!doit) return;
+    const double v0 = base[e];
+    const double v1 = n > 1 ? double(base[e + step]) : 0.0;
+    const double v2 = n > 2 ? double(base[e + 2 * step]) : 0.0;
+    base[e] = float(v0 + (((k.B1 + k.B2) + k.B3) * v0 + (k.B2 + k.B3) * v1 + k.B3 * v2) / k.B);
+}
+
 // One full forward + backward blur of `nlines` interleaved lines of length n held in shared memory
 // (line j, element i at buf[i * pitch + j]), nseg segments per line, threads = nlines * nseg. Thread t
 // handles line t / nseg, segment t % nseg when seg_major, else line t % nlines, segment t / nlines; the
@@ -127,10 +137,11 @@ __device__ void blur_lines(float* buf, int pitch, int nlines, int n, int nseg, c
     const int nt = nlines * nseg;
     double* cs = carry + t;
 
+    const bool adj = q.adjoint != 0;
     // ---- forward ----
     if (active && a < n) {
         double s1 = 0.0, s2 = 0.0, s3 = 0.0;
-        if (seg == 0) s1 = s2 = s3 = double(base[0]);
+        if (seg == 0 && !adj) s1 = s2 = s3 = double(base[0]);
         seg_forward(k, base, pitch, a, b, s1, s2, s3, false);
         cs[0] = s1;
         cs[nt] = s2;
@@ -143,7 +154,7 @@ __device__ void blur_lines(float* buf, int pitch, int nlines, int n, int nseg, c
     if (active && a < n) {
         double s1, s2, s3;
         if (seg == 0) {
-            s1 = s2 = s3 = double(base[0]);
+            s1 = s2 = s3 = adj ? 0.0 : double(base[0]);
         } else {
             const double* prev = cs - cstep;
             s1 = prev[0];
@@ -153,10 +164,16 @@ __device__ void blur_lines(float* buf, int pitch, int nlines, int n, int nseg, c
         seg_forward(k, base, pitch, a, b, s1, s2, s3, true);
     }
     __syncthreads();
+    if (adj) {
+        // the forward blur's anticausal pass starts from y[n..n+2] = u[n-1]: its transpose adds
+        // ((B1 + B2 + B3) l[n-1] + (B2 + B3) l[n-2] + B3 l[n-3]) / B to sample n-1
+        edge_fold(k, base, (n - 1) * pitch, -pitch, n, active && seg == 0);
+        __syncthreads();
+    }
     // ---- backward ----
     if (active && a < n) {
         double s1 = 0.0, s2 = 0.0, s3 = 0.0;
-        if (seg == last) s1 = s2 = s3 = double(base[(n - 1) * pitch]);
+        if (seg == last && !adj) s1 = s2 = s3 = double(base[(n - 1) * pitch]);
         seg_backward(k, base, pitch, a, b, s1, s2, s3, false);
         cs[0] = s1;
         cs[nt] = s2;
@@ -167,7 +184,7 @@ __device__ void blur_lines(float* buf, int pitch, int nlines, int n, int nseg, c
     if (active && a < n) {
         double s1, s2, s3;
         if (seg == last) {
-            s1 = s2 = s3 = double(base[(n - 1) * pitch]);
+            s1 = s2 = s3 = adj ? 0.0 : double(base[(n - 1) * pitch]);
         } else {
             const double* prev = cs + cstep;
             s1 = prev[0];
@@ -177,6 +194,11 @@ __device__ void blur_lines(float* buf, int pitch, int nlines, int n, int nseg, c
         seg_backward(k, base, pitch, a, b, s1, s2, s3, true);
     }
     __syncthreads();
+    if (adj) {
+        // the forward blur's causal pass starts from w[-1..-3] = x[0]: its transpose folds into sample 0
+        edge_fold(k, base, 0, pitch, n, active && seg == 0);
+        __syncthreads();
+    }
 }
 
 // 16-byte asynchronous copy global -> shared (both addresses 16-byte aligned), and the wait for all of

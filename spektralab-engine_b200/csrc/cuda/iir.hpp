@@ -23,7 +23,9 @@ struct IirChannel {
 
 struct IirLaunch {
     int32_t seg_len;
-    int32_t pad;
+    // 1: the transpose of the blur, for the adjoint of the render: both passes from a zero state, then a
+    // correction at the far edge of each pass for the replicated edge state of the forward blur
+    int32_t adjoint;
     IirChannel ch[3 * SPKB_MAX_COMPONENTS];  // [component * 3 + channel]
 };
 

@@ -1066,6 +1066,42 @@ SPK_API spk_status spkx_session_develop_debug(spk_session* session, const char* 
     });
 }
 
+SPK_API spk_status spk_render_vjp(spk_session* session, const char* tier, uint32_t film_seed, const float* grad_output,
+                                  float* grad_input, double* grad_params, uint32_t n_params, float* output) {
+    last_error::clear();
+    if (!session) return invalid("session is NULL");
+    if (grad_output && !grad_input) return invalid("grad_input is NULL while grad_output is given");
+    if (!grad_output && !output) return invalid("neither grad_output nor output is given");
+    if (n_params > 0 && !grad_params) return invalid("grad_params is NULL with n_params > 0");
+    return guarded([&] {
+        Session& s = *S(session);
+        std::lock_guard<std::mutex> lock(s.m);
+        auto t = parse_tier(tier);
+        if (!t) fail_invalid("unknown tier");
+        s.check_tier(*t);
+        DeviceGuard dg(s.engine->device);
+        RenderCtx ctx{s.pool, s.stream};
+        ctx.pitch_um = s.pitch_um();
+        const size_t bytes = s.source.pixels() * 3 * sizeof(float);
+        DevBuffer dy, dgy, dgx;
+        if (output) dy = s.pool.acquire(bytes);
+        if (grad_output) {
+            dgy = s.pool.acquire(bytes);
+            dgx = s.pool.acquire(bytes);
+            cuda_check(cudaMemcpyAsync(dgy.ptr(), grad_output, bytes, cudaMemcpyHostToDevice, s.stream), "copy");
+        }
+        render_vjp(ctx, s.pipe, s.live, s.source, film_seed, s.hal, output ? dy.as<float>() : nullptr,
+                   grad_output ? dgy.as<float>() : nullptr, grad_output ? dgx.as<float>() : nullptr,
+                   grad_output ? grad_params : nullptr, grad_output ? n_params : 0u);
+        if (output) cuda_check(cudaMemcpyAsync(output, dy.ptr(), bytes, cudaMemcpyDeviceToHost, s.stream), "copy");
+        if (grad_output)
+            cuda_check(cudaMemcpyAsync(grad_input, dgx.ptr(), bytes, cudaMemcpyDeviceToHost, s.stream), "copy");
+        cuda_check(cudaStreamSynchronize(s.stream), "render adjoint");
+        cuda_check(cudaGetLastError(), "render adjoint");
+        return SPK_OK;
+    });
+}
+
 SPK_API spk_status spkx_session_setup_json(spk_session* session, double pitch_um, char** out_json) {
     last_error::clear();
     if (!session) return invalid("session is NULL");

@@ -5,6 +5,7 @@
 
 #include "../cuda/iir.hpp"
 #include "../cuda/launch.hpp"
+#include "../cuda/vjp.hpp"
 #include "blur_plan.h"
 #include "status.hpp"
 
@@ -331,7 +332,7 @@ void fill_launch(dev::IirLaunch& q, const std::vector<MixtureComponent>& comps, 
 // raw := a raw + b M(raw) with the block-parallel recursive kernels, when every channel of every
 // component is on the recursive branch and the lines fit in shared memory; false otherwise.
 bool iir_mixture_mix(RenderCtx& ctx, const Plane& raw, const std::vector<MixtureComponent>& comps, const Vec3& a,
-                     const Vec3& b) {
+                     const Vec3& b, bool adjoint = false) {
     if (comps.empty() || comps.size() > SPKB_MAX_COMPONENTS) return false;
     for (const MixtureComponent& m : comps)
         for (int c = 0; c < 3; ++c)
@@ -346,6 +347,7 @@ bool iir_mixture_mix(RenderCtx& ctx, const Plane& raw, const std::vector<Mixture
     const int Lc = dev::iir_col_seg_len(raw.h);
     fill_launch(q.rows, comps, Lr);
     fill_launch(q.cols, comps, Lc);
+    q.rows.adjoint = q.cols.adjoint = adjoint ? 1 : 0;
     std::vector<Plane> tmp;
     float* tp[SPKB_MAX_COMPONENTS] = {};
     for (size_t c = 0; c < comps.size(); ++c) {
@@ -378,61 +380,67 @@ void check_supported(const ParamSet& p) {
     if (!geometry_identity) refuse("a crop, rotation, quarter turn or flip (geometry)");
 }
 
-Plane develop(RenderCtx& ctx, const Pipeline& p, const Plane& source, uint32_t film_seed,
-              const std::optional<HalationOverride>& hov, float* counts_out) {
-    const FilmSetup& f = *p.film;
-    const ParamSet& b = f.params;
-    const uint32_t w = source.w, h = source.h;
-    Plane H = make_plane(ctx.pool, w, h);
-    {
-        Stage st(ctx, "expose");
-        ExposeArgs a{};
-        for (int i = 0; i < 9; ++i) a.a[i] = f.input_matrix_f32[size_t(i)];
-        a.gain = f32(std::pow(2.0, b.f(P::exposure_compensation_ev)));
-        a.apply_gain = a.gain != 1.0f;
-        a.L = f.L;
-        a.n = uint32_t(source.pixels());
-        dev::expose(source.data(), H.data(), p.dev.table.as<float>(), a, ctx.stream);
-    }
-    if (b.f(P::lens_blur_um) > 0.0) {
-        Stage st(ctx, "lens_blur");
-        const double s = b.f(P::lens_blur_um) / ctx.pitch_um;
-        if (s > 0.0) {
-            Plane Hb = make_plane(ctx.pool, w, h);
-            gaussian(ctx, H, Hb, Vec3{s, s, s});
-            H = std::move(Hb);
+namespace {
+
+ExposeArgs expose_args(const FilmSetup& f, size_t pixels) {
+    ExposeArgs a{};
+    for (int i = 0; i < 9; ++i) a.a[i] = f.input_matrix_f32[size_t(i)];
+    a.gain = f32(std::pow(2.0, f.params.f(P::exposure_compensation_ev)));
+    a.apply_gain = a.gain != 1.0f;
+    a.L = f.L;
+    a.n = uint32_t(pixels);
+    return a;
+}
+
+// the camera lens blur of the film side in pixels (0: none)
+double film_lens_blur_px(const RenderCtx& ctx, const FilmSetup& f) {
+    const double um = f.params.f(P::lens_blur_um);
+    return um > 0.0 ? um / ctx.pitch_um : 0.0;
+}
+
+// the film's halation stages: the override's bounce mixture, or the film preset's plan at this pitch
+HalationPlan film_halation(const RenderCtx& ctx, const FilmSetup& f, const std::optional<HalationOverride>& hov) {
+    HalationPlan pl;
+    if (hov) {
+        pl.bounce = !hov->comps.empty();
+        pl.bounce_comps = hov->comps;
+        for (size_t c = 0; c < 3; ++c) {
+            const double A = hov->strength[c];
+            pl.mix_a[c] = 1.0 / (1.0 + A);
+            pl.mix_b[c] = A / (1.0 + A);
         }
+        return pl;
     }
-    {
-        HalationPlan pl;
-        if (hov) {
-            pl.bounce = !hov->comps.empty();
-            pl.bounce_comps = hov->comps;
-            for (size_t c = 0; c < 3; ++c) {
-                const double A = hov->strength[c];
-                pl.mix_a[c] = 1.0 / (1.0 + A);
-                pl.mix_b[c] = A / (1.0 + A);
-            }
-        } else {
-            if (f.halation.back_reflection && f.halation.active && f.halation.headroom_ev > 0.0 && f.halation.amount > 0.0)
-                fail_user("the back-reflection halation preset (highlight headroom) is outside this B200 build's render path");
-            pl = halation_plan(f.halation, ctx.pitch_um);
-        }
-        if (pl.scatter || pl.bounce) {
-            Stage st(ctx, "halation");
-            if (pl.scatter && !iir_mixture_mix(ctx, H, pl.scatter_comps, pl.scatter_a, pl.scatter_b)) {
-                Plane m = make_plane(ctx.pool, w, h);
-                gaussian_mixture(ctx, H, m, pl.scatter_comps);
-                lincomb(ctx, pl.scatter_a, H, pl.scatter_b, &m, H);
-            }
-            if (pl.bounce && !iir_mixture_mix(ctx, H, pl.bounce_comps, pl.mix_a, pl.mix_b)) {
-                Plane Hh = make_plane(ctx.pool, w, h);
-                gaussian_mixture(ctx, H, Hh, pl.bounce_comps);
-                lincomb(ctx, pl.mix_a, H, pl.mix_b, &Hh, H);
-            }
-        }
+    if (f.halation.back_reflection && f.halation.active && f.halation.headroom_ev > 0.0 && f.halation.amount > 0.0)
+        fail_user("the back-reflection halation preset (highlight headroom) is outside this B200 build's render path");
+    return halation_plan(f.halation, ctx.pitch_um);
+}
+
+// raw := a raw + b M(raw) for the scatter, then the bounce mixture
+void apply_halation(RenderCtx& ctx, const HalationPlan& pl, Plane& H) {
+    if (pl.scatter && !iir_mixture_mix(ctx, H, pl.scatter_comps, pl.scatter_a, pl.scatter_b)) {
+        Plane m = make_plane(ctx.pool, H.w, H.h);
+        gaussian_mixture(ctx, H, m, pl.scatter_comps);
+        lincomb(ctx, pl.scatter_a, H, pl.scatter_b, &m, H);
     }
+    if (pl.bounce && !iir_mixture_mix(ctx, H, pl.bounce_comps, pl.mix_a, pl.mix_b)) {
+        Plane Hh = make_plane(ctx.pool, H.w, H.h);
+        gaussian_mixture(ctx, H, Hh, pl.bounce_comps);
+        lincomb(ctx, pl.mix_a, H, pl.mix_b, &Hh, H);
+    }
+}
+
+struct DevelopPlan {
     DevelopArgs da{};
+    bool grain = false;
+    double final_blur = 0.0, amount = 1.0;
+};
+
+// the develop kernel's arguments for a frame of width w and the grain's final blur and strength
+DevelopPlan develop_plan(const RenderCtx& ctx, const Pipeline& p, uint32_t w, uint32_t film_seed, float* counts_out) {
+    const FilmSetup& f = *p.film;
+    DevelopPlan dp;
+    DevelopArgs& da = dp.da;
     da.cx = p.dev.curves.as<float>();
     da.cinv = da.cx + f.K;
     da.cy = da.cx + 2 * size_t(f.K);
@@ -440,17 +448,14 @@ Plane develop(RenderCtx& ctx, const Pipeline& p, const Plane& source, uint32_t f
     da.cgrid = axis_grid(f.cx.data(), f.K, 1);
     da.width = w;
     da.counts_out = counts_out;
-    Plane neg = make_plane(ctx.pool, w, h);
     const GrainSetup* g = f.grain.get();
-    const bool grain = g && g->active && g->amount > 0.0;
-    if (!grain) {
-        Stage st(ctx, "develop");
-        dev::develop(H.data(), neg.data(), da, w, h, ctx.stream);
-        return neg;
-    }
+    dp.grain = g && g->active && g->amount > 0.0;
+    if (!dp.grain) return dp;
     const GrainConstants kc = grain_constants(*g, ctx.pitch_um);
     if (kc.sublayers && (kc.dye || kc.micro))
         fail_user("grain dye clouds or micro-structure (pixel pitch below about 2 um) are outside this B200 build's render path");
+    dp.final_blur = kc.final_blur;
+    dp.amount = g->amount;
     da.grain = 1;
     da.seed = film_seed;
     da.positive = g->positive ? 1u : 0u;
@@ -477,15 +482,50 @@ Plane develop(RenderCtx& ctx, const Pipeline& p, const Plane& source, uint32_t f
     } else {
         da.mode = 2;  // SIMPLE
     }
+    return dp;
+}
+
+}  // namespace
+
+Plane develop(RenderCtx& ctx, const Pipeline& p, const Plane& source, uint32_t film_seed,
+              const std::optional<HalationOverride>& hov, float* counts_out) {
+    const FilmSetup& f = *p.film;
+    const uint32_t w = source.w, h = source.h;
+    Plane H = make_plane(ctx.pool, w, h);
+    {
+        Stage st(ctx, "expose");
+        dev::expose(source.data(), H.data(), p.dev.table.as<float>(), expose_args(f, source.pixels()), ctx.stream);
+    }
+    if (const double s = film_lens_blur_px(ctx, f); s > 0.0) {
+        Stage st(ctx, "lens_blur");
+        Plane Hb = make_plane(ctx.pool, w, h);
+        gaussian(ctx, H, Hb, Vec3{s, s, s});
+        H = std::move(Hb);
+    }
+    {
+        const HalationPlan pl = film_halation(ctx, f, hov);
+        if (pl.scatter || pl.bounce) {
+            Stage st(ctx, "halation");
+            apply_halation(ctx, pl, H);
+        }
+    }
+    const DevelopPlan dp = develop_plan(ctx, p, w, film_seed, counts_out);
+    const DevelopArgs& da = dp.da;
+    Plane neg = make_plane(ctx.pool, w, h);
+    if (!dp.grain) {
+        Stage st(ctx, "develop");
+        dev::develop(H.data(), neg.data(), da, w, h, ctx.stream);
+        return neg;
+    }
     Plane G = make_plane(ctx.pool, w, h);
     {
         Stage st(ctx, "develop");
         dev::develop(H.data(), G.data(), da, w, h, ctx.stream);
     }
-    if (kc.final_blur > 0.0) {
+    if (dp.final_blur > 0.0) {
         Stage st(ctx, "grain_blur");
-        const double s = kc.final_blur;
-        if (g->amount == 1.0) {  // the blurred grain is the negative
+        const double s = dp.final_blur;
+        if (dp.amount == 1.0) {  // the blurred grain is the negative
             gaussian(ctx, G, neg, Vec3{s, s, s});
             return neg;
         }
@@ -495,13 +535,13 @@ Plane develop(RenderCtx& ctx, const Pipeline& p, const Plane& source, uint32_t f
     }
     {
         Stage st(ctx, "grain_mix");
-        if (g->amount == 1.0) {
+        if (dp.amount == 1.0) {
             dev::copy(G.data(), neg.data(), G.pixels(), ctx.stream);
         } else {
             DevelopArgs dd = da;
             dd.grain = 0;
             dev::develop(H.data(), neg.data(), dd, w, h, ctx.stream);
-            const double k = g->amount;
+            const double k = dp.amount;
             lincomb(ctx, Vec3{1.0 - k, 1.0 - k, 1.0 - k}, neg, Vec3{k, k, k}, &G, neg);
         }
     }
@@ -587,6 +627,247 @@ void print_scan_encode(RenderCtx& ctx, const Pipeline& p, const LiveParams& live
         Stage st(ctx, "encode");
         dev::encode(rgb.data(), gpl ? gpl.data() : nullptr, img->dev, w, h, e, ctx.stream);
     }
+}
+
+
+// ---- the adjoint of the render ------------------------------------------------------------------------
+
+namespace {
+
+// g := G^T g for the Gaussian of one sigma on every channel: the transposed FIR passes, or the
+// block-parallel recursive kernels in transpose mode
+void gaussian_adjoint(RenderCtx& ctx, Plane& g, double sigma) {
+    const Branch br = blur_branch(sigma);
+    if (br == Branch::Identity) return;
+    if (br == Branch::Fir) {
+        const bool no_iir[3] = {false, false, false};
+        const FirTaps t = fir_taps(Vec3{sigma, sigma, sigma}, no_iir);
+        if (t.r == 0) return;
+        Plane tmp = make_plane(ctx.pool, g.w, g.h);
+        dev::fir_pass_adjoint(g.data(), tmp.data(), g.w, g.h, t.r, t.taps[0], 0, ctx.stream);
+        dev::fir_pass_adjoint(tmp.data(), g.data(), g.w, g.h, t.r, t.taps[0], 1, ctx.stream);
+        return;
+    }
+    const std::vector<MixtureComponent> one{MixtureComponent{Vec3{1.0, 1.0, 1.0}, Vec3{sigma, sigma, sigma}}};
+    if (!iir_mixture_mix(ctx, g, one, Vec3{0.0, 0.0, 0.0}, Vec3{1.0, 1.0, 1.0}, true))
+        fail_unsupported("the transposed recursive blur needs the frame's lines in shared memory");
+}
+
+double common_sigma(const MixtureComponent& m) {
+    if (!(m.sigma[0] == m.sigma[1] && m.sigma[1] == m.sigma[2]))
+        fail_unsupported("the render's adjoint takes halation components with one sigma for the three channels");
+    return m.sigma[0];
+}
+
+// g := a g + b sum_k w_k G_k^T g, the transpose of the mixture stage raw := a raw + b sum_k w_k G_k(raw)
+void mixture_adjoint(RenderCtx& ctx, Plane& g, const std::vector<MixtureComponent>& comps, const Vec3& a,
+                     const Vec3& b) {
+    if (iir_mixture_mix(ctx, g, comps, a, b, true)) return;
+    Plane acc = make_plane(ctx.pool, g.w, g.h);
+    Plane t = make_plane(ctx.pool, g.w, g.h);
+    for (size_t k = 0; k < comps.size(); ++k) {
+        dev::copy(g.data(), t.data(), g.pixels(), ctx.stream);
+        gaussian_adjoint(ctx, t, common_sigma(comps[k]));
+        if (k == 0) lincomb(ctx, comps[k].weight, t, Vec3{0.0, 0.0, 0.0}, nullptr, acc);
+        else lincomb(ctx, Vec3{1.0, 1.0, 1.0}, acc, comps[k].weight, &t, acc);
+    }
+    lincomb(ctx, a, g, b, &acc, g);
+}
+
+// The print stage in the adjoint's form, with the tangents of its per-print constants along
+// print_exposure (k = print_exposure exactly) and the two filter shifts (binary64 central differences
+// of the set-up, step 1e-4).
+dev::VjpPrintArgs vjp_print_args(const Pipeline& p, const LiveParams& live, uint32_t n) {
+    const PrintSetup& s = *p.print;
+    const PrintRun r = compute_run(s, live);
+    dev::VjpPrintArgs a{};
+    std::memcpy(a.enl_eps, r.enl32.eps, sizeof a.enl_eps);
+    std::memcpy(a.enl_beta, r.enl32.beta, sizeof a.enl_beta);
+    std::memcpy(a.enl_wt, r.enl32.wt, sizeof a.enl_wt);
+    std::memcpy(a.scan_eps, s.scan32.eps, sizeof a.scan_eps);
+    std::memcpy(a.scan_beta, s.scan32.beta, sizeof a.scan_beta);
+    std::memcpy(a.scan_wt, s.scan32.wt, sizeof a.scan_wt);
+    for (int c = 0; c < 3; ++c) {
+        a.g[c] = f32(r.g[c]);
+        a.o[c] = f32(r.o[c]);
+    }
+    a.k_gain = r.k_gain;
+    a.t_k[0] = 1.0f;
+    constexpr double h = 1e-4;
+    for (int j = 1; j < dev::kVjpPrintParams; ++j) {
+        LiveParams lp = live, lm = live;
+        double& vp = j == 1 ? lp.m_filter_shift : lp.y_filter_shift;
+        double& vm = j == 1 ? lm.m_filter_shift : lm.y_filter_shift;
+        vp += h;
+        vm -= h;
+        const PrintRun rp = compute_run(s, lp), rm = compute_run(s, lm);
+        for (int i = 0; i < 3 * SPKB_NL; ++i) {
+            a.t_eps[j][i] = f32((rp.eps_n[size_t(i)] - rm.eps_n[size_t(i)]) / (2.0 * h));
+            a.t_wt[j][i] = f32((rp.w_n[size_t(i)] - rm.w_n[size_t(i)]) / (2.0 * h));
+        }
+        for (int l = 0; l < SPKB_NL; ++l) a.t_beta[j][l] = f32((rp.beta_n[size_t(l)] - rm.beta_n[size_t(l)]) / (2.0 * h));
+        for (int c = 0; c < 3; ++c) {
+            a.t_g[j][c] = f32((rp.g[c] - rm.g[c]) / (2.0 * h));
+            a.t_o[j][c] = f32((rp.o[c] - rm.o[c]) / (2.0 * h));
+        }
+    }
+    a.printed = s.scanned ? 0 : 1;
+    a.paper = p.dev.paper.as<float>();
+    a.paper_K = s.paper_K;
+    if (!s.paper_tab.empty()) a.paper_grid = axis_grid(s.paper_tab.data(), s.paper_K, 1);
+    std::memcpy(a.to_rgb, s.to_rgb, sizeof a.to_rgb);
+    a.cam = s.cam_args;
+    a.cmax = p.dev.cmax.as<float>();
+    a.n = n;
+    return a;
+}
+
+}  // namespace
+
+void render_vjp(RenderCtx& ctx, const Pipeline& p, const LiveParams& live, const Plane& source, uint32_t film_seed,
+                const std::optional<HalationOverride>& hov, float* y_out, const float* g_y, float* g_x,
+                double* grad_params, uint32_t n_params) {
+    const FilmSetup& f = *p.film;
+    const PrintSetup& ps = *p.print;
+    const uint32_t w = source.w, h = source.h;
+    const size_t n = source.pixels();
+    // ---- forward, keeping what the adjoint needs ----
+    Plane H0 = make_plane(ctx.pool, w, h);
+    const ExposeArgs ea = expose_args(f, n);
+    dev::expose(source.data(), H0.data(), p.dev.table.as<float>(), ea, ctx.stream);
+    const double s_lens = film_lens_blur_px(ctx, f);
+    Plane H1 = H0;
+    if (s_lens > 0.0) {
+        H1 = make_plane(ctx.pool, w, h);
+        gaussian(ctx, H0, H1, Vec3{s_lens, s_lens, s_lens});
+    }
+    const HalationPlan pl = film_halation(ctx, f, hov);
+    Plane H2 = H1;  // after the scatter stage
+    if (pl.scatter) {
+        H2 = make_plane(ctx.pool, w, h);
+        dev::copy(H1.data(), H2.data(), n, ctx.stream);
+        HalationPlan only = pl;
+        only.bounce = false;
+        apply_halation(ctx, only, H2);
+    }
+    Plane H3 = H2;  // after the bounce stage: the exposure the develop stage reads
+    if (pl.bounce) {
+        H3 = make_plane(ctx.pool, w, h);
+        dev::copy(H2.data(), H3.data(), n, ctx.stream);
+        HalationPlan only = pl;
+        only.scatter = false;
+        apply_halation(ctx, only, H3);
+    }
+    DevBuffer counts = ctx.pool.acquire(n * 9 * sizeof(float));
+    const DevelopPlan dp = develop_plan(ctx, p, w, film_seed, counts.as<float>());
+    if (dp.grain && (dp.da.mode != 0 || dp.amount != 1.0))
+        fail_unsupported("the render's adjoint takes sub-layer grain at full strength (or no grain)");
+    Plane G = make_plane(ctx.pool, w, h);
+    dev::develop(H3.data(), G.data(), dp.da, w, h, ctx.stream);
+    Plane neg = G;
+    if (dp.grain && dp.final_blur > 0.0) {
+        neg = make_plane(ctx.pool, w, h);
+        gaussian(ctx, G, neg, Vec3{dp.final_blur, dp.final_blur, dp.final_blur});
+    }
+    const dev::VjpPrintArgs va = vjp_print_args(p, live, uint32_t(n));
+    PrintArgs pa{};
+    {
+        const PrintRun r = compute_run(ps, live);
+        pa.enl = spectral_pairs(r.enl32);
+        pa.scan = spectral_pairs(ps.scan32);
+        for (int c = 0; c < 3; ++c) {
+            pa.g[c] = f32(r.g[c]);
+            pa.o[c] = f32(r.o[c]);
+        }
+        pa.k_gain = r.k_gain;
+        pa.printed = va.printed;
+        pa.paper = va.paper;
+        pa.paper_K = va.paper_K;
+        pa.paper_grid = va.paper_grid;
+        std::memcpy(pa.to_rgb, ps.to_rgb, sizeof pa.to_rgb);
+        pa.cam = ps.cam_args;
+        pa.cmax = va.cmax;
+        pa.n = uint32_t(n);
+    }
+    Plane P = make_plane(ctx.pool, w, h);
+    dev::print(neg.data(), P.data(), pa, ctx.stream);
+    const double sb = ps.scanner_lens_blur_px, su = ps.unsharp_sigma_full * ctx.rho_tier, am = ps.unsharp_amount;
+    const bool unsharp = su > 0.0 && am > 0.0;
+    Plane B = P;
+    if (sb > 0.0) {
+        B = make_plane(ctx.pool, w, h);
+        gaussian(ctx, P, B, Vec3{sb, sb, sb});
+    }
+    Plane Y = B;
+    if (unsharp) {
+        Plane Gs = make_plane(ctx.pool, w, h);
+        gaussian(ctx, B, Gs, Vec3{su, su, su});
+        Y = make_plane(ctx.pool, w, h);
+        lincomb(ctx, Vec3{1.0 + am, 1.0 + am, 1.0 + am}, B, Vec3{-am, -am, -am}, &Gs, Y);
+    }
+    if (y_out) cuda_check(cudaMemcpyAsync(y_out, Y.data(), Y.bytes(), cudaMemcpyDeviceToDevice, ctx.stream), "copy");
+    if (!g_y) return;
+
+    // ---- adjoint ----
+    const uint32_t ncomp = hov ? uint32_t(hov->comps.size()) : 0u;
+    const uint32_t n_all = dev::kVjpPrintParams + 2 * ncomp;
+    DevBuffer dparams = ctx.pool.acquire(sizeof(double) * (dev::kVjpPrintParams + 3 * 3 * 2 * SPKB_MAX_COMPONENTS));
+    cuda_check(cudaMemsetAsync(dparams.ptr(), 0, sizeof(double) * (dev::kVjpPrintParams + 3 * 3 * 2 * SPKB_MAX_COMPONENTS),
+                               ctx.stream),
+               "memset");
+    double* d_print = dparams.as<double>();
+    double* d_dots = d_print + dev::kVjpPrintParams;  // [k][weight 3 | sigma 3]
+    Plane g = make_plane(ctx.pool, w, h);
+    cuda_check(cudaMemcpyAsync(g.data(), g_y, g.bytes(), cudaMemcpyDeviceToDevice, ctx.stream), "copy");
+    if (unsharp) {  // g_B = (1 + a) g_Y - a Gs^T g_Y
+        Plane t = make_plane(ctx.pool, w, h);
+        dev::copy(g.data(), t.data(), n, ctx.stream);
+        gaussian_adjoint(ctx, t, su);
+        lincomb(ctx, Vec3{1.0 + am, 1.0 + am, 1.0 + am}, g, Vec3{-am, -am, -am}, &t, g);
+    }
+    if (sb > 0.0) gaussian_adjoint(ctx, g, sb);  // g_P
+    Plane gn = make_plane(ctx.pool, w, h);
+    dev::vjp_print(neg.data(), g.data(), gn.data(), d_print, va, ctx.stream);
+    if (dp.grain && dp.final_blur > 0.0) gaussian_adjoint(ctx, gn, dp.final_blur);  // g_G
+    dev::vjp_develop(H3.data(), counts.as<float>(), gn.data(), g.data(), dp.da, w, h, ctx.stream);  // g_H3
+    if (pl.bounce) {
+        if (hov) {  // the override's weights and sigmas, from the exposure entering the bounce stage (H2)
+            Plane Gk = make_plane(ctx.pool, w, h), Gp = make_plane(ctx.pool, w, h);
+            for (uint32_t k = 0; k < ncomp; ++k) {
+                const double sg = common_sigma(hov->comps[k]);
+                gaussian(ctx, H2, Gk, Vec3{sg, sg, sg});
+                dev::dot3(g.data(), Gk.data(), n, d_dots + 6 * k, ctx.stream);
+                constexpr double eps = 2e-3;
+                const double sp = sg * (1.0 + eps), sm = sg * (1.0 - eps);
+                gaussian(ctx, H2, Gk, Vec3{sp, sp, sp});
+                gaussian(ctx, H2, Gp, Vec3{sm, sm, sm});
+                const double inv = 1.0 / (sp - sm);
+                lincomb(ctx, Vec3{inv, inv, inv}, Gk, Vec3{-inv, -inv, -inv}, &Gp, Gk);
+                dev::dot3(g.data(), Gk.data(), n, d_dots + 6 * k + 3, ctx.stream);
+            }
+        }
+        mixture_adjoint(ctx, g, pl.bounce_comps, pl.mix_a, pl.mix_b);  // g_H2
+    }
+    if (pl.scatter) mixture_adjoint(ctx, g, pl.scatter_comps, pl.scatter_a, pl.scatter_b);  // g_H1
+    if (s_lens > 0.0) gaussian_adjoint(ctx, g, s_lens);  // g_H0
+    dev::vjp_expose(source.data(), g.data(), g_x, p.dev.table.as<float>(), ea, ctx.stream);
+    double hp[dev::kVjpPrintParams + 6 * SPKB_MAX_COMPONENTS];
+    cuda_check(cudaMemcpyAsync(hp, dparams.ptr(), sizeof hp, cudaMemcpyDeviceToHost, ctx.stream), "copy");
+    cuda_check(cudaStreamSynchronize(ctx.stream), "render adjoint");
+    if (!grad_params) return;
+    std::vector<double> all(n_all, 0.0);
+    for (int j = 0; j < dev::kVjpPrintParams; ++j) all[size_t(j)] = hp[j];
+    for (uint32_t k = 0; k < ncomp; ++k) {
+        const double* dk = hp + dev::kVjpPrintParams + 6 * k;
+        double gw = 0.0, gs = 0.0;
+        for (int c = 0; c < 3; ++c) {
+            gw += pl.mix_b[c] * dk[c];
+            gs += pl.mix_b[c] * hov->comps[k].weight[c] * dk[3 + c];
+        }
+        all[dev::kVjpPrintParams + k] = gw;
+        all[dev::kVjpPrintParams + ncomp + k] = gs;
+    }
+    for (uint32_t j = 0; j < n_params; ++j) grad_params[j] = j < n_all ? all[j] : 0.0;
 }
 
 }  // namespace spkb

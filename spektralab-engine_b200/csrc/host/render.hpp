@@ -68,6 +68,20 @@ Plane develop(RenderCtx& ctx, const Pipeline& p, const Plane& source, uint32_t f
 void print_scan_encode(RenderCtx& ctx, const Pipeline& p, const LiveParams& live, const Plane& negative,
                        OutputImage* img);
 
+// The adjoint of the render. The differentiated output y is the scanned linear RGB (print, scanner lens
+// blur and unsharp mask; before the output transfer function and the 16-bit encode) of the source frame,
+// developed with the grain counts of film_seed held fixed. Device pointers, 3 floats per pixel:
+//   y_out (may be null)  receives y;
+//   g_y (null: y only)   the gradient of a loss with respect to y;
+//   g_x                  receives the gradient with respect to the source frame.
+// grad_params (host, n_params entries, may be null) receives the gradient with respect to
+//   [print_exposure, m_filter_shift, y_filter_shift, halation weight 0..K-1, halation sigma 0..K-1],
+// K the components of the halation override (none without one). A weight's or sigma's gradient is along
+// a common change of its three channels.
+void render_vjp(RenderCtx& ctx, const Pipeline& p, const LiveParams& live, const Plane& source, uint32_t film_seed,
+                const std::optional<HalationOverride>& hov, float* y_out, const float* g_y, float* g_x,
+                double* grad_params, uint32_t n_params);
+
 // The blur machinery on device planes (exposed for the tests' stage entry points).
 void gaussian(RenderCtx& ctx, const Plane& in, const Plane& dst, const Vec3& sigma);
 void gaussian_mixture(RenderCtx& ctx, const Plane& in, const Plane& out, const std::vector<MixtureComponent>& comps);

@@ -25,6 +25,7 @@ private:
 [[noreturn]] inline void fail_io(const std::string& msg) { fail(SPK_ERR_IO, msg); }
 [[noreturn]] inline void fail_internal(const std::string& msg) { fail(SPK_ERR_INTERNAL, msg); }
 [[noreturn]] inline void fail_invalid(const std::string& msg) { fail(SPK_ERR_INVALID_ARG, msg); }
+[[noreturn]] inline void fail_unsupported(const std::string& msg) { fail(SPK_ERR_UNSUPPORTED, msg); }
 [[noreturn]] inline void fail_cancelled() { fail(SPK_ERR_CANCELLED, "render cancelled"); }
 
 namespace last_error {

@@ -100,6 +100,7 @@ EXT = {
     "spkx_gaussian": (I32, [FP, FP, U32, U32, DP]),
     "spkx_setup_json": (I32, [C, C, ctypes.c_double, PS]),
     "spkx_session_develop_debug": (I32, [P, C, U32, FP, FP]),
+    "spk_render_vjp": (I32, [P, C, U32, FP, FP, DP, U32, FP]),
 }
 
 REF_EXT = {
@@ -187,7 +188,7 @@ class Engine:
         s = self.L.lib.spk_open(self.h, ctypes.byref(si), d, ctypes.byref(out))
         if not s:
             raise SpkError(-2, self.L.last_error())
-        return Session(self, s, self.L.take_json(out))
+        return Session(self, s, self.L.take_json(out), (h, w))
 
 
 class Result:
@@ -214,11 +215,12 @@ class Result:
 
 
 class Session:
-    def __init__(self, engine, handle, reply):
+    def __init__(self, engine, handle, reply, shape=None):
         self.E = engine
         self.L = engine.L
         self.h = handle
         self.reply = reply
+        self.shape = shape  # (height, width) of the source frame
 
     def close(self):
         if self.h:
@@ -253,6 +255,27 @@ class Session:
 
     def reprint(self, tier="full"):
         return self._render(self.L.lib.spk_reprint, tier)
+
+    def render_linear(self, film_seed, tier="full"):
+        """The scanned linear RGB (the output spk_render_vjp differentiates), (h, w, 3) float32, with the
+        grain counts of film_seed."""
+        h, w = self.shape
+        y = np.empty((h, w, 3), np.float32)
+        self.L.check(self.L.lib.spk_render_vjp(self.h, tier.encode(), film_seed, None, None, None, 0,
+                                                y.ctypes.data_as(FP)))
+        return y
+
+    def render_vjp(self, grad_output, film_seed, n_params=0, tier="full", want_output=False):
+        """spk_render_vjp: (grad_input (h, w, 3) float32, grad_params float64[n_params][, output])."""
+        h, w = self.shape
+        gy = np.ascontiguousarray(grad_output, np.float32)
+        gx = np.empty((h, w, 3), np.float32)
+        gp = np.zeros(max(n_params, 1), np.float64)
+        y = np.empty((h, w, 3), np.float32) if want_output else None
+        self.L.check(self.L.lib.spk_render_vjp(self.h, tier.encode(), film_seed, gy.ctypes.data_as(FP),
+                                                gx.ctypes.data_as(FP), gp.ctypes.data_as(DP), n_params,
+                                                y.ctypes.data_as(FP) if want_output else None))
+        return (gx, gp[:n_params], y) if want_output else (gx, gp[:n_params])
 
     def render_result(self, tier="full", reprint=False):
         """spk_render / spk_reprint without a copy: a Result that owns the spk_result (its pinned host

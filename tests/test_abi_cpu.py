@@ -26,7 +26,8 @@ def test_headers_declare_the_reference_entry_points():
     names = set(declared())
     for n in sc.ABI:
         assert n in names, n
-    assert len([n for n in names if n.startswith("spk_")]) == 26
+    # the reference's 26, plus the render's adjoint (spk_render_vjp) in the extension header
+    assert {n for n in names if n.startswith("spk_")} == set(sc.ABI) | {"spk_render_vjp"}
 
 
 def test_library_exports_every_declared_symbol(lib):

@@ -1,0 +1,105 @@
+"""The render's adjoint, spk_render_vjp (gpu), against binary64 central differences of the oracle.
+
+The differentiated output is the scanned linear RGB with the grain held as fixed noise: the device's
+Poisson counts for the film seed (spkx_session_develop_debug) are fed to the float64 oracle
+(orc_render_linear), whose loss is differenced along a direction of the frame and along each parameter
+[print_exposure, m_filter_shift, y_filter_shift, halation weights, halation sigmas]. The loss is the L2
+distance to a target rendered with perturbed parameters.
+"""
+
+import numpy as np
+import pytest
+
+from conftest import BASE, sc, setup_f64
+
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+SEED = 7
+W, H = 96, 72
+STRENGTH = (0.03, 0.03, 0.03)
+PARAMS = np.array([1.0, 0.05, -0.04, 0.02, 0.02, 8.0, 40.0])  # pe, m, y, w0, w1, s0, s1
+DELTA = dict(BASE, grain_active=True, scanner_lens_blur=1.5)
+PITCH = 35000.0 / max(W, H)
+TOL = 2e-3  # relative, gradient against the central difference
+
+
+def halation(p):
+    return ([((p[3],) * 3, (p[5],) * 3), ((p[4],) * 3, (p[6],) * 3)], STRENGTH)
+
+
+def delta_of(p):
+    return dict(DELTA, print_exposure=float(p[0]), m_filter_shift=float(p[1]), y_filter_shift=float(p[2]))
+
+
+def oracle_linear(lib, resources, img64, counts, p):
+    f64 = setup_f64(lib, resources, delta_of(p), PITCH)["f64"]
+    o = oracle.Oracle(f64, seed=SEED, halation=halation(p), print_exposure=float(p[0]))
+    return o.render_linear(img64, counts)
+
+
+@pytest.fixture(scope="module")
+def case(engine, lib, resources):
+    img = sc.synthetic_image(W, H, 3)
+    with engine.open(img, delta_of(PARAMS)) as s:
+        s.set_halation(*halation(PARAMS))
+        _, counts = s.develop_debug("full", SEED, W, H)
+        y = s.render_linear(SEED)
+        # the target: the same frame with perturbed parameters
+        q = PARAMS * np.array([1.1, 1.0, 1.0, 1.25, 0.8, 1.1, 0.9]) + np.array([0, 0.02, 0.03, 0, 0, 0, 0])
+    with engine.open(img, delta_of(q)) as s2:
+        s2.set_halation(*halation(q))
+        target = s2.render_linear(SEED).astype(np.float64)
+    with engine.open(img, delta_of(PARAMS)) as s:
+        s.set_halation(*halation(PARAMS))
+        gy = (y.astype(np.float64) - target).astype(np.float32)
+        gx, gp = s.render_vjp(gy, SEED, len(PARAMS))
+    return dict(img=img, counts=counts, y=y, target=target, gx=gx, gp=gp)
+
+
+def loss(lib, resources, case, img64, p):
+    y = oracle_linear(lib, resources, img64, case["counts"], p)
+    return 0.5 * float(np.sum((y - case["target"]) ** 2))
+
+
+def test_forward_matches_oracle(lib, resources, case):
+    y64 = oracle_linear(lib, resources, case["img"].astype(np.float64), case["counts"], PARAMS)
+    err = np.abs(case["y"] - y64) / np.maximum(np.abs(y64), 1e-3)
+    assert err.max() < 1e-3, err.max()
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2])
+def test_image_gradient(lib, resources, case, seed):
+    rng = np.random.default_rng(seed)
+    x = case["img"].astype(np.float64)
+    v = rng.standard_normal(x.shape) * x
+    eps = 1e-6
+    fd = (loss(lib, resources, case, x + eps * v, PARAMS) - loss(lib, resources, case, x - eps * v, PARAMS)) / (2 * eps)
+    got = float(np.sum(case["gx"].astype(np.float64) * v))
+    assert abs(got - fd) <= TOL * abs(fd), (got, fd)
+
+
+@pytest.mark.parametrize("j,step", [(0, 1e-4), (1, 1e-4), (2, 1e-4), (3, 1e-5), (4, 1e-5), (5, 1e-3), (6, 1e-2)])
+def test_parameter_gradient(lib, resources, case, j, step):
+    x = case["img"].astype(np.float64)
+    pp, pm = PARAMS.copy(), PARAMS.copy()
+    pp[j] += step
+    pm[j] -= step
+    fd = (loss(lib, resources, case, x, pp) - loss(lib, resources, case, x, pm)) / (2 * step)
+    got = float(case["gp"][j])
+    assert abs(got - fd) <= TOL * abs(fd) + 1e-9, (j, got, fd)
+
+
+def test_autograd_function(engine, case):
+    import torch
+
+    import spk_torch
+
+    img = torch.from_numpy(case["img"].copy()).requires_grad_(True)
+    params = torch.tensor(PARAMS, dtype=torch.float64, requires_grad=True)
+    y = spk_torch.render_linear(img, params, engine, DELTA, STRENGTH, SEED)
+    loss_t = 0.5 * ((y.double() - torch.from_numpy(case["target"])) ** 2).sum()
+    loss_t.backward()
+    np.testing.assert_allclose(img.grad.numpy(), case["gx"], rtol=1e-5, atol=1e-7)
+    np.testing.assert_allclose(params.grad.numpy(), case["gp"], rtol=1e-5, atol=1e-9)
