@@ -261,6 +261,164 @@ def run_e2e(args, eng, img, delta, pg, local, world):
     return e2e
 
 
+VJP_SIZE = 1024
+VJP_SEED = 7
+VJP_HALATION = ([((0.02, 0.02, 0.02), (8, 8, 8)), ((0.02, 0.02, 0.02), (40, 40, 40))], (0.03, 0.03, 0.03))
+VJP_PARAMS = 7  # print_exposure, m_filter_shift, y_filter_shift, 2 halation weights, 2 halation sigmas
+
+
+def run_vjp(args):
+    """The render's adjoint (spk_render_vjp) on a 1024 x 1024 frame: the scanned linear RGB with the grain
+    held fixed (film seed 7), the gradient of an L2 loss against a target rendered with perturbed
+    parameters, with respect to the frame and 7 parameters. Wall time per call through the C ABI (host
+    arrays in and out); the forward-only call (output alone) beside it."""
+    resources = synth_resources.ensure(sc.RESOURCES)
+    lib = sc.load()
+    n = VJP_SIZE
+    ff = film_format_for_grains(lib, resources, n)
+    delta = dict(BASE, film_format_mm=ff)
+    eng = lib.engine(resources, device=0)
+    img = sc.synthetic_image(n, n, VJP_SEED)
+    with eng.open(img, dict(delta, print_exposure=1.1)) as t:
+        t.set_halation([((0.025,) * 3, (8, 8, 8)), ((0.015,) * 3, (44, 44, 44))], VJP_HALATION[1])
+        target = t.render_linear(VJP_SEED)
+    with eng.open(img, delta) as s:
+        s.set_halation(*VJP_HALATION)
+        y = s.render_linear(VJP_SEED)
+        gy = y - target
+        for _ in range(args.warmup):
+            s.render_vjp(gy, VJP_SEED, VJP_PARAMS)
+        fwd, bwd = [], []
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            s.render_linear(VJP_SEED)
+            t1 = time.perf_counter()
+            gx, gp = s.render_vjp(gy, VJP_SEED, VJP_PARAMS)
+            t2 = time.perf_counter()
+            fwd.append(t1 - t0)
+            bwd.append(t2 - t1)
+    eng.close()
+    ms = 1000.0 * statistics.median(bwd)
+    line = {"metric": "VJP ms/frame", "value": ms, "unit": "ms", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "render adjoint, 1024x1024, grain fixed (seed 7)", "width": n, "height": n,
+                       "params": ["print_exposure", "m_filter_shift", "y_filter_shift", "halation_weight_0",
+                                  "halation_weight_1", "halation_sigma_0", "halation_sigma_1"],
+                       "halation_sigma_px": [8, 40]},
+            "forward_ms": 1000.0 * statistics.median(fwd),
+            "note": "wall time per spk_render_vjp call with host arrays (forward recomputed inside); "
+                    "gradient accuracy is checked against binary64 central differences in tests/test_gpu_vjp.py",
+            "grad_params": [float(v) for v in gp], "grad_input_l2": float(np.sqrt(np.sum(gx.astype(np.float64) ** 2)))}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+BATCH_FRAMES = 64
+BATCH_SEED = 3
+
+
+def batch_workload():
+    """64 frames, sizes uniform in [256, 4096] x [256, 2732], print_exposure uniform in [0.7, 1.4], a
+    halation sigma pair (sigma0 in [5, 30], sigma1 in [40, 160] px, weight 1 each, strength 0.03), seed 3."""
+    rng = np.random.default_rng(BATCH_SEED)
+    frames = []
+    for i in range(BATCH_FRAMES):
+        w, h = int(rng.integers(256, 4097)), int(rng.integers(256, 2733))
+        ex = float(rng.uniform(0.7, 1.4))
+        s0, s1 = float(rng.uniform(5, 30)), float(rng.uniform(40, 160))
+        frames.append((w, h, ex, s0, s1))
+    return frames
+
+
+def run_batch(args):
+    """Batched renders (spkx_render_batch) of 64 frames of mixed sizes, then 64 batched reprints, against
+    the same frames through per-frame spk_render / spk_reprint calls. Aggregate megapixels/s over wall
+    time (results in pinned host memory); per-frame latency: a plain call's wall time, a batched frame's
+    completion on the device from the batch's start."""
+    resources = synth_resources.ensure(sc.RESOURCES)
+    lib = sc.load()
+    eng = lib.engine(resources, device=0)
+    frames = batch_workload()
+    mpx = sum(w * h for w, h, *_ in frames) / 1e6
+    images = [sc.synthetic_image(w, h, i) for i, (w, h, *_) in enumerate(frames)]
+
+    def open_all():
+        ss = []
+        for img, (w, h, ex, s0, s1) in zip(images, frames):
+            s = eng.open(img, dict(BASE, film_format_mm=35.0, print_exposure=ex))
+            s.set_halation([((1, 1, 1), (s0,) * 3), ((1, 1, 1), (s1,) * 3)], (0.03, 0.03, 0.03))
+            ss.append(s)
+        return ss
+
+    def reprint_exposures(ss):
+        for s, (w, h, ex, *_) in zip(ss, frames):
+            s.set_params({"print_exposure": min(1.4, ex * 1.1)})
+
+    def plain(ss, reprint):
+        lat = []
+        t0 = time.perf_counter()
+        for s in ss:
+            a = time.perf_counter()
+            with s.render_result("full", reprint=reprint):
+                pass
+            lat.append(1000.0 * (time.perf_counter() - a))
+        return time.perf_counter() - t0, lat
+
+    def batched(ss, reprint):
+        t0 = time.perf_counter()
+        res, info = eng.render_batch(ss, "full", reprint=reprint)
+        wall = time.perf_counter() - t0
+        for r in res:
+            r.free()
+        return wall, info
+
+    # warm-up and tuning: one plain pass and one batched pass of the same shape, untimed
+    for mode in ("plain", "batch"):
+        ss = open_all()
+        if mode == "plain":
+            plain(ss, False)
+        else:
+            batched(ss, False)
+            reprint_exposures(ss)
+            batched(ss, True)
+        for s in ss:
+            s.close()
+    ss = open_all()
+    p_render, lat_pr = plain(ss, False)
+    reprint_exposures(ss)
+    p_reprint, lat_pp = plain(ss, True)
+    for s in ss:
+        s.close()
+    ss = open_all()
+    b_render, info_r = batched(ss, False)
+    reprint_exposures(ss)
+    b_reprint, info_p = batched(ss, True)
+    for s in ss:
+        s.close()
+    eng.close()
+
+    def pct(v):
+        return {"p50": float(np.percentile(v, 50)), "p99": float(np.percentile(v, 99))}
+
+    line = {"metric": "batched render megapixels/s", "value": mpx / b_render, "unit": "Mpx/s", "n_gpus": 1,
+            "steps": 1, "warmup": 1, "ms_per_step": 1000.0 * b_render, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "64 frames 256x256..4096x2732 (seed 3), render then reprint", "frames": BATCH_FRAMES,
+                       "megapixels": mpx, "print_exposure": "uniform [0.7, 1.4]",
+                       "halation_sigma_px": "uniform [5, 30] and [40, 160]"},
+            "render": {"batched_mpx_s": mpx / b_render, "plain_mpx_s": mpx / p_render,
+                       "batched_ms": 1000.0 * b_render, "plain_ms": 1000.0 * p_render,
+                       "latency_ms_batched": pct(info_r["frame_done_ms"]), "latency_ms_plain": pct(lat_pr),
+                       "plan": info_r.get("plan")},
+            "reprint": {"batched_mpx_s": mpx / b_reprint, "plain_mpx_s": mpx / p_reprint,
+                        "batched_ms": 1000.0 * b_reprint, "plain_ms": 1000.0 * p_reprint,
+                        "latency_ms_batched": pct(info_p["frame_done_ms"]), "latency_ms_plain": pct(lat_pp),
+                        "plan": info_p.get("plan")}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -271,12 +429,19 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     ap.add_argument("--width", type=int, default=3840, help="frame width (the benchmark workload is 3840)")
     ap.add_argument("--height", type=int, default=2160, help="frame height (the benchmark workload is 2160)")
+    ap.add_argument("--config", default="render", choices=["render", "vjp", "batch"],
+                    help="render: the 4K render + reprint (the headline); vjp: the render's adjoint on 1024x1024; "
+                         "batch: 64 frames of mixed sizes, batched against per-frame calls")
     args = ap.parse_args()
     global W, H
     W, H = args.width, args.height
     if args.impl == "reference":
         return run_reference(args)
     args.warmup = max(args.warmup, 3)
+    if args.config == "vjp":
+        return run_vjp(args)
+    if args.config == "batch":
+        return run_batch(args)
 
     rank, local, world, pg = dist_init(args.gpus)
     resources = synth_resources.ensure(sc.RESOURCES)

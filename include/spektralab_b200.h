@@ -80,6 +80,29 @@ SPK_API spk_status spkx_philox(const uint32_t* counters, const uint32_t* keys, u
  * by the engine's FIR / recursive branch rule */
 SPK_API spk_status spkx_gaussian(const float* in, float* out, uint32_t w, uint32_t h, const double* sigma3);
 
+/* ---- batched renders (no counterpart in the reference engine) ----
+ *
+ * spkx_render_batch(sessions, n, tier, reprint, results, out_json)
+ *   spk_render (reprint = 0) or spk_reprint (reprint != 0) of n distinct sessions of one engine in one call;
+ *   results[i] is what that call would give sessions[i], pixel for pixel, and is released with
+ *   spk_result_free. The film side of each frame runs on its session's stream; the print side of the frames
+ *   runs as one CUDA graph: per-frame launches spread over worker streams, or one persistent print launch and
+ *   one persistent scanner launch for every frame. The first batch of a list of frame sizes times each plan
+ *   on the device and keeps the fastest for that list. results[i].elapsed_ms is the time from the start of
+ *   the call's device work to that frame's result in host memory. out_json (may be NULL) receives
+ *   {"plan": ..., "tuning_ms": ..., "frame_done_ms": [...]}. On failure every result is zeroed.
+ *   SPK_ERR_INVALID_ARG: NULL arrays, n = 0, a session twice, sessions of different engines, unknown tier.
+ */
+SPK_API spk_status spkx_render_batch(spk_session* const* sessions, uint32_t n, const char* tier, int32_t reprint,
+                                     spk_result* results, char** out_json);
+
+/* spkx_engine_batch_plan(engine, plan)
+ *   pins the plan of every later spkx_render_batch of this engine ("frames:K", K 1..16: per-frame launches on
+ *   K worker streams; "persistent:S:C": items of S pixels, S even, over C CTAs); NULL or "" restores the
+ *   timed choice. SPK_ERR_INVALID_ARG for any other string.
+ */
+SPK_API spk_status spkx_engine_batch_plan(spk_engine* engine, const char* plan);
+
 /* ---- the render's adjoint (no counterpart in the reference engine) ----
  *
  * spk_render_vjp(session, tier, film_seed, grad_output, grad_input, grad_params, n_params, output)

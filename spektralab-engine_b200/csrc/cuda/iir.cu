@@ -363,8 +363,8 @@ void iir_mixture(float* raw, float* const* tmp, float* acc, uint32_t w, uint32_t
     IirPlanes planes{};
     for (uint32_t c = 0; c < m.ncomp; ++c) planes.p[c] = tmp[c];
     const size_t sr = iir_rows_smem(w), sc = iir_cols_smem(h);
-    cudaFuncSetAttribute(k_iir_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sr));
-    cudaFuncSetAttribute(k_iir_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sc));
+    ensure_smem(reinterpret_cast<const void*>(k_iir_rows), int(sr));
+    ensure_smem(reinterpret_cast<const void*>(k_iir_cols), int(sc));
     {
         Probe p("iir_rows", s);
         k_iir_rows<<<h, kRowThreads, sr, s>>>(raw, planes, w, h, m);

@@ -10,6 +10,8 @@
 #include <stdint.h>
 
 #include <atomic>
+#include <map>
+#include <mutex>
 
 #include "../grain_sampler.h"
 #include "../kernel_args.h"
@@ -601,6 +603,18 @@ Probe::Probe(const char* name, cudaStream_t st) : s(st) {
 }
 Probe::~Probe() {
     if (t_hook) t_hook->after(s);
+}
+
+void ensure_smem(const void* kernel, int bytes) {
+    static std::mutex m;
+    static std::map<std::pair<const void*, int>, int> done;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> g(m);
+    int& cur = done[{kernel, dev}];
+    if (bytes <= cur) return;
+    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    cur = bytes;
 }
 
 void set_launch_hook(LaunchHook* hook) { t_hook = hook; }

@@ -27,6 +27,10 @@ struct Probe {
     ~Probe();
 };
 
+// Raises a kernel's dynamic shared-memory limit to `bytes` on the current device, once (a later call asking
+// no more is a no-op), so that launches inside a stream capture make no attribute call.
+void ensure_smem(const void* kernel, int bytes);
+
 // RGB -> film exposure H (Mitchell bicubic of the spectral table, L x L float4 texels), times the
 // compensation gain.
 void expose(const float* rgb, float* h, const float* table4, const ExposeArgs& a, cudaStream_t s);
@@ -66,6 +70,19 @@ void scan_encode(const float* rgb, uint16_t* out, uint32_t w, uint32_t h, const 
 // out must not alias in. fir_tile_fits tells whether the tiled kernel takes this frame and radius.
 bool fir_tile_fits(uint32_t w, uint32_t h, int r);
 void fir_tile(const float* in, float* out, uint32_t w, uint32_t h, int r, const float* taps, cudaStream_t s);
+
+// The print and scanner stages of many frames, each in one persistent launch of `ctas` CTAs: print over
+// items of item_px pixels (item_frame / item_first per item, ordered by frame; frames in device memory),
+// the scanner over the frames' concatenated 32 x 32 tile lists (frames in device memory, ordered by
+// first_tile; r1, r2 the radii every frame shares, or -1 for frames that differ).
+void print_batch(const BatchPrintFrame* frames, const uint32_t* item_frame, const uint32_t* item_first,
+                 uint32_t n_items, uint32_t item_px, uint32_t ctas, cudaStream_t s);
+void scan_encode_batch(const BatchScanFrame* frames, uint32_t n_frames, uint32_t n_tiles, int r1, int r2,
+                       uint32_t ctas, cudaStream_t s);
+// Sets the scanner kernels' shared-memory limits on the current device (before a stream capture).
+void scan_prepare();
+uint32_t scan_tiles(uint32_t w, uint32_t h);  // 32 x 32 tiles of a w x h frame
+uint32_t scan_tiles_x(uint32_t w);
 
 // host frame (channels 3 or 4, already on the device) -> interleaved RGB plane, non-finite -> 0
 void source_copy(const float* raw, float* out, size_t pixels, uint32_t channels, cudaStream_t s);

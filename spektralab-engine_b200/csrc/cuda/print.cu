@@ -204,11 +204,10 @@ __device__ __forceinline__ float print_density(const PrintArgs& a, uint32_t c, f
     return paper_lookup(a.paper, a.paper_K, a.paper_grid, c, l);
 }
 
-__global__ void __launch_bounds__(kPrintThreads) k_print(const float* __restrict__ neg, float* __restrict__ rgb,
-                                                         const __grid_constant__ PrintArgs a) {
-    const uint32_t p0 = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
-    if (p0 >= a.n) return;
-    const bool two = p0 + 1 < a.n;
+// pixels p0 and p0 + 1 (when p0 + 1 < n) of one frame
+__device__ __forceinline__ void print_pair(const PrintArgs& a, const float* __restrict__ neg, float* __restrict__ rgb,
+                                           uint32_t p0, uint32_t n) {
+    const bool two = p0 + 1 < n;
     const float* s0 = neg + 3 * size_t(p0);
     const float* s1 = two ? s0 + 3 : s0;
     float2 d0 = make_float2(s0[0], s1[0]), d1 = make_float2(s0[1], s1[1]), d2 = make_float2(s0[2], s1[2]);
@@ -237,6 +236,45 @@ __global__ void __launch_bounds__(kPrintThreads) k_print(const float* __restrict
     }
 }
 
+__global__ void __launch_bounds__(kPrintThreads) k_print(const float* __restrict__ neg, float* __restrict__ rgb,
+                                                         const __grid_constant__ PrintArgs a) {
+    const uint32_t p0 = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
+    if (p0 >= a.n) return;
+    print_pair(a, neg, rgb, p0, a.n);
+}
+
+// The print stage of many frames in one persistent launch. Work item i covers `item_px` pixels of frame
+// item_frame[i] from pixel item_first[i]; the CTAs take items i = blockIdx.x, blockIdx.x + gridDim.x, ...
+// (items are ordered by frame, so a CTA mostly stays on one frame) and stage the frame's arguments in
+// shared memory when the frame changes.
+__global__ void __launch_bounds__(kPrintThreads) k_print_batch(const BatchPrintFrame* __restrict__ frames,
+                                                               const uint32_t* __restrict__ item_frame,
+                                                               const uint32_t* __restrict__ item_first,
+                                                               uint32_t n_items, uint32_t item_px) {
+    __shared__ __align__(16) PrintArgs sa;
+    __shared__ const float* s_neg;
+    __shared__ float* s_rgb;
+    uint32_t cur = 0xFFFFFFFFu;
+    for (uint32_t it = blockIdx.x; it < n_items; it += gridDim.x) {
+        const uint32_t f = item_frame[it];
+        if (f != cur) {
+            __syncthreads();
+            const uint4* src = reinterpret_cast<const uint4*>(&frames[f].args);
+            uint4* dst = reinterpret_cast<uint4*>(&sa);
+            for (uint32_t i = threadIdx.x; i < sizeof(PrintArgs) / 16; i += blockDim.x) dst[i] = src[i];
+            if (threadIdx.x == 0) {
+                s_neg = frames[f].neg;
+                s_rgb = frames[f].rgb;
+            }
+            __syncthreads();
+            cur = f;
+        }
+        const uint32_t first = item_first[it];
+        for (uint32_t p0 = first + 2 * threadIdx.x; p0 < min(first + item_px, sa.n); p0 += 2 * blockDim.x)
+            print_pair(sa, s_neg, s_rgb, p0, sa.n);
+    }
+}
+
 }  // namespace
 
 void print(const float* neg, float* rgb, const PrintArgs& a, cudaStream_t s) {
@@ -244,6 +282,13 @@ void print(const float* neg, float* rgb, const PrintArgs& a, cudaStream_t s) {
     const uint32_t threads = (a.n + 1) / 2;
     Probe p("print", s);
     k_print<<<(threads + kPrintThreads - 1) / kPrintThreads, kPrintThreads, 0, s>>>(neg, rgb, a);
+}
+
+void print_batch(const BatchPrintFrame* frames, const uint32_t* item_frame, const uint32_t* item_first,
+                 uint32_t n_items, uint32_t item_px, uint32_t ctas, cudaStream_t s) {
+    if (n_items == 0) return;
+    Probe p("print_batch", s);
+    k_print_batch<<<ctas, kPrintThreads, 0, s>>>(frames, item_frame, item_first, n_items, item_px);
 }
 
 }  // namespace spkb::dev

@@ -32,10 +32,10 @@ constexpr int kTW = 32, kTH = 32, kThreads = 256, kWarps = kThreads / 32;
 // half-sample symmetric reflection, exact for p in [-n, 2n)
 __device__ __forceinline__ int reflect_near(int p, int n) { return p < 0 ? -1 - p : (p >= n ? 2 * n - 1 - p : p); }
 
+// One 32 x 32 output tile at (x0, y0) of a frame; smem as sized by scan_smem_bytes for the radii.
 template <int R1, int R2>
-__global__ void __launch_bounds__(kThreads) k_scan_encode(const float* __restrict__ rgb, uint16_t* __restrict__ out,
-                                                          int w, int h, const __grid_constant__ ScanArgs a) {
-    extern __shared__ float smem[];
+__device__ __forceinline__ void scan_tile(const ScanArgs& a, const float* __restrict__ rgb, uint16_t* __restrict__ out,
+                                          int w, int h, int x0, int y0, float* smem) {
     const int r1 = R1 >= 0 ? R1 : a.r1, r2 = R2 >= 0 ? R2 : a.r2, R = r1 + r2;
     const int PC = 3 * (kTW + 2 * R);  // floats per row of the print tile and the first vertical pass
     const int PR = kTH + 2 * R;
@@ -43,7 +43,6 @@ __global__ void __launch_bounds__(kThreads) k_scan_encode(const float* __restric
     const int BC = 3 * (kTW + 2 * r2);
     float* A = smem;
     float* B = smem + PR * PC;
-    const int x0 = blockIdx.x * kTW, y0 = blockIdx.y * kTH;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
     // 1. the print output at (y0 - R + i, x0 - R + j), reflected; pixels more than R past an edge are
@@ -156,6 +155,34 @@ __global__ void __launch_bounds__(kThreads) k_scan_encode(const float* __restric
     }
 }
 
+template <int R1, int R2>
+__global__ void __launch_bounds__(kThreads) k_scan_encode(const float* __restrict__ rgb, uint16_t* __restrict__ out,
+                                                          int w, int h, const __grid_constant__ ScanArgs a) {
+    extern __shared__ float smem[];
+    scan_tile<R1, R2>(a, rgb, out, w, h, blockIdx.x * kTW, blockIdx.y * kTH, smem);
+}
+
+// The scanner stage of many frames in one persistent launch: the CTAs take tiles t = blockIdx.x,
+// blockIdx.x + gridDim.x, ... of the frames' concatenated tile lists (row-major within a frame).
+template <int R1, int R2>
+__global__ void __launch_bounds__(kThreads) k_scan_encode_batch(const BatchScanFrame* __restrict__ frames,
+                                                                uint32_t n_frames, uint32_t n_tiles) {
+    extern __shared__ float smem[];
+    for (uint32_t t = blockIdx.x; t < n_tiles; t += gridDim.x) {
+        uint32_t lo = 0, hi = n_frames;  // the last frame whose first tile is <= t
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) / 2;
+            if (frames[mid].first_tile <= t) lo = mid;
+            else hi = mid;
+        }
+        const BatchScanFrame& f = frames[lo];
+        const uint32_t local = t - f.first_tile;
+        const uint32_t ty = local / f.tiles_x, tx = local - ty * f.tiles_x;
+        __syncthreads();  // the previous tile's reads of shared memory are done
+        scan_tile<R1, R2>(f.args, f.rgb, f.out, int(f.w), int(f.h), int(tx) * kTW, int(ty) * kTH, smem);
+    }
+}
+
 // A separable FIR Gaussian with one tap vector for the three channels, both passes in one tiled kernel:
 // the vertical pass at the tile's rows (every column of the haloed tile; a halo column holds the
 // reflected source column, so its vertical result is that of the reflected column), then the horizontal
@@ -214,7 +241,7 @@ size_t scan_smem_bytes(int r1, int r2) {
 template <int R1, int R2>
 void launch_scan(const float* rgb, uint16_t* out, uint32_t w, uint32_t h, const ScanArgs& a, cudaStream_t s) {
     const size_t smem = scan_smem_bytes(a.r1, a.r2);  // at most 96 KB (r1 = r2 = 9)
-    cudaFuncSetAttribute(k_scan_encode<R1, R2>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    ensure_smem(reinterpret_cast<const void*>(k_scan_encode<R1, R2>), int(smem));
     const dim3 g((w + kTW - 1) / kTW, (h + kTH - 1) / kTH);
     k_scan_encode<R1, R2><<<g, kThreads, smem, s>>>(rgb, out, int(w), int(h), a);
 }
@@ -236,10 +263,39 @@ void scan_encode(const float* rgb, uint16_t* out, uint32_t w, uint32_t h, const 
 }
 
 namespace {
+template <int R1, int R2>
+void launch_scan_batch(const BatchScanFrame* frames, uint32_t n_frames, uint32_t n_tiles, uint32_t ctas, size_t smem,
+                       cudaStream_t s) {
+    ensure_smem(reinterpret_cast<const void*>(k_scan_encode_batch<R1, R2>), int(smem));
+    k_scan_encode_batch<R1, R2><<<ctas, kThreads, smem, s>>>(frames, n_frames, n_tiles);
+}
+}  // namespace
+
+void scan_prepare() {
+    const int max_smem = int(scan_smem_bytes(SPKB_FIR_MAX_R, SPKB_FIR_MAX_R));
+    ensure_smem(reinterpret_cast<const void*>(k_scan_encode<5, 2>), int(scan_smem_bytes(5, 2)));
+    ensure_smem(reinterpret_cast<const void*>(k_scan_encode<0, 2>), int(scan_smem_bytes(0, 2)));
+    ensure_smem(reinterpret_cast<const void*>(k_scan_encode<-1, -1>), max_smem);
+    ensure_smem(reinterpret_cast<const void*>(k_scan_encode_batch<5, 2>), int(scan_smem_bytes(5, 2)));
+    ensure_smem(reinterpret_cast<const void*>(k_scan_encode_batch<-1, -1>), max_smem);
+}
+
+uint32_t scan_tiles(uint32_t w, uint32_t h) { return ((w + kTW - 1) / kTW) * ((h + kTH - 1) / kTH); }
+uint32_t scan_tiles_x(uint32_t w) { return (w + kTW - 1) / kTW; }
+
+void scan_encode_batch(const BatchScanFrame* frames, uint32_t n_frames, uint32_t n_tiles, int r1, int r2,
+                       uint32_t ctas, cudaStream_t s) {
+    if (n_tiles == 0) return;
+    Probe p("scan_encode_batch", s);
+    if (r1 == 5 && r2 == 2) launch_scan_batch<5, 2>(frames, n_frames, n_tiles, ctas, scan_smem_bytes(5, 2), s);
+    else launch_scan_batch<-1, -1>(frames, n_frames, n_tiles, ctas, scan_smem_bytes(SPKB_FIR_MAX_R, SPKB_FIR_MAX_R), s);
+}
+
+namespace {
 template <int R>
 void launch_fir_tile(const float* in, float* out, uint32_t w, uint32_t h, const ScanArgs& a, cudaStream_t s) {
     const size_t smem = size_t(2 * kTH + 2 * a.r1) * size_t(3 * (kTW + 2 * a.r1)) * sizeof(float);
-    cudaFuncSetAttribute(k_fir_tile<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+    ensure_smem(reinterpret_cast<const void*>(k_fir_tile<R>), int(smem));
     const dim3 g((w + kTW - 1) / kTW, (h + kTH - 1) / kTH);
     k_fir_tile<R><<<g, kThreads, smem, s>>>(in, out, int(w), int(h), a);
 }

@@ -6,11 +6,13 @@
 // The device work is this build's own: one CUDA stream and one scratch pool per session, the source
 // frame and the per-tier negatives resident in device memory, the result copied once to pinned host
 // memory.
+#include <algorithm>
 #include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <set>
 
@@ -92,6 +94,31 @@ public:
     std::mutex pipelines_m;
     std::vector<std::pair<std::string, Pipeline>> pipelines;  // most recent last
     static constexpr size_t kPipelineCache = 8;
+
+    // Batched renders (spkx_render_batch): one at a time per engine, on their own streams. The plan chosen
+    // for a list of frame sizes is kept, and so is the instantiated graph of each (plan, sizes) pair, which a
+    // later batch of the same shape updates in place.
+    std::mutex batch_m;
+    cudaStream_t batch_stream = nullptr;
+    std::vector<cudaStream_t> workers;
+    std::vector<cudaEvent_t> frame_events;  // one per frame slot: completion, recorded inside the graph
+    std::vector<cudaEvent_t> join_events;   // one per worker stream
+    cudaEvent_t fork_event = nullptr, start_event = nullptr;
+    std::map<std::string, std::string> tuned;
+    std::string pinned_plan;  // set by spkx_engine_batch_plan: used for every batch, no tuning
+    std::map<std::string, cudaGraphExec_t> graphs;
+    static constexpr size_t kGraphCache = 16;
+
+    ~Engine() {
+        if (batch_stream) cudaStreamSynchronize(batch_stream);
+        for (auto& [k, g] : graphs) cudaGraphExecDestroy(g);
+        for (cudaStream_t w : workers) cudaStreamDestroy(w);
+        for (cudaEvent_t ev : frame_events) cudaEventDestroy(ev);
+        for (cudaEvent_t ev : join_events) cudaEventDestroy(ev);
+        if (fork_event) cudaEventDestroy(fork_event);
+        if (start_event) cudaEventDestroy(start_event);
+        if (batch_stream) cudaStreamDestroy(batch_stream);
+    }
 };
 
 struct TierState {
@@ -411,6 +438,371 @@ spk_status render_common(spk_session* session, const char* tier, spk_result* out
     });
     if (st != SPK_OK) release_result(out);
     return st;
+}
+
+// ---- batched renders ------------------------------------------------------------------------------
+//
+// A batch renders many sessions' frames with one call. The film side of each frame runs on its session's
+// stream as in spk_render (sessions develop concurrently); the print side and the scanner of every frame
+// whose scanner takes the tiled kernel go into ONE CUDA graph on the engine's batch stream, launched after
+// all the negatives are ready. Two plan families build that graph:
+//   frames:K          each frame's print and scanner launches on one of K worker streams (round robin),
+//                     forked from and joined to the batch stream; the frames overlap on the device;
+//   persistent:S:C    one print launch and one scanner launch for all frames: C CTAs walking items of S
+//                     pixels (print) and the frames' concatenated 32 x 32 tile lists (scanner).
+// Every plan runs the same per-pixel and per-tile code as spk_render, so the pixels are those of singles.
+// The first batch of a list of frame sizes times each candidate plan on the device and keeps the fastest.
+
+struct BatchFrame {
+    Session* s = nullptr;
+    OutputImage* img = nullptr;
+    Plane rgb;
+    const float* neg = nullptr;
+    PrintArgs pa{};
+    ScanArgs sa{};
+    bool fused = false;      // print and scanner inside the batch graph
+    bool reused = false;     // the tier's negative was cached (reprint)
+    bool developed = false;  // the tier's negative was made by this batch
+    cudaEvent_t ready = nullptr;
+};
+
+const char* const kBatchPlans[] = {"frames:4", "frames:16", "persistent:2048:592", "persistent:8192:1184"};
+constexpr size_t kMaxWorkers = 16;
+
+// A plan string: "frames:K" (1 <= K <= 16) or "persistent:S:C" (S even, 2 .. 2^20 pixels; 1 <= C <= 65535).
+bool valid_plan(const std::string& p) {
+    auto number = [](const std::string& t, unsigned long lo, unsigned long hi, unsigned long& v) {
+        if (t.empty() || t.size() > 9 || t.find_first_not_of("0123456789") != std::string::npos) return false;
+        v = std::stoul(t);
+        return v >= lo && v <= hi;
+    };
+    unsigned long a = 0, b = 0;
+    if (p.rfind("frames:", 0) == 0) return number(p.substr(7), 1, kMaxWorkers, a);
+    if (p.rfind("persistent:", 0) != 0) return false;
+    const std::string rest = p.substr(11);
+    const size_t c = rest.find(':');
+    if (c == std::string::npos) return false;
+    return number(rest.substr(0, c), 2, 1ul << 20, a) && a % 2 == 0 && number(rest.substr(c + 1), 1, 65535, b);
+}
+
+void batch_resources(Engine& e, size_t n_frames, size_t n_workers) {
+    if (!e.batch_stream) cuda_check(cudaStreamCreateWithFlags(&e.batch_stream, cudaStreamNonBlocking), "batch stream");
+    if (!e.fork_event) cuda_check(cudaEventCreateWithFlags(&e.fork_event, cudaEventDisableTiming), "batch event");
+    if (!e.start_event) cuda_check(cudaEventCreate(&e.start_event), "batch event");
+    while (e.workers.size() < n_workers) {
+        cudaStream_t w = nullptr;
+        cuda_check(cudaStreamCreateWithFlags(&w, cudaStreamNonBlocking), "batch worker stream");
+        e.workers.push_back(w);
+        cudaEvent_t j = nullptr;
+        cuda_check(cudaEventCreateWithFlags(&j, cudaEventDisableTiming), "batch event");
+        e.join_events.push_back(j);
+    }
+    while (e.frame_events.size() < n_frames) {
+        cudaEvent_t ev = nullptr;
+        cuda_check(cudaEventCreate(&ev), "batch event");
+        e.frame_events.push_back(ev);
+    }
+}
+
+// Captures body(batch_stream) into a graph, brings the engine's executable graph for `key` up to date
+// (updated in place when the topology is unchanged, else instantiated afresh) and launches it.
+template <class F>
+void launch_captured(Engine& e, const std::string& key, F&& body) {
+    cudaStream_t bs = e.batch_stream;
+    cuda_check(cudaStreamBeginCapture(bs, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
+    try {
+        body(bs);
+    } catch (...) {
+        cudaGraph_t g = nullptr;
+        cudaStreamEndCapture(bs, &g);
+        if (g) cudaGraphDestroy(g);
+        (void)cudaGetLastError();
+        throw;
+    }
+    cudaGraph_t graph = nullptr;
+    cuda_check(cudaStreamEndCapture(bs, &graph), "cudaStreamEndCapture");
+    cudaGraphExec_t exec = nullptr;
+    auto it = e.graphs.find(key);
+    if (it != e.graphs.end()) {
+        cudaGraphExecUpdateResultInfo info{};
+        if (cudaGraphExecUpdate(it->second, graph, &info) == cudaSuccess) {
+            exec = it->second;
+        } else {
+            (void)cudaGetLastError();
+            cudaGraphExecDestroy(it->second);
+            e.graphs.erase(it);
+        }
+    }
+    if (!exec) {
+        const cudaError_t err = cudaGraphInstantiate(&exec, graph, 0);
+        if (err != cudaSuccess) {
+            cudaGraphDestroy(graph);
+            cuda_check(err, "cudaGraphInstantiate");
+        }
+        if (e.graphs.size() >= Engine::kGraphCache) {
+            cudaGraphExecDestroy(e.graphs.begin()->second);
+            e.graphs.erase(e.graphs.begin());
+        }
+        e.graphs[key] = exec;
+    }
+    cudaGraphDestroy(graph);
+    cuda_check(cudaGraphLaunch(exec, bs), "cudaGraphLaunch");
+}
+
+// Enqueues the print side of the fused frames under `plan` on the batch stream (graph launch and, for the
+// persistent plans, the upload of the frame tables before it). Each fused frame's result is copied to its
+// pinned host image inside the graph, and frame_events[slot] marks its completion.
+void run_plan(Engine& e, const std::string& plan, const std::string& shape, std::vector<BatchFrame>& fr,
+              const std::vector<size_t>& slots, DevBuffer& tables) {
+    cudaStream_t bs = e.batch_stream;
+    const std::string key = plan + "|" + shape;
+    if (plan.rfind("frames:", 0) == 0) {
+        const size_t K = std::min<size_t>(std::stoul(plan.substr(7)), std::max<size_t>(slots.size(), 1));
+        launch_captured(e, key, [&](cudaStream_t s) {
+            cuda_check(cudaEventRecord(e.fork_event, s), "fork");
+            for (size_t k = 0; k < K; ++k) cuda_check(cudaStreamWaitEvent(e.workers[k], e.fork_event, 0), "fork");
+            for (size_t j = 0; j < slots.size(); ++j) {
+                BatchFrame& f = fr[slots[j]];
+                cudaStream_t ws = e.workers[j % K];
+                dev::print(f.neg, f.rgb.data(), f.pa, ws);
+                dev::scan_encode(f.rgb.data(), f.img->dev, f.rgb.w, f.rgb.h, f.sa, ws);
+                cuda_check(cudaMemcpyAsync(f.img->host, f.img->dev, f.img->bytes, cudaMemcpyDeviceToHost, ws),
+                           "result copy");
+                cuda_check(cudaEventRecordWithFlags(e.frame_events[slots[j]], ws, cudaEventRecordExternal), "frame");
+            }
+            for (size_t k = 0; k < K; ++k) {
+                cuda_check(cudaEventRecord(e.join_events[k], e.workers[k]), "join");
+                cuda_check(cudaStreamWaitEvent(s, e.join_events[k], 0), "join");
+            }
+        });
+        return;
+    }
+    // persistent:S:C
+    const size_t c1 = plan.find(':'), c2 = plan.find(':', c1 + 1);
+    const uint32_t item_px = uint32_t(std::stoul(plan.substr(c1 + 1, c2 - c1 - 1)));
+    const uint32_t ctas = uint32_t(std::stoul(plan.substr(c2 + 1)));
+    const size_t n = slots.size();
+    std::vector<BatchPrintFrame> pf(n);
+    std::vector<BatchScanFrame> sf(n);
+    std::vector<uint32_t> item_frame, item_first;
+    uint32_t tiles = 0;
+    int r1 = fr[slots[0]].sa.r1, r2 = fr[slots[0]].sa.r2;
+    for (size_t j = 0; j < n; ++j) {
+        BatchFrame& f = fr[slots[j]];
+        pf[j].args = f.pa;
+        pf[j].neg = f.neg;
+        pf[j].rgb = f.rgb.data();
+        for (uint32_t p = 0; p < f.pa.n; p += item_px) {
+            item_frame.push_back(uint32_t(j));
+            item_first.push_back(p);
+        }
+        sf[j].args = f.sa;
+        sf[j].rgb = f.rgb.data();
+        sf[j].out = f.img->dev;
+        sf[j].w = f.rgb.w;
+        sf[j].h = f.rgb.h;
+        sf[j].tiles_x = dev::scan_tiles_x(f.rgb.w);
+        sf[j].first_tile = tiles;
+        tiles += dev::scan_tiles(f.rgb.w, f.rgb.h);
+        if (f.sa.r1 != r1 || f.sa.r2 != r2) r1 = r2 = -1;
+    }
+    const uint32_t n_items = uint32_t(item_frame.size());
+    auto up16 = [](size_t b) { return (b + 15) / 16 * 16; };
+    const size_t o_sf = up16(n * sizeof(BatchPrintFrame));
+    const size_t o_if = o_sf + up16(n * sizeof(BatchScanFrame));
+    const size_t o_ip = o_if + up16(n_items * sizeof(uint32_t));
+    const size_t bytes = o_ip + up16(n_items * sizeof(uint32_t));
+    std::vector<unsigned char> blob(bytes, 0);
+    std::memcpy(blob.data(), pf.data(), n * sizeof(BatchPrintFrame));
+    std::memcpy(blob.data() + o_sf, sf.data(), n * sizeof(BatchScanFrame));
+    std::memcpy(blob.data() + o_if, item_frame.data(), n_items * sizeof(uint32_t));
+    std::memcpy(blob.data() + o_ip, item_first.data(), n_items * sizeof(uint32_t));
+    Pool pool(bs);
+    tables = pool.acquire(bytes);
+    unsigned char* d = tables.as<unsigned char>();
+    cuda_check(cudaMemcpyAsync(d, blob.data(), bytes, cudaMemcpyHostToDevice, bs), "batch tables");
+    // the pageable source is staged before cudaMemcpyAsync returns, so blob may go at scope exit
+    launch_captured(e, key, [&](cudaStream_t s) {
+        dev::print_batch(reinterpret_cast<const BatchPrintFrame*>(d), reinterpret_cast<const uint32_t*>(d + o_if),
+                         reinterpret_cast<const uint32_t*>(d + o_ip), n_items, item_px, ctas, s);
+        dev::scan_encode_batch(reinterpret_cast<const BatchScanFrame*>(d + o_sf), uint32_t(n), tiles, r1, r2, ctas, s);
+        for (size_t j = 0; j < n; ++j) {
+            BatchFrame& f = fr[slots[j]];
+            cuda_check(cudaMemcpyAsync(f.img->host, f.img->dev, f.img->bytes, cudaMemcpyDeviceToHost, s),
+                       "result copy");
+            cuda_check(cudaEventRecordWithFlags(e.frame_events[slots[j]], s, cudaEventRecordExternal), "frame");
+        }
+    });
+}
+
+void render_batch(std::vector<Session*> ss, const char* tier_name, bool reprint, spk_result* out, std::string* info) {
+    const std::optional<Tier> t = parse_tier(tier_name);
+    if (!t) fail_invalid(std::string("unknown tier '") + (tier_name ? tier_name : "") + "'; expected live, preview or full");
+    if (ss.empty()) fail_invalid("a batch needs at least one session");
+    Engine& e = *ss[0]->engine;
+    {
+        std::vector<Session*> order = ss;
+        std::sort(order.begin(), order.end());
+        for (size_t i = 0; i < order.size(); ++i) {
+            if (!order[i]) fail_invalid("a session of the batch is NULL");
+            if (i && order[i] == order[i - 1]) fail_invalid("a session appears twice in the batch");
+            if (order[i]->engine != &e) fail_invalid("the sessions of a batch must share one engine");
+        }
+    }
+    // sessions locked in address order (no lock-order cycle with other batches), then the engine's batch
+    std::vector<Session*> order = ss;
+    std::sort(order.begin(), order.end());
+    std::vector<std::unique_lock<std::mutex>> locks;
+    locks.reserve(order.size());
+    for (Session* s : order) locks.emplace_back(s->m);
+    std::lock_guard<std::mutex> bl(e.batch_m);
+    DeviceGuard dg(e.device);
+
+    const size_t n = ss.size();
+    std::vector<BatchFrame> fr(n);
+    DevBuffer tables;
+    std::string plan;
+    double tuning_ms = 0.0;
+    std::vector<double> done_ms(n, 0.0);
+    try {
+        batch_resources(e, n, kMaxWorkers);
+        dev::scan_prepare();
+        cudaStream_t bs = e.batch_stream;
+        const auto t0 = std::chrono::steady_clock::now();
+        cuda_check(cudaEventRecord(e.start_event, bs), "batch start");
+        std::vector<size_t> slots;
+        std::string shape = std::string(tier_name);
+        for (size_t i = 0; i < n; ++i) {
+            Session& s = *ss[i];
+            BatchFrame& f = fr[i];
+            f.s = &s;
+            TierState& ts = s.tiers[int(*t)];
+            f.reused = reprint && static_cast<bool>(ts.negative);
+            s.progress_id = "p" + std::to_string(g_next_id++);
+            s.cancel.store(false);
+            s.nodes_done.store(0);
+            s.nodes_total = f.reused ? 1 : 2;
+            s.done = false;
+            s.check_tier(*t);
+            RenderCtx ctx{s.pool, s.stream};
+            ctx.rho_tier = 1.0;
+            if (!f.reused) {
+                f.developed = true;
+                develop_tier(s, *t, ctx);
+            }
+            ctx.pitch_um = ts.pitch_um;
+            s.node();
+            f.img = output_acquire(e.device, s.source.w, s.source.h);
+            f.neg = ts.negative.data();
+            f.fused = scan_args(s.pipe, ctx.rho_tier, s.source.w, s.source.h, f.img->stride_px, f.sa);
+            if (f.fused) {
+                f.pa = print_args(s.pipe, s.live, uint32_t(ts.negative.pixels()));
+                f.rgb = make_plane(s.pool, s.source.w, s.source.h);
+                cuda_check(cudaEventCreateWithFlags(&f.ready, cudaEventDisableTiming), "batch event");
+                cuda_check(cudaEventRecord(f.ready, s.stream), "frame ready");
+                cuda_check(cudaStreamWaitEvent(bs, f.ready, 0), "frame ready");
+                slots.push_back(i);
+                shape += "," + std::to_string(s.source.w) + "x" + std::to_string(s.source.h);
+            } else {
+                // the scanner's separate passes: the frame stays on its session's stream
+                print_scan_encode(ctx, s.pipe, s.live, ts.negative, f.img);
+                cuda_check(cudaMemcpyAsync(f.img->host, f.img->dev, f.img->bytes, cudaMemcpyDeviceToHost, s.stream),
+                           "result copy");
+                cuda_check(cudaEventRecord(e.frame_events[i], s.stream), "frame");
+            }
+        }
+        if (!slots.empty()) {
+            auto tuned = e.tuned.find(shape);
+            if (!e.pinned_plan.empty()) {
+                plan = e.pinned_plan;
+            } else if (tuned != e.tuned.end()) {
+                plan = tuned->second;
+            } else {
+                // every candidate renders the whole batch; the pixels agree, so the last run's stand
+                cudaEvent_t a = nullptr, b = nullptr;
+                cuda_check(cudaEventCreate(&a), "batch event");
+                cuda_check(cudaEventCreate(&b), "batch event");
+                float best = 0.0f;
+                try {
+                    for (const char* cand : kBatchPlans) {
+                        DevBuffer tb;
+                        cuda_check(cudaEventRecord(a, bs), "tuning");
+                        run_plan(e, cand, shape, fr, slots, tb);
+                        cuda_check(cudaEventRecord(b, bs), "tuning");
+                        cuda_check(cudaEventSynchronize(b), "tuning");
+                        float ms = 0.0f;
+                        cuda_check(cudaEventElapsedTime(&ms, a, b), "tuning");
+                        tuning_ms += ms;
+                        if (plan.empty() || ms < best) {
+                            best = ms;
+                            plan = cand;
+                        }
+                    }
+                } catch (...) {
+                    cudaEventDestroy(a);
+                    cudaEventDestroy(b);
+                    throw;
+                }
+                cudaEventDestroy(a);
+                cudaEventDestroy(b);
+                e.tuned[shape] = plan;
+            }
+            run_plan(e, plan, shape, fr, slots, tables);
+        }
+        cuda_check(cudaStreamSynchronize(bs), "batch");
+        for (size_t i = 0; i < n; ++i) {
+            cuda_check(cudaStreamSynchronize(ss[i]->stream), "batch");
+            float ms = 0.0f;
+            if (cudaEventElapsedTime(&ms, e.start_event, e.frame_events[i]) == cudaSuccess) {
+                done_ms[i] = ms;
+            } else {
+                (void)cudaGetLastError();
+                done_ms[i] = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+            }
+        }
+        cuda_check(cudaGetLastError(), "batch");
+    } catch (...) {
+        if (e.batch_stream) (void)cudaStreamSynchronize(e.batch_stream);
+        for (BatchFrame& f : fr) {
+            if (f.s) (void)cudaStreamSynchronize(f.s->stream);
+            if (f.img) output_release(f.img);
+            f.img = nullptr;
+            if (f.developed) f.s->tiers[int(*t)].negative = Plane{};
+            if (f.ready) cudaEventDestroy(f.ready);
+        }
+        try {
+            throw;
+        } catch (const Error& err) {
+            if (err.status() == SPK_ERR_CANCELLED || err.status() == SPK_ERR_INVALID_ARG) throw;
+            fail_gpu(err.what());
+        } catch (const std::bad_alloc&) {
+            fail_gpu("out of memory");
+        }
+    }
+    json::Value r;
+    json::Array dms;
+    for (size_t i = 0; i < n; ++i) {
+        BatchFrame& f = fr[i];
+        if (f.ready) cudaEventDestroy(f.ready);
+        Session& s = *f.s;
+        s.done = true;
+        spk_result& o = out[i];
+        o.rgba16 = f.img->host;
+        o.texture = f.img;
+        o.width = f.img->width;
+        o.height = f.img->height;
+        o.row_stride_px = f.img->stride_px;
+        o.elapsed_ms = done_ms[i];
+        o.reprint = f.reused ? 1 : 0;
+        o.negative_was_cached = f.reused ? 1 : 0;
+        std::memset(o.progress_id, 0, sizeof o.progress_id);
+        std::strncpy(o.progress_id, s.progress_id.c_str(), sizeof o.progress_id - 1);
+        dms.push_back(json::Value(done_ms[i]));
+    }
+    r["plan"] = plan.empty() ? std::string("none") : plan;
+    r["tuning_ms"] = tuning_ms;
+    r["frame_done_ms"] = json::Value(std::move(dms));
+    if (info) *info = json::write(r);
 }
 
 }  // namespace
@@ -826,6 +1218,43 @@ SPK_API spk_status spkx_session_negative(spk_session* session, const char* tier,
         cuda_check(cudaStreamSynchronize(s.stream), "negative copy");
         return SPK_OK;
     });
+}
+
+SPK_API spk_status spkx_engine_batch_plan(spk_engine* engine, const char* plan) {
+    last_error::clear();
+    if (!engine) return invalid("engine is NULL");
+    const std::string p = plan ? plan : "";
+    if (!p.empty() && !valid_plan(p))
+        return invalid("batch plan must be \"frames:K\" (K 1..16) or \"persistent:S:C\" (S even, 2..1048576; C 1..65535)");
+    return guarded([&] {
+        Engine& e = *E(engine);
+        std::lock_guard<std::mutex> g(e.batch_m);
+        e.pinned_plan = p;
+        return SPK_OK;
+    });
+}
+
+// Batched renders: this build's extension (no reference counterpart; spk_render per session is the
+// reference's only entry, src/abi/abi.cpp:293-308, and every result here is the one spk_render gives).
+SPK_API spk_status spkx_render_batch(spk_session* const* sessions, uint32_t n, const char* tier, int32_t reprint,
+                                     spk_result* results, char** out_json) {
+    last_error::clear();
+    if (out_json) *out_json = nullptr;
+    if (!sessions) return invalid("sessions is NULL");
+    if (!results) return invalid("results is NULL");
+    if (n == 0) return invalid("a batch needs at least one session");
+    std::memset(results, 0, sizeof(spk_result) * n);
+    const int32_t st = guarded([&] {
+        std::vector<Session*> ss(n);
+        for (uint32_t i = 0; i < n; ++i) ss[i] = S(sessions[i]);
+        std::string info;
+        render_batch(ss, tier, reprint != 0, results, &info);
+        put_json(out_json, info);
+        return SPK_OK;
+    });
+    if (st != SPK_OK)
+        for (uint32_t i = 0; i < n; ++i) release_result(&results[i]);
+    return st;
 }
 
 }  // extern "C"

@@ -273,7 +273,20 @@ IirCoefs blur_iir_coefs(const double sigma[3], const bool iir[3]) {
     return iir_coefs(Vec3{sigma[0], sigma[1], sigma[2]}, iir);
 }
 
+namespace {
+bool iir_mixture_mix(RenderCtx& ctx, const Plane& raw, const std::vector<MixtureComponent>& comps, const Vec3& a,
+                     const Vec3& b, bool adjoint = false);
+}  // namespace
+
 void gaussian(RenderCtx& ctx, const Plane& in, const Plane& dst, const Vec3& sigma) {
+    // one recursive sigma on every channel: the block-parallel kernels, as a one-component mixture
+    // dst := 0 dst + 1 G(dst) (the same recurrence as the line kernels, evaluated by segments)
+    if (sigma[0] == sigma[1] && sigma[1] == sigma[2] && blur_branch(sigma[0]) == Branch::Iir &&
+        dev::iir_mixture_fits(in.w, in.h)) {
+        if (!same(in, dst)) dev::copy(in.data(), dst.data(), in.pixels(), ctx.stream);
+        const std::vector<MixtureComponent> one{MixtureComponent{Vec3{1.0, 1.0, 1.0}, sigma}};
+        if (iir_mixture_mix(ctx, dst, one, Vec3{0.0, 0.0, 0.0}, Vec3{1.0, 1.0, 1.0})) return;
+    }
     encode_blur(ctx, in, dst, sigma, Fuse{});
 }
 
@@ -332,7 +345,7 @@ void fill_launch(dev::IirLaunch& q, const std::vector<MixtureComponent>& comps, 
 // raw := a raw + b M(raw) with the block-parallel recursive kernels, when every channel of every
 // component is on the recursive branch and the lines fit in shared memory; false otherwise.
 bool iir_mixture_mix(RenderCtx& ctx, const Plane& raw, const std::vector<MixtureComponent>& comps, const Vec3& a,
-                     const Vec3& b, bool adjoint = false) {
+                     const Vec3& b, bool adjoint) {
     if (comps.empty() || comps.size() > SPKB_MAX_COMPONENTS) return false;
     for (const MixtureComponent& m : comps)
         for (int c = 0; c < 3; ++c)
@@ -548,10 +561,8 @@ Plane develop(RenderCtx& ctx, const Pipeline& p, const Plane& source, uint32_t f
     return neg;
 }
 
-void print_scan_encode(RenderCtx& ctx, const Pipeline& p, const LiveParams& live, const Plane& negative,
-                       OutputImage* img) {
+PrintArgs print_args(const Pipeline& p, const LiveParams& live, uint32_t pixels) {
     const PrintSetup& s = *p.print;
-    const uint32_t w = negative.w, h = negative.h;
     const PrintRun r = compute_run(s, live);
     PrintArgs a{};
     a.enl = spectral_pairs(r.enl32);
@@ -568,46 +579,65 @@ void print_scan_encode(RenderCtx& ctx, const Pipeline& p, const LiveParams& live
     std::memcpy(a.to_rgb, s.to_rgb, sizeof a.to_rgb);
     a.cam = s.cam_args;
     a.cmax = p.dev.cmax.as<float>();
-    a.n = uint32_t(negative.pixels());
+    a.n = pixels;
+    return a;
+}
+
+namespace {
+EncodeArgs encode_args(const PrintSetup& s, uint32_t stride_px) {
+    EncodeArgs e{};
+    std::memcpy(e.m_nid, s.m_nid, sizeof e.m_nid);
+    e.cctf_active = s.cctf ? 1 : 0;
+    e.cctf_mode = s.cctf_mode;
+    e.stride = stride_px;
+    return e;
+}
+}  // namespace
+
+bool scan_args(const Pipeline& p, double rho_tier, uint32_t w, uint32_t h, uint32_t stride_px, ScanArgs& sa) {
+    const PrintSetup& s = *p.print;
+    const double sb = s.scanner_lens_blur_px;
+    const double su = s.unsharp_sigma_full * rho_tier;
+    const double am = s.unsharp_amount;
+    const bool unsharp = su > 0.0 && am > 0.0;
+    const Branch bb = blur_branch(sb), bu = unsharp ? blur_branch(su) : Branch::Identity;
+    if (bb == Branch::Iir || bu == Branch::Iir) return false;
+    const bool no_iir[3] = {false, false, false};
+    const FirTaps t1 = fir_taps(Vec3{sb, sb, sb}, no_iir);
+    const FirTaps t2 = fir_taps(Vec3{su, su, su}, no_iir);
+    sa = ScanArgs{};
+    sa.r1 = t1.r;
+    std::memcpy(sa.t1, t1.taps[0], sizeof sa.t1);
+    sa.r2 = unsharp ? t2.r : 0;
+    if (unsharp) std::memcpy(sa.t2, t2.taps[0], sizeof sa.t2);
+    if (sa.r1 == 0) sa.t1[0] = 1.0f;
+    if (sa.r2 == 0) sa.t2[0] = 1.0f;
+    if (!dev::scan_encode_fits(w, h, sa.r1, sa.r2)) return false;
+    sa.e = encode_args(s, stride_px);
+    sa.e.unsharp = unsharp ? 1 : 0;
+    sa.e.lincomb_a = f32(1.0 + am);
+    sa.e.lincomb_b = f32(-am);
+    return true;
+}
+
+void print_scan_encode(RenderCtx& ctx, const Pipeline& p, const LiveParams& live, const Plane& negative,
+                       OutputImage* img) {
+    const PrintSetup& s = *p.print;
+    const uint32_t w = negative.w, h = negative.h;
+    const PrintArgs a = print_args(p, live, uint32_t(negative.pixels()));
     Plane rgb = make_plane(ctx.pool, w, h);
     {
         Stage st(ctx, "print");
         dev::print(negative.data(), rgb.data(), a, ctx.stream);
     }
-    EncodeArgs e{};
-    std::memcpy(e.m_nid, s.m_nid, sizeof e.m_nid);
-    e.cctf_active = s.cctf ? 1 : 0;
-    e.cctf_mode = s.cctf_mode;
-    e.stride = img->stride_px;
-    {
+    ScanArgs sa;
+    if (scan_args(p, ctx.rho_tier, w, h, img->stride_px, sa)) {
         // the scanner's blurs on the FIR branch: one tiled pass from the print output to RGBA16
-        const double sb = s.scanner_lens_blur_px;
-        const double su = s.unsharp_sigma_full * ctx.rho_tier;
-        const double am = s.unsharp_amount;
-        const bool unsharp = su > 0.0 && am > 0.0;
-        const Branch bb = blur_branch(sb), bu = unsharp ? blur_branch(su) : Branch::Identity;
-        const bool no_iir[3] = {false, false, false};
-        ScanArgs sa{};
-        if (bb != Branch::Iir && bu != Branch::Iir) {
-            const FirTaps t1 = fir_taps(Vec3{sb, sb, sb}, no_iir);
-            const FirTaps t2 = fir_taps(Vec3{su, su, su}, no_iir);
-            sa.r1 = t1.r;
-            std::memcpy(sa.t1, t1.taps[0], sizeof sa.t1);
-            sa.r2 = unsharp ? t2.r : 0;
-            if (unsharp) std::memcpy(sa.t2, t2.taps[0], sizeof sa.t2);
-            if (sa.r1 == 0) sa.t1[0] = 1.0f;
-            if (sa.r2 == 0) sa.t2[0] = 1.0f;
-        }
-        if (bb != Branch::Iir && bu != Branch::Iir && dev::scan_encode_fits(w, h, sa.r1, sa.r2)) {
-            sa.e = e;
-            sa.e.unsharp = unsharp ? 1 : 0;
-            sa.e.lincomb_a = f32(1.0 + am);
-            sa.e.lincomb_b = f32(-am);
-            Stage st(ctx, "scanner");
-            dev::scan_encode(rgb.data(), img->dev, w, h, sa, ctx.stream);
-            return;
-        }
+        Stage st(ctx, "scanner");
+        dev::scan_encode(rgb.data(), img->dev, w, h, sa, ctx.stream);
+        return;
     }
+    EncodeArgs e = encode_args(s, img->stride_px);
     Plane gpl;
     {
         Stage st(ctx, "scanner");

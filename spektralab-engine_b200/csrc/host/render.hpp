@@ -64,6 +64,12 @@ struct Timer : dev::LaunchHook {
 Plane develop(RenderCtx& ctx, const Pipeline& p, const Plane& source, uint32_t film_seed,
               const std::optional<HalationOverride>& hov, float* counts_out = nullptr);
 
+// The print kernel's arguments for a negative of `pixels` pixels at the live parameters.
+PrintArgs print_args(const Pipeline& p, const LiveParams& live, uint32_t pixels);
+// The fused scanner kernel's arguments for a w x h frame written with row pitch stride_px; false when the
+// frame or the scanner's blurs need the separate passes (a recursive blur, a frame narrower than the halo).
+bool scan_args(const Pipeline& p, double rho_tier, uint32_t w, uint32_t h, uint32_t stride_px, ScanArgs& out);
+
 // print side: negative -> RGBA16 into img->dev (row pitch img->stride_px); no host copy
 void print_scan_encode(RenderCtx& ctx, const Pipeline& p, const LiveParams& live, const Plane& negative,
                        OutputImage* img);

@@ -36,7 +36,6 @@ struct IirCoefs {
 // Accumulation of a blur's last pass: out = v, out = 0 + w v, or out = acc + w v.
 enum AccMode { ACC_NONE = 0, ACC_ZERO = 1, ACC_PLANE = 2 };
 
-// Film-side point work after halation: log10 exposure, density curves, grain draw.
 // Direct index into an ascending binary32 axis x[0..K-1]: g(v) = clamp(int((v - x0) s), 0, K - 2). The
 // host sets `active` only after checking that g is within one of the bisection's interval for every v
 // in (x[0], x[K-1]); the kernel then corrects g by one comparison on each side. Inactive: bisection.
@@ -45,6 +44,7 @@ struct AxisGrid {
     int32_t active;
 };
 
+// Film-side point work after halation: log10 exposure, density curves, grain draw.
 struct DevelopArgs {
     // curves: x[K], inv[K], y[3K] (channel-major)
     const float* cx;
@@ -109,7 +109,7 @@ struct Cam16Args {
 };
 
 // The print kernel: negative density -> linear output RGB.
-struct PrintArgs {
+struct alignas(16) PrintArgs {
     SpectralPairs enl;
     SpectralPairs scan;
     float g[3], o[3];
@@ -143,4 +143,20 @@ struct ScanArgs {
     int32_t r2;                              // unsharp blur radius (0 when unsharp is off)
     float t2[2 * SPKB_FIR_MAX_R + 1];
     EncodeArgs e;
+};
+
+// One frame of a batched print launch (k_print_batch): its arguments and planes.
+struct alignas(16) BatchPrintFrame {
+    PrintArgs args;
+    const float* neg;
+    float* rgb;
+};
+
+// One frame of a batched scanner launch (k_scan_encode_batch): its tiles are first_tile ..
+// first_tile + tiles_x * tiles_y - 1 of the launch's tile list.
+struct BatchScanFrame {
+    ScanArgs args;
+    const float* rgb;
+    uint16_t* out;
+    uint32_t w, h, tiles_x, first_tile;
 };

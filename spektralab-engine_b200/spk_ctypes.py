@@ -101,6 +101,8 @@ EXT = {
     "spkx_setup_json": (I32, [C, C, ctypes.c_double, PS]),
     "spkx_session_develop_debug": (I32, [P, C, U32, FP, FP]),
     "spk_render_vjp": (I32, [P, C, U32, FP, FP, DP, U32, FP]),
+    "spkx_render_batch": (I32, [ctypes.POINTER(P), U32, C, I32, ctypes.POINTER(SpkResult), PS]),
+    "spkx_engine_batch_plan": (I32, [P, C]),
 }
 
 REF_EXT = {
@@ -189,6 +191,27 @@ class Engine:
         if not s:
             raise SpkError(-2, self.L.last_error())
         return Session(self, s, self.L.take_json(out), (h, w))
+
+    def batch_plan(self, plan=None):
+        """Pins the plan of later render_batch calls (None: timed choice)."""
+        self.L.check(self.L.lib.spkx_engine_batch_plan(self.h, plan.encode() if plan else None))
+
+    def render_batch(self, sessions, tier="full", reprint=False):
+        """spkx_render_batch over Session objects of this engine: ([Result, ...], info dict). Each Result owns
+        its spk_result until .free()."""
+        n = len(sessions)
+        hs = (P * max(n, 1))(*[s.h for s in sessions])
+        rs = (SpkResult * max(n, 1))()
+        out = ctypes.c_char_p()
+        self.L.check(self.L.lib.spkx_render_batch(hs, n, tier.encode() if tier is not None else None, int(reprint),
+                                                  rs, ctypes.byref(out)))
+        info = self.L.take_json(out)
+        results = []
+        for i in range(n):
+            r = SpkResult()
+            ctypes.memmove(ctypes.byref(r), ctypes.byref(rs[i]), ctypes.sizeof(SpkResult))
+            results.append(Result(self.L, r))
+        return results, info
 
 
 class Result:
