@@ -314,6 +314,112 @@ def run_vjp(args):
     return 0
 
 
+PREC_W, PREC_H = 6144, 4096
+PREC_SEED = 0
+PREC_MODES = ("fp32", "tf32", "bf16", "bf16x3", "fp64")
+
+
+def tensor_flops_per_px(mode, bins):
+    """Tensor-core FLOPs the spectral-mode kernel issues per pixel (both integrals): M x N x K MMAs with
+    N = 16 and K the wavelengths padded to 32, twice for the BF16 hi + lo split of the A operand."""
+    if mode not in ("tf32", "bf16", "bf16x3"):
+        return 0
+    k = (bins + 31) // 32 * 32
+    return 2 * 2 * 16 * k * (2 if mode == "bf16x3" else 1)
+
+
+def run_precision(args):
+    """The print's spectral integrals in each arithmetic on a 6144 x 4096 frame of dye densities (uniform
+    in [0, 3], seed 0), at 81 (5 nm) and 401 (1 nm) wavelengths. Per mode: the print kernel's device time
+    (CUDA events around its launch, inputs resident on the device, L2 flushed before each call) and the
+    error against the same print with both integrals in binary64 (mode fp64): the enlarger integral's
+    max and mean over pixels of max_k |R - R64| / max_k |R64|, and the 16-bit output after the scan
+    (LSB16). fp32 at 81 wavelengths is the binary32 print kernel, its integral taken from the
+    spectral-mode kernel's binary32 path (the same operations); at 401 it is that path."""
+    import torch
+
+    resources = synth_resources.ensure(sc.RESOURCES)
+    lib = sc.load()
+    eng = lib.engine(resources, device=0)
+    torch.cuda.set_device(0)
+    w = args.width if args.width != 3840 else PREC_W
+    h = args.height if args.height != 2160 else PREC_H
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(PREC_SEED)
+    neg = torch.rand((h, w, 3), generator=gen, device="cuda", dtype=torch.float32) * 3.0
+    stride = (w + 31) // 32 * 32
+    out = torch.empty((h, stride, 4), dtype=torch.int16, device="cuda")
+    ref_out = torch.empty_like(out)
+    scratch = torch.empty_like(out)
+    con = torch.empty((h, w, 3), dtype=torch.float32, device="cuda")
+    ref_con = torch.empty_like(con)
+    flush = torch.empty(64 << 20, dtype=torch.int32, device="cuda")
+    mpx = w * h / 1e6
+    s = eng.open(sc.synthetic_image(64, 48, 5), dict(BASE, grain_active=False))
+
+    def run(mode, bins, contraction, rgba):
+        s.set_print_mode(mode, bins)
+        return s.print_negative(neg.data_ptr(), w, h, rgba.data_ptr(), stride,
+                                contraction.data_ptr() if contraction is not None else None)
+
+    def errors(R, rgba):
+        R64 = ref_con.double()
+        rel = (R.double() - R64).abs().amax(-1) / R64.abs().amax(-1)
+        d = ((rgba[:, :w, :3].int() & 0xFFFF) - (ref_out[:, :w, :3].int() & 0xFFFF)).abs()
+        return {"integral_rel_max": float(rel.max()), "integral_rel_mean": float(rel.mean()),
+                "lsb16_max": int(d.max()), "lsb16_mean": float(d.float().mean()),
+                "lsb16_frac_gt1": float((d > 1).float().mean())}
+
+    table = {}
+    with Clocks(0) as clk:
+        for bins in (81, 401):
+            run("fp64", bins, ref_con, ref_out)
+            for mode in PREC_MODES:
+                times = []
+                for k in range(args.warmup + args.steps):
+                    flush.fill_(k)
+                    ms = run(mode, bins, None, out)
+                    if k >= args.warmup:
+                        times.append(ms)
+                row = {"print_ms": statistics.median(times)}
+                row["mpx_s"] = mpx / (row["print_ms"] / 1000.0)
+                tf = tensor_flops_per_px(mode, bins) * w * h
+                if tf:
+                    row["tensor_tflops_issued"] = tf / (row["print_ms"] / 1000.0) / 1e12
+                if mode != "fp64":
+                    if mode == "fp32" and bins == 81:
+                        run("fp32_generic", bins, con, scratch)
+                    else:
+                        run(mode, bins, con, out)
+                    row.update(errors(con, out))
+                table[f"{mode}@{bins}"] = row
+    s.close()
+    eng.close()
+    torch.cuda.synchronize()
+    head = table["bf16x3@81"]
+    try:
+        with open(MEASURED_PEAKS) as f:
+            tpeak, tkind = float(json.load(f)["bf16_tflops"]), "measured (MEASURED_PEAKS bf16_tflops)"
+    except (OSError, KeyError, ValueError):
+        tpeak, tkind = 1590.0, "fallback"
+    line = {"metric": "print Mpx/s, split-BF16 tensor cores, 81 wavelengths", "value": head["mpx_s"],
+            "unit": "Mpx/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": head["print_ms"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "bf16x3", "data": "synthetic",
+            "config": {"workload": f"print spectral integrals, {w}x{h} dye densities uniform [0, 3] (seed 0), "
+                                   "81 and 401 wavelengths", "width": w, "height": h,
+                       "l2": "flushed (256 MiB write) before each call"},
+            "modes": table,
+            "roofline": {"bound": "tensor", "achieved": head["tensor_tflops_issued"], "peak": tpeak,
+                         "unit": "TFLOP/s", "frac": head["tensor_tflops_issued"] / tpeak, "traffic": None,
+                         "kernel": "print_spectral (bf16x3)", "peak_source": tkind,
+                         "note": "tensor FLOPs issued (N padded to 16, K to 32); the kernel is bound by "
+                                 "the exponentials and operand splits on the CUDA cores"},
+            "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 BATCH_FRAMES = 64
 BATCH_SEED = 3
 
@@ -429,9 +535,11 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg (profiling runs)")
     ap.add_argument("--width", type=int, default=3840, help="frame width (the benchmark workload is 3840)")
     ap.add_argument("--height", type=int, default=2160, help="frame height (the benchmark workload is 2160)")
-    ap.add_argument("--config", default="render", choices=["render", "vjp", "batch"],
+    ap.add_argument("--config", default="render", choices=["render", "vjp", "batch", "precision"],
                     help="render: the 4K render + reprint (the headline); vjp: the render's adjoint on 1024x1024; "
-                         "batch: 64 frames of mixed sizes, batched against per-frame calls")
+                         "batch: 64 frames of mixed sizes, batched against per-frame calls; precision: the "
+                         "print's spectral integrals in fp32 / tf32 / bf16 / split bf16 against binary64 on "
+                         "6144x4096 densities")
     args = ap.parse_args()
     global W, H
     W, H = args.width, args.height
@@ -442,6 +550,8 @@ def main():
         return run_vjp(args)
     if args.config == "batch":
         return run_batch(args)
+    if args.config == "precision":
+        return run_precision(args)
 
     rank, local, world, pg = dist_init(args.gpus)
     resources = synth_resources.ensure(sc.RESOURCES)

@@ -103,6 +103,31 @@ SPK_API spk_status spkx_render_batch(spk_session* const* sessions, uint32_t n, c
  */
 SPK_API spk_status spkx_engine_batch_plan(spk_engine* engine, const char* plan);
 
+/* ---- the print's spectral integrals on the tensor cores (no counterpart in the reference engine) ----
+ *
+ * spkx_session_set_print_mode(session, mode, bins)
+ *   selects the arithmetic of the print's two spectral integrals (enlarger and scan, reference
+ *   kernels/print.metal:165-189) for the session's later renders, reprints and spkx_print_negative calls:
+ *     "fp32"          the binary32 print kernel (the default; at 401 wavelengths the spectral-mode kernel's
+ *                     binary32 path, which performs the same operations)
+ *     "fp32_generic"  the spectral-mode kernel's binary32 path (at 81 wavelengths equal to "fp32" bit for bit)
+ *     "fp64"          both integrals in binary64 from the binary64 set-up tables
+ *     "tf32", "bf16"  the sums over wavelengths on the tensor cores (tcgen05), binary32 accumulation
+ *     "bf16x3"        the same with BF16 hi + lo splits of both operands (all four products)
+ *   bins: 81 (the resources' 5 nm grid) or 401 (1 nm, the binary64 tables interpolated linearly).
+ *   The stages around the integrals stay binary32. SPK_ERR_INVALID_ARG for another mode or bins.
+ *
+ * spkx_print_negative(session, negative, width, height, rgba16, row_stride_px, contraction, print_ms)
+ *   the print side of a render (print, scanner, output encode) of a given negative with the session's
+ *   parameters and print mode. negative: device memory, width x height x 3 floats (dye densities);
+ *   rgba16: device memory, row pitch row_stride_px pixels; contraction (device, may be NULL; spectral-mode
+ *   kernels only) receives the enlarger integral R_k of every pixel (3 floats); print_ms (host, may be
+ *   NULL) receives the device time of the print kernel. Synchronous on the session's stream.
+ */
+SPK_API spk_status spkx_session_set_print_mode(spk_session* session, const char* mode, uint32_t bins);
+SPK_API spk_status spkx_print_negative(spk_session* session, const float* negative, uint32_t width, uint32_t height,
+                                       uint16_t* rgba16, uint32_t row_stride_px, float* contraction, double* print_ms);
+
 /* ---- the render's adjoint (no counterpart in the reference engine) ----
  *
  * spk_render_vjp(session, tier, film_seed, grad_output, grad_input, grad_params, n_params, output)

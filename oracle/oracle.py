@@ -61,6 +61,7 @@ def lib():
         L.orc_print.argtypes = [ctypes.POINTER(OracleSetup), PD, I32, I32, U16, PD]
         L.orc_render_linear.argtypes = [ctypes.POINTER(OracleSetup), PD, I32, I32, FP, PD]
         L.orc_gaussian.argtypes = [PD, PD, I32, I32, PD]
+        L.orc_spectral.argtypes = [PD, PD, PD, I32, PD, ctypes.c_int64, PD]
         L.orc_gaussian.restype = None
         L.orc_poisson.argtypes = [FP, FP, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32]
         L.orc_poisson.restype = None
@@ -213,6 +214,19 @@ class Oracle:
         lib().orc_print(ctypes.byref(self.s), neg.ctypes.data_as(PD), w, h,
                         out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint16)), lin.ctypes.data_as(PD))
         return out, lin
+
+
+def spectral(eps, beta, wt, densities):
+    """The print's spectral integral in binary64 (orc_spectral): eps (nl, 3), beta (nl,), wt (nl, 3),
+    densities (..., 3) -> (..., 3)."""
+    eps = np.ascontiguousarray(eps, np.float64)
+    beta = np.ascontiguousarray(beta, np.float64)
+    wt = np.ascontiguousarray(wt, np.float64)
+    d = np.ascontiguousarray(densities, np.float64)
+    out = np.zeros(d.shape, np.float64)
+    lib().orc_spectral(eps.ctypes.data_as(PD), beta.ctypes.data_as(PD), wt.ctypes.data_as(PD), len(beta),
+                       d.ctypes.data_as(PD), d.size // 3, out.ctypes.data_as(PD))
+    return out
 
 
 def gaussian(plane, sigma3):

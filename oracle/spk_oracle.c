@@ -286,13 +286,23 @@ int orc_develop(const OracleSetup* s, const float* rgb, int32_t w, int32_t h, co
 
 /* ---- print (reference kernels/print.metal:29-127, :165-317) -------------------------------------- */
 
-static void spectral(const double* eps, const double* beta, const double* wt, const double d[3], double r[3]) {
+static void spectral_n(const double* eps, const double* beta, const double* wt, int32_t nl, const double d[3],
+                       double r[3]) {
     r[0] = r[1] = r[2] = 0.0;
-    for (int l = 0; l < 81; ++l) {
+    for (int32_t l = 0; l < nl; ++l) {
         const double D = ((d[0] * eps[3 * l] + d[1] * eps[3 * l + 1]) + d[2] * eps[3 * l + 2]) + beta[l];
         const double T = pow(10.0, -D);
         for (int k = 0; k < 3; ++k) r[k] += T * wt[3 * l + k];
     }
+}
+
+static void spectral(const double* eps, const double* beta, const double* wt, const double d[3], double r[3]) {
+    spectral_n(eps, beta, wt, 81, d, r);
+}
+
+void orc_spectral(const double* eps, const double* beta, const double* wt, int32_t nl, const double* d, int64_t n,
+                  double* out) {
+    for (int64_t p = 0; p < n; ++p) spectral_n(eps, beta, wt, nl, d + 3 * p, out + 3 * p);
 }
 
 static double paper(const OracleSetup* s, int c, double v) {

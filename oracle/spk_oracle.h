@@ -79,6 +79,11 @@ int orc_print(const OracleSetup* s, const double* negative, int32_t w, int32_t h
 int orc_render_linear(const OracleSetup* s, const double* rgb, int32_t w, int32_t h, const float* counts,
                       double* out_linear);
 
+/* The print's spectral integral (reference kernels/print.metal:165-189) at nl wavelengths for n pixels:
+ * out[p][k] = sum_l 10^-(sum_c d[p][c] eps[l][c] + beta[l]) wt[l][k], binary64, ascending l. */
+void orc_spectral(const double* eps, const double* beta, const double* wt, int32_t nl, const double* d, int64_t n,
+                  double* out);
+
 /* The Gaussian of a w x h x 3 plane, per-channel sigma in pixels, in binary64 with the engine's
  * branch rule (FIR below 3, Young-van Vliet above) */
 void orc_gaussian(const double* in, double* out, int32_t w, int32_t h, const double sigma[3]);

@@ -57,6 +57,14 @@ void develop(const float* exposure, float* out, const DevelopArgs& a, uint32_t w
 // negative density -> linear output RGB (enlarger, gain, paper, scan, XYZ -> RGB, CAM16 gamut).
 void print(const float* neg, float* rgb, const PrintArgs& a, cudaStream_t s);
 
+// The print stage with the spectral integrals in the given SpectralMode (print_tc.cu): host_tab the
+// tables on the host (their binary32 part goes into the kernel's parameters), tab the same in device
+// memory; host_tab.nl_pad must be 96 or SPKB_NL_MAX. contraction (may be null) receives the enlarger
+// integral R_k of every pixel (3 floats). *err (device) is or-ed with 1 when a tensor-core wait gave up.
+void print_spectral(const PrintArgs& a, const SpectralTablesN& host_tab, const SpectralTablesN* tab, int mode,
+                    const float* neg, float* rgb, uint32_t n, float* contraction, uint32_t* err, cudaStream_t s);
+bool print_spectral_supported(uint32_t nl_pad);
+
 // (optional unsharp combine with g) -> transfer function -> RGBA16 with row pitch e.stride.
 void encode(const float* rgb, const float* g, uint16_t* out, uint32_t w, uint32_t h, const EncodeArgs& e,
             cudaStream_t s);

@@ -142,6 +142,8 @@ public:
     SeedSequence seeds;
     TierState tiers[3];
     std::optional<HalationOverride> hal;
+    int print_mode = -1;  // spkx_session_set_print_mode: -1 the binary32 print kernel, else a SpectralMode
+    uint32_t print_bins = SPKB_NL;
     std::atomic<bool> cancel{false};
     std::string progress_id;
     std::atomic<uint32_t> nodes_done{0};
@@ -386,6 +388,8 @@ void render(Session& s, const char* tier_name, bool reprint, spk_result* out) {
         s.check_tier(*t);  // a tier this build cannot make is a render failure (SPK_ERR_GPU), as in the reference
         RenderCtx ctx{s.pool, s.stream};
         ctx.rho_tier = 1.0;
+        ctx.print_mode = s.print_mode;
+        ctx.print_bins = s.print_bins;
         if (!reuse) {
             developed = true;
             develop_tier(s, *t, ctx);
@@ -686,6 +690,8 @@ void render_batch(std::vector<Session*> ss, const char* tier_name, bool reprint,
             s.check_tier(*t);
             RenderCtx ctx{s.pool, s.stream};
             ctx.rho_tier = 1.0;
+            ctx.print_mode = s.print_mode;
+            ctx.print_bins = s.print_bins;
             if (!f.reused) {
                 f.developed = true;
                 develop_tier(s, *t, ctx);
@@ -694,7 +700,8 @@ void render_batch(std::vector<Session*> ss, const char* tier_name, bool reprint,
             s.node();
             f.img = output_acquire(e.device, s.source.w, s.source.h);
             f.neg = ts.negative.data();
-            f.fused = scan_args(s.pipe, ctx.rho_tier, s.source.w, s.source.h, f.img->stride_px, f.sa);
+            // a session on the spectral-mode print kernel stays on its own stream
+            f.fused = s.print_mode < 0 && scan_args(s.pipe, ctx.rho_tier, s.source.w, s.source.h, f.img->stride_px, f.sa);
             if (f.fused) {
                 f.pa = print_args(s.pipe, s.live, uint32_t(ts.negative.pixels()));
                 f.rgb = make_plane(s.pool, s.source.w, s.source.h);
@@ -838,6 +845,8 @@ std::string session_profile(Session& s, const char* tier_name, bool reprint, uin
             dev::set_launch_hook(&timer);
             RenderCtx ctx{s.pool, s.stream};
             ctx.timer = &timer;
+            ctx.print_mode = s.print_mode;
+            ctx.print_bins = s.print_bins;
             cudaEventRecord(a, s.stream);
             if (!reprint || !ts.negative) {
                 ctx.pitch_um = s.pitch_um();
@@ -1216,6 +1225,78 @@ SPK_API spk_status spkx_session_negative(spk_session* session, const char* tier,
         cuda_check(cudaMemcpyAsync(out, ts.negative.data(), ts.negative.bytes(), cudaMemcpyDeviceToHost, s.stream),
                    "negative copy");
         cuda_check(cudaStreamSynchronize(s.stream), "negative copy");
+        return SPK_OK;
+    });
+}
+
+SPK_API spk_status spkx_session_set_print_mode(spk_session* session, const char* mode, uint32_t bins) {
+    last_error::clear();
+    if (!session || !mode) return invalid("a required pointer is NULL");
+    const std::string m(mode);
+    int code = -2;
+    if (m == "fp32") code = -1;
+    if (m == "fp32_generic") code = SPKB_SPEC_F32;
+    if (m == "fp64") code = SPKB_SPEC_F64;
+    if (m == "tf32") code = SPKB_SPEC_TF32;
+    if (m == "bf16") code = SPKB_SPEC_BF16;
+    if (m == "bf16x3") code = SPKB_SPEC_BF16X3;
+    if (code == -2) return invalid("print mode must be fp32, fp32_generic, fp64, tf32, bf16 or bf16x3");
+    if (bins != SPKB_NL && bins != 401) return invalid("print wavelengths must be 81 or 401");
+    if (code == -1 && bins != SPKB_NL) code = SPKB_SPEC_F32;  // the binary32 print kernel holds 81 wavelengths
+    return guarded([&] {
+        Session& s = *S(session);
+        std::lock_guard<std::mutex> lock(s.m);
+        s.print_mode = code;
+        s.print_bins = bins;
+        return SPK_OK;
+    });
+}
+
+SPK_API spk_status spkx_print_negative(spk_session* session, const float* negative, uint32_t width, uint32_t height,
+                                       uint16_t* rgba16, uint32_t row_stride_px, float* contraction, double* print_ms) {
+    last_error::clear();
+    if (!session || !negative || !rgba16) return invalid("a required pointer is NULL");
+    if (width == 0 || height == 0 || uint64_t(width) * height > kMaxPixels) return invalid("frame size out of range");
+    if (row_stride_px < width) return invalid("row_stride_px is below the width");
+    return guarded([&] {
+        Session& s = *S(session);
+        std::lock_guard<std::mutex> lock(s.m);
+        if (contraction && s.print_mode < 0)
+            fail_invalid("the enlarger integral is written by the spectral-mode print kernel only");
+        DeviceGuard dg(s.engine->device);
+        Plane neg = make_plane(s.pool, width, height);
+        cuda_check(cudaMemcpyAsync(neg.data(), negative, neg.bytes(), cudaMemcpyDeviceToDevice, s.stream), "negative");
+        OutputImage img{};
+        img.dev = rgba16;
+        img.width = width;
+        img.height = height;
+        img.stride_px = row_stride_px;
+        img.device = s.engine->device;
+        RenderCtx ctx{s.pool, s.stream};
+        ctx.print_mode = s.print_mode;
+        ctx.print_bins = s.print_bins;
+        ctx.contraction_out = contraction;
+        Timer timer;
+        struct HookGuard {
+            ~HookGuard() { dev::set_launch_hook(nullptr); }
+        } hook_guard;
+        if (print_ms) {
+            ctx.timer = &timer;
+            dev::set_launch_hook(&timer);
+        }
+        print_scan_encode(ctx, s.pipe, s.live, neg, &img);
+        cuda_check(cudaStreamSynchronize(s.stream), "print");
+        cuda_check(cudaGetLastError(), "print");
+        if (print_ms) {
+            *print_ms = 0.0;
+            for (const Timer::Mark& k : timer.kernels) {
+                const std::string name(k.name);
+                if (name != "print" && name != "print_spectral") continue;
+                float ms = 0.0f;
+                cuda_check(cudaEventElapsedTime(&ms, k.a, k.b), "print timing");
+                *print_ms += ms;
+            }
+        }
         return SPK_OK;
     });
 }

@@ -1,7 +1,9 @@
 #include "render.hpp"
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <memory>
 
 #include "../cuda/iir.hpp"
 #include "../cuda/launch.hpp"
@@ -561,6 +563,80 @@ Plane develop(RenderCtx& ctx, const Pipeline& p, const Plane& source, uint32_t f
     return neg;
 }
 
+namespace {
+uint16_t bf16_rn(float x) {
+    uint32_t u;
+    std::memcpy(&u, &x, 4);
+    u += 0x7FFFu + ((u >> 16) & 1u);
+    return uint16_t(u >> 16);
+}
+float bf16_value(uint16_t h) {
+    const uint32_t u = uint32_t(h) << 16;
+    float f;
+    std::memcpy(&f, &u, 4);
+    return f;
+}
+
+// One integral of the spectral-mode kernel from its binary64 tables at the resources' 81 wavelengths
+// (eps [l][c], beta [l], wt [l][k]) and their binary32 narrowings t32. At 81 wavelengths the binary32
+// values are the print kernel's (spectral_pairs); at 1 nm the binary64 tables are interpolated linearly and
+// a bin's weight is a fifth of a 5 nm bin's, so that the sum approximates the same integral.
+void fill_spectral_pass(SpectralTablesN& t, uint32_t pass, const double* eps64, const double* beta64,
+                        const double* wt64, const SpectralTables& t32) {
+    constexpr double kNegLog2Of10 = -3.32192809488736234787;
+    const uint32_t nl = t.nl, np = t.nl_pad;
+    const double step = double(SPKB_NL - 1) / double(nl - 1);
+    for (uint32_t l = 0; l < nl; ++l) {
+        double eps[3], wt[3], beta;
+        float e32[3], w32[3];
+        if (nl == SPKB_NL) {
+            beta = beta64[l];
+            for (int c = 0; c < 3; ++c) {
+                eps[c] = eps64[3 * l + c];
+                wt[c] = wt64[3 * l + c];
+                e32[c] = f32(double(t32.eps[3 * l + c]) * kNegLog2Of10);
+                w32[c] = f32(double(t32.wt[3 * l + c]) * std::pow(10.0, -double(t32.beta[l])));
+            }
+        } else {
+            const double x = double(l) * step;
+            const uint32_t i = std::min(uint32_t(x), uint32_t(SPKB_NL - 2));
+            const double f = x - double(i);
+            beta = (1.0 - f) * beta64[i] + f * beta64[i + 1];
+            for (int c = 0; c < 3; ++c) {
+                eps[c] = (1.0 - f) * eps64[3 * i + c] + f * eps64[3 * (i + 1) + c];
+                wt[c] = ((1.0 - f) * wt64[3 * i + c] + f * wt64[3 * (i + 1) + c]) * step;
+                e32[c] = f32(eps[c] * kNegLog2Of10);
+                w32[c] = f32(wt[c] * std::pow(10.0, -beta));
+            }
+        }
+        for (uint32_t c = 0; c < 3; ++c) {
+            t.e64[pass][l][c] = eps[c] * kNegLog2Of10;
+            t.w64[pass][l][c] = wt[c] * std::pow(10.0, -beta);
+            t.e_pairs[pass][l / 2][2 * c + (l & 1)] = e32[c];
+            t.w[pass][l][c] = w32[c];
+            const uint16_t hi = bf16_rn(w32[c]);
+            const uint16_t lo = bf16_rn(w32[c] - bf16_value(hi));
+            auto at = [&](uint32_t n, uint32_t bytes) {  // element index of (n, l) in the B tile
+                const uint32_t b = ((n / 8) * (np * bytes / 16) + (l * bytes) / 16) * 128 + (n % 8) * 16 + (l * bytes) % 16;
+                return b / bytes;
+            };
+            t.b_bf16[pass][at(c, 2)] = hi;
+            t.b_bf16[pass][at(3 + c, 2)] = lo;
+            t.b_tf32[pass][at(c, 4)] = w32[c];
+        }
+    }
+}
+}  // namespace
+
+void spectral_tables_n(const PrintSetup& s, const PrintRun& r, uint32_t bins, SpectralTablesN& t) {
+    if (bins != SPKB_NL && bins != 401) fail_invalid("spectral print: 81 or 401 wavelengths");
+    std::memset(&t, 0, sizeof t);
+    t.nl = bins;
+    t.nl_pad = (bins + 31) / 32 * 32;
+    fill_spectral_pass(t, 0, r.eps_n.data(), r.beta_n.data(), r.w_n.data(), r.enl32);
+    fill_spectral_pass(t, 1, s.scan_eps.data(), s.scan_beta.data(), s.scan_wt.data(), s.scan32);
+}
+
 PrintArgs print_args(const Pipeline& p, const LiveParams& live, uint32_t pixels) {
     const PrintSetup& s = *p.print;
     const PrintRun r = compute_run(s, live);
@@ -620,15 +696,43 @@ bool scan_args(const Pipeline& p, double rho_tier, uint32_t w, uint32_t h, uint3
     return true;
 }
 
+namespace {
+// negative -> linear output RGB by the binary32 print kernel, or by the spectral-mode kernel when the
+// context asks for one (its tables and arguments uploaded for the call, its wait status read back)
+void print_stage(RenderCtx& ctx, const Pipeline& p, const LiveParams& live, const Plane& negative, const Plane& rgb) {
+    const uint32_t n = uint32_t(negative.pixels());
+    const PrintArgs a = print_args(p, live, n);
+    if (ctx.print_mode < 0) {
+        dev::print(negative.data(), rgb.data(), a, ctx.stream);
+        return;
+    }
+    auto tabs = std::make_unique<SpectralTablesN>();
+    spectral_tables_n(*p.print, compute_run(*p.print, live), ctx.print_bins, *tabs);
+    if (!dev::print_spectral_supported(tabs->nl_pad)) fail_invalid("spectral print: 81 or 401 wavelengths");
+    DevBuffer tab_d = ctx.pool.acquire(sizeof(SpectralTablesN));
+    DevBuffer err_d = ctx.pool.acquire(16);
+    // a pageable source: the copy has read it when the call returns
+    cuda_check(cudaMemcpyAsync(tab_d.ptr(), tabs.get(), sizeof(SpectralTablesN), cudaMemcpyHostToDevice, ctx.stream),
+               "spectral tables");
+    cuda_check(cudaMemsetAsync(err_d.ptr(), 0, 16, ctx.stream), "print status");
+    dev::print_spectral(a, *tabs, tab_d.as<SpectralTablesN>(), ctx.print_mode, negative.data(), rgb.data(), n,
+                        ctx.contraction_out, err_d.as<uint32_t>(), ctx.stream);
+    cuda_check(cudaGetLastError(), "print_spectral");
+    uint32_t err = 0;
+    cuda_check(cudaMemcpyAsync(&err, err_d.ptr(), 4, cudaMemcpyDeviceToHost, ctx.stream), "print status");
+    cuda_check(cudaStreamSynchronize(ctx.stream), "print");
+    if (err) fail_gpu("print: a tensor-core wait gave up");
+}
+}  // namespace
+
 void print_scan_encode(RenderCtx& ctx, const Pipeline& p, const LiveParams& live, const Plane& negative,
                        OutputImage* img) {
     const PrintSetup& s = *p.print;
     const uint32_t w = negative.w, h = negative.h;
-    const PrintArgs a = print_args(p, live, uint32_t(negative.pixels()));
     Plane rgb = make_plane(ctx.pool, w, h);
     {
         Stage st(ctx, "print");
-        dev::print(negative.data(), rgb.data(), a, ctx.stream);
+        print_stage(ctx, p, live, negative, rgb);
     }
     ScanArgs sa;
     if (scan_args(p, ctx.rho_tier, w, h, img->stride_px, sa)) {

@@ -41,6 +41,12 @@ struct RenderCtx {
     double rho_tier = 1.0;
     // optional per-stage timing: events recorded around each stage when set
     struct Timer* timer = nullptr;
+    // the print stage: -1 the binary32 print kernel, else a SpectralMode of the spectral-mode kernel at
+    // print_bins wavelengths (81, or 401 resampled to 1 nm); contraction_out (device, may be null) then
+    // receives the enlarger integral of every pixel (3 floats)
+    int print_mode = -1;
+    uint32_t print_bins = SPKB_NL;
+    float* contraction_out = nullptr;
 };
 
 // Stage timing with CUDA events on the render stream (bench and profile entry points).
@@ -63,6 +69,9 @@ struct Timer : dev::LaunchHook {
 // counts_out: nullptr, or device memory for 9 floats per pixel receiving the grain's Poisson counts
 Plane develop(RenderCtx& ctx, const Pipeline& p, const Plane& source, uint32_t film_seed,
               const std::optional<HalationOverride>& hov, float* counts_out = nullptr);
+
+// The spectral-mode kernel's tables of a print set-up at the live print run, at 81 or 401 wavelengths.
+void spectral_tables_n(const PrintSetup& s, const PrintRun& r, uint32_t bins, SpectralTablesN& out);
 
 // The print kernel's arguments for a negative of `pixels` pixels at the live parameters.
 PrintArgs print_args(const Pipeline& p, const LiveParams& live, uint32_t pixels);

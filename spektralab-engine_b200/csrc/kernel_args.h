@@ -90,6 +90,40 @@ struct SpectralPairs {
     F32Pair w[SPKB_NL * 3];  // [l][k]
 };
 
+// The arithmetic of the print's two spectral integrals in the spectral-mode print kernel
+// (k_print_spectral): binary32 or binary64 on the CUDA cores, or the sum over wavelengths on the tensor
+// cores (tcgen05) with binary32 accumulation: TF32 operands, BF16 operands, or BF16 hi + lo splits of
+// both operands (T w = (Th + Tl)(wh + wl), four products).
+#define SPKB_NL_MAX 416  // wavelength samples of the spectral-mode kernel: 401 (1 nm) padded to 32
+enum SpectralMode : int32_t {
+    SPKB_SPEC_F32 = 0,
+    SPKB_SPEC_F64 = 1,
+    SPKB_SPEC_TF32 = 2,
+    SPKB_SPEC_BF16 = 3,
+    SPKB_SPEC_BF16X3 = 4,
+};
+
+// The print's two spectral integrals at nl wavelengths for the spectral-mode kernel, in device memory.
+// Pass 0 is the enlarger (film densities -> print exposure), pass 1 the scan (print densities -> XYZ);
+// in both, R_k = sum_l 2^(sum_c d_c e_c(l)) w_k(l) with e_c = -log2(10) eps_c and w_k = wt_k 10^-beta.
+// Every table is zero from nl to nl_pad.
+struct SpectralTablesN {
+    uint32_t nl, nl_pad;  // nl_pad: nl rounded up to a multiple of 32
+    uint32_t pad_[2];
+    // e in wavelength pairs: [pass][l / 2] = {e0(l), e0(l+1), e1(l), e1(l+1), e2(l), e2(l+1), 0, 0}
+    float e_pairs[2][SPKB_NL_MAX / 2][8];
+    float w[2][SPKB_NL_MAX][4];    // [pass][l] = {w0, w1, w2, 0}
+    double e64[2][SPKB_NL_MAX][4];  // the binary64 values, before narrowing
+    double w64[2][SPKB_NL_MAX][4];
+    // The tensor cores' B operand of each pass: 16 rows n by nl_pad columns l, K-major without swizzle:
+    // element (n, l) at byte ((n / 8) * (nl_pad * S / 16) + (l * S) / 16) * 128 + (n % 8) * 16 + (l * S) % 16,
+    // S the element size (8-row by 16-byte core matrices, the K direction's fastest).
+    //   bf16: rows 0..2 bf16(w_k), rows 3..5 bf16(w_k - bf16(w_k)), rows 6..15 zero;
+    //   tf32: rows 0..2 w_k (binary32; the tensor core reads its TF32 part), rows 3..15 zero.
+    uint16_t b_bf16[2][16 * SPKB_NL_MAX];
+    float b_tf32[2][16 * SPKB_NL_MAX];
+};
+
 // CAM16-UCS gamut compression constants (reference kernels/print_shared.h:74-100 field meanings).
 struct Cam16Args {
     uint32_t rows, cols;

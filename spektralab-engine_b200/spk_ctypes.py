@@ -103,6 +103,8 @@ EXT = {
     "spk_render_vjp": (I32, [P, C, U32, FP, FP, DP, U32, FP]),
     "spkx_render_batch": (I32, [ctypes.POINTER(P), U32, C, I32, ctypes.POINTER(SpkResult), PS]),
     "spkx_engine_batch_plan": (I32, [P, C]),
+    "spkx_session_set_print_mode": (I32, [P, C, U32]),
+    "spkx_print_negative": (I32, [P, P, U32, U32, P, U32, P, ctypes.POINTER(ctypes.c_double)]),
 }
 
 REF_EXT = {
@@ -333,6 +335,17 @@ class Session:
         self.L.check(self.L.lib.spkx_session_develop_debug(self.h, tier.encode(), seed, neg.ctypes.data_as(FP),
                                                            cnt.ctypes.data_as(FP) if counts else None))
         return neg, cnt
+
+    def set_print_mode(self, mode, bins=81):
+        """spkx_session_set_print_mode: fp32, fp32_generic, fp64, tf32, bf16 or bf16x3 at 81 or 401 wavelengths."""
+        self.L.check(self.L.lib.spkx_session_set_print_mode(self.h, mode.encode(), bins))
+
+    def print_negative(self, negative_ptr, width, height, rgba16_ptr, row_stride_px, contraction_ptr=None):
+        """spkx_print_negative on device pointers (ints); returns the print kernel's device time in ms."""
+        ms = ctypes.c_double()
+        self.L.check(self.L.lib.spkx_print_negative(self.h, negative_ptr, width, height, rgba16_ptr, row_stride_px,
+                                                    contraction_ptr, ctypes.byref(ms)))
+        return ms.value
 
     def setup_json(self, pitch_um):
         out = ctypes.c_char_p()
