@@ -264,13 +264,15 @@ def run_e2e(args, eng, img, delta, pg, local, world):
 VJP_SIZE = 1024
 VJP_SEED = 7
 VJP_HALATION = ([((0.02, 0.02, 0.02), (8, 8, 8)), ((0.02, 0.02, 0.02), (40, 40, 40))], (0.03, 0.03, 0.03))
-VJP_PARAMS = 7  # print_exposure, m_filter_shift, y_filter_shift, 2 halation weights, 2 halation sigmas
+# print_exposure, m_filter_shift, y_filter_shift, 2 halation weights, 2 halation sigmas, then 16
+# density-curve parameters per film layer (hat functions over each layer's curve table)
+VJP_PARAMS = 7 + 48
 
 
 def run_vjp(args):
     """The render's adjoint (spk_render_vjp) on a 1024 x 1024 frame: the scanned linear RGB with the grain
     held fixed (film seed 7), the gradient of an L2 loss against a target rendered with perturbed
-    parameters, with respect to the frame and 7 parameters. Wall time per call through the C ABI (host
+    parameters, with respect to the frame and 55 parameters. Wall time per call through the C ABI (host
     arrays in and out); the forward-only call (output alone) beside it."""
     resources = synth_resources.ensure(sc.RESOURCES)
     lib = sc.load()
@@ -304,12 +306,13 @@ def run_vjp(args):
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": "render adjoint, 1024x1024, grain fixed (seed 7)", "width": n, "height": n,
                        "params": ["print_exposure", "m_filter_shift", "y_filter_shift", "halation_weight_0",
-                                  "halation_weight_1", "halation_sigma_0", "halation_sigma_1"],
+                                  "halation_weight_1", "halation_sigma_0", "halation_sigma_1"] +
+                                 [f"curve_{c}_{j}" for c in range(3) for j in range(16)],
                        "halation_sigma_px": [8, 40]},
             "forward_ms": 1000.0 * statistics.median(fwd),
             "note": "wall time per spk_render_vjp call with host arrays (forward recomputed inside); "
                     "gradient accuracy is checked against binary64 central differences in tests/test_gpu_vjp.py",
-            "grad_params": [float(v) for v in gp], "grad_input_l2": float(np.sqrt(np.sum(gx.astype(np.float64) ** 2)))}
+            "grad_params": [float(v) for v in gp[:7]], "grad_curve_l1": float(np.abs(gp[7:]).sum()), "grad_input_l2": float(np.sqrt(np.sum(gx.astype(np.float64) ** 2)))}
     print(json.dumps(line), flush=True)
     return 0
 

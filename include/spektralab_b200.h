@@ -138,9 +138,12 @@ SPK_API spk_status spkx_print_negative(spk_session* session, const float* negati
  *     grad_output  (NULL: the output alone is computed) the gradient of a loss with respect to it;
  *     grad_input   receives the gradient with respect to the session's source frame (RGB).
  *   grad_params (n_params doubles) receives the gradient with respect to
- *     [print_exposure, m_filter_shift, y_filter_shift, halation weight 0..K-1, halation sigma 0..K-1],
+ *     [print_exposure, m_filter_shift, y_filter_shift, halation weight 0..K-1, halation sigma 0..K-1,
+ *      density-curve parameter theta[c][j] for film layer c = 0..2 and node j = 0..15 at 3 + 2K + 16c + j],
  *   K the components set by spkx_session_set_halation (none otherwise; entries past the list are 0). A
- *   halation weight or sigma is taken as one value for the three channels.
+ *   halation weight or sigma is taken as one value for the three channels. theta[c][j] adds
+ *   theta phi_j(k) to entry k of layer c's K-entry density-curve table, phi_j(k) = max(0, 1 - |15k/(K-1) - j|)
+ *   (16 hat functions over the table; the curve's lookup interpolates the perturbed entries linearly).
  *   Blur passes are recomputed, not stored; the recursive blurs run transposed. Refused with
  *   SPK_ERR_UNSUPPORTED: grain below full strength or without sub-layers, halation components whose
  *   three channels differ in sigma.

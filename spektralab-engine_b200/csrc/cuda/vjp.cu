@@ -104,61 +104,102 @@ __global__ void k_vjp_expose(const float* __restrict__ rgb, const float* __restr
 
 // ---- develop, grain as fixed noise (reference kernels/film.metal:242-261, fx_grain.metal:39-97) ------
 
-template <int N>
-__device__ __forceinline__ Dual<N> curve_d(const float* __restrict__ x, const float* __restrict__ inv,
-                                           const float* __restrict__ y, uint32_t K, const AxisGrid& g,
-                                           const Dual<N>& v) {
-    if (v.v <= __ldg(x)) return dconst<N>(__ldg(y));
-    if (v.v >= __ldg(x + K - 1)) return dconst<N>(__ldg(y + K - 1));
-    const uint32_t l = axis_index(x, 1, K, g, v.v);
-    const Dual<N> t = (v - __ldg(x + l)) * __ldg(inv + l);
-    const float y0 = __ldg(y + l);
-    return y0 + t * (__ldg(y + l + 1) - y0);
+// the hat functions of the density-curve parameters at table entry k: phi_j(k) (1 - f) and phi_{j+1}(k) f
+__device__ __forceinline__ void curve_basis(uint32_t k, uint32_t K, uint32_t& j, float& f) {
+    const float u = float(k) * (float(kVjpCurveNodes - 1) / float(K - 1));
+    j = min(uint32_t(u), uint32_t(kVjpCurveNodes - 2));
+    f = u - float(j);
 }
 
 __global__ void k_vjp_develop(const float* __restrict__ exposure, const float* __restrict__ counts,
-                              const float* __restrict__ g_neg, float* __restrict__ g_exp, uint32_t w, uint32_t h,
-                              const __grid_constant__ DevelopArgs q) {
-    using D1 = Dual<1>;
+                              const float* __restrict__ g_neg, float* __restrict__ g_exp, double* __restrict__ g_nodes,
+                              uint32_t w, uint32_t h, const __grid_constant__ DevelopArgs q) {
+    using D2 = Dual<2>;  // tangents: the exposure, and the density the curve returns
+    __shared__ float acc[3 * kVjpCurveNodes];
+    const uint32_t tid = threadIdx.y * blockDim.x + threadIdx.x, nt = blockDim.x * blockDim.y;
+    if (g_nodes) {
+        for (uint32_t i = tid; i < 3u * kVjpCurveNodes; i += nt) acc[i] = 0.0f;
+        __syncthreads();
+    }
     const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t y = blockIdx.y * blockDim.y + threadIdx.y;
-    if (x >= w || y >= h) return;
-    const uint32_t pixel = y * q.width + x;
-    const size_t o = 3 * (size_t(y) * w + x);
-    for (uint32_t c = 0; c < 3; ++c) {
-        const D1 H = dvar<1>(exposure[o + c], 0);
-        const D1 L = dlog10(dfmax(H, 0.0f) + 1e-10f);
-        const D1 D = curve_d(q.cx, q.cinv, q.cy + size_t(c) * q.K, q.K, q.cgrid, L);
-        D1 out = D;
-        if (q.grain) {
-            const D1 v = q.positive ? -D : D;
-            const uint32_t K = q.gK;
-            D1 dl[3];
-            if (v.v <= __ldg(q.axis + c)) {
-                for (uint32_t l = 0; l < 3u; ++l) dl[l] = dconst<1>(__ldg(q.layers + l * 3u + c));
-            } else if (v.v >= __ldg(q.axis + 3u * (K - 1u) + c)) {
-                for (uint32_t l = 0; l < 3u; ++l) dl[l] = dconst<1>(__ldg(q.layers + ((K - 1u) * 3u + l) * 3u + c));
+    if (x < w && y < h) {
+        const uint32_t pixel = y * q.width + x;
+        const size_t o = 3 * (size_t(y) * w + x);
+        for (uint32_t c = 0; c < 3; ++c) {
+            const D2 H = dvar<2>(exposure[o + c], 0);
+            const D2 L = dlog10(dfmax(H, 0.0f) + 1e-10f);
+            // the curve lookup (reference kernels/film.metal:84-101), keeping its interval l and fraction t
+            const float* cy = q.cy + size_t(c) * q.K;
+            D2 D;
+            uint32_t l = 0;
+            float t = 0.0f;
+            if (L.v <= __ldg(q.cx)) {
+                D = dconst<2>(__ldg(cy));
+            } else if (L.v >= __ldg(q.cx + q.K - 1)) {
+                D = dconst<2>(__ldg(cy + q.K - 1));
+                l = q.K - 2;
+                t = 1.0f;
             } else {
-                const uint32_t j = axis_index(q.axis + c, 3u, K, q.ggrid[c], v.v);
-                const D1 t = (v - __ldg(q.axis + 3u * j + c)) * __ldg(q.ginv + 3u * j + c);
-                for (uint32_t l = 0; l < 3u; ++l) {
-                    const float y0 = __ldg(q.layers + (j * 3u + l) * 3u + c);
-                    const float y1 = __ldg(q.layers + ((j + 1u) * 3u + l) * 3u + c);
-                    dl[l] = y0 + t * (y1 - y0);
+                l = axis_index(q.cx, 1, q.K, q.cgrid, L.v);
+                const D2 td = (L - __ldg(q.cx + l)) * __ldg(q.cinv + l);
+                const float y0 = __ldg(cy + l);
+                D = y0 + td * (__ldg(cy + l + 1) - y0);
+                t = td.v;
+            }
+            D.d[1] = 1.0f;
+            D2 out = D;
+            if (q.grain) {
+                const D2 v = q.positive ? -D : D;
+                const uint32_t K = q.gK;
+                D2 dl[3];
+                if (v.v <= __ldg(q.axis + c)) {
+                    for (uint32_t k = 0; k < 3u; ++k) dl[k] = dconst<2>(__ldg(q.layers + k * 3u + c));
+                } else if (v.v >= __ldg(q.axis + 3u * (K - 1u) + c)) {
+                    for (uint32_t k = 0; k < 3u; ++k) dl[k] = dconst<2>(__ldg(q.layers + ((K - 1u) * 3u + k) * 3u + c));
+                } else {
+                    const uint32_t j = axis_index(q.axis + c, 3u, K, q.ggrid[c], v.v);
+                    const D2 tg = (v - __ldg(q.axis + 3u * j + c)) * __ldg(q.ginv + 3u * j + c);
+                    for (uint32_t k = 0; k < 3u; ++k) {
+                        const float y0 = __ldg(q.layers + (j * 3u + k) * 3u + c);
+                        const float y1 = __ldg(q.layers + ((j + 1u) * 3u + k) * 3u + c);
+                        dl[k] = y0 + tg * (y1 - y0);
+                    }
+                }
+                D2 G = dconst<2>(0.0f);
+                for (uint32_t k = 0; k < 3u; ++k) {
+                    const uint32_t lc = k * 3u + c;
+                    const D2 qd = dclamp((dl[k] + q.dmin_l[lc]) / q.sat_d[lc], 1e-6f, 0.999999f);
+                    const D2 sat = 1.0f - (qd * q.uniformity[c]) * 0.999999f;
+                    const float cnt = counts[size_t(pixel) * 9 + c * 3 + k];
+                    G = G + cnt * ((q.sat_d[lc] / q.count[lc]) * sat);
+                }
+                if (q.shift) G = G + (-q.dmin_c[c]);
+                out = G;
+            }
+            const float gn = g_neg[o + c];
+            g_exp[o + c] = gn * out.d[0];
+            if (g_nodes) {
+                const float gd = gn * out.d[1];
+                if (gd != 0.0f) {
+                    uint32_t j;
+                    float f;
+                    curve_basis(l, q.K, j, f);
+                    atomicAdd(&acc[c * kVjpCurveNodes + j], gd * (1.0f - t) * (1.0f - f));
+                    atomicAdd(&acc[c * kVjpCurveNodes + j + 1], gd * (1.0f - t) * f);
+                    if (t != 0.0f) {
+                        curve_basis(l + 1, q.K, j, f);
+                        atomicAdd(&acc[c * kVjpCurveNodes + j], gd * t * (1.0f - f));
+                        atomicAdd(&acc[c * kVjpCurveNodes + j + 1], gd * t * f);
+                    }
                 }
             }
-            D1 G = dconst<1>(0.0f);
-            for (uint32_t l = 0; l < 3u; ++l) {
-                const uint32_t lc = l * 3u + c;
-                const D1 qd = dclamp((dl[l] + q.dmin_l[lc]) / q.sat_d[lc], 1e-6f, 0.999999f);
-                const D1 sat = 1.0f - (qd * q.uniformity[c]) * 0.999999f;
-                const float k = counts[size_t(pixel) * 9 + c * 3 + l];
-                G = G + k * ((q.sat_d[lc] / q.count[lc]) * sat);
-            }
-            if (q.shift) G = G + (-q.dmin_c[c]);
-            out = G;
         }
-        g_exp[o + c] = g_neg[o + c] * out.d[0];
+    }
+    if (g_nodes) {
+        __syncthreads();
+        for (uint32_t i = tid; i < 3u * kVjpCurveNodes; i += nt)
+            if (acc[i] != 0.0f) atomicAdd(g_nodes + i, double(acc[i]));
     }
 }
 
@@ -403,11 +444,11 @@ void vjp_print(const float* neg, const float* g_print, float* g_neg, double* gra
 }
 
 void vjp_develop(const float* exposure, const float* counts, const float* g_neg, float* g_exposure,
-                 const DevelopArgs& a, uint32_t w, uint32_t h, cudaStream_t s) {
+                 double* g_nodes, const DevelopArgs& a, uint32_t w, uint32_t h, cudaStream_t s) {
     if (uint64_t(w) * h == 0) return;
     const dim3 b(32, 4), g((w + 31) / 32, (h + 3) / 4);
     Probe p("vjp_develop", s);
-    k_vjp_develop<<<g, b, 0, s>>>(exposure, counts, g_neg, g_exposure, w, h, a);
+    k_vjp_develop<<<g, b, 0, s>>>(exposure, counts, g_neg, g_exposure, g_nodes, w, h, a);
 }
 
 void vjp_expose(const float* rgb, const float* g_h, float* g_rgb, const float* table4, const ExposeArgs& a,

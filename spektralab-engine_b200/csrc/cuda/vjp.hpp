@@ -14,6 +14,10 @@
 namespace spkb::dev {
 
 constexpr int kVjpPrintParams = 3;  // print_exposure, m_filter_shift, y_filter_shift
+// Density-curve parameters: per film layer c, 16 hat functions on the entries of its K-entry curve table,
+// phi_j(k) = max(0, 1 - |u_k - j|) with u_k = 15 k / (K - 1). theta[c][j] adds theta phi_j(k) to every entry
+// y_c[k], so the lookup's linear interpolation gives dD/dtheta_j = (1 - t) phi_j(l) + t phi_j(l + 1).
+constexpr int kVjpCurveNodes = 16;
 
 // The print stage in the adjoint's form: the set-up's narrowed tables as they are (no packing), and the
 // tangents of the enlarger tables and gains along each print-side parameter (formed on the host by
@@ -41,8 +45,10 @@ void vjp_print(const float* neg, const float* g_print, float* g_neg, double* gra
 
 // g_exposure = J^T g_neg per pixel and channel of the develop stage: log10, density curve, sub-layer
 // densities and the grain value with the counts held fixed (counts: 9 floats per pixel [c][l]).
+// g_nodes (may be null): g_nodes[c * 16 + j] += the sum over pixels of g_neg_c dneg_c/dtheta[c][j]
+// (binary64 accumulation).
 void vjp_develop(const float* exposure, const float* counts, const float* g_neg, float* g_exposure,
-                 const DevelopArgs& a, uint32_t w, uint32_t h, cudaStream_t s);
+                 double* g_nodes, const DevelopArgs& a, uint32_t w, uint32_t h, cudaStream_t s);
 
 // g_rgb = J^T g_h per pixel of the expose stage (RGB -> film exposure through the spectral table).
 void vjp_expose(const float* rgb, const float* g_h, float* g_rgb, const float* table4, const ExposeArgs& a,

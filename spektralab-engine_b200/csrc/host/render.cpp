@@ -944,13 +944,15 @@ void render_vjp(RenderCtx& ctx, const Pipeline& p, const LiveParams& live, const
 
     // ---- adjoint ----
     const uint32_t ncomp = hov ? uint32_t(hov->comps.size()) : 0u;
-    const uint32_t n_all = dev::kVjpPrintParams + 2 * ncomp;
-    DevBuffer dparams = ctx.pool.acquire(sizeof(double) * (dev::kVjpPrintParams + 3 * 3 * 2 * SPKB_MAX_COMPONENTS));
-    cuda_check(cudaMemsetAsync(dparams.ptr(), 0, sizeof(double) * (dev::kVjpPrintParams + 3 * 3 * 2 * SPKB_MAX_COMPONENTS),
-                               ctx.stream),
-               "memset");
+    constexpr uint32_t kNodes = 3 * dev::kVjpCurveNodes;
+    const uint32_t n_all = dev::kVjpPrintParams + 2 * ncomp + kNodes;
+    // device accumulators: print parameters | per component [weight 3 | sigma 3] | curve parameters
+    constexpr size_t kAcc = dev::kVjpPrintParams + 6 * SPKB_MAX_COMPONENTS + kNodes;
+    DevBuffer dparams = ctx.pool.acquire(sizeof(double) * kAcc);
+    cuda_check(cudaMemsetAsync(dparams.ptr(), 0, sizeof(double) * kAcc, ctx.stream), "memset");
     double* d_print = dparams.as<double>();
     double* d_dots = d_print + dev::kVjpPrintParams;  // [k][weight 3 | sigma 3]
+    double* d_nodes = d_dots + 6 * SPKB_MAX_COMPONENTS;
     Plane g = make_plane(ctx.pool, w, h);
     cuda_check(cudaMemcpyAsync(g.data(), g_y, g.bytes(), cudaMemcpyDeviceToDevice, ctx.stream), "copy");
     if (unsharp) {  // g_B = (1 + a) g_Y - a Gs^T g_Y
@@ -963,7 +965,7 @@ void render_vjp(RenderCtx& ctx, const Pipeline& p, const LiveParams& live, const
     Plane gn = make_plane(ctx.pool, w, h);
     dev::vjp_print(neg.data(), g.data(), gn.data(), d_print, va, ctx.stream);
     if (dp.grain && dp.final_blur > 0.0) gaussian_adjoint(ctx, gn, dp.final_blur);  // g_G
-    dev::vjp_develop(H3.data(), counts.as<float>(), gn.data(), g.data(), dp.da, w, h, ctx.stream);  // g_H3
+    dev::vjp_develop(H3.data(), counts.as<float>(), gn.data(), g.data(), d_nodes, dp.da, w, h, ctx.stream);  // g_H3
     if (pl.bounce) {
         if (hov) {  // the override's weights and sigmas, from the exposure entering the bounce stage (H2)
             Plane Gk = make_plane(ctx.pool, w, h), Gp = make_plane(ctx.pool, w, h);
@@ -985,7 +987,7 @@ void render_vjp(RenderCtx& ctx, const Pipeline& p, const LiveParams& live, const
     if (pl.scatter) mixture_adjoint(ctx, g, pl.scatter_comps, pl.scatter_a, pl.scatter_b);  // g_H1
     if (s_lens > 0.0) gaussian_adjoint(ctx, g, s_lens);  // g_H0
     dev::vjp_expose(source.data(), g.data(), g_x, p.dev.table.as<float>(), ea, ctx.stream);
-    double hp[dev::kVjpPrintParams + 6 * SPKB_MAX_COMPONENTS];
+    double hp[kAcc];
     cuda_check(cudaMemcpyAsync(hp, dparams.ptr(), sizeof hp, cudaMemcpyDeviceToHost, ctx.stream), "copy");
     cuda_check(cudaStreamSynchronize(ctx.stream), "render adjoint");
     if (!grad_params) return;
@@ -1001,6 +1003,8 @@ void render_vjp(RenderCtx& ctx, const Pipeline& p, const LiveParams& live, const
         all[dev::kVjpPrintParams + k] = gw;
         all[dev::kVjpPrintParams + ncomp + k] = gs;
     }
+    for (uint32_t i = 0; i < kNodes; ++i)
+        all[dev::kVjpPrintParams + 2 * ncomp + i] = hp[dev::kVjpPrintParams + 6 * SPKB_MAX_COMPONENTS + i];
     for (uint32_t j = 0; j < n_params; ++j) grad_params[j] = j < n_all ? all[j] : 0.0;
 }
 

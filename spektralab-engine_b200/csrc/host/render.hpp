@@ -90,9 +90,10 @@ void print_scan_encode(RenderCtx& ctx, const Pipeline& p, const LiveParams& live
 //   g_y (null: y only)   the gradient of a loss with respect to y;
 //   g_x                  receives the gradient with respect to the source frame.
 // grad_params (host, n_params entries, may be null) receives the gradient with respect to
-//   [print_exposure, m_filter_shift, y_filter_shift, halation weight 0..K-1, halation sigma 0..K-1],
+//   [print_exposure, m_filter_shift, y_filter_shift, halation weight 0..K-1, halation sigma 0..K-1,
+//    density-curve parameter (layer c, node j) at 3 + 2K + 16 c + j],
 // K the components of the halation override (none without one). A weight's or sigma's gradient is along
-// a common change of its three channels.
+// a common change of its three channels; the curve parameters are the hat functions of vjp.hpp.
 void render_vjp(RenderCtx& ctx, const Pipeline& p, const LiveParams& live, const Plane& source, uint32_t film_seed,
                 const std::optional<HalationOverride>& hov, float* y_out, const float* g_y, float* g_x,
                 double* grad_params, uint32_t n_params);

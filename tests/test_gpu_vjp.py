@@ -3,8 +3,9 @@
 The differentiated output is the scanned linear RGB with the grain held as fixed noise: the device's
 Poisson counts for the film seed (spkx_session_develop_debug) are fed to the float64 oracle
 (orc_render_linear), whose loss is differenced along a direction of the frame and along each parameter
-[print_exposure, m_filter_shift, y_filter_shift, halation weights, halation sigmas]. The loss is the L2
-distance to a target rendered with perturbed parameters.
+[print_exposure, m_filter_shift, y_filter_shift, halation weights, halation sigmas, and the 48
+density-curve parameters: 16 hat functions over each layer's curve table]. The loss is the L2 distance
+to a target rendered with perturbed parameters.
 """
 
 import numpy as np
@@ -23,6 +24,7 @@ PARAMS = np.array([1.0, 0.05, -0.04, 0.02, 0.02, 8.0, 40.0])  # pe, m, y, w0, w1
 DELTA = dict(BASE, grain_active=True, scanner_lens_blur=1.5)
 PITCH = 35000.0 / max(W, H)
 TOL = 2e-3  # relative, gradient against the central difference
+N_CURVE = 3 * 16
 
 
 def halation(p):
@@ -54,7 +56,7 @@ def case(engine, lib, resources):
     with engine.open(img, delta_of(PARAMS)) as s:
         s.set_halation(*halation(PARAMS))
         gy = (y.astype(np.float64) - target).astype(np.float32)
-        gx, gp = s.render_vjp(gy, SEED, len(PARAMS))
+        gx, gp = s.render_vjp(gy, SEED, len(PARAMS) + N_CURVE)
     return dict(img=img, counts=counts, y=y, target=target, gx=gx, gp=gp)
 
 
@@ -91,6 +93,26 @@ def test_parameter_gradient(lib, resources, case, j, step):
     assert abs(got - fd) <= TOL * abs(fd) + 1e-9, (j, got, fd)
 
 
+@pytest.mark.parametrize("c,j", [(0, 4), (1, 7), (2, 10), (0, 12), (2, 2)])
+def test_curve_parameter_gradient(lib, resources, case, c, j):
+    x = case["img"].astype(np.float64)
+    f64 = setup_f64(lib, resources, delta_of(PARAMS), PITCH)["f64"]
+    K = len(f64["curve_x"])
+    phi = np.maximum(0.0, 1.0 - np.abs(np.arange(K) * 15.0 / (K - 1) - j))
+    step = 1e-4
+
+    def loss_at(sign):
+        y = np.array(f64["curve_y"], np.float64)
+        y[c * K:(c + 1) * K] += sign * step * phi
+        o = oracle.Oracle(dict(f64, curve_y=y), seed=SEED, halation=halation(PARAMS), print_exposure=float(PARAMS[0]))
+        return 0.5 * float(np.sum((o.render_linear(x, case["counts"]) - case["target"]) ** 2))
+
+    fd = (loss_at(1.0) - loss_at(-1.0)) / (2 * step)
+    got = float(case["gp"][len(PARAMS) + 16 * c + j])
+    # a node whose hat functions no pixel's lookup reaches has both at 0
+    assert abs(got - fd) <= TOL * abs(fd) + 1e-9, (c, j, got, fd)
+
+
 def test_autograd_function(engine, case):
     import torch
 
@@ -102,4 +124,4 @@ def test_autograd_function(engine, case):
     loss_t = 0.5 * ((y.double() - torch.from_numpy(case["target"])) ** 2).sum()
     loss_t.backward()
     np.testing.assert_allclose(img.grad.numpy(), case["gx"], rtol=1e-5, atol=1e-7)
-    np.testing.assert_allclose(params.grad.numpy(), case["gp"], rtol=1e-5, atol=1e-9)
+    np.testing.assert_allclose(params.grad.numpy(), case["gp"][:len(PARAMS)], rtol=1e-5, atol=1e-9)
