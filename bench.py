@@ -487,14 +487,15 @@ def run_batch(args):
         return wall, info
 
     # warm-up and tuning: one plain pass and one batched pass of the same shape, untimed
+    tuning = {}
     for mode in ("plain", "batch"):
         ss = open_all()
         if mode == "plain":
             plain(ss, False)
         else:
-            batched(ss, False)
+            _, tuning["render"] = batched(ss, False)
             reprint_exposures(ss)
-            batched(ss, True)
+            _, tuning["reprint"] = batched(ss, True)
         for s in ss:
             s.close()
     ss = open_all()
@@ -523,11 +524,13 @@ def run_batch(args):
             "render": {"batched_mpx_s": mpx / b_render, "plain_mpx_s": mpx / p_render,
                        "batched_ms": 1000.0 * b_render, "plain_ms": 1000.0 * p_render,
                        "latency_ms_batched": pct(info_r["frame_done_ms"]), "latency_ms_plain": pct(lat_pr),
-                       "plan": info_r.get("plan")},
+                       "plan": info_r.get("plan"),
+                       "tuning_candidates_ms": tuning["render"].get("candidates_ms")},
             "reprint": {"batched_mpx_s": mpx / b_reprint, "plain_mpx_s": mpx / p_reprint,
                         "batched_ms": 1000.0 * b_reprint, "plain_ms": 1000.0 * p_reprint,
                         "latency_ms_batched": pct(info_p["frame_done_ms"]), "latency_ms_plain": pct(lat_pp),
-                        "plan": info_p.get("plan")}}
+                        "plan": info_p.get("plan"),
+                        "tuning_candidates_ms": tuning["reprint"].get("candidates_ms")}}
     print(json.dumps(line), flush=True)
     return 0
 

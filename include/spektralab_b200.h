@@ -90,7 +90,8 @@ SPK_API spk_status spkx_gaussian(const float* in, float* out, uint32_t w, uint32
  *   one persistent scanner launch for every frame. The first batch of a list of frame sizes times each plan
  *   on the device and keeps the fastest for that list. results[i].elapsed_ms is the time from the start of
  *   the call's device work to that frame's result in host memory. out_json (may be NULL) receives
- *   {"plan": ..., "tuning_ms": ..., "frame_done_ms": [...]}. On failure every result is zeroed.
+ *   {"plan": ..., "tuning_ms": ..., "frame_done_ms": [...]}, with "candidates_ms" (each plan's device time)
+ *   after a timed choice. On failure every result is zeroed.
  *   SPK_ERR_INVALID_ARG: NULL arrays, n = 0, a session twice, sessions of different engines, unknown tier.
  */
 SPK_API spk_status spkx_render_batch(spk_session* const* sessions, uint32_t n, const char* tier, int32_t reprint,

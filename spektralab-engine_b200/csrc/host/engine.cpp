@@ -102,6 +102,7 @@ public:
     cudaStream_t batch_stream = nullptr;
     std::vector<cudaStream_t> workers;
     std::vector<cudaEvent_t> frame_events;  // one per frame slot: completion, recorded inside the graph
+    std::vector<cudaEvent_t> ready_events;  // one per frame slot: the frame's negative is ready
     std::vector<cudaEvent_t> join_events;   // one per worker stream
     cudaEvent_t fork_event = nullptr, start_event = nullptr;
     std::map<std::string, std::string> tuned;
@@ -114,6 +115,7 @@ public:
         for (auto& [k, g] : graphs) cudaGraphExecDestroy(g);
         for (cudaStream_t w : workers) cudaStreamDestroy(w);
         for (cudaEvent_t ev : frame_events) cudaEventDestroy(ev);
+        for (cudaEvent_t ev : ready_events) cudaEventDestroy(ev);
         for (cudaEvent_t ev : join_events) cudaEventDestroy(ev);
         if (fork_event) cudaEventDestroy(fork_event);
         if (start_event) cudaEventDestroy(start_event);
@@ -448,8 +450,8 @@ spk_status render_common(spk_session* session, const char* tier, spk_result* out
 //
 // A batch renders many sessions' frames with one call. The film side of each frame runs on its session's
 // stream as in spk_render (sessions develop concurrently); the print side and the scanner of every frame
-// whose scanner takes the tiled kernel go into ONE CUDA graph on the engine's batch stream, launched after
-// all the negatives are ready. Two plan families build that graph:
+// whose scanner takes the tiled kernel go into ONE CUDA graph on the engine's batch stream. Two plan
+// families build that graph:
 //   frames:K          each frame's print and scanner launches on one of K worker streams (round robin),
 //                     forked from and joined to the batch stream; the frames overlap on the device;
 //   persistent:S:C    one print launch and one scanner launch for all frames: C CTAs walking items of S
@@ -467,7 +469,7 @@ struct BatchFrame {
     bool fused = false;      // print and scanner inside the batch graph
     bool reused = false;     // the tier's negative was cached (reprint)
     bool developed = false;  // the tier's negative was made by this batch
-    cudaEvent_t ready = nullptr;
+    cudaEvent_t ready = nullptr;  // the engine's ready event of the frame's slot
 };
 
 const char* const kBatchPlans[] = {"frames:4", "frames:16", "persistent:2048:592", "persistent:8192:1184"};
@@ -506,12 +508,18 @@ void batch_resources(Engine& e, size_t n_frames, size_t n_workers) {
         cuda_check(cudaEventCreate(&ev), "batch event");
         e.frame_events.push_back(ev);
     }
+    while (e.ready_events.size() < n_frames) {
+        cudaEvent_t ev = nullptr;
+        cuda_check(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "batch event");
+        e.ready_events.push_back(ev);
+    }
 }
 
 // Captures body(batch_stream) into a graph, brings the engine's executable graph for `key` up to date
-// (updated in place when the topology is unchanged, else instantiated afresh) and launches it.
+// (updated in place when the topology is unchanged, else instantiated afresh) and launches it, between
+// the timing events t0 and t1 when given.
 template <class F>
-void launch_captured(Engine& e, const std::string& key, F&& body) {
+void launch_captured(Engine& e, const std::string& key, F&& body, cudaEvent_t t0 = nullptr, cudaEvent_t t1 = nullptr) {
     cudaStream_t bs = e.batch_stream;
     cuda_check(cudaStreamBeginCapture(bs, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
     try {
@@ -550,37 +558,47 @@ void launch_captured(Engine& e, const std::string& key, F&& body) {
         e.graphs[key] = exec;
     }
     cudaGraphDestroy(graph);
+    if (t0) cuda_check(cudaEventRecord(t0, bs), "graph timing");
     cuda_check(cudaGraphLaunch(exec, bs), "cudaGraphLaunch");
+    if (t1) cuda_check(cudaEventRecord(t1, bs), "graph timing");
 }
 
 // Enqueues the print side of the fused frames under `plan` on the batch stream (graph launch and, for the
 // persistent plans, the upload of the frame tables before it). Each fused frame's result is copied to its
-// pinned host image inside the graph, and frame_events[slot] marks its completion.
+// pinned host image inside the graph, and frame_events[slot] marks its completion. In the per-frame plans
+// each frame waits inside the graph for its own negative (its ready event), so a frame prints while
+// later frames still develop; the persistent plans wait for every negative before their launch. The
+// graph launch is bracketed by t0 and t1 when given.
 void run_plan(Engine& e, const std::string& plan, const std::string& shape, std::vector<BatchFrame>& fr,
-              const std::vector<size_t>& slots, DevBuffer& tables) {
+              const std::vector<size_t>& slots, DevBuffer& tables, cudaEvent_t t0 = nullptr, cudaEvent_t t1 = nullptr) {
     cudaStream_t bs = e.batch_stream;
     const std::string key = plan + "|" + shape;
     if (plan.rfind("frames:", 0) == 0) {
         const size_t K = std::min<size_t>(std::stoul(plan.substr(7)), std::max<size_t>(slots.size(), 1));
-        launch_captured(e, key, [&](cudaStream_t s) {
-            cuda_check(cudaEventRecord(e.fork_event, s), "fork");
-            for (size_t k = 0; k < K; ++k) cuda_check(cudaStreamWaitEvent(e.workers[k], e.fork_event, 0), "fork");
-            for (size_t j = 0; j < slots.size(); ++j) {
-                BatchFrame& f = fr[slots[j]];
-                cudaStream_t ws = e.workers[j % K];
-                dev::print(f.neg, f.rgb.data(), f.pa, ws);
-                dev::scan_encode(f.rgb.data(), f.img->dev, f.rgb.w, f.rgb.h, f.sa, ws);
-                cuda_check(cudaMemcpyAsync(f.img->host, f.img->dev, f.img->bytes, cudaMemcpyDeviceToHost, ws),
-                           "result copy");
-                cuda_check(cudaEventRecordWithFlags(e.frame_events[slots[j]], ws, cudaEventRecordExternal), "frame");
-            }
-            for (size_t k = 0; k < K; ++k) {
-                cuda_check(cudaEventRecord(e.join_events[k], e.workers[k]), "join");
-                cuda_check(cudaStreamWaitEvent(s, e.join_events[k], 0), "join");
-            }
-        });
+        launch_captured(
+            e, key,
+            [&](cudaStream_t s) {
+                cuda_check(cudaEventRecord(e.fork_event, s), "fork");
+                for (size_t k = 0; k < K; ++k) cuda_check(cudaStreamWaitEvent(e.workers[k], e.fork_event, 0), "fork");
+                for (size_t j = 0; j < slots.size(); ++j) {
+                    BatchFrame& f = fr[slots[j]];
+                    cudaStream_t ws = e.workers[j % K];
+                    cuda_check(cudaStreamWaitEvent(ws, f.ready, cudaEventWaitExternal), "frame ready");
+                    dev::print(f.neg, f.rgb.data(), f.pa, ws);
+                    dev::scan_encode(f.rgb.data(), f.img->dev, f.rgb.w, f.rgb.h, f.sa, ws);
+                    cuda_check(cudaMemcpyAsync(f.img->host, f.img->dev, f.img->bytes, cudaMemcpyDeviceToHost, ws),
+                               "result copy");
+                    cuda_check(cudaEventRecordWithFlags(e.frame_events[slots[j]], ws, cudaEventRecordExternal), "frame");
+                }
+                for (size_t k = 0; k < K; ++k) {
+                    cuda_check(cudaEventRecord(e.join_events[k], e.workers[k]), "join");
+                    cuda_check(cudaStreamWaitEvent(s, e.join_events[k], 0), "join");
+                }
+            },
+            t0, t1);
         return;
     }
+    for (size_t slot : slots) cuda_check(cudaStreamWaitEvent(bs, fr[slot].ready, 0), "frame ready");
     // persistent:S:C
     const size_t c1 = plan.find(':'), c2 = plan.find(':', c1 + 1);
     const uint32_t item_px = uint32_t(std::stoul(plan.substr(c1 + 1, c2 - c1 - 1)));
@@ -626,17 +644,21 @@ void run_plan(Engine& e, const std::string& plan, const std::string& shape, std:
     unsigned char* d = tables.as<unsigned char>();
     cuda_check(cudaMemcpyAsync(d, blob.data(), bytes, cudaMemcpyHostToDevice, bs), "batch tables");
     // the pageable source is staged before cudaMemcpyAsync returns, so blob may go at scope exit
-    launch_captured(e, key, [&](cudaStream_t s) {
-        dev::print_batch(reinterpret_cast<const BatchPrintFrame*>(d), reinterpret_cast<const uint32_t*>(d + o_if),
-                         reinterpret_cast<const uint32_t*>(d + o_ip), n_items, item_px, ctas, s);
-        dev::scan_encode_batch(reinterpret_cast<const BatchScanFrame*>(d + o_sf), uint32_t(n), tiles, r1, r2, ctas, s);
-        for (size_t j = 0; j < n; ++j) {
-            BatchFrame& f = fr[slots[j]];
-            cuda_check(cudaMemcpyAsync(f.img->host, f.img->dev, f.img->bytes, cudaMemcpyDeviceToHost, s),
-                       "result copy");
-            cuda_check(cudaEventRecordWithFlags(e.frame_events[slots[j]], s, cudaEventRecordExternal), "frame");
-        }
-    });
+    launch_captured(
+        e, key,
+        [&](cudaStream_t s) {
+            dev::print_batch(reinterpret_cast<const BatchPrintFrame*>(d), reinterpret_cast<const uint32_t*>(d + o_if),
+                             reinterpret_cast<const uint32_t*>(d + o_ip), n_items, item_px, ctas, s);
+            dev::scan_encode_batch(reinterpret_cast<const BatchScanFrame*>(d + o_sf), uint32_t(n), tiles, r1, r2, ctas,
+                                   s);
+            for (size_t j = 0; j < n; ++j) {
+                BatchFrame& f = fr[slots[j]];
+                cuda_check(cudaMemcpyAsync(f.img->host, f.img->dev, f.img->bytes, cudaMemcpyDeviceToHost, s),
+                           "result copy");
+                cuda_check(cudaEventRecordWithFlags(e.frame_events[slots[j]], s, cudaEventRecordExternal), "frame");
+            }
+        },
+        t0, t1);
 }
 
 void render_batch(std::vector<Session*> ss, const char* tier_name, bool reprint, spk_result* out, std::string* info) {
@@ -667,6 +689,7 @@ void render_batch(std::vector<Session*> ss, const char* tier_name, bool reprint,
     DevBuffer tables;
     std::string plan;
     double tuning_ms = 0.0;
+    json::Value candidates = json::Object{};  // the timed plans of a tuning pass: device ms each
     std::vector<double> done_ms(n, 0.0);
     try {
         batch_resources(e, n, kMaxWorkers);
@@ -705,9 +728,8 @@ void render_batch(std::vector<Session*> ss, const char* tier_name, bool reprint,
             if (f.fused) {
                 f.pa = print_args(s.pipe, s.live, uint32_t(ts.negative.pixels()));
                 f.rgb = make_plane(s.pool, s.source.w, s.source.h);
-                cuda_check(cudaEventCreateWithFlags(&f.ready, cudaEventDisableTiming), "batch event");
+                f.ready = e.ready_events[i];
                 cuda_check(cudaEventRecord(f.ready, s.stream), "frame ready");
-                cuda_check(cudaStreamWaitEvent(bs, f.ready, 0), "frame ready");
                 slots.push_back(i);
                 shape += "," + std::to_string(s.source.w) + "x" + std::to_string(s.source.h);
             } else {
@@ -725,7 +747,9 @@ void render_batch(std::vector<Session*> ss, const char* tier_name, bool reprint,
             } else if (tuned != e.tuned.end()) {
                 plan = tuned->second;
             } else {
-                // every candidate renders the whole batch; the pixels agree, so the last run's stand
+                // every candidate renders the whole batch; the pixels agree, so the last run's stand. The
+                // negatives are complete first, so that each candidate's time is its graph's alone.
+                for (size_t slot : slots) cuda_check(cudaEventSynchronize(fr[slot].ready), "frame ready");
                 cudaEvent_t a = nullptr, b = nullptr;
                 cuda_check(cudaEventCreate(&a), "batch event");
                 cuda_check(cudaEventCreate(&b), "batch event");
@@ -733,13 +757,12 @@ void render_batch(std::vector<Session*> ss, const char* tier_name, bool reprint,
                 try {
                     for (const char* cand : kBatchPlans) {
                         DevBuffer tb;
-                        cuda_check(cudaEventRecord(a, bs), "tuning");
-                        run_plan(e, cand, shape, fr, slots, tb);
-                        cuda_check(cudaEventRecord(b, bs), "tuning");
+                        run_plan(e, cand, shape, fr, slots, tb, a, b);
                         cuda_check(cudaEventSynchronize(b), "tuning");
                         float ms = 0.0f;
                         cuda_check(cudaEventElapsedTime(&ms, a, b), "tuning");
                         tuning_ms += ms;
+                        candidates[cand] = double(ms);
                         if (plan.empty() || ms < best) {
                             best = ms;
                             plan = cand;
@@ -775,7 +798,6 @@ void render_batch(std::vector<Session*> ss, const char* tier_name, bool reprint,
             if (f.img) output_release(f.img);
             f.img = nullptr;
             if (f.developed) f.s->tiers[int(*t)].negative = Plane{};
-            if (f.ready) cudaEventDestroy(f.ready);
         }
         try {
             throw;
@@ -790,7 +812,6 @@ void render_batch(std::vector<Session*> ss, const char* tier_name, bool reprint,
     json::Array dms;
     for (size_t i = 0; i < n; ++i) {
         BatchFrame& f = fr[i];
-        if (f.ready) cudaEventDestroy(f.ready);
         Session& s = *f.s;
         s.done = true;
         spk_result& o = out[i];
@@ -808,6 +829,7 @@ void render_batch(std::vector<Session*> ss, const char* tier_name, bool reprint,
     }
     r["plan"] = plan.empty() ? std::string("none") : plan;
     r["tuning_ms"] = tuning_ms;
+    if (!candidates.as_object().empty()) r["candidates_ms"] = std::move(candidates);
     r["frame_done_ms"] = json::Value(std::move(dms));
     if (info) *info = json::write(r);
 }
