@@ -51,6 +51,15 @@ SPK_API spk_status spkx_session_negative(spk_session* session, const char* tier,
 SPK_API spk_status spkx_session_develop_debug(spk_session* session, const char* tier, uint32_t film_seed,
                                               float* negative, float* counts);
 
+/* spkx_session_develop_draws(session, tier, film_seed, counts, lambdas)
+ *   the grain's draws of a develop with the given film seed (sub-layer grain): counts and lambdas receive
+ *   9 floats per pixel each, [c][l], the Poisson count and the lambda it was drawn with. Draw (c, l) of
+ *   pixel y * width + x uses the sampler's stream c + 10 l, so spkx_sampler_poisson over one (c, l)
+ *   plane of lambdas, with that stream and seed, reproduces the counts.
+ */
+SPK_API spk_status spkx_session_develop_draws(spk_session* session, const char* tier, uint32_t film_seed, float* counts,
+                                             float* lambdas);
+
 /* spkx_session_setup_json(session, out_json)
  *   the narrowed kernel constants of the session's pipeline, for set-up parity checks:
  *   input matrix, curve tables, grain tables and constants at a given pitch, enlarger and scan

@@ -430,6 +430,7 @@ __global__ void __launch_bounds__(kDrawWarps * 32) k_develop_layers(const float*
             lam[c * 3 + l][tid] =
                 live ? spk_sublayer_lambda(dl[l] + q.dmin_l[lc], q.sat_d[lc], q.count[lc], q.uniformity[c], &sat)
                      : 0.0f;
+            if (q.lam_out && live) q.lam_out[size_t(pixel) * 9 + c * 3 + l] = lam[c * 3 + l][tid];
             scale[c * 3 + l][tid] = SPK_MUL(SPK_DIV(q.sat_d[lc], q.count[lc]), sat);
         }
     }

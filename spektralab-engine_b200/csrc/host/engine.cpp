@@ -1598,6 +1598,31 @@ SPK_API spk_status spkx_session_develop_debug(spk_session* session, const char* 
     });
 }
 
+SPK_API spk_status spkx_session_develop_draws(spk_session* session, const char* tier, uint32_t seed, float* counts,
+                                              float* lambdas) {
+    last_error::clear();
+    if (!session || !counts || !lambdas) return invalid("a required pointer is NULL");
+    return guarded([&] {
+        Session& s = *S(session);
+        std::lock_guard<std::mutex> lock(s.m);
+        auto t = parse_tier(tier);
+        if (!t) fail_invalid("unknown tier");
+        s.check_tier(*t);
+        DeviceGuard dg(s.engine->device);
+        RenderCtx ctx{s.pool, s.stream};
+        ctx.pitch_um = s.pitch_um();
+        const size_t bytes = s.source.pixels() * 9 * sizeof(float);
+        DevBuffer dc = s.pool.acquire(bytes), dl = s.pool.acquire(bytes);
+        cuda_check(cudaMemsetAsync(dc.ptr(), 0, bytes, s.stream), "memset");
+        cuda_check(cudaMemsetAsync(dl.ptr(), 0, bytes, s.stream), "memset");
+        Plane neg = develop(ctx, s.pipe, s.source, seed, s.hal, dc.as<float>(), dl.as<float>());
+        cuda_check(cudaMemcpyAsync(counts, dc.ptr(), bytes, cudaMemcpyDeviceToHost, s.stream), "copy");
+        cuda_check(cudaMemcpyAsync(lambdas, dl.ptr(), bytes, cudaMemcpyDeviceToHost, s.stream), "copy");
+        cuda_check(cudaStreamSynchronize(s.stream), "develop");
+        return SPK_OK;
+    });
+}
+
 SPK_API spk_status spk_render_vjp(spk_session* session, const char* tier, uint32_t film_seed, const float* grad_output,
                                   float* grad_input, double* grad_params, uint32_t n_params, float* output) {
     last_error::clear();

@@ -452,7 +452,8 @@ struct DevelopPlan {
 };
 
 // the develop kernel's arguments for a frame of width w and the grain's final blur and strength
-DevelopPlan develop_plan(const RenderCtx& ctx, const Pipeline& p, uint32_t w, uint32_t film_seed, float* counts_out) {
+DevelopPlan develop_plan(const RenderCtx& ctx, const Pipeline& p, uint32_t w, uint32_t film_seed, float* counts_out,
+                         float* lam_out = nullptr) {
     const FilmSetup& f = *p.film;
     DevelopPlan dp;
     DevelopArgs& da = dp.da;
@@ -463,6 +464,7 @@ DevelopPlan develop_plan(const RenderCtx& ctx, const Pipeline& p, uint32_t w, ui
     da.cgrid = axis_grid(f.cx.data(), f.K, 1);
     da.width = w;
     da.counts_out = counts_out;
+    da.lam_out = lam_out;
     const GrainSetup* g = f.grain.get();
     dp.grain = g && g->active && g->amount > 0.0;
     if (!dp.grain) return dp;
@@ -503,7 +505,7 @@ DevelopPlan develop_plan(const RenderCtx& ctx, const Pipeline& p, uint32_t w, ui
 }  // namespace
 
 Plane develop(RenderCtx& ctx, const Pipeline& p, const Plane& source, uint32_t film_seed,
-              const std::optional<HalationOverride>& hov, float* counts_out) {
+              const std::optional<HalationOverride>& hov, float* counts_out, float* lam_out) {
     const FilmSetup& f = *p.film;
     const uint32_t w = source.w, h = source.h;
     Plane H = make_plane(ctx.pool, w, h);
@@ -524,7 +526,7 @@ Plane develop(RenderCtx& ctx, const Pipeline& p, const Plane& source, uint32_t f
             apply_halation(ctx, pl, H);
         }
     }
-    const DevelopPlan dp = develop_plan(ctx, p, w, film_seed, counts_out);
+    const DevelopPlan dp = develop_plan(ctx, p, w, film_seed, counts_out, lam_out);
     const DevelopArgs& da = dp.da;
     Plane neg = make_plane(ctx.pool, w, h);
     if (!dp.grain) {

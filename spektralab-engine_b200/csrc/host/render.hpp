@@ -66,9 +66,10 @@ struct Timer : dev::LaunchHook {
 };
 
 // film side: raw source plane -> developed negative density plane (a fresh persistent plane)
-// counts_out: nullptr, or device memory for 9 floats per pixel receiving the grain's Poisson counts
+// counts_out: nullptr, or device memory for 9 floats per pixel receiving the grain's Poisson counts;
+// lam_out: nullptr, or the same for the draws' lambdas (sub-layer grain)
 Plane develop(RenderCtx& ctx, const Pipeline& p, const Plane& source, uint32_t film_seed,
-              const std::optional<HalationOverride>& hov, float* counts_out = nullptr);
+              const std::optional<HalationOverride>& hov, float* counts_out = nullptr, float* lam_out = nullptr);
 
 // The spectral-mode kernel's tables of a print set-up at the live print run, at 81 or 401 wavelengths.
 void spectral_tables_n(const PrintSetup& s, const PrintRun& r, uint32_t bins, SpectralTablesN& out);

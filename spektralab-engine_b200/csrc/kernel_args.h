@@ -70,6 +70,7 @@ struct DevelopArgs {
     const float* layers;  // [(k*3 + l)*3 + c]
     uint32_t width;       // pixel index = y * width + x keys the draws
     float* counts_out;    // test hook: the Poisson counts, [pixel][c][l]; nullptr in renders
+    float* lam_out;       // test hook: the draws' lambdas, [pixel][c][l] (sub-layer grain); nullptr in renders
 };
 
 // Per-wavelength tables of one spectral integral (already neutralised).

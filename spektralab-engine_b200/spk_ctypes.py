@@ -100,6 +100,7 @@ EXT = {
     "spkx_gaussian": (I32, [FP, FP, U32, U32, DP]),
     "spkx_setup_json": (I32, [C, C, ctypes.c_double, PS]),
     "spkx_session_develop_debug": (I32, [P, C, U32, FP, FP]),
+    "spkx_session_develop_draws": (I32, [P, C, U32, FP, FP]),
     "spk_render_vjp": (I32, [P, C, U32, FP, FP, DP, U32, FP]),
     "spkx_render_batch": (I32, [ctypes.POINTER(P), U32, C, I32, ctypes.POINTER(SpkResult), PS]),
     "spkx_engine_batch_plan": (I32, [P, C]),
@@ -346,6 +347,14 @@ class Session:
         self.L.check(self.L.lib.spkx_print_negative(self.h, negative_ptr, width, height, rgba16_ptr, row_stride_px,
                                                     contraction_ptr, ctypes.byref(ms)))
         return ms.value
+
+    def develop_draws(self, tier, seed, w, h):
+        """(counts, lambdas), each (h, w, 9) float32 [c][l]: the grain's draws of one develop."""
+        cnt = np.zeros((h, w, 9), np.float32)
+        lam = np.zeros((h, w, 9), np.float32)
+        self.L.check(self.L.lib.spkx_session_develop_draws(self.h, tier.encode(), seed, cnt.ctypes.data_as(FP),
+                                                           lam.ctypes.data_as(FP)))
+        return cnt, lam
 
     def setup_json(self, pitch_um):
         out = ctypes.c_char_p()

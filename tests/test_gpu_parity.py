@@ -99,6 +99,39 @@ def test_sampler_bit_exact(lib):
     assert np.array_equal(ln, oracle.lognormal(ln.size, 1.0, 0.2, 100, 9))
 
 
+def film_format_for(lib, resources, grains, long_edge):
+    """film_format_mm giving a mean of `grains` grains per sub-layer and pixel (counts scale with the
+    square of the pixel pitch)."""
+    import ctypes
+    p0 = 10.0
+    out = ctypes.c_char_p()
+    lib.check(lib.lib.spkx_setup_json(resources.encode(), json.dumps(BASE).encode(), p0, ctypes.byref(out)))
+    counts = lib.take_json(out)["f64"]["grain_count"]
+    return p0 * (grains / float(np.mean(counts))) ** 0.5 * long_edge / 1000.0
+
+
+# (the film format stays within the schema's 4..200 mm: a wide frame for the fine pitch of 40 grains, which
+# still stays above the pitch where dye clouds begin)
+@pytest.mark.parametrize("w,h,seed,grains", [(300, 200, FIRST_SEED, 600.0), (401, 73, 12345, 600.0),
+                                             (800, 48, 99, 40.0)])
+def test_develop_draws_match_sampler(engine, lib, resources, w, h, seed, grains):
+    """Every grain draw of the develop kernel (its first attempts run in lockstep, the rest deferred and
+    finished apart) equals the shared sampler's count for the same lambda, pixel, stream and seed; at 40
+    grains per pixel the low densities take the product method (lambda < 10)."""
+    img = sc.synthetic_image(w, h, 5)
+    delta = dict(BASE, grain_active=True, film_format_mm=film_format_for(lib, resources, grains, max(w, h)))
+    with engine.open(img, delta) as s:
+        s.set_halation(*CFG1)
+        counts, lam = s.develop_draws("full", seed, w, h)
+    assert (lam >= 10).any()
+    if grains < 100:
+        assert (lam < 10).any()
+    for c in range(3):
+        for l in range(3):
+            want = oracle.poisson(lam[..., c * 3 + l].ravel(), c + 10 * l, seed)
+            assert np.array_equal(counts[..., c * 3 + l].ravel(), want), (c, l)
+
+
 def test_philox_on_device(lib):
     rng = np.random.default_rng(0)
     ctr = rng.integers(0, 2 ** 32, (1024, 4), dtype=np.uint64).astype(np.uint32)

@@ -23,7 +23,7 @@ STRENGTH = (0.03, 0.03, 0.03)
 PARAMS = np.array([1.0, 0.05, -0.04, 0.02, 0.02, 8.0, 40.0])  # pe, m, y, w0, w1, s0, s1
 DELTA = dict(BASE, grain_active=True, scanner_lens_blur=1.5)
 PITCH = 35000.0 / max(W, H)
-TOL = 2e-3  # relative, gradient against the central difference
+TOL = 1e-4  # relative, gradient against the binary64 central difference (the adjoint's accuracy gate)
 N_CURVE = 3 * 16
 
 
@@ -76,7 +76,8 @@ def test_image_gradient(lib, resources, case, seed):
     rng = np.random.default_rng(seed)
     x = case["img"].astype(np.float64)
     v = rng.standard_normal(x.shape) * x
-    eps = 1e-6
+    # the curve tables are piecewise linear: a step small enough that few pixels cross a table node
+    eps = 1e-7
     fd = (loss(lib, resources, case, x + eps * v, PARAMS) - loss(lib, resources, case, x - eps * v, PARAMS)) / (2 * eps)
     got = float(np.sum(case["gx"].astype(np.float64) * v))
     assert abs(got - fd) <= TOL * abs(fd), (got, fd)
