@@ -145,37 +145,53 @@ class Clocks:
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def dist_init(gpus):
+def dist_init(gpus, backend="nccl"):
+    """One rank per GPU (torchrun's RANK / LOCAL_RANK / WORLD_SIZE / MASTER_*): (rank, local rank, world,
+    process group or None, the device the group's tensors live on). backend "gloo" runs the same steps on
+    the CPU (the tests' two-process check)."""
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     pg = None
+    device = f"cuda:{local}" if backend == "nccl" else "cpu"
     if world > 1:
         import datetime
 
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
         pg = dist
-    return rank, local, world, pg
+    return rank, local, world, pg, device
 
 
-def reduce_max(pg, local, value):
+def reduce_max(pg, device, value):
+    """The maximum of value over the ranks (every rank gets it)."""
     if pg is None:
         return value
     import torch
-    t = torch.tensor([value], dtype=torch.float64, device=f"cuda:{local}")
+    t = torch.tensor([value], dtype=torch.float64, device=device)
     pg.all_reduce(t, op=pg.ReduceOp.MAX)
     return float(t.item())
 
 
-def barrier(pg, local):
+def barrier(pg, device):
     if pg is None:
         return
     import torch
-    pg.barrier(device_ids=[local])
-    torch.cuda.synchronize(local)
+    if device.startswith("cuda"):
+        idx = int(device.split(":")[1])
+        pg.barrier(device_ids=[idx])
+        torch.cuda.synchronize(idx)
+    else:
+        pg.barrier()
+
+
+def replica_throughput(world, steps, dev_ms_max):
+    """frames/s of the whole job: every rank renders and reprints `steps` frames of its own; the job takes
+    the slowest rank's device time (replicas: no exchange between ranks)."""
+    return world * steps / (dev_ms_max / 1000.0)
 
 
 def cpu_reference_sample(resources, film_format_mm, steps=1):
@@ -228,7 +244,7 @@ def run_reference(args):
     return 0
 
 
-def run_e2e(args, eng, img, delta, pg, local, world):
+def run_e2e(args, eng, img, delta, pg, dev, world):
     """The workload through the C ABI with host buffers: spk_open from pinned host memory, spk_render,
     spk_set_params, spk_reprint, both results copied to pinned host memory and read in place."""
     import torch
@@ -249,13 +265,13 @@ def run_e2e(args, eng, img, delta, pg, local, world):
 
     for _ in range(args.warmup):
         e2e_step()
-    barrier(pg, local)
+    barrier(pg, dev)
     t0 = time.perf_counter()
     stride = 0
     for _ in range(args.steps):
         stride, _ = e2e_step()
-    e2e_s = reduce_max(pg, local, time.perf_counter() - t0)
-    barrier(pg, local)
+    e2e_s = reduce_max(pg, dev, time.perf_counter() - t0)
+    barrier(pg, dev)
     e2e = {"value": world * args.steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": W * H * 3 * 4,
            "d2h_bytes_per_step": 2 * stride * H * 8}
     return e2e
@@ -565,7 +581,7 @@ def main():
     if args.config == "precision":
         return run_precision(args)
 
-    rank, local, world, pg = dist_init(args.gpus)
+    rank, local, world, pg, dev = dist_init(args.gpus)
     resources = synth_resources.ensure(sc.RESOURCES)
     lib = sc.load()
     ff = film_format_for_grains(lib, resources, W)
@@ -581,22 +597,22 @@ def main():
     sess.set_params({"print_exposure": 1.2})
     sess.profile("full", True, args.warmup)
     sess.set_params({"print_exposure": 1.0})
-    barrier(pg, local)
+    barrier(pg, dev)
     # clocks are sampled every 100 ms from one second of untimed load before the timed steps to their end
     with Clocks(local) as clk:
         t_heat = time.perf_counter()
         while time.perf_counter() - t_heat < 1.0:
             sess.profile("full", False, 1)
-        barrier(pg, local)
+        barrier(pg, dev)
         t0 = time.perf_counter()
         pr = sess.profile("full", False, args.steps)
         sess.set_params({"print_exposure": 1.2})
         pp = sess.profile("full", True, args.steps)
         wall = time.perf_counter() - t0
-    barrier(pg, local)
+    barrier(pg, dev)
     dev_ms = sum(pr["total_ms"]) + sum(pp["total_ms"])
-    dev_ms_max = reduce_max(pg, local, dev_ms)
-    value = world * args.steps / (dev_ms_max / 1000.0)
+    dev_ms_max = reduce_max(pg, dev, dev_ms)
+    value = replica_throughput(world, args.steps, dev_ms_max)
     render_ms = sum(pr["total_ms"]) / args.steps
     reprint_ms = sum(pp["total_ms"]) / args.steps
     launches = int(pr["launches"] + pp["launches"])
@@ -639,7 +655,7 @@ def main():
     # ---- end to end through the C ABI with host buffers ----
     e2e = None
     if not args.no_e2e:
-        e2e = run_e2e(args, eng, img, delta, pg, local, world)
+        e2e = run_e2e(args, eng, img, delta, pg, dev, world)
     eng.close()
 
     cpu = None

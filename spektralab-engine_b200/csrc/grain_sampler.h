@@ -239,6 +239,7 @@ SPK_HD float spk_cosf(float x) {
 /* ---- the sampler ---- */
 
 #define SPK_TWO_PI 6.283185307179586f
+#define SPK_LOG_TWO_PI 0x1.d67f1ep+0f /* spk_logf(SPK_TWO_PI), bit for bit (0x3FEB3F8F) */
 
 SPK_HD float spk_lgamma_k(float x) {
     if (x == 1.0f || x == 2.0f) return 0.0f;
@@ -254,7 +255,7 @@ SPK_HD float spk_lgamma_k(float x) {
     g = SPK_ADD(SPK_MUL(g, x2), 7.936507936507937e-04f);
     g = SPK_ADD(SPK_MUL(g, x2), -2.777777777777778e-03f);
     g = SPK_ADD(SPK_MUL(g, x2), 8.333333333333333e-02f);
-    const float t1 = SPK_ADD(SPK_DIV(g, x0), SPK_MUL(0.5f, spk_logf(SPK_TWO_PI)));
+    const float t1 = SPK_ADD(SPK_DIV(g, x0), SPK_MUL(0.5f, SPK_LOG_TWO_PI));
     float gl = SPK_SUB(SPK_ADD(t1, SPK_MUL(SPK_SUB(x0, 0.5f), spk_logf(x0))), x0);
     if (x <= 7.0f) {
         for (int i = 0; i < n; ++i) {
@@ -268,7 +269,7 @@ SPK_HD float spk_lgamma_k(float x) {
 /* PTRS in pieces, so that a caller can run every draw's first attempt in lockstep and finish the
  * rest apart. Attempt `it` of a draw takes uniforms 2 it (U) and 2 it + 1 (V) of its stream. */
 typedef struct {
-    float lam, loglam, b, a, invalpha, vr;
+    float lam, loglam, b, a, invalpha, loginvalpha, vr;
 } spk_ptrs;
 
 #define SPK_PTRS_REJECT 0
@@ -284,10 +285,11 @@ SPK_HD void spk_ptrs_init(spk_ptrs* p, float lam) {
     p->vr = SPK_SUB(0.9277f, SPK_DIV(3.6224f, SPK_SUB(p->b, 2.0f)));
 }
 
-/* the constants only the full test reads: log lam and 1 / alpha (after spk_ptrs_init) */
+/* the constants only the full test reads: log lam, 1 / alpha and its log (after spk_ptrs_init) */
 SPK_HD void spk_ptrs_init_test(spk_ptrs* p) {
     p->loglam = spk_logf(p->lam);
     p->invalpha = SPK_ADD(1.1239f, SPK_DIV(1.1328f, SPK_SUB(p->b, 3.4f)));
+    p->loginvalpha = spk_logf(p->invalpha);
 }
 
 /* the candidate k of an attempt and its two squeezes */
@@ -305,7 +307,7 @@ SPK_HD int spk_ptrs_squeeze(const spk_ptrs* p, float u, float V, float* k_out, f
 
 /* the full acceptance test: log V + log(1/alpha) - log(a / us^2 + b) <= -lam + k log lam - log k! */
 SPK_HD int spk_ptrs_test(const spk_ptrs* p, float V, float k, float us) {
-    const float L = SPK_SUB(SPK_ADD(spk_logf(V), spk_logf(p->invalpha)),
+    const float L = SPK_SUB(SPK_ADD(spk_logf(V), p->loginvalpha),
                             spk_logf(SPK_ADD(SPK_DIV(p->a, SPK_MUL(us, us)), p->b)));
     const float Rt = SPK_SUB(SPK_ADD(-p->lam, SPK_MUL(k, p->loglam)), spk_lgamma_k(SPK_ADD(k, 1.0f)));
     return L <= Rt;

@@ -64,6 +64,9 @@ def test_elementary_functions_error_bounds():
     assert np.abs(got - np.cos(cx.astype(np.float64))).max() <= 2e-7
     assert L.orc_logf(0.0) == -np.inf and np.isnan(L.orc_logf(-1.0))
     assert L.orc_expf(-200.0) == 0.0 and L.orc_expf(100.0) == np.inf
+    # the sampler's lgamma takes log(2 pi) as a constant: the sampler's own log of SPK_TWO_PI, bit for bit
+    two_pi = np.float32(6.283185307179586)
+    assert np.float32(L.orc_logf(float(two_pi))).view(np.uint32) == 0x3FEB3F8F
 
 
 def test_sampler_against_reference():
