@@ -338,8 +338,14 @@ void fill_launch(dev::IirLaunch& q, const std::vector<MixtureComponent>& comps, 
             d.B1 = k.B1;
             d.B2 = k.B2;
             d.B3 = k.B3;
-            // M^(2^p): the map through L 2^p steps, iterated directly
-            for (int p = 0; p < dev::kIirScanSteps; ++p) entry_map(k, L << p, d.Mp[p]);
+            // M^(2^p), the map through L 2^p steps: the map through L steps, then squared (7 products of
+            // 3 x 3 matrices instead of 381 L steps of the recurrence on the host before every launch)
+            entry_map(k, L, d.Mp[0]);
+            for (int p = 1; p < dev::kIirScanSteps; ++p)
+                for (int r = 0; r < 3; ++r)
+                    for (int c2 = 0; c2 < 3; ++c2)
+                        d.Mp[p][r][c2] = (d.Mp[p - 1][r][0] * d.Mp[p - 1][0][c2] + d.Mp[p - 1][r][1] * d.Mp[p - 1][1][c2]) +
+                                         d.Mp[p - 1][r][2] * d.Mp[p - 1][2][c2];
             d.active = 1;
         }
 }
