@@ -73,6 +73,11 @@ void encode(const float* rgb, const float* g, uint16_t* out, uint32_t w, uint32_
 // transfer function, RGBA16. scan_encode_fits tells whether the tiled kernel takes this frame and these radii.
 bool scan_encode_fits(uint32_t w, uint32_t h, int r1, int r2);
 void scan_encode(const float* rgb, uint16_t* out, uint32_t w, uint32_t h, const ScanArgs& a, cudaStream_t s);
+// the same for output rows row0 .. row1 - 1 only (row0 a multiple of scan_tile_rows(); the rows' halo of
+// the print output must be written)
+void scan_encode_rows(const float* rgb, uint16_t* out, uint32_t w, uint32_t h, uint32_t row0, uint32_t row1,
+                      const ScanArgs& a, cudaStream_t s);
+constexpr uint32_t scan_tile_rows() { return 32; }
 
 // A separable FIR (taps[0..2r], the same for the three channels) with both passes in one tiled kernel;
 // out must not alias in. fir_tile_fits tells whether the tiled kernel takes this frame and radius.

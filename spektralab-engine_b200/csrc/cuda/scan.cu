@@ -28,6 +28,7 @@ namespace spkb::dev {
 namespace {
 
 constexpr int kTW = 32, kTH = 32, kThreads = 256, kWarps = kThreads / 32;
+static_assert(uint32_t(kTH) == scan_tile_rows(), "row bands start on tile rows");
 
 // half-sample symmetric reflection, exact for p in [-n, 2n)
 __device__ __forceinline__ int reflect_near(int p, int n) { return p < 0 ? -1 - p : (p >= n ? 2 * n - 1 - p : p); }
@@ -157,9 +158,9 @@ __device__ __forceinline__ void scan_tile(const ScanArgs& a, const float* __rest
 
 template <int R1, int R2>
 __global__ void __launch_bounds__(kThreads) k_scan_encode(const float* __restrict__ rgb, uint16_t* __restrict__ out,
-                                                          int w, int h, const __grid_constant__ ScanArgs a) {
+                                                          int w, int h, int row0, const __grid_constant__ ScanArgs a) {
     extern __shared__ float smem[];
-    scan_tile<R1, R2>(a, rgb, out, w, h, blockIdx.x * kTW, blockIdx.y * kTH, smem);
+    scan_tile<R1, R2>(a, rgb, out, w, h, blockIdx.x * kTW, row0 + int(blockIdx.y) * kTH, smem);
 }
 
 // The scanner stage of many frames in one persistent launch: the CTAs take tiles t = blockIdx.x,
@@ -239,11 +240,12 @@ size_t scan_smem_bytes(int r1, int r2) {
 }
 
 template <int R1, int R2>
-void launch_scan(const float* rgb, uint16_t* out, uint32_t w, uint32_t h, const ScanArgs& a, cudaStream_t s) {
+void launch_scan(const float* rgb, uint16_t* out, uint32_t w, uint32_t h, uint32_t row0, uint32_t row1,
+                 const ScanArgs& a, cudaStream_t s) {
     const size_t smem = scan_smem_bytes(a.r1, a.r2);  // at most 96 KB (r1 = r2 = 9)
     ensure_smem(reinterpret_cast<const void*>(k_scan_encode<R1, R2>), int(smem));
-    const dim3 g((w + kTW - 1) / kTW, (h + kTH - 1) / kTH);
-    k_scan_encode<R1, R2><<<g, kThreads, smem, s>>>(rgb, out, int(w), int(h), a);
+    const dim3 g((w + kTW - 1) / kTW, (row1 - row0 + kTH - 1) / kTH);
+    k_scan_encode<R1, R2><<<g, kThreads, smem, s>>>(rgb, out, int(w), int(h), int(row0), a);
 }
 
 }  // namespace
@@ -254,12 +256,17 @@ bool scan_encode_fits(uint32_t w, uint32_t h, int r1, int r2) {
            h >= uint32_t(R) + 1 && (uint64_t(h) + kTH - 1) / kTH <= 65535u;
 }
 
-void scan_encode(const float* rgb, uint16_t* out, uint32_t w, uint32_t h, const ScanArgs& a, cudaStream_t s) {
-    if (uint64_t(w) * h == 0) return;
+void scan_encode_rows(const float* rgb, uint16_t* out, uint32_t w, uint32_t h, uint32_t row0, uint32_t row1,
+                      const ScanArgs& a, cudaStream_t s) {
+    if (uint64_t(w) * h == 0 || row1 <= row0) return;
     Probe p("scan_encode", s);
-    if (a.r1 == 5 && a.r2 == 2) launch_scan<5, 2>(rgb, out, w, h, a, s);
-    else if (a.r1 == 0 && a.r2 == 2) launch_scan<0, 2>(rgb, out, w, h, a, s);
-    else launch_scan<-1, -1>(rgb, out, w, h, a, s);
+    if (a.r1 == 5 && a.r2 == 2) launch_scan<5, 2>(rgb, out, w, h, row0, row1, a, s);
+    else if (a.r1 == 0 && a.r2 == 2) launch_scan<0, 2>(rgb, out, w, h, row0, row1, a, s);
+    else launch_scan<-1, -1>(rgb, out, w, h, row0, row1, a, s);
+}
+
+void scan_encode(const float* rgb, uint16_t* out, uint32_t w, uint32_t h, const ScanArgs& a, cudaStream_t s) {
+    scan_encode_rows(rgb, out, w, h, 0, h, a, s);
 }
 
 namespace {

@@ -134,6 +134,8 @@ public:
     std::string id;
     std::mutex m;
     cudaStream_t stream = nullptr;
+    cudaStream_t copy_stream = nullptr;     // the result's copy to host memory, in row bands
+    std::vector<cudaEvent_t> band_events;  // their events (grown by the print side as needed)
     Pool pool;
     bool product_defaults = false;
     Plane source;
@@ -161,6 +163,11 @@ public:
             cudaStreamSynchronize(stream);
             cudaStreamDestroy(stream);
         }
+        if (copy_stream) {
+            cudaStreamSynchronize(copy_stream);
+            cudaStreamDestroy(copy_stream);
+        }
+        for (cudaEvent_t e : band_events) cudaEventDestroy(e);
     }
 
     void digest(ParamSet& p, const Profile& f) const {
@@ -308,6 +315,7 @@ Session* open_session(Engine& e, const void* data, bool device_ptr, uint32_t w, 
     s->engine = &e;
     s->product_defaults = d.product_defaults.value_or(false);
     cuda_check(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    cuda_check(cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking), "cudaStreamCreate");
     s->pool.set_stream(s->stream);
     ParamSet p;
     for (const auto& [fid, v] : d.fields)
@@ -399,14 +407,19 @@ void render(Session& s, const char* tier_name, bool reprint, spk_result* out) {
         ctx.pitch_um = ts.pitch_um;
         s.node();
         img = output_acquire(s.engine->device, s.source.w, s.source.h);
-        print_scan_encode(ctx, s.pipe, s.live, ts.negative, img);
-        cuda_check(cudaMemcpyAsync(img->host, img->dev, img->bytes, cudaMemcpyDeviceToHost, s.stream), "result copy");
+        ctx.copy_stream = s.copy_stream;
+        ctx.band_events = &s.band_events;
+        if (!print_scan_encode(ctx, s.pipe, s.live, ts.negative, img, true))
+            cuda_check(cudaMemcpyAsync(img->host, img->dev, img->bytes, cudaMemcpyDeviceToHost, s.stream),
+                       "result copy");
         cuda_check(cudaStreamSynchronize(s.stream), "render");
         cuda_check(cudaGetLastError(), "render");
     } catch (...) {
+        // band copies may still be writing the image's host pixels
+        (void)cudaStreamSynchronize(s.copy_stream);
+        (void)cudaStreamSynchronize(s.stream);
         if (img) output_release(img);
         if (developed) ts.negative = Plane{};
-        (void)cudaStreamSynchronize(s.stream);
         try {
             throw;
         } catch (const Error& e) {

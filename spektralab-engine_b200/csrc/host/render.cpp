@@ -733,21 +733,69 @@ void print_stage(RenderCtx& ctx, const Pipeline& p, const LiveParams& live, cons
 }
 }  // namespace
 
-void print_scan_encode(RenderCtx& ctx, const Pipeline& p, const LiveParams& live, const Plane& negative,
-                       OutputImage* img) {
+namespace {
+constexpr uint32_t kBandRows = 8 * dev::scan_tile_rows();
+
+// The print and the tiled scanner in row bands, each band's RGBA16 rows copied to the host on the copy
+// stream while the next band's kernels run. Band b's scanner reads the print output up to kernel radius
+// r1 + r2 rows past its last row, so the print runs that far ahead; the print is per pixel and the scanner
+// per tile, so the bands write what the whole-frame launches write.
+void print_scan_banded(RenderCtx& ctx, const Pipeline& p, const LiveParams& live, const Plane& negative,
+                       const Plane& rgb, OutputImage* img, const ScanArgs& sa) {
+    const uint32_t w = negative.w, h = negative.h;
+    const uint32_t halo = uint32_t(sa.r1 + sa.r2);
+    const uint32_t nb = (h + kBandRows - 1) / kBandRows;
+    std::vector<cudaEvent_t>& ev = *ctx.band_events;
+    while (ev.size() < nb + 1) {
+        cudaEvent_t e = nullptr;
+        cuda_check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "band event");
+        ev.push_back(e);
+    }
+    PrintArgs a = print_args(p, live, 0);
+    const size_t row_bytes = size_t(img->stride_px) * 4 * sizeof(uint16_t);
+    uint32_t printed = 0;
+    for (uint32_t b = 0; b < nb; ++b) {
+        const uint32_t r0 = b * kBandRows, r1 = std::min(h, r0 + kBandRows);
+        const uint32_t need = std::min(h, r1 + halo);
+        if (need > printed) {
+            a.n = (need - printed) * w;
+            dev::print(negative.data() + size_t(printed) * w * 3, rgb.data() + size_t(printed) * w * 3, a, ctx.stream);
+            printed = need;
+        }
+        dev::scan_encode_rows(rgb.data(), img->dev, w, h, r0, r1, sa, ctx.stream);
+        cuda_check(cudaEventRecord(ev[b], ctx.stream), "band event");
+        cuda_check(cudaStreamWaitEvent(ctx.copy_stream, ev[b], 0), "band event");
+        cuda_check(cudaMemcpyAsync(reinterpret_cast<unsigned char*>(img->host) + size_t(r0) * row_bytes,
+                                   reinterpret_cast<const unsigned char*>(img->dev) + size_t(r0) * row_bytes,
+                                   size_t(r1 - r0) * row_bytes, cudaMemcpyDeviceToHost, ctx.copy_stream),
+                   "result copy");
+    }
+    cuda_check(cudaEventRecord(ev[nb], ctx.copy_stream), "band event");
+    cuda_check(cudaStreamWaitEvent(ctx.stream, ev[nb], 0), "band event");
+}
+}  // namespace
+
+bool print_scan_encode(RenderCtx& ctx, const Pipeline& p, const LiveParams& live, const Plane& negative,
+                       OutputImage* img, bool to_host) {
     const PrintSetup& s = *p.print;
     const uint32_t w = negative.w, h = negative.h;
     Plane rgb = make_plane(ctx.pool, w, h);
+    ScanArgs sa;
+    const bool tiled = scan_args(p, ctx.rho_tier, w, h, img->stride_px, sa);
+    if (to_host && tiled && ctx.print_mode < 0 && ctx.copy_stream && ctx.band_events && h > kBandRows) {
+        Stage st(ctx, "print_scanner");
+        print_scan_banded(ctx, p, live, negative, rgb, img, sa);
+        return true;
+    }
     {
         Stage st(ctx, "print");
         print_stage(ctx, p, live, negative, rgb);
     }
-    ScanArgs sa;
-    if (scan_args(p, ctx.rho_tier, w, h, img->stride_px, sa)) {
+    if (tiled) {
         // the scanner's blurs on the FIR branch: one tiled pass from the print output to RGBA16
         Stage st(ctx, "scanner");
         dev::scan_encode(rgb.data(), img->dev, w, h, sa, ctx.stream);
-        return;
+        return false;
     }
     EncodeArgs e = encode_args(s, img->stride_px);
     Plane gpl;
@@ -769,6 +817,7 @@ void print_scan_encode(RenderCtx& ctx, const Pipeline& p, const LiveParams& live
         Stage st(ctx, "encode");
         dev::encode(rgb.data(), gpl ? gpl.data() : nullptr, img->dev, w, h, e, ctx.stream);
     }
+    return false;
 }
 
 

@@ -47,6 +47,10 @@ struct RenderCtx {
     int print_mode = -1;
     uint32_t print_bins = SPKB_NL;
     float* contraction_out = nullptr;
+    // the print side's copy to the output image's host pixels, in row bands on copy_stream (events from
+    // band_events, grown as needed), overlapping the next band's kernels; null: no banded copy
+    cudaStream_t copy_stream = nullptr;
+    std::vector<cudaEvent_t>* band_events = nullptr;
 };
 
 // Stage timing with CUDA events on the render stream (bench and profile entry points).
@@ -80,9 +84,11 @@ PrintArgs print_args(const Pipeline& p, const LiveParams& live, uint32_t pixels)
 // frame or the scanner's blurs need the separate passes (a recursive blur, a frame narrower than the halo).
 bool scan_args(const Pipeline& p, double rho_tier, uint32_t w, uint32_t h, uint32_t stride_px, ScanArgs& out);
 
-// print side: negative -> RGBA16 into img->dev (row pitch img->stride_px); no host copy
-void print_scan_encode(RenderCtx& ctx, const Pipeline& p, const LiveParams& live, const Plane& negative,
-                       OutputImage* img);
+// print side: negative -> RGBA16 into img->dev (row pitch img->stride_px). With to_host and a copy stream
+// in ctx, the rows are also copied to img->host, band by band as they are written, and true is returned
+// (the stream then orders after the copies); false: no host copy was made.
+bool print_scan_encode(RenderCtx& ctx, const Pipeline& p, const LiveParams& live, const Plane& negative,
+                       OutputImage* img, bool to_host = false);
 
 // The adjoint of the render. The differentiated output y is the scanned linear RGB (print, scanner lens
 // blur and unsharp mask; before the output transfer function and the 16-bit encode) of the source frame,
