@@ -61,10 +61,10 @@ N_SM = 148
 # From the ncu capture summarised in profiles/render_kernels_2048x2048_ncu.md (one 2048 x 2048 render +
 # reprint, --set full): DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) and warp instructions
 # (smsp__inst_executed.sum) per pixel of each kernel's launch. Traffic scales with the pixels launched.
-NCU_TRAFFIC_PER_PX = {"expose": 14.17, "iir_rows": 25.03, "iir_cols": 54.04, "develop_layers": 14.08,
-                      "fir_tile": 14.24, "print": 13.00, "scan_encode": 13.13}
-NCU_WARP_INST_PER_PX = {"expose": 15.07, "iir_rows": 18.28, "iir_cols": 13.01, "develop_layers": 174.92,
-                        "fir_tile": 10.06, "print": 60.29, "scan_encode": 28.16}
+NCU_TRAFFIC_PER_PX = {"expose": 14.20, "iir_rows": 25.09, "iir_cols": 54.05,
+                      "develop_layers": 14.39, "fir_tile": 14.46, "print": 12.94, "scan_encode": 13.29}
+NCU_WARP_INST_PER_PX = {"expose": 15.07, "iir_rows": 18.37, "iir_cols": 13.05,
+                        "develop_layers": 171.30, "fir_tile": 10.06, "print": 60.29, "scan_encode": 28.23}
 
 
 def workload_name():
