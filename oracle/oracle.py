@@ -41,6 +41,8 @@ class OracleSetup(ctypes.Structure):
         ("cmax", PD), ("lc_active", I32),
         ("scanner_lens_blur", D), ("unsharp_sigma", D), ("unsharp_amount", D),
         ("cctf_active", I32), ("cctf_mode", I32), ("m_nid", D * 9),
+        ("couplers", I32), ("n_dir", I32), ("coupler_m", D * 9), ("dmax", D * 3), ("cy0", PD),
+        ("dir_w", (D * 3) * MAXC), ("dir_s", (D * 3) * MAXC),
     ]
 
 
@@ -179,6 +181,17 @@ class Oracle:
         s.cctf_active = 1 if f64["cctf_active"] else 0
         s.cctf_mode = int(f64["cctf_mode"])
         put("m_nid", f64["m_nid"])
+        cp = f64.get("couplers")
+        if cp and cp["active"]:
+            s.couplers = 1
+            put("coupler_m", cp["m"])
+            put("dmax", cp["dmax"])
+            s.cy0 = buf(cp["y0"])
+            s.n_dir = len(cp["dir"])
+            for k, (w, sg) in enumerate(cp["dir"]):
+                for c in range(3):
+                    s.dir_w[k][c] = w[c]
+                    s.dir_s[k][c] = sg[c]
         self.s = s
 
     def render(self, rgb, counts=None):

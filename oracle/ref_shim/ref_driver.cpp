@@ -11,6 +11,7 @@
 
 #include "film/film_internal.hpp"
 #include "film_shared.h"
+#include "fx/dir_blur.hpp"
 #include "fx/fx_internal.hpp"
 #include "fx/grain.hpp"
 #include "fx/halation.hpp"
@@ -65,7 +66,7 @@ Built build(Engine& e, const char* delta_text) {
 }
 
 // develop() with the bounce mixture replaced (stage order of src/film/develop.cpp:101-236 for the
-// identity geometry, no auto exposure, no boost, no headroom and no couplers)
+// identity geometry, no auto exposure, no boost and no headroom)
 gpu::Plane develop_override(core::RenderContext& ctx, const film::FilmSetup& setup, const gpu::Plane& src,
                             uint32_t seed, uint32_t n, const double* weights, const double* sigmas,
                             const double* strength) {
@@ -114,12 +115,41 @@ gpu::Plane develop_override(core::RenderContext& ctx, const film::FilmSetup& set
         bt.dispatch_1d(ctx.kernel("spk_film_log"), a.n, {gpu::Arg::plane(plane), gpu::Arg::value(a)});
         bt.commit_and_wait();
     }
+    // the curves develop into a second plane when the couplers need the log exposure again
+    gpu::Plane developed = s.couplers ? ctx.scratch(plane.w, plane.h) : plane;
     {
         SpkFilmCurvesArgs a{uint32_t(plane.pixels()), s.curves.K, 0u};
         gpu::Batch bt = ctx.gpu.batch();
         bt.dispatch_1d(ctx.kernel("spk_film_curves"), a.n,
-                       {gpu::Arg::plane(plane), gpu::Arg::plane(plane), gpu::Arg::buffer(s.curve_buffer), gpu::Arg::value(a)});
+                       {gpu::Arg::plane(plane), gpu::Arg::plane(developed), gpu::Arg::buffer(s.curve_buffer),
+                        gpu::Arg::value(a)});
         bt.commit_and_wait();
+    }
+    if (s.couplers) {
+        // DIR couplers (src/film/develop.cpp:203-226): the first development becomes the inhibitor source,
+        // is diffused, and corrects the log exposure before the second lookup through the curves
+        SpkFilmCouplerArgs ca{};
+        ca.n = uint32_t(developed.pixels());
+        ca.positive = s.positive ? 1u : 0u;
+        for (size_t i = 0; i < 9; ++i) ca.m[i] = s.coupler_m_f32[i];
+        for (size_t c = 0; c < 3; ++c) ca.dmax[c] = s.dmax_f32[c];
+        {
+            gpu::Batch bt = ctx.gpu.batch();
+            bt.dispatch_1d(ctx.kernel("spk_film_coupler_source"), ca.n,
+                           {gpu::Arg::plane(developed), gpu::Arg::value(ca)});
+            bt.commit_and_wait();
+        }
+        fx::dir_diffusion_blur(ctx, developed);
+        SpkFilmCouplerApplyArgs aa{uint32_t(plane.pixels()), s.curves.K};
+        {
+            gpu::Batch bt = ctx.gpu.batch();
+            bt.dispatch_1d(ctx.kernel("spk_film_coupler_apply"), aa.n,
+                           {gpu::Arg::plane(plane), gpu::Arg::plane(developed), gpu::Arg::buffer(s.curve_buffer),
+                            gpu::Arg::value(aa)});
+            bt.commit_and_wait();
+        }
+    } else {
+        plane = developed;
     }
     if (s.grain) fx::grain(ctx, plane, *s.grain, seed);
     gpu::Plane negative = ctx.gpu.persistent_plane(plane.w, plane.h, gpu::MemTag::Negative);

@@ -199,9 +199,9 @@ static size_t search_right(const double* x, size_t K, size_t stride, double v) {
     return lo;
 }
 
-static double curve(const OracleSetup* s, int c, double v) {
+static double curve_y(const OracleSetup* s, const double* table, int c, double v) {
     const double* x = s->cx;
-    const double* y = s->cy + (size_t)c * s->K;
+    const double* y = table + (size_t)c * s->K;
     if (v <= x[0]) return y[0];
     if (v >= x[s->K - 1]) return y[s->K - 1];
     const size_t lo = search_right(x, (size_t)s->K, 1, v);
@@ -209,6 +209,8 @@ static double curve(const OracleSetup* s, int c, double v) {
     const double t = (v - x[l]) * s->cinv[l];
     return y[l] + t * (y[l + 1] - y[l]);
 }
+
+static double curve(const OracleSetup* s, int c, double v) { return curve_y(s, s->cy, c, v); }
 
 static double grain_value(const OracleSetup* s, double D, int c, uint32_t pixel, const float* counts) {
     const double v = s->positive ? -D : D;
@@ -261,6 +263,23 @@ static int develop_impl(const OracleSetup* s, const float* rgb, const double* rg
     double* D = (double*)malloc(N * sizeof(double));
 #pragma omp parallel for
     for (size_t i = 0; i < N; ++i) D[i] = curve(s, (int)(i % 3), log10(fmax(H[i], 0.0) + 1e-10));
+    if (s->couplers) {
+        /* the correction from the first development, its diffusion, then the pre-inverted curve */
+        double* chi = (double*)malloc(N * sizeof(double));
+#pragma omp parallel for
+        for (size_t p = 0; p < n; ++p) {
+            double sv[3];
+            for (int c = 0; c < 3; ++c) sv[c] = s->positive ? s->dmax[c] - D[3 * p + c] : D[3 * p + c];
+            for (int m = 0; m < 3; ++m)
+                chi[3 * p + m] = (sv[0] * s->coupler_m[m] + sv[1] * s->coupler_m[3 + m]) + sv[2] * s->coupler_m[6 + m];
+        }
+        const double zero[3] = {0.0, 0.0, 0.0}, one[3] = {1.0, 1.0, 1.0};
+        if (s->n_dir > 0) mixture_mix(chi, w, h, s->n_dir, s->dir_w, s->dir_s, zero, one);
+#pragma omp parallel for
+        for (size_t i = 0; i < N; ++i)
+            D[i] = curve_y(s, s->cy0, (int)(i % 3), log10(fmax(H[i], 0.0) + 1e-10) - chi[i]);
+        free(chi);
+    }
     if (!s->grain) {
         memcpy(neg, D, N * sizeof(double));
     } else {

@@ -60,6 +60,13 @@ typedef struct {
     double scanner_lens_blur, unsharp_sigma, unsharp_amount;
     int32_t cctf_active, cctf_mode;
     double m_nid[9];
+    /* DIR couplers (reference src/film/develop.cpp:203-226): chi_m := sum_c s_c M[c][m] with
+     * s := positive ? dmax - D : D from the first development D, chi := sum_k dir_w[k] G(dir_s[k]) chi,
+     * then the density is the pre-inverted curve cy0 at log10 exposure - chi */
+    int32_t couplers, n_dir;
+    double coupler_m[9], dmax[3];
+    const double* cy0; /* 3K, channel-major */
+    double dir_w[ORC_MAX_COMP][3], dir_s[ORC_MAX_COMP][3];
 } OracleSetup;
 
 /* The whole render of a w x h frame; rgb is 3 floats per pixel (already non-finite-cleaned),

@@ -297,6 +297,26 @@ __device__ __forceinline__ float grain_draw(float d, float D, float n, float u, 
     return SPK_MUL(k, SPK_MUL(SPK_DIV(D, n), sat));
 }
 
+// DIR couplers' source (reference kernels/film.metal:242-276): L = log10(max(H, 0) + 1e-10), D = the curve at
+// L, s_c = positive ? dmax_c - D_c : D_c, chi_m = (s_0 M[0][m] + s_1 M[1][m]) + s_2 M[2][m], each operation
+// rounded as written
+__global__ void k_coupler_source(const float* __restrict__ exposure, float* __restrict__ chi,
+                                 const __grid_constant__ CouplerArgs q) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= q.n) return;
+    float sv[3];
+#pragma unroll
+    for (uint32_t c = 0; c < 3; ++c) {
+        const float L = log10f(fmaxf(exposure[3 * size_t(i) + c], 0.0f) + 1e-10f);
+        const float D = curve_lookup(q.cx, q.cinv, q.cy + size_t(c) * q.K, q.K, q.cgrid, L);
+        sv[c] = q.positive ? __fsub_rn(q.dmax[c], D) : D;
+    }
+#pragma unroll
+    for (uint32_t m = 0; m < 3; ++m)
+        chi[3 * size_t(i) + m] = __fadd_rn(__fadd_rn(__fmul_rn(sv[0], q.m[m]), __fmul_rn(sv[1], q.m[3 + m])),
+                                           __fmul_rn(sv[2], q.m[6 + m]));
+}
+
 __global__ void k_develop(const float* __restrict__ exposure, float* __restrict__ out, uint32_t w, uint32_t h,
                           const __grid_constant__ DevelopArgs q) {
     const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
@@ -305,7 +325,8 @@ __global__ void k_develop(const float* __restrict__ exposure, float* __restrict_
     const uint32_t pixel = y * q.width + x;
     const size_t o = 3 * (size_t(y) * w + x);
     for (uint32_t c = 0; c < 3; ++c) {
-        const float L = log10f(fmaxf(exposure[o + c], 0.0f) + 1e-10f);
+        float L = log10f(fmaxf(exposure[o + c], 0.0f) + 1e-10f);
+        if (q.chi) L = __fsub_rn(L, q.chi[o + c]);  // DIR couplers: the corrected log exposure, the y0 curve
         const float D = curve_lookup(q.cx, q.cinv, q.cy + size_t(c) * q.K, q.K, q.cgrid, L);
         if (!q.grain) {
             out[o + c] = D;
@@ -419,7 +440,8 @@ __global__ void __launch_bounds__(kDrawWarps * 32) k_develop_layers(const float*
     for (int c = 0; c < 3; ++c) {
         float dl[3] = {0.0f, 0.0f, 0.0f};
         if (live) {
-            const float L = log10f(fmaxf(exposure[o + c], 0.0f) + 1e-10f);
+            float L = log10f(fmaxf(exposure[o + c], 0.0f) + 1e-10f);
+            if (q.chi) L = __fsub_rn(L, q.chi[o + c]);  // DIR couplers: the corrected log exposure, the y0 curve
             const float D = curve_lookup(q.cx, q.cinv, q.cy + size_t(c) * q.K, q.K, q.cgrid, L);
             layer_densities(q, uint32_t(c), q.positive ? -D : D, dl);
         }
@@ -676,6 +698,12 @@ void develop(const float* exposure, float* out, const DevelopArgs& a, uint32_t w
     const dim3 b(32, 4), g(div_up(w, 32), div_up(h, 4));
     Probe p("develop", s);
     k_develop<<<g, b, 0, s>>>(exposure, out, w, h, a);
+}
+
+void coupler_source(const float* exposure, float* chi, const CouplerArgs& a, cudaStream_t s) {
+    if (a.n == 0) return;
+    Probe p("coupler_source", s);
+    k_coupler_source<<<div_up(a.n, 256), 256, 0, s>>>(exposure, chi, a);
 }
 
 void encode(const float* rgb, const float* g, uint16_t* out, uint32_t w, uint32_t h, const EncodeArgs& e,

@@ -51,6 +51,9 @@ void lincomb(const float* x, const float* y, float* out, size_t pixels, const fl
              cudaStream_t s);
 void copy(const float* x, float* out, size_t pixels, cudaStream_t s);
 
+// DIR couplers: exposure -> the coupler correction chi (before its diffusion blur).
+void coupler_source(const float* exposure, float* chi, const CouplerArgs& a, cudaStream_t s);
+
 // log10 exposure -> density curves -> grain draw (grain mode) or density (no grain).
 void develop(const float* exposure, float* out, const DevelopArgs& a, uint32_t w, uint32_t h, cudaStream_t s);
 

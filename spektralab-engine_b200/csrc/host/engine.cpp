@@ -1404,6 +1404,23 @@ json::Value setup_f64(const FilmSetup& f, const PrintSetup& p, const PrintRun& r
     r["curve_x"] = arr(cx.data(), K);
     r["curve_inv"] = arr(cinv.data(), K);
     r["curve_y"] = arr(cy.data(), 3 * K);
+    {
+        // DIR couplers: the matrix, D_max, the pre-inverted curve and the diffusion mixture at this pitch
+        json::Value cp;
+        cp["active"] = f.couplers;
+        cp["m"] = arr(f.coupler_m.data(), 9);
+        cp["dmax"] = arr(f.dmax.data(), 3);
+        cp["y0"] = arr(f.cy0_64.data(), f.cy0_64.size());
+        json::Array dir;
+        for (const MixtureComponent& m : dir_diffusion_components(pitch_um)) {
+            json::Array pair;
+            pair.push_back(arr(m.weight.data(), 3));
+            pair.push_back(arr(m.sigma.data(), 3));
+            dir.push_back(json::Value(std::move(pair)));
+        }
+        cp["dir"] = json::Value(std::move(dir));
+        r["couplers"] = std::move(cp);
+    }
     if (f.grain && f.grain->K) {
         const GrainSetup& g = *f.grain;
         const GrainConstants kc = grain_constants(g, pitch_um);

@@ -32,10 +32,11 @@ void upload_tables(Pool& pool, cudaStream_t s, Pipeline& p) {
             for (size_t c = 0; c < 3; ++c) t4[4 * i + c] = f.table32[3 * i + c];
         upload(pool, s, p.dev.table, t4.data(), t4.size() * sizeof(float));
     }
-    std::vector<float> c(5 * size_t(f.K));
+    std::vector<float> c(8 * size_t(f.K));
     std::memcpy(c.data(), f.cx.data(), f.K * sizeof(float));
     std::memcpy(c.data() + f.K, f.cinv.data(), f.K * sizeof(float));
     std::memcpy(c.data() + 2 * f.K, f.cy.data(), 3 * f.K * sizeof(float));
+    std::memcpy(c.data() + 5 * f.K, f.cy0.data(), 3 * f.K * sizeof(float));
     upload(pool, s, p.dev.curves, c.data(), c.size() * sizeof(float));
     if (f.grain && f.grain->K) {
         upload(pool, s, p.dev.gaxis, f.grain->axis.data(), f.grain->axis.size() * sizeof(float));
@@ -387,7 +388,6 @@ void check_supported(const ParamSet& p) {
         fail_user(what + " is outside this B200 build's render path");
     };
     if (p.b(P::auto_exposure)) refuse("auto_exposure=true (the meter)");
-    if (p.b(P::dir_couplers_active)) refuse("dir_couplers_active=true (DIR couplers)");
     if (p.b(P::glare_active) && p.f(P::glare_amount) > 0.0) refuse("glare_active=true (print glare)");
     if (p.b(P::input_cctf_decoding)) refuse("input_cctf_decoding=true (input transfer decode)");
     if (p.f(P::halation_boost_ev) != 0.0) refuse("halation_boost_ev != 0 (highlight boost)");
@@ -510,6 +510,72 @@ DevelopPlan develop_plan(const RenderCtx& ctx, const Pipeline& p, uint32_t w, ui
 
 }  // namespace
 
+std::vector<MixtureComponent> dir_diffusion_components(double pitch_um) {
+    constexpr double kCoreUm = 20.0, kTailUm = 200.0, kTailWeight = 0.06;
+    std::vector<MixtureComponent> comps;
+    MixtureComponent core;
+    const double s = kCoreUm / pitch_um;
+    for (int c = 0; c < 3; ++c) {
+        core.weight[c] = 1.0 - kTailWeight;
+        core.sigma[c] = s;
+    }
+    comps.push_back(core);
+    const double lam = kTailUm / pitch_um;
+    for (const MixtureComponent& m : exponential_surrogate(Vec3{kTailWeight, kTailWeight, kTailWeight}, Vec3{lam, lam, lam}))
+        comps.push_back(m);
+    return comps;
+}
+
+namespace {
+// DIR couplers (reference src/film/develop.cpp:203-226): the correction chi from the first development of
+// the exposure H, blurred by the diffusion mixture; the develop then reads the pre-inverted curve y0 at the
+// log exposure minus chi (da.cy, da.chi set here).
+Plane dir_couplers(RenderCtx& ctx, const Pipeline& p, const Plane& H, DevelopArgs& da) {
+    const FilmSetup& f = *p.film;
+    if (!(ctx.pitch_um > 0.0)) fail_internal("DIR couplers without a pixel pitch");
+    CouplerArgs q{};
+    q.cx = da.cx;
+    q.cinv = da.cinv;
+    q.cy = da.cy;
+    q.K = da.K;
+    q.cgrid = da.cgrid;
+    q.positive = f.positive ? 1u : 0u;
+    for (int i = 0; i < 9; ++i) q.m[i] = f.coupler_m_f32[size_t(i)];
+    for (int c = 0; c < 3; ++c) q.dmax[c] = f.dmax_f32[size_t(c)];
+    q.n = uint32_t(H.pixels());
+    Plane chi = make_plane(ctx.pool, H.w, H.h);
+    dev::coupler_source(H.data(), chi.data(), q, ctx.stream);
+    // the diffusion: the FIR components (the 20 um core below 60 um pitch) into a side plane, the recursive
+    // ones (the tail's surrogate) in one block-parallel mixture launch pair in place, then their sum
+    const std::vector<MixtureComponent> comps = dir_diffusion_components(ctx.pitch_um);
+    std::vector<MixtureComponent> fir, iir;
+    for (const MixtureComponent& m : comps) {
+        bool rec = true;
+        for (int c = 0; c < 3; ++c) rec = rec && blur_branch(m.sigma[c]) == Branch::Iir;
+        (rec ? iir : fir).push_back(m);
+    }
+    if (iir.empty() || fir.size() > 1 || !dev::iir_mixture_fits(chi.w, chi.h)) {
+        gaussian_mixture(ctx, chi, chi, comps);
+    } else {
+        Plane core;
+        if (!fir.empty()) {
+            core = make_plane(ctx.pool, chi.w, chi.h);
+            Fuse f;
+            f.mode = ACC_ZERO;
+            f.acc = &core;
+            f.weight = fir[0].weight;
+            encode_blur(ctx, chi, core, fir[0].sigma, f);
+        }
+        if (!iir_mixture_mix(ctx, chi, iir, Vec3{0.0, 0.0, 0.0}, Vec3{1.0, 1.0, 1.0}))
+            fail_internal("DIR diffusion: the recursive mixture was refused");
+        if (core) lincomb(ctx, Vec3{1.0, 1.0, 1.0}, core, Vec3{1.0, 1.0, 1.0}, &chi, chi);
+    }
+    da.cy = da.cx + 5 * size_t(f.K);
+    da.chi = chi.data();
+    return chi;
+}
+}  // namespace
+
 Plane develop(RenderCtx& ctx, const Pipeline& p, const Plane& source, uint32_t film_seed,
               const std::optional<HalationOverride>& hov, float* counts_out, float* lam_out) {
     const FilmSetup& f = *p.film;
@@ -532,7 +598,12 @@ Plane develop(RenderCtx& ctx, const Pipeline& p, const Plane& source, uint32_t f
             apply_halation(ctx, pl, H);
         }
     }
-    const DevelopPlan dp = develop_plan(ctx, p, w, film_seed, counts_out, lam_out);
+    DevelopPlan dp = develop_plan(ctx, p, w, film_seed, counts_out, lam_out);
+    Plane chi;
+    if (f.couplers) {
+        Stage st(ctx, "couplers");
+        chi = dir_couplers(ctx, p, H, dp.da);
+    }
     const DevelopArgs& da = dp.da;
     Plane neg = make_plane(ctx.pool, w, h);
     if (!dp.grain) {
@@ -953,6 +1024,7 @@ void render_vjp(RenderCtx& ctx, const Pipeline& p, const LiveParams& live, const
     const DevelopPlan dp = develop_plan(ctx, p, w, film_seed, counts.as<float>());
     if (dp.grain && (dp.da.mode != 0 || dp.amount != 1.0))
         fail_unsupported("the render's adjoint takes sub-layer grain at full strength (or no grain)");
+    if (f.couplers) fail_unsupported("the render's adjoint does not take DIR couplers");
     Plane G = make_plane(ctx.pool, w, h);
     dev::develop(H3.data(), G.data(), dp.da, w, h, ctx.stream);
     Plane neg = G;

@@ -19,7 +19,7 @@ namespace spkb {
 // A film/print set-up pair with its device tables, built once per pipeline.
 struct DeviceTables {
     DevBuffer table;              // L x L spectral table, float4 texels (R, G, B, 0)
-    DevBuffer curves;             // x[K] | inv[K] | y[3K]
+    DevBuffer curves;             // x[K] | inv[K] | y[3K] | y0[3K] (the DIR couplers' pre-inverted curve)
     DevBuffer gaxis, ginv, glayers;
     DevBuffer paper;              // x[K] | r[K] | y[K][3]
     DevBuffer cmax;               // 64 x 720
@@ -104,6 +104,10 @@ bool print_scan_encode(RenderCtx& ctx, const Pipeline& p, const LiveParams& live
 void render_vjp(RenderCtx& ctx, const Pipeline& p, const LiveParams& live, const Plane& source, uint32_t film_seed,
                 const std::optional<HalationOverride>& hov, float* y_out, const float* g_y, float* g_x,
                 double* grad_params, uint32_t n_params);
+
+// The DIR-coupler diffusion (reference src/fx/dir_blur.hpp:15-19, dir_blur.cpp:14-38) at a pixel pitch: a
+// core Gaussian of 20 um with weight 1 - 0.06 and the exponential surrogate of a 200 um tail with weight 0.06.
+std::vector<MixtureComponent> dir_diffusion_components(double pitch_um);
 
 // The blur machinery on device planes (exposed for the tests' stage entry points).
 void gaussian(RenderCtx& ctx, const Plane& in, const Plane& dst, const Vec3& sigma);

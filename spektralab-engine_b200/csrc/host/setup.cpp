@@ -79,7 +79,6 @@ HalationParams resolve_halation(const Profile& film, const ParamSet& p) {
     return h;
 }
 
-namespace {
 // An exponential PSF as three Gaussians (reference src/fx/gaussian.cpp:55-66).
 std::array<MixtureComponent, 3> exponential_surrogate(const Vec3& weight, const Vec3& lambda_px) {
     static constexpr double kA[3] = {0.1633, 0.6496, 0.1870};
@@ -92,7 +91,6 @@ std::array<MixtureComponent, 3> exponential_surrogate(const Vec3& weight, const 
         }
     return out;
 }
-}  // namespace
 
 HalationPlan halation_plan(const HalationParams& h, double p) {
     HalationPlan pl;
@@ -465,6 +463,14 @@ std::shared_ptr<FilmSetup> build_film_setup(const ParamSet& p, std::shared_ptr<c
     s->cinv.assign(K, 0.0f);
     s->cy.resize(3 * K);
     s->cy0.resize(3 * K);
+    s->cy0_64.resize(3 * K);
+    s->couplers = p.b(P::dir_couplers_active);
+    s->coupler_m = m;
+    for (size_t i = 0; i < 9; ++i) s->coupler_m_f32[i] = f32(m[i]);
+    for (size_t c = 0; c < 3; ++c) {
+        s->dmax[c] = film.dmax[c];
+        s->dmax_f32[c] = f32(film.dmax[c]);
+    }
     const std::vector<double>& le = film.log_exposure;
     for (size_t k = 0; k < K; ++k) {
         s->cx[k] = f32(le[k] / gamma);
@@ -485,7 +491,10 @@ std::shared_ptr<FilmSetup> build_film_setup(const ParamSet& p, std::shared_ptr<c
             xs[k] = le[k] - sum;
             ys[k] = film.normalized(k, mm);
         }
-        for (size_t k = 0; k < K; ++k) s->cy0[mm * K + k] = f32(interp(le[k], xs, ys));
+        for (size_t k = 0; k < K; ++k) {
+            s->cy0_64[mm * K + k] = interp(le[k], xs, ys);
+            s->cy0[mm * K + k] = f32(s->cy0_64[mm * K + k]);
+        }
     }
     return s;
 }

@@ -84,6 +84,8 @@ struct GrainConstants {
     double micro_sigma = 0, micro_blur = 0, final_blur = 0;
 };
 GrainConstants grain_constants(const GrainSetup& g, double pitch_um);
+// An exponential PSF of scale lambda_px as three Gaussians of total weight `weight`.
+std::array<MixtureComponent, 3> exponential_surrogate(const Vec3& weight, const Vec3& lambda_px);
 inline constexpr double kGrainDmin[3] = {0.03, 0.03, 0.03};
 
 // ---- film set-up (reference src/film/setup.cpp:353-419) ----
@@ -102,6 +104,14 @@ struct FilmSetup {
     std::shared_ptr<GrainSetup> grain;
     uint32_t K = 0;
     std::vector<float> cx, cinv, cy, cy0;  // curve tables, y channel-major
+    // DIR couplers (reference src/film/setup.cpp:25-95, :402-406): the coupler matrix M[donor][receiver],
+    // the stock's D_max, and the pre-inverted curve y0 (cy0; binary64 in cy0_64, channel-major)
+    bool couplers = false;
+    Mat3 coupler_m{};
+    std::array<float, 9> coupler_m_f32{};
+    Vec3 dmax{};
+    std::array<float, 3> dmax_f32{};
+    std::vector<double> cy0_64;
 };
 std::shared_ptr<FilmSetup> build_film_setup(const ParamSet& p, std::shared_ptr<const Profile> film,
                                             const Resources& res);

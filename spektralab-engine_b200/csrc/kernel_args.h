@@ -71,6 +71,23 @@ struct DevelopArgs {
     uint32_t width;       // pixel index = y * width + x keys the draws
     float* counts_out;    // test hook: the Poisson counts, [pixel][c][l]; nullptr in renders
     float* lam_out;       // test hook: the draws' lambdas, [pixel][c][l] (sub-layer grain); nullptr in renders
+    // DIR couplers: the blurred correction plane chi (interleaved RGB), subtracted from the log exposure
+    // before the curve lookup, with cy then the pre-inverted curve y0; nullptr without couplers
+    const float* chi;
+};
+
+// DIR couplers' source (reference kernels/film.metal:242-276): the first development of the exposure
+// through the density curve (x, inv, y), then chi_m = sum_c s_c M[c][m], s_c = positive ? dmax_c - D_c : D_c.
+struct CouplerArgs {
+    const float* cx;
+    const float* cinv;
+    const float* cy;
+    uint32_t K;
+    AxisGrid cgrid;
+    uint32_t positive;
+    float m[9];           // M[c * 3 + m], c the donor layer
+    float dmax[3];
+    uint32_t n;           // pixels
 };
 
 // Per-wavelength tables of one spectral integral (already neutralised).

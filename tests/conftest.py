@@ -73,3 +73,19 @@ def lsb_stats(a, b):
 
 def golden(name):
     return np.load(os.path.join(GOLDEN, name))
+
+
+def coupler_steep_mask(f64, D, slope=50.0, margin=1e-5):
+    """Values of the negative D (h, w, 3) that the couplers' pre-inverted curve y0 reaches inside a
+    segment steeper than `slope` (density per log10 exposure), away from its two ends by `margin`. Where
+    the forward development folds, y0 climbs by up to two densities within one knot spacing (and is flat
+    on either side), so a binary32 rounding of L - chi (about 1e-7) moves D by slope x 1e-7: the
+    reference's binary32 arithmetic and the binary64 oracle part there by up to a few 1e-4."""
+    x = np.asarray(f64["curve_x"])
+    y0 = np.asarray(f64["couplers"]["y0"]).reshape(3, -1)
+    mask = np.zeros(D.shape, bool)
+    for c in range(3):
+        s = np.diff(y0[c]) / np.diff(x)
+        for k in np.where(s > slope)[0]:
+            mask[..., c] |= (D[..., c] > y0[c][k] + margin) & (D[..., c] < y0[c][k + 1] - margin)
+    return mask, float(max((np.diff(y0[c]) / np.diff(x)).max() for c in range(3)))

@@ -14,7 +14,7 @@ import numpy as np
 import pytest
 
 import oracle
-from conftest import BASE, GOLDEN, golden, lsb_stats, sc, setup_f64
+from conftest import BASE, GOLDEN, coupler_steep_mask, golden, lsb_stats, sc, setup_f64
 
 pytestmark = pytest.mark.gpu
 CFG1 = ([((1, 1, 1), (8, 8, 8)), ((1, 1, 1), (40, 40, 40))], (0.02, 0.02, 0.02))
@@ -85,6 +85,61 @@ def test_fp64_gate_fixed_noise(engine, lib, resources, case):
     assert st["frac_gt1"] <= 1e-4, st
     assert st["max"] <= 64, st
     np.testing.assert_allclose(neg, neg64, rtol=0, atol=5e-5)
+
+
+@pytest.mark.parametrize("amount", [0.5, 1.0])
+def test_couplers_within_one_lsb_of_reference(engine, lib, resources, ref, ref_engine, amount):
+    """DIR couplers (reference src/film/develop.cpp:203-226) on the device against the reference engine,
+    without grain: render and reprint within 1 LSB16 on every pixel whose negative the pre-inverted curve
+    does not reach through its fold, the negatives within 2e-5 there (coupler_steep_mask)."""
+    import ctypes
+    w, h = 200, 136
+    img = sc.synthetic_image(w, h, 3)
+    delta = dict(BASE, grain_active=False, dir_couplers_active=True, dir_couplers_amount=amount)
+    a, b = render_pair(engine, img, delta)
+    with engine.open(img, delta) as s:
+        neg_dev, _ = s.develop_debug("full", FIRST_SEED, w, h)
+    out = np.zeros((2, h, w, 4), np.uint16)
+    neg = np.zeros((h, w, 3), np.float32)
+    ex = (ctypes.c_double * 2)(1.0, 1.2)
+    z = (ctypes.c_double * 3)(0, 0, 0)
+    ref.check(ref.lib.spkref_render(ref_engine.h, img.ctypes.data_as(sc.FP), w, h, json.dumps(delta).encode(), 0, z,
+                                    z, z, ex, 2, out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint16)),
+                                    neg.ctypes.data_as(sc.FP)))
+    f64 = setup_f64(lib, resources, delta, 35000.0 / max(w, h))["f64"]
+    steep, _ = coupler_steep_mask(f64, neg)
+    assert steep.mean() < 0.01
+    assert np.abs(neg_dev - neg)[~steep].max() <= 2e-5
+    flat = ~steep.any(-1)
+    assert lsb_stats(a[flat][None], out[0][flat][None])["max"] <= 1
+    assert lsb_stats(b[flat][None], out[1][flat][None])["max"] <= 1
+
+
+def test_couplers_fp64_gate_fixed_noise(engine, lib, resources):
+    """DIR couplers with grain against the float64 oracle, the device's own Poisson counts as fixed noise:
+    the RGBA within 1 LSB16 on all but a handful of pixels away from the pre-inverted curve's fold (the
+    developed density, before the grain, inside the fold's steep segment; widened by the final blur's
+    radius of 2 pixels, which spreads the fold's binary32 differences to the neighbours)."""
+    from scipy.ndimage import binary_dilation
+    w, h = 384, 256
+    img = sc.synthetic_image(w, h, 0)
+    delta = dict(BASE, grain_active=True, dir_couplers_active=True, dir_couplers_amount=1.0)
+    with engine.open(img, delta) as s:
+        a, _ = s.render("full")
+        neg, counts = s.develop_debug("full", FIRST_SEED, w, h)
+    f64 = setup_f64(lib, resources, delta, 35000.0 / max(w, h))["f64"]
+    out, neg64 = oracle.Oracle(f64, seed=FIRST_SEED).render(img, counts=counts)
+    plain = setup_f64(lib, resources, dict(delta, grain_active=False), 35000.0 / max(w, h))["f64"]
+    fold = coupler_steep_mask(plain, oracle.Oracle(plain).render(img)[1])[0].any(-1)
+    flat = ~binary_dilation(fold, np.ones((5, 5), bool))
+    st = lsb_stats(a[flat][None], out[flat][None])
+    d = np.abs(a.astype(np.int64) - out.astype(np.int64))[..., :3].max(-1)
+    info = dict(st, fold=float(fold.mean()), flat=float(flat.mean()), gt1_all=int((d > 1).sum()),
+                gt1_fold=int((d[fold] > 1).sum()), gt1_flat=int((d[flat] > 1).sum()),
+                neg_flat=float(np.abs(neg - neg64)[flat].max()))
+    assert st["frac_gt1"] <= 1e-4, info
+    assert st["max"] <= 64, info
+    assert fold.mean() < 0.02 and flat.mean() > 0.75, info  # the fold is a thin contour; widened, a sixth of the frame
 
 
 def test_sampler_bit_exact(lib):

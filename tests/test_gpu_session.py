@@ -71,11 +71,21 @@ def test_unknown_tier_and_result_zeroed(engine, lib):
 
 def test_outside_render_path_is_refused(engine):
     img = sc.synthetic_image(8, 8, 0)
-    for extra in ({"auto_exposure": True}, {"dir_couplers_active": True}, {"glare_active": True},
-                  {"geometry_flip_h": True}):
+    for extra in ({"auto_exposure": True}, {"glare_active": True}, {"geometry_flip_h": True}):
         with pytest.raises(sc.SpkError) as e:
             engine.open(img, dict(BASE, **extra))
         assert e.value.status == sc.SPK_ERR_USER and "outside this B200 build" in str(e.value)
+
+
+def test_couplers_have_no_adjoint(engine):
+    """The DIR couplers render; the adjoint (spk_render_vjp) refuses them as outside its parameters."""
+    img = sc.synthetic_image(16, 12, 0)
+    with engine.open(img, dict(BASE, grain_active=False, dir_couplers_active=True)) as s:
+        a, _ = s.render("full")
+        assert (a[..., 3] == 65535).all()
+        with pytest.raises(sc.SpkError) as e:
+            s.render_vjp(np.ones((12, 16, 3), np.float32), 1)
+        assert e.value.status == sc.SPK_ERR_UNSUPPORTED and "DIR couplers" in str(e.value)
 
 
 def test_channels_and_nonfinite_inputs(engine):

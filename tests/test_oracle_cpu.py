@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 
 import oracle
-from conftest import BASE, GOLDEN, golden, lsb_stats, sc, setup_f64
+from conftest import coupler_steep_mask, BASE, GOLDEN, golden, lsb_stats, sc, setup_f64
 
 KAT = [
     ((0, 0, 0, 0), (0, 0), (0x6627E8D5, 0xE169C58D, 0xBC57AC4C, 0x9B00DBD8)),
@@ -150,3 +150,42 @@ def test_render_against_reference_golden(lib, resources):
             assert np.median(dn) < 1e-5 and abs(neg.mean() - g[f"{name}_negative"].mean()) < 1e-3, name
             assert s["frac_gt1"] < 0.5, (name, s)
         assert (out[..., 3] == 65535).all()
+
+
+@pytest.mark.parametrize("amount", [0.5, 1.0, 4.0])
+def test_couplers_against_reference(lib, resources, ref, ref_engine, amount):
+    """DIR couplers (reference src/film/develop.cpp:203-226): the float64 oracle's render against the
+    reference engine itself, without grain: the negatives within 2e-5 and the RGBA within 1 LSB16, except
+    where the pre-inverted curve is steep (coupler_steep_mask); there within its slope times 4 binary32
+    rounding steps of the log exposure. At the schema's largest amount (4) y0 is flat but for one step, and
+    the negative holds channels at zero density: the print's gamut compression of those saturated colours
+    parts binary32 from binary64 by a few LSB16 on a handful of pixels."""
+    import ctypes
+    w, h = 160, 120
+    img = sc.synthetic_image(w, h, 3)
+    delta = dict(BASE, grain_active=False, dir_couplers_active=True, dir_couplers_amount=amount)
+    out = np.zeros((1, h, w, 4), np.uint16)
+    neg = np.zeros((h, w, 3), np.float32)
+    ex = (ctypes.c_double * 1)(1.0)
+    z = (ctypes.c_double * 3)(0, 0, 0)
+    ref.check(ref.lib.spkref_render(ref_engine.h, img.ctypes.data_as(sc.FP), w, h, json.dumps(delta).encode(), 0, z,
+                                    z, z, ex, 1, out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint16)),
+                                    neg.ctypes.data_as(sc.FP)))
+    f64 = setup_f64(lib, resources, delta, 35000.0 / max(w, h))["f64"]
+    assert f64["couplers"]["active"]
+    got, neg64 = oracle.Oracle(f64).render(img)
+    steep, slope = coupler_steep_mask(f64, neg64)
+    assert steep.mean() < 0.01
+    dn = np.abs(neg64 - neg)
+    assert dn[~steep].max() <= 2e-5
+    assert dn[steep].max(initial=0) <= slope * 4 * 2.0 ** -23 * 4
+    flat = ~steep.any(-1)
+    st = lsb_stats(got[flat][None], out[0][flat][None])
+    if amount <= 1.0:
+        assert st["max"] <= 1, st
+    else:
+        assert st["frac_gt1"] <= 1e-3 and st["max"] <= 8, st
+    # the couplers change the negative
+    plain, neg_plain = oracle.Oracle(setup_f64(lib, resources, dict(delta, dir_couplers_active=False),
+                                               35000.0 / max(w, h))["f64"]).render(img)
+    assert np.abs(neg_plain - neg64).max() > 1e-2
