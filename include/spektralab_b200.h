@@ -42,6 +42,14 @@ SPK_API spk_status spkx_session_profile(spk_session* session, const char* tier, 
  */
 SPK_API spk_status spkx_session_negative(spk_session* session, const char* tier, float* out, size_t capacity_floats);
 
+/* spkx_session_tier_image(session, tier, out, capacity_floats, width, height)
+ *   the tier's image (the frame downscaled to the tier's long edge, made on first use and kept; the frame
+ *   itself when it fits): its size in *width, *height and, when out is not NULL and capacity_floats
+ *   holds 3 floats per pixel, its pixels.
+ */
+SPK_API spk_status spkx_session_tier_image(spk_session* session, const char* tier, float* out, size_t capacity_floats,
+                                          uint32_t* width, uint32_t* height);
+
 /* spkx_session_develop_debug(session, tier, film_seed, negative, counts)
  *   develop the tier's frame once more with the given film seed, without touching the cache:
  *   negative receives 3 floats per pixel, counts (may be NULL) the grain's Poisson counts, 9 floats per

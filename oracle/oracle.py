@@ -65,6 +65,9 @@ def lib():
         L.orc_gaussian.argtypes = [PD, PD, I32, I32, PD]
         L.orc_spectral.argtypes = [PD, PD, PD, I32, PD, ctypes.c_int64, PD]
         L.orc_gaussian.restype = None
+        L.orc_downscale.argtypes = [FP, I32, I32, I32, I32, FP]
+        L.orc_prepare.argtypes = [FP, I32, I32, I32, I32, PD, PD, ctypes.POINTER(I32), ctypes.POINTER(I32)]
+        L.orc_render64.argtypes = [ctypes.POINTER(OracleSetup), PD, I32, I32, FP, U16, PD]
         L.orc_poisson.argtypes = [FP, FP, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32]
         L.orc_poisson.restype = None
         L.orc_lognormal.argtypes = [FP, ctypes.c_uint32, ctypes.c_float, ctypes.c_float, ctypes.c_uint32,
@@ -86,7 +89,7 @@ def lib():
 class Oracle:
     """An OracleSetup plus the arrays it points into (kept alive here)."""
 
-    def __init__(self, f64, seed=0, halation=None, print_exposure=None):
+    def __init__(self, f64, seed=0, halation=None, print_exposure=None, rho_tier=1.0):
         s = OracleSetup()
         self.keep = []
 
@@ -176,7 +179,7 @@ class Oracle:
         s.cmax = buf(f64["cmax"])
         s.lc_active = 1
         s.scanner_lens_blur = f64["scanner_lens_blur"]
-        s.unsharp_sigma = f64["unsharp_sigma"]
+        s.unsharp_sigma = f64["unsharp_sigma"] * rho_tier  # the unsharp mask's sigma scales with the tier
         s.unsharp_amount = f64["unsharp_amount"]
         s.cctf_active = 1 if f64["cctf_active"] else 0
         s.cctf_mode = int(f64["cctf_mode"])
@@ -205,6 +208,20 @@ class Oracle:
             cp = counts.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
         lib().orc_render(ctypes.byref(self.s), rgb.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), w, h, cp,
                          out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint16)), neg.ctypes.data_as(PD))
+        return out, neg
+
+    def render64(self, rgb64, counts=None):
+        """render() of a binary64 frame (the output of prepare())."""
+        rgb64 = np.ascontiguousarray(rgb64, np.float64)
+        h, w, _ = rgb64.shape
+        out = np.zeros((h, w, 4), np.uint16)
+        neg = np.zeros((h, w, 3), np.float64)
+        cp = None
+        if counts is not None:
+            counts = np.ascontiguousarray(counts, np.float32)
+            cp = counts.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+        lib().orc_render64(ctypes.byref(self.s), rgb64.ctypes.data_as(PD), w, h, cp,
+                           out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint16)), neg.ctypes.data_as(PD))
         return out, neg
 
     def render_linear(self, rgb64, counts):
@@ -240,6 +257,48 @@ def spectral(eps, beta, wt, densities):
     lib().orc_spectral(eps.ctypes.data_as(PD), beta.ctypes.data_as(PD), wt.ctypes.data_as(PD), len(beta),
                        d.ctypes.data_as(PD), d.size // 3, out.ctypes.data_as(PD))
     return out
+
+
+def downscale_size(w, h, long_edge):
+    """The tier image's size (reference src/session/tiers.cpp:50-57)."""
+    m = max(w, h)
+    if long_edge == 0 or m <= long_edge:
+        return w, h
+    s = long_edge / m
+    return max(1, int(np.floor(w * s))), max(1, int(np.floor(h * s)))
+
+
+def downscale(rgb, long_edge):
+    """The tier image of a float32 frame at a target long edge (orc_downscale; the frame itself when it
+    fits)."""
+    rgb = np.ascontiguousarray(rgb, np.float32)
+    h, w, _ = rgb.shape
+    ow, oh = downscale_size(w, h, long_edge)
+    if (ow, oh) == (w, h):
+        return rgb.copy()
+    out = np.zeros((oh, ow, 3), np.float32)
+    FP = ctypes.POINTER(ctypes.c_float)
+    lib().orc_downscale(rgb.ctypes.data_as(FP), w, h, ow, oh, out.ctypes.data_as(FP))
+    return out
+
+
+GEOMETRY_KEYS = ("geometry_crop_x", "geometry_crop_y", "geometry_crop_w", "geometry_crop_h",
+                 "geometry_rotation_deg", "geometry_quarter_turns", "geometry_flip_h", "geometry_flip_v")
+GEOMETRY_DEFAULTS = (0.0, 0.0, 1.0, 1.0, 0.0, 0, False, False)
+
+
+def prepare(rgb, delta, cctf_mode):
+    """The input decode (when delta has input_cctf_decoding) and the geometry of delta's geometry_* keys,
+    in binary64 (orc_prepare): float32 frame -> float64 frame of the geometry's output size."""
+    rgb = np.ascontiguousarray(rgb, np.float32)
+    h, w, _ = rgb.shape
+    geo = (ctypes.c_double * 8)(*[float(delta.get(k, d)) for k, d in zip(GEOMETRY_KEYS, GEOMETRY_DEFAULTS)])
+    out = np.zeros(h * w * 3, np.float64)
+    ow, oh = I32(), I32()
+    lib().orc_prepare(rgb.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), w, h,
+                      1 if delta.get("input_cctf_decoding") else 0, int(cctf_mode), geo, out.ctypes.data_as(PD),
+                      ctypes.byref(ow), ctypes.byref(oh))
+    return out[: oh.value * ow.value * 3].reshape(oh.value, ow.value, 3)
 
 
 def gaussian(plane, sigma3):

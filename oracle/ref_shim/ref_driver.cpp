@@ -20,6 +20,7 @@
 #include "print/internal.hpp"
 #include "print/print.hpp"
 #include "session/engine.hpp"
+#include "session/tiers.hpp"
 #include "spektralab.h"
 #include "util/error.hpp"
 #include "util/json.hpp"
@@ -285,6 +286,22 @@ __attribute__((visibility("default"))) int32_t spkref_print(void* handle, double
 }
 
 __attribute__((visibility("default"))) void spkref_close(void* handle) { delete static_cast<RefSession*>(handle); }
+
+/* spkref_downscale(rgb, w, h, long_edge, out, out_w, out_h): the reference's CPU tier downscale
+ * (src/session/tiers.cpp:196-227) at a target long edge; out holds w h 3 floats */
+__attribute__((visibility("default"))) int32_t spkref_downscale(const float* rgb, uint32_t w, uint32_t h,
+                                                                uint32_t long_edge, float* out, uint32_t* out_w,
+                                                                uint32_t* out_h) {
+    try {
+        const session::Size o = session::downscale_size(w, h, long_edge);
+        session::downscale_cpu(rgb, w, h, out, o.w, o.h);
+        *out_w = o.w;
+        *out_h = o.h;
+        return SPK_OK;
+    } catch (const std::exception& ex) {
+        return fail_status(ex);
+    }
+}
 
 /* spkref_setup_json(engine, delta, pitch_um, out_json): the reference's narrowed kernel constants under the
  * same keys as the B200 build's spkx_session_setup_json */

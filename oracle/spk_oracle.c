@@ -522,6 +522,211 @@ int orc_render(const OracleSetup* s, const float* rgb, int32_t w, int32_t h, con
     return 0;
 }
 
+int orc_render64(const OracleSetup* s, const double* rgb, int32_t w, int32_t h, const float* counts,
+                 uint16_t* out, double* out_negative) {
+    const size_t N = (size_t)w * h * 3;
+    double* neg = (double*)malloc(N * sizeof(double));
+    develop_impl(s, NULL, rgb, w, h, counts, neg);
+    orc_print(s, neg, w, h, out, NULL);
+    if (out_negative) memcpy(out_negative, neg, N * sizeof(double));
+    free(neg);
+    return 0;
+}
+
+/* ---- before the film path: tier downscale, decode, geometry ---- */
+
+/* "c b | a b c d | c b": period 2 (n - 1) (reference src/util/numeric.cpp:134-140) */
+static int64_t mirror_i(int64_t i, int64_t n) {
+    if (n <= 1) return 0;
+    const int64_t period = 2 * (n - 1);
+    int64_t m = i % period;
+    if (m < 0) m += period;
+    return m < n ? m : period - m;
+}
+
+/* gaussian taps with sigma = max(0, (n / m - 1) / 2), radius floor(4 sigma + 0.5), binary64 normalised
+ * in ascending k and narrowed; returns the radius (taps holds 2 r + 1 values) */
+static int tier_taps(int32_t n, int32_t m, float** taps) {
+    const double sigma = fmax(0.0, ((double)n / (double)m - 1.0) / 2.0);
+    const int r = sigma > 0.0 ? (int)floor(4.0 * sigma + 0.5) : 0;
+    *taps = (float*)malloc((size_t)(2 * r + 1) * sizeof(float));
+    if (r == 0) {
+        (*taps)[0] = 1.0f;
+        return 0;
+    }
+    double* w = (double*)malloc((size_t)(2 * r + 1) * sizeof(double));
+    double sum = 0.0;
+    for (int k = -r; k <= r; ++k) {
+        const double t = (double)k / sigma;
+        w[k + r] = exp(-0.5 * t * t);
+        sum += w[k + r];
+    }
+    for (int k = 0; k <= 2 * r; ++k) (*taps)[k] = (float)(w[k] / sum);
+    free(w);
+    return r;
+}
+
+/* output o -> the source coordinate (o + 1/2) n / m - 1/2 as num / den, mirrored into [0, n - 1] */
+static void tier_sample(int64_t N, int64_t M, int64_t o, uint32_t* i0, uint32_t* i1, float* t) {
+    const int64_t den = 2 * M;
+    int64_t num = (2 * o + 1) * N - M;
+    if (num > den * (N - 1)) num = 2 * den * (N - 1) - num;
+    if (num < 0) num = -num;
+    int64_t a = num / den;
+    if (a > N - 1) a = N - 1;
+    *i0 = (uint32_t)a;
+    *i1 = (uint32_t)(a + 1 < N - 1 ? a + 1 : N - 1);
+    *t = (float)(num - a * den) / (float)den;
+}
+
+int orc_downscale(const float* src, int32_t w, int32_t h, int32_t ow, int32_t oh, float* dst) {
+    const size_t N = (size_t)w * h * 3;
+    float* a = (float*)malloc(N * sizeof(float));
+    float* b = (float*)malloc(N * sizeof(float));
+    memcpy(a, src, N * sizeof(float));
+    float *ty, *tx;
+    const int ry = tier_taps(h, oh, &ty), rx = tier_taps(w, ow, &tx);
+    if (ry > 0) {
+#pragma omp parallel for
+        for (int32_t y = 0; y < h; ++y)
+            for (int32_t x = 0; x < w; ++x)
+                for (int c = 0; c < 3; ++c) {
+                    float acc = 0.0f;
+                    for (int k = -ry; k <= ry; ++k)
+                        acc = fmaf(ty[k + ry], a[3 * ((size_t)mirror_i(y + k, h) * w + x) + c], acc);
+                    b[3 * ((size_t)y * w + x) + c] = acc;
+                }
+        float* t = a;
+        a = b;
+        b = t;
+    }
+    if (rx > 0) {
+#pragma omp parallel for
+        for (int32_t y = 0; y < h; ++y)
+            for (int32_t x = 0; x < w; ++x)
+                for (int c = 0; c < 3; ++c) {
+                    float acc = 0.0f;
+                    for (int k = -rx; k <= rx; ++k)
+                        acc = fmaf(tx[k + rx], a[3 * ((size_t)y * w + mirror_i(x + k, w)) + c], acc);
+                    b[3 * ((size_t)y * w + x) + c] = acc;
+                }
+        float* t = a;
+        a = b;
+        b = t;
+    }
+#pragma omp parallel for
+    for (int32_t oy = 0; oy < oh; ++oy) {
+        uint32_t y0, y1;
+        float tyv;
+        tier_sample(h, oh, oy, &y0, &y1, &tyv);
+        for (int32_t ox = 0; ox < ow; ++ox) {
+            uint32_t x0, x1;
+            float txv;
+            tier_sample(w, ow, ox, &x0, &x1, &txv);
+            for (int c = 0; c < 3; ++c) {
+                const float pa = a[3 * ((size_t)y0 * w + x0) + c], pb = a[3 * ((size_t)y0 * w + x1) + c];
+                const float pd = a[3 * ((size_t)y1 * w + x0) + c], pe = a[3 * ((size_t)y1 * w + x1) + c];
+                const float top = fmaf(txv, pb - pa, pa), bot = fmaf(txv, pe - pd, pd);
+                dst[3 * ((size_t)oy * ow + ox) + c] = fmaf(tyv, bot - top, top);
+            }
+        }
+    }
+    free(tx);
+    free(ty);
+    free(a);
+    free(b);
+    return 0;
+}
+
+/* the inverse transfer functions in binary64 */
+static double decode64(double v, int mode) {
+    switch (mode) {
+        case 0:
+            return v <= 0.040449936 ? v / 12.92 : pow((v + 0.055) / 1.055, 2.4);
+        case 1:
+            return v < 16.0 / 512.0 ? v / 16.0 : pow(v, 1.8);
+        case 2:
+            return pow(v, 563.0 / 256.0);
+        case 3: {
+            const double bp = 1.099 * pow(0.018, 0.45) - 0.099;
+            return v < bp ? v / 4.5 : pow((v + 0.099) / 1.099, 1.0 / 0.45);
+        }
+        default:
+            return v;
+    }
+}
+
+/* the clamped bilinear axis of geometry_cpu: f <= 0 or f >= n - 1 clamps with t = 0 */
+static void geo_axis(double f, int32_t n, int32_t* i0, int32_t* i1, double* t) {
+    if (f <= 0.0) {
+        *i0 = 0;
+        *t = 0.0;
+    } else if (f >= (double)(n - 1)) {
+        *i0 = n - 1;
+        *t = 0.0;
+    } else {
+        const double fl = floor(f);
+        *i0 = (int32_t)fl;
+        *t = f - fl;
+    }
+    *i1 = *i0 + 1 < n - 1 ? *i0 + 1 : n - 1;
+}
+
+int orc_prepare(const float* src, int32_t w, int32_t h, int32_t decode, int32_t mode, const double geo[8],
+                double* dst, int32_t* out_w, int32_t* out_h) {
+    const size_t N = (size_t)w * h * 3;
+    double* d = (double*)malloc(N * sizeof(double));
+    for (size_t i = 0; i < N; ++i) d[i] = decode ? decode64((double)src[i], mode) : (double)src[i];
+    const double cx = geo[0], cy = geo[1], cw = geo[2], ch = geo[3], deg = geo[4];
+    const int q = (((int)geo[5] % 4) + 4) % 4;
+    const int fh = geo[6] != 0.0, fv = geo[7] != 0.0;
+    if (cx == 0.0 && cy == 0.0 && cw == 1.0 && ch == 1.0 && deg == 0.0 && q == 0 && !fh && !fv) {
+        memcpy(dst, d, N * sizeof(double));
+        *out_w = w;
+        *out_h = h;
+        free(d);
+        return 0;
+    }
+    /* the output size is the rounded crop (sides exchanged by an odd quarter turn); output pixel centres
+     * (u, v) map through the turn and flips, scale to the crop, rotate about its centre */
+    const double CW = fmax(1.0, round(cw * w)), CH = fmax(1.0, round(ch * h));
+    const double OW = (q & 1) ? CH : CW, OH = (q & 1) ? CW : CH;
+    const double sx = cw * w / CW, sy = ch * h / CH, hx = cw * w / 2.0, hy = ch * h / 2.0;
+    const double ccx = (cx + cw / 2.0) * w - 0.5, ccy = (cy + ch / 2.0) * h - 0.5;
+    const double th = deg * 3.14159265358979323846 / 180.0, ca = cos(th), sa = sin(th);
+    const int32_t ow = (int32_t)OW, oh = (int32_t)OH;
+#pragma omp parallel for
+    for (int32_t oy = 0; oy < oh; ++oy)
+        for (int32_t ox = 0; ox < ow; ++ox) {
+            double U0 = ox + 0.5, V0 = oy + 0.5;
+            if (fh) U0 = OW - U0;
+            if (fv) V0 = OH - V0;
+            double u, v;
+            switch (q) {
+                case 0: u = U0; v = V0; break;
+                case 1: v = OW - U0; u = V0; break;
+                case 2: u = OW - U0; v = OH - V0; break;
+                default: v = U0; u = OH - V0; break;
+            }
+            const double P = sx * u - hx, Q = sy * v - hy;
+            const double fx = ccx + (P * ca - Q * sa), fy = ccy + (P * sa + Q * ca);
+            int32_t x0, x1, y0, y1;
+            double tx, ty;
+            geo_axis(fx, w, &x0, &x1, &tx);
+            geo_axis(fy, h, &y0, &y1, &ty);
+            for (int c = 0; c < 3; ++c) {
+                const double a = d[3 * ((size_t)y0 * w + x0) + c], b = d[3 * ((size_t)y0 * w + x1) + c];
+                const double e0 = d[3 * ((size_t)y1 * w + x0) + c], e1 = d[3 * ((size_t)y1 * w + x1) + c];
+                const double top = a * (1.0 - tx) + b * tx, bot = e0 * (1.0 - tx) + e1 * tx;
+                dst[3 * ((size_t)oy * ow + ox) + c] = top * (1.0 - ty) + bot * ty;
+            }
+        }
+    *out_w = ow;
+    *out_h = oh;
+    free(d);
+    return 0;
+}
+
 /* ---- the shared binary32 sampler ---- */
 
 void orc_poisson(const float* lam, float* counts, uint32_t n, uint32_t stream, uint32_t seed) {

@@ -95,6 +95,24 @@ void orc_spectral(const double* eps, const double* beta, const double* wt, int32
  * branch rule (FIR below 3, Young-van Vliet above) */
 void orc_gaussian(const double* in, double* out, int32_t w, int32_t h, const double sigma[3]);
 
+/* The tier downscale (reference src/session/tiers.cpp:99-227, session.metal:19-91), restated in the
+ * binary32 arithmetic that the reference specifies for both its GPU and CPU paths (taps narrowed from
+ * binary64, fmaf in ascending tap order, mirror edges, exact-integer bilinear tables), so that every
+ * implementation gives the same bits: src w x h x 3 -> dst ow x oh x 3. Returns 0. */
+int orc_downscale(const float* src, int32_t w, int32_t h, int32_t ow, int32_t oh, float* dst);
+
+/* The input transfer decode (reference kernels/film.metal:104-142; mode 0 sRGB, 1 ProPhoto, 2 Adobe,
+ * 3 BT.709, 4 identity; decode = 0 skips it) and the crop / rotation / quarter turn / flip geometry
+ * (src/film/geometry.cpp:45-157: geo = {crop_x, crop_y, crop_w, crop_h, rotation_deg, quarter_turns,
+ * flip_h, flip_v}), both in binary64: src w x h x 3 -> dst of the geometry's output size, written to
+ * *ow, *oh (dst holds at least w h 3 doubles: the crop never exceeds the frame). Returns 0. */
+int orc_prepare(const float* src, int32_t w, int32_t h, int32_t decode, int32_t mode, const double geo[8],
+                double* dst, int32_t* ow, int32_t* oh);
+
+/* orc_render on a binary64 frame (the output of orc_prepare). */
+int orc_render64(const OracleSetup* s, const double* rgb, int32_t w, int32_t h, const float* counts,
+                 uint16_t* out_rgba, double* out_negative);
+
 /* The shared binary32 sampler (grain_sampler.h), for the bit-exactness tests. */
 void orc_poisson(const float* lam, float* counts, uint32_t n, uint32_t stream, uint32_t seed);
 void orc_lognormal(float* out, uint32_t n, float mean, float sd, uint32_t stream, uint32_t seed);

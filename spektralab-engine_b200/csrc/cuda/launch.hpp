@@ -31,6 +31,13 @@ struct Probe {
 // no more is a no-op), so that launches inside a stream capture make no attribute call.
 void ensure_smem(const void* kernel, int bytes);
 
+// Tier downscale: the vertical prefilter src -> dst (same size), then the horizontal prefilter at the
+// bilinear sample points fused with the blend, v (in_w x in_h) -> dst (out_w x out_h).
+void tier_blur_v(const float* src, float* dst, const TierBlurArgs& a, cudaStream_t s);
+void tier_resample(const float* v, float* dst, const TierResampleArgs& a, cudaStream_t s);
+// Input transfer decode and geometry: src (src_w x src_h) -> dst (dst_w x dst_h).
+void prepare(const float* src, float* dst, const PrepareArgs& a, cudaStream_t s);
+
 // RGB -> film exposure H (Mitchell bicubic of the spectral table, L x L float4 texels), times the
 // compensation gain.
 void expose(const float* rgb, float* h, const float* table4, const ExposeArgs& a, cudaStream_t s);

@@ -22,6 +22,7 @@
 #include "spektralab.h"
 #include "spektralab_b200.h"
 #include "status.hpp"
+#include "tiers.hpp"
 
 namespace spkb {
 
@@ -124,6 +125,8 @@ public:
 };
 
 struct TierState {
+    Plane source;            // the tier's image (the frame itself when it fits the tier)
+    uint32_t long_edge = 0;  // of the tier's image
     Plane negative;
     double pitch_um = 0.0;
 };
@@ -156,7 +159,7 @@ public:
 
     ~Session() {
         // stream-ordered buffers are freed on the stream, so they go before it does
-        for (TierState& t : tiers) t.negative = Plane{};
+        for (TierState& t : tiers) t = TierState{};
         source = Plane{};
         pipe = Pipeline{};
         if (stream) {
@@ -197,20 +200,25 @@ public:
         return pl;
     }
 
-    // tier source: the frame itself when its long edge fits the tier (reference src/session/tiers.cpp:55-64)
-    void check_tier(Tier t) const {
-        const uint32_t M = std::max(source.w, source.h);
-        uint32_t L = 0;
-        if (t == Tier::Live) L = uint32_t(params.i(P::preview_long_edge));
-        if (t == Tier::Preview) L = 3400;
-        if (L != 0 && M > L)
-            fail_user("tier '" + std::string(t == Tier::Live ? "live" : "preview") +
-                      "' needs a downscale of this frame, which is outside this B200 build's render path; "
-                      "render the 'full' tier");
+    // The tier's image, downscaled from the frame on first use and kept (reference
+    // src/session/session.cpp:282-292, src/session/tiers.cpp:39-64): live at preview_long_edge, preview at
+    // 3400 px, full the frame itself; a frame that fits the tier is its own tier image.
+    TierState& tier_source(Tier t) {
+        TierState& ts = tiers[int(t)];
+        if (!ts.source) {
+            uint32_t L = 0;
+            if (t == Tier::Live) L = uint32_t(params.i(P::preview_long_edge));
+            if (t == Tier::Preview) L = kPreviewLongEdge;
+            ts.source = downscale(pool, stream, source, L);
+            ts.long_edge = std::max(ts.source.w, ts.source.h);
+        }
+        return ts;
     }
-
-    double pitch_um() const {
-        return 1000.0 * params.f(P::film_format_mm) / double(std::max(source.w, source.h));
+    // rho_tier: the tier image's long edge over the frame's (never L / M: the floor can give L - 1)
+    double rho(const TierState& ts) const { return double(ts.long_edge) / double(std::max(source.w, source.h)); }
+    // the develop's pixel pitch at the tier's long edge
+    double tier_pitch_um(const TierState& ts) const {
+        return 1000.0 * params.f(P::film_format_mm) / double(ts.long_edge);
     }
 
     void node() {
@@ -370,12 +378,12 @@ Session* open_session(Engine& e, const void* data, bool device_ptr, uint32_t w, 
 
 // develop the tier (reference src/session/session.cpp:327-340): drop its negative, draw the film seed
 void develop_tier(Session& s, Tier t, RenderCtx& ctx) {
-    TierState& ts = s.tiers[int(t)];
+    TierState& ts = s.tier_source(t);
     ts.negative = Plane{};
     const uint32_t seed = s.params.b(P::grain_active) ? s.seeds.next() : kNoGrainFilmSeed;
-    ctx.pitch_um = s.pitch_um();
+    ctx.pitch_um = s.tier_pitch_um(ts);
     s.node();
-    ts.negative = develop(ctx, s.pipe, s.source, seed, s.hal);
+    ts.negative = develop(ctx, s.pipe, ts.source, seed, s.hal);
     ts.pitch_um = ctx.pitch_um;
 }
 
@@ -395,9 +403,9 @@ void render(Session& s, const char* tier_name, bool reprint, spk_result* out) {
     bool developed = false;
     OutputImage* img = nullptr;
     try {
-        s.check_tier(*t);  // a tier this build cannot make is a render failure (SPK_ERR_GPU), as in the reference
+        s.tier_source(*t);  // a failed downscale is a render failure (SPK_ERR_GPU), as in the reference
         RenderCtx ctx{s.pool, s.stream};
-        ctx.rho_tier = 1.0;
+        ctx.rho_tier = s.rho(ts);
         ctx.print_mode = s.print_mode;
         ctx.print_bins = s.print_bins;
         if (!reuse) {
@@ -406,7 +414,7 @@ void render(Session& s, const char* tier_name, bool reprint, spk_result* out) {
         }
         ctx.pitch_um = ts.pitch_um;
         s.node();
-        img = output_acquire(s.engine->device, s.source.w, s.source.h);
+        img = output_acquire(s.engine->device, ts.negative.w, ts.negative.h);
         ctx.copy_stream = s.copy_stream;
         ctx.band_events = &s.band_events;
         if (!print_scan_encode(ctx, s.pipe, s.live, ts.negative, img, true))
@@ -723,9 +731,9 @@ void render_batch(std::vector<Session*> ss, const char* tier_name, bool reprint,
             s.nodes_done.store(0);
             s.nodes_total = f.reused ? 1 : 2;
             s.done = false;
-            s.check_tier(*t);
+            s.tier_source(*t);
             RenderCtx ctx{s.pool, s.stream};
-            ctx.rho_tier = 1.0;
+            ctx.rho_tier = s.rho(ts);
             ctx.print_mode = s.print_mode;
             ctx.print_bins = s.print_bins;
             if (!f.reused) {
@@ -734,17 +742,18 @@ void render_batch(std::vector<Session*> ss, const char* tier_name, bool reprint,
             }
             ctx.pitch_um = ts.pitch_um;
             s.node();
-            f.img = output_acquire(e.device, s.source.w, s.source.h);
+            const uint32_t nw = ts.negative.w, nh = ts.negative.h;
+            f.img = output_acquire(e.device, nw, nh);
             f.neg = ts.negative.data();
             // a session on the spectral-mode print kernel stays on its own stream
-            f.fused = s.print_mode < 0 && scan_args(s.pipe, ctx.rho_tier, s.source.w, s.source.h, f.img->stride_px, f.sa);
+            f.fused = s.print_mode < 0 && scan_args(s.pipe, ctx.rho_tier, nw, nh, f.img->stride_px, f.sa);
             if (f.fused) {
                 f.pa = print_args(s.pipe, s.live, uint32_t(ts.negative.pixels()));
-                f.rgb = make_plane(s.pool, s.source.w, s.source.h);
+                f.rgb = make_plane(s.pool, nw, nh);
                 f.ready = e.ready_events[i];
                 cuda_check(cudaEventRecord(f.ready, s.stream), "frame ready");
                 slots.push_back(i);
-                shape += "," + std::to_string(s.source.w) + "x" + std::to_string(s.source.h);
+                shape += "," + std::to_string(nw) + "x" + std::to_string(nh);
             } else {
                 // the scanner's separate passes: the frame stays on its session's stream
                 print_scan_encode(ctx, s.pipe, s.live, ts.negative, f.img);
@@ -855,11 +864,10 @@ std::string session_profile(Session& s, const char* tier_name, bool reprint, uin
     std::lock_guard<std::mutex> lock(s.m);
     const std::optional<Tier> t = parse_tier(tier_name);
     if (!t) fail_invalid("unknown tier");
-    s.check_tier(*t);
     DeviceGuard dg(s.engine->device);
-    TierState& ts = s.tiers[int(*t)];
+    TierState& ts = s.tier_source(*t);
     DevBuffer flush = s.pool.acquire(size_t(256) << 20);
-    OutputImage* img = output_acquire(s.engine->device, s.source.w, s.source.h);
+    OutputImage* img = nullptr;  // acquired at the negative's size (a geometry changes it)
     json::Value stages = json::Object{};
     json::Value kernels = json::Object{};
     json::Array totals;
@@ -880,16 +888,18 @@ std::string session_profile(Session& s, const char* tier_name, bool reprint, uin
             dev::set_launch_hook(&timer);
             RenderCtx ctx{s.pool, s.stream};
             ctx.timer = &timer;
+            ctx.rho_tier = s.rho(ts);
             ctx.print_mode = s.print_mode;
             ctx.print_bins = s.print_bins;
             cudaEventRecord(a, s.stream);
             if (!reprint || !ts.negative) {
-                ctx.pitch_um = s.pitch_um();
+                ctx.pitch_um = s.tier_pitch_um(ts);
                 const uint32_t seed = s.params.b(P::grain_active) ? s.seeds.next() : kNoGrainFilmSeed;
-                ts.negative = develop(ctx, s.pipe, s.source, seed, s.hal);
+                ts.negative = develop(ctx, s.pipe, ts.source, seed, s.hal);
                 ts.pitch_um = ctx.pitch_um;
             }
             ctx.pitch_um = ts.pitch_um;
+            if (!img) img = output_acquire(s.engine->device, ts.negative.w, ts.negative.h);
             print_scan_encode(ctx, s.pipe, s.live, ts.negative, img);
             cudaEventRecord(b, s.stream);
             cuda_check(cudaStreamSynchronize(s.stream), "profile step");
@@ -915,19 +925,19 @@ std::string session_profile(Session& s, const char* tier_name, bool reprint, uin
     } catch (...) {
         cudaEventDestroy(a);
         cudaEventDestroy(b);
-        output_release(img);
+        if (img) output_release(img);
         throw;
     }
     cudaEventDestroy(a);
     cudaEventDestroy(b);
-    output_release(img);
+    if (img) output_release(img);
     json::Value r;
     r["steps"] = steps;
     r["total_ms"] = std::move(totals);
     r["stages"] = std::move(stages);
     r["kernels"] = std::move(kernels);  // per kernel name: the duration of every launch, all steps
     r["launches"] = double(dev::launch_count() - launches0 - flushes);
-    r["pixels"] = double(s.source.pixels());
+    r["pixels"] = double(ts.negative ? ts.negative.pixels() : ts.source.pixels());
     return json::write(r);
 }
 
@@ -993,7 +1003,7 @@ SPK_API const char* spk_capabilities(spk_engine* engine) {
     c["backend"] = "cuda sm_100a";
     c["device"] = e->device;
     c["effect_versions"] =
-        "halation=reference;grain=reference;glare=absent;print_spatial=reference;dir_couplers=absent";
+        "halation=reference;grain=reference;glare=absent;print_spatial=reference;dir_couplers=reference";
     e->capabilities = json::write(c);
     return e->capabilities.c_str();
 }
@@ -1004,15 +1014,19 @@ SPK_API const char* spk_memory_report(spk_engine* engine) {
     if (!engine) return "";
     Engine* e = E(engine);
     std::lock_guard<std::mutex> g(e->m);
-    size_t live = 0, negs = 0;
+    size_t live = 0, negs = 0, tiers = 0;
     for (Session* s : e->sessions) {
         live += s->pool.live_bytes();
-        for (const TierState& t : s->tiers) negs += t.negative ? t.negative.bytes() : 0;
+        for (const TierState& t : s->tiers) {
+            negs += t.negative ? t.negative.bytes() : 0;
+            if (t.source && t.source.data() != s->source.data()) tiers += t.source.bytes();
+        }
     }
     json::Value r;
     r["pool_live_bytes"] = double(live);
     r["pool_reserved_bytes"] = double(device_pool_reserved(e->device));
     r["cached_negative_bytes"] = double(negs);
+    r["tier_image_bytes"] = double(tiers);
     r["sessions"] = unsigned(e->sessions.size());
     e->memory_report = json::write(r);
     return e->memory_report.c_str();
@@ -1092,11 +1106,19 @@ SPK_API spk_status spk_set_params(spk_session* session, const char* delta_text, 
             s.seeds = SeedSequence{};
         }
         s.live = LiveParams::from(cand);
+        const uint32_t old_live = uint32_t(s.params.i(P::preview_long_edge));
         s.params = cand;
         s.film = film;
         s.print = print;
         if (d.any_shoot)
             for (TierState& t : s.tiers) t.negative = Plane{};
+        // a new preview_long_edge that changes the live tier's size drops the live tier's image and negative
+        // (reference src/session/session.cpp:247-251)
+        if (d.has_preview_long_edge) {
+            const Size2 a = downscale_size(s.source.w, s.source.h, old_live);
+            const Size2 b = downscale_size(s.source.w, s.source.h, uint32_t(s.params.i(P::preview_long_edge)));
+            if (a.w != b.w || a.h != b.h) s.tiers[int(Tier::Live)] = TierState{};
+        }
         json::Value r;
         r["invalidated"] = d.any_shoot ? "shoot" : "print";
         r["params"] = s.params.to_json();
@@ -1241,6 +1263,29 @@ SPK_API spk_status spkx_session_profile(spk_session* session, const char* tier, 
     if (!session) return invalid("session is NULL");
     return guarded([&] {
         put_json(out_json, session_profile(*S(session), tier, reprint != 0, steps));
+        return SPK_OK;
+    });
+}
+
+SPK_API spk_status spkx_session_tier_image(spk_session* session, const char* tier, float* out, size_t capacity,
+                                          uint32_t* width, uint32_t* height) {
+    last_error::clear();
+    if (!session || !width || !height) return invalid("a required pointer is NULL");
+    return guarded([&] {
+        Session& s = *S(session);
+        std::lock_guard<std::mutex> lock(s.m);
+        auto t = parse_tier(tier);
+        if (!t) fail_invalid("unknown tier");
+        DeviceGuard dg(s.engine->device);
+        const TierState& ts = s.tier_source(*t);
+        *width = ts.source.w;
+        *height = ts.source.h;
+        if (out) {
+            if (capacity < 3 * ts.source.pixels()) fail_invalid("output capacity too small");
+            cuda_check(cudaMemcpyAsync(out, ts.source.data(), ts.source.bytes(), cudaMemcpyDeviceToHost, s.stream),
+                       "tier image copy");
+            cuda_check(cudaStreamSynchronize(s.stream), "tier image copy");
+        }
         return SPK_OK;
     });
 }
@@ -1399,6 +1444,7 @@ json::Value setup_f64(const FilmSetup& f, const PrintSetup& p, const PrintRun& r
     }
     json::Value r;
     r["input_matrix"] = arr(f.input_matrix.data(), 9);
+    r["input_cctf_mode"] = int(f.input_space.cctf);
     r["gain"] = std::pow(2.0, f.params.f(P::exposure_compensation_ev));
     r["table"] = arr(f.table64.data(), f.table64.size());
     r["curve_x"] = arr(cx.data(), K);
@@ -1608,21 +1654,20 @@ SPK_API spk_status spkx_session_develop_debug(spk_session* session, const char* 
         std::lock_guard<std::mutex> lock(s.m);
         auto t = parse_tier(tier);
         if (!t) fail_invalid("unknown tier");
-        s.check_tier(*t);
         DeviceGuard dg(s.engine->device);
+        TierState& ts = s.tier_source(*t);
         RenderCtx ctx{s.pool, s.stream};
-        ctx.pitch_um = s.pitch_um();
+        ctx.pitch_um = s.tier_pitch_um(ts);
+        const Size2 ns = prepared_size(s.params, ts.source.w, ts.source.h);
+        const size_t cbytes = size_t(ns.w) * ns.h * 9 * sizeof(float);
         DevBuffer dc;
         if (counts) {
-            dc = s.pool.acquire(s.source.pixels() * 9 * sizeof(float));
-            cuda_check(cudaMemsetAsync(dc.ptr(), 0, s.source.pixels() * 9 * sizeof(float), s.stream), "memset");
+            dc = s.pool.acquire(cbytes);
+            cuda_check(cudaMemsetAsync(dc.ptr(), 0, cbytes, s.stream), "memset");
         }
-        Plane neg = develop(ctx, s.pipe, s.source, seed, s.hal, counts ? dc.as<float>() : nullptr);
+        Plane neg = develop(ctx, s.pipe, ts.source, seed, s.hal, counts ? dc.as<float>() : nullptr);
         cuda_check(cudaMemcpyAsync(negative, neg.data(), neg.bytes(), cudaMemcpyDeviceToHost, s.stream), "copy");
-        if (counts)
-            cuda_check(cudaMemcpyAsync(counts, dc.ptr(), s.source.pixels() * 9 * sizeof(float), cudaMemcpyDeviceToHost,
-                                       s.stream),
-                       "copy");
+        if (counts) cuda_check(cudaMemcpyAsync(counts, dc.ptr(), cbytes, cudaMemcpyDeviceToHost, s.stream), "copy");
         cuda_check(cudaStreamSynchronize(s.stream), "develop");
         return SPK_OK;
     });
@@ -1637,15 +1682,16 @@ SPK_API spk_status spkx_session_develop_draws(spk_session* session, const char* 
         std::lock_guard<std::mutex> lock(s.m);
         auto t = parse_tier(tier);
         if (!t) fail_invalid("unknown tier");
-        s.check_tier(*t);
         DeviceGuard dg(s.engine->device);
+        TierState& ts = s.tier_source(*t);
         RenderCtx ctx{s.pool, s.stream};
-        ctx.pitch_um = s.pitch_um();
-        const size_t bytes = s.source.pixels() * 9 * sizeof(float);
+        ctx.pitch_um = s.tier_pitch_um(ts);
+        const Size2 ns = prepared_size(s.params, ts.source.w, ts.source.h);
+        const size_t bytes = size_t(ns.w) * ns.h * 9 * sizeof(float);
         DevBuffer dc = s.pool.acquire(bytes), dl = s.pool.acquire(bytes);
         cuda_check(cudaMemsetAsync(dc.ptr(), 0, bytes, s.stream), "memset");
         cuda_check(cudaMemsetAsync(dl.ptr(), 0, bytes, s.stream), "memset");
-        Plane neg = develop(ctx, s.pipe, s.source, seed, s.hal, dc.as<float>(), dl.as<float>());
+        Plane neg = develop(ctx, s.pipe, ts.source, seed, s.hal, dc.as<float>(), dl.as<float>());
         cuda_check(cudaMemcpyAsync(counts, dc.ptr(), bytes, cudaMemcpyDeviceToHost, s.stream), "copy");
         cuda_check(cudaMemcpyAsync(lambdas, dl.ptr(), bytes, cudaMemcpyDeviceToHost, s.stream), "copy");
         cuda_check(cudaStreamSynchronize(s.stream), "develop");
@@ -1665,10 +1711,12 @@ SPK_API spk_status spk_render_vjp(spk_session* session, const char* tier, uint32
         std::lock_guard<std::mutex> lock(s.m);
         auto t = parse_tier(tier);
         if (!t) fail_invalid("unknown tier");
-        s.check_tier(*t);
         DeviceGuard dg(s.engine->device);
+        TierState& ts = s.tier_source(*t);
+        if (ts.source.w != s.source.w || ts.source.h != s.source.h)
+            fail_unsupported("the render's adjoint runs on a tier whose image is the frame itself (no downscale)");
         RenderCtx ctx{s.pool, s.stream};
-        ctx.pitch_um = s.pitch_um();
+        ctx.pitch_um = s.tier_pitch_um(ts);
         const size_t bytes = s.source.pixels() * 3 * sizeof(float);
         DevBuffer dy, dgy, dgx;
         if (output) dy = s.pool.acquire(bytes);

@@ -10,6 +10,7 @@
 #include "../cuda/vjp.hpp"
 #include "blur_plan.h"
 #include "status.hpp"
+#include "tiers.hpp"
 
 namespace spkb {
 
@@ -389,16 +390,10 @@ void check_supported(const ParamSet& p) {
     };
     if (p.b(P::auto_exposure)) refuse("auto_exposure=true (the meter)");
     if (p.b(P::glare_active) && p.f(P::glare_amount) > 0.0) refuse("glare_active=true (print glare)");
-    if (p.b(P::input_cctf_decoding)) refuse("input_cctf_decoding=true (input transfer decode)");
     if (p.f(P::halation_boost_ev) != 0.0) refuse("halation_boost_ev != 0 (highlight boost)");
     if (p.b(P::scanner_white_correction) || p.b(P::scanner_black_correction))
         refuse("scanner white/black correction (levels)");
     if (p.b(P::extended_dynamic_range)) refuse("extended_dynamic_range=true (EDR tone map)");
-    const bool geometry_identity = p.f(P::geometry_crop_x) == 0.0 && p.f(P::geometry_crop_y) == 0.0 &&
-                                   p.f(P::geometry_crop_w) == 1.0 && p.f(P::geometry_crop_h) == 1.0 &&
-                                   p.f(P::geometry_rotation_deg) == 0.0 && p.i(P::geometry_quarter_turns) % 4 == 0 &&
-                                   !p.b(P::geometry_flip_h) && !p.b(P::geometry_flip_v);
-    if (!geometry_identity) refuse("a crop, rotation, quarter turn or flip (geometry)");
 }
 
 namespace {
@@ -576,9 +571,14 @@ Plane dir_couplers(RenderCtx& ctx, const Pipeline& p, const Plane& H, DevelopArg
 }
 }  // namespace
 
-Plane develop(RenderCtx& ctx, const Pipeline& p, const Plane& source, uint32_t film_seed,
+Plane develop(RenderCtx& ctx, const Pipeline& p, const Plane& tier_source, uint32_t film_seed,
               const std::optional<HalationOverride>& hov, float* counts_out, float* lam_out) {
     const FilmSetup& f = *p.film;
+    Plane source = tier_source;
+    if (f.decode || !geometry_identity(f.params)) {
+        Stage st(ctx, "prepare");
+        source = prepare_source(ctx.pool, ctx.stream, tier_source, f.params, f.decode, uint32_t(f.input_space.cctf));
+    }
     const uint32_t w = source.w, h = source.h;
     Plane H = make_plane(ctx.pool, w, h);
     {
@@ -1025,6 +1025,8 @@ void render_vjp(RenderCtx& ctx, const Pipeline& p, const LiveParams& live, const
     if (dp.grain && (dp.da.mode != 0 || dp.amount != 1.0))
         fail_unsupported("the render's adjoint takes sub-layer grain at full strength (or no grain)");
     if (f.couplers) fail_unsupported("the render's adjoint does not take DIR couplers");
+    if (f.decode || !geometry_identity(f.params))
+        fail_unsupported("the render's adjoint does not take the input transfer decode or a geometry");
     Plane G = make_plane(ctx.pool, w, h);
     dev::develop(H3.data(), G.data(), dp.da, w, h, ctx.stream);
     Plane neg = G;

@@ -434,6 +434,7 @@ std::shared_ptr<FilmSetup> build_film_setup(const ParamSet& p, std::shared_ptr<c
     auto cs = colour_space(blob, space);
     if (!cs) fail_user("input_color_space '" + space + "' is not a colour space in the constants blob");
     s->input_space = *cs;
+    s->decode = p.b(P::input_cctf_decoding);
     auto I = illuminant(blob, film.reference_illuminant);
     if (!I) fail_user("film '" + film.id + "': unknown reference_illuminant '" + film.reference_illuminant + "'");
     s->illuminant_xy = chromaticity(blob, *I);

@@ -94,6 +94,7 @@ struct FilmSetup {
     std::shared_ptr<const Profile> profile;
     bool positive = false;
     ColourSpace input_space;
+    bool decode = false;          // input_cctf_decoding: the input space's transfer function is undone first
     std::array<double, 2> illuminant_xy{};
     Mat3 input_matrix{};
     std::array<float, 9> input_matrix_f32{};

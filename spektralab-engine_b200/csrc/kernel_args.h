@@ -90,6 +90,43 @@ struct CouplerArgs {
     uint32_t n;           // pixels
 };
 
+// Tier downscale (reference src/session/tiers.cpp:137-183, kernels/session.metal:19-91): a vertical
+// Gaussian prefilter over the frame (k_tier_blur_v), then one pass per output pixel that evaluates the
+// horizontal prefilter at the four points its bilinear sample reads and blends them. Mirror edges,
+// taps -r..r ascending, acc = fma(w_k, x, acc) from 0; the index tables are the host's exact integers.
+struct TierBlurArgs {
+    const float* taps;  // 2 r + 1
+    uint32_t w, h;
+    int32_t r;          // >= 1
+};
+struct TierResampleArgs {
+    const float* taps_x;  // 2 rx + 1 (rx = 0: no horizontal prefilter)
+    const uint32_t* xi;   // [2 out_w]: i0, i1
+    const float* xt;      // [out_w]
+    const uint32_t* yi;   // [2 out_h]
+    const float* yt;      // [out_h]
+    uint32_t in_w, in_h, out_w, out_h;
+    int32_t rx;
+};
+
+// Input transfer decode and geometry (reference kernels/film.metal:104-173, src/film/geometry.cpp:45-107)
+// in one pass over the output: each bilinear tap is decoded before the blend, which gives the values of
+// the decode pass followed by the geometry pass. The kernel forms the plan's binary64 column and row
+// terms itself, by the host plan's operations (no contraction), and splits them into two binary32 as the
+// reference's host does before its launch.
+struct PrepareArgs {
+    int32_t decode;         // 0: the input is linear
+    uint32_t mode;          // transfer function: 0 sRGB, 1 ProPhoto, 2 Adobe, 3 BT.709, 4 identity
+    float bt709_bp, bt709_exp;
+    int32_t geometry;       // 0: identity (dst = decoded src, same size)
+    uint32_t quarter, flip_h, flip_v;
+    uint32_t src_w, src_h, dst_w, dst_h;
+    double sx, sy, hx, hy;  // per-axis scale and half extent of the crop, in source pixels
+    double ca, sa;          // cos and sin of the rotation
+    double ow, oh;          // the output size
+    double cx, cy;          // the crop centre in source pixel coordinates
+};
+
 // Per-wavelength tables of one spectral integral (already neutralised).
 struct SpectralTables {
     float eps[SPKB_NL * 3];  // [l][c]

@@ -93,6 +93,7 @@ EXT = {
     "spkx_session_set_halation": (I32, [P, U32, DP, DP, DP]),
     "spkx_session_profile": (I32, [P, C, I32, U32, PS]),
     "spkx_session_negative": (I32, [P, C, FP, ctypes.c_size_t]),
+    "spkx_session_tier_image": (I32, [P, C, FP, ctypes.c_size_t, ctypes.POINTER(U32), ctypes.POINTER(U32)]),
     "spkx_session_setup_json": (I32, [P, ctypes.c_double, PS]),
     "spkx_sampler_poisson": (I32, [FP, FP, U32, U32, U32]),
     "spkx_sampler_lognormal": (I32, [FP, U32, ctypes.c_float, ctypes.c_float, U32, U32]),
@@ -117,7 +118,19 @@ REF_EXT = {
     "spkref_develop": (I32, [P]),
     "spkref_print": (I32, [P, ctypes.c_double, ctypes.POINTER(ctypes.c_uint16)]),
     "spkref_close": (None, [P]),
+    "spkref_downscale": (I32, [FP, U32, U32, U32, FP, ctypes.POINTER(U32), ctypes.POINTER(U32)]),
 }
+
+
+def reference_downscale(ref, rgb, long_edge):
+    """The reference engine's CPU tier downscale (spkref_downscale) of a float32 frame."""
+    img = np.ascontiguousarray(rgb, np.float32)
+    h, w, _ = img.shape
+    out = np.zeros(h * w * 3, np.float32)
+    ow, oh = U32(), U32()
+    ref.check(ref.lib.spkref_downscale(img.ctypes.data_as(FP), w, h, long_edge, out.ctypes.data_as(FP),
+                                       ctypes.byref(ow), ctypes.byref(oh)))
+    return out[: ow.value * oh.value * 3].reshape(oh.value, ow.value, 3)
 
 
 class SpkError(RuntimeError):
@@ -324,6 +337,16 @@ class Session:
         out = ctypes.c_char_p()
         self.L.check(self.L.lib.spkx_session_profile(self.h, tier.encode(), int(reprint), steps, ctypes.byref(out)))
         return self.L.take_json(out)
+
+    def tier_image(self, tier):
+        """spkx_session_tier_image: the tier's image, (h, w, 3) float32."""
+        w, h = U32(), U32()
+        self.L.check(self.L.lib.spkx_session_tier_image(self.h, tier.encode(), None, 0, ctypes.byref(w),
+                                                        ctypes.byref(h)))
+        buf = np.empty((h.value, w.value, 3), np.float32)
+        self.L.check(self.L.lib.spkx_session_tier_image(self.h, tier.encode(), buf.ctypes.data_as(FP), buf.size,
+                                                        ctypes.byref(w), ctypes.byref(h)))
+        return buf
 
     def negative(self, tier, w, h):
         buf = np.empty((h, w, 3), np.float32)

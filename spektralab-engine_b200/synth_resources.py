@@ -37,7 +37,7 @@ import sys
 
 import numpy as np
 
-FORMAT_VERSION = "synthetic-resources-v1"
+FORMAT_VERSION = "synthetic-resources-v2"
 FILM_STOCK = "synthetic_negative_400"
 PAPER_STOCK = "synthetic_paper"
 L_TABLE = 192  # the engine's spectral-upsampling table size (src/film/film_internal.hpp:19)
@@ -85,6 +85,9 @@ def npm(primaries, white):
 SPACES = {
     "ProPhoto RGB": ((0.7347, 0.2653, 0.1596, 0.8404, 0.0366, 0.0001), (0.3457, 0.3585)),
     "sRGB": ((0.64, 0.33, 0.30, 0.60, 0.15, 0.06), (0.3127, 0.3290)),
+    # inputs for the transfer-function decode tests (published primaries, D65 white)
+    "Adobe RGB (1998)": ((0.64, 0.33, 0.21, 0.71, 0.15, 0.06), (0.3127, 0.3290)),
+    "ITU-R BT.709": ((0.64, 0.33, 0.30, 0.60, 0.15, 0.06), (0.3127, 0.3290)),
 }
 
 # Published cone-response matrices (CIECAM02's CAT02; CAM16's M16, Li et al. 2017).

@@ -1,0 +1,123 @@
+"""The steps before the film path on the device (marked gpu): the tier downscale, the input decode and the
+geometry, through the C ABI.
+
+  * the tier image is bit-identical to the oracle's binary32 restatement of the reference's downscale
+    (which the CPU tests pin to the reference's own bits);
+  * renders on the live and full tiers with decode and geometry are within 1 LSB16 of the reference
+    engine (oracle/_ref, through its own spk_open / spk_render) without grain, and of the float64 oracle
+    with the device's grain counts as fixed noise;
+  * session rules: the live tier follows preview_long_edge, a new size drops its image and negative.
+"""
+
+import numpy as np
+import pytest
+
+import oracle
+from conftest import BASE, lsb_stats, sc
+from test_tiers_cpu import GEOMETRIES, encoded, oracle_render, ref_render
+
+pytestmark = pytest.mark.gpu
+FIRST_SEED = 0x4ABEA221
+
+
+@pytest.mark.parametrize("w,h,L", [(1000, 600, 800), (1203, 811, 800), (2000, 50, 1000), (850, 850, 849),
+                                   (900, 4000, 3000), (4000, 2250, 1600)])
+def test_tier_image_bit_exact(engine, w, h, L):
+    img = sc.synthetic_image(w, h, 21)
+    with engine.open(img, dict(BASE, preview_long_edge=L)) as s:
+        got = s.tier_image("live")
+    want = oracle.downscale(img, L)
+    assert got.shape == want.shape
+    assert np.array_equal(got, want)
+
+
+def test_preview_tier_and_fitting_frames(engine):
+    img = sc.synthetic_image(3600, 1800, 22)
+    with engine.open(img, BASE) as s:
+        prev = s.tier_image("preview")
+        assert prev.shape == (1700, 3400, 3)
+        assert np.array_equal(prev, oracle.downscale(img, 3400))
+        assert np.array_equal(s.tier_image("full"), img)  # the full tier is the frame
+    small = sc.synthetic_image(640, 480, 23)
+    with engine.open(small, BASE) as s:
+        assert np.array_equal(s.tier_image("live"), small)  # a frame that fits the tier is its own image
+
+
+@pytest.mark.parametrize("geo", sorted(GEOMETRIES))
+def test_decode_geometry_within_one_lsb_of_reference(engine, ref, ref_engine, geo):
+    w, h = 200, 136
+    img = encoded(sc.synthetic_image(w, h, 24))
+    delta = dict(BASE, grain_active=False, input_cctf_decoding=True, **GEOMETRIES[geo])
+    with engine.open(img, delta) as s:
+        a, _ = s.render("full")
+    want = ref_render(ref_engine, img, delta, "full")
+    assert a.shape == want.shape
+    assert lsb_stats(a, want)["max"] <= 1
+
+
+@pytest.mark.parametrize("space", ["sRGB", "Adobe RGB (1998)", "ITU-R BT.709"])
+def test_decode_spaces_within_one_lsb_of_reference(engine, ref, ref_engine, space):
+    w, h = 128, 96
+    img = encoded(sc.synthetic_image(w, h, 25), 0.45)
+    delta = dict(BASE, grain_active=False, input_cctf_decoding=True, input_color_space=space)
+    with engine.open(img, delta) as s:
+        a, _ = s.render("full")
+    assert lsb_stats(a, ref_render(ref_engine, img, delta, "full"))["max"] <= 1
+
+
+def test_live_tier_within_one_lsb_of_reference(engine, ref, ref_engine):
+    """The live tier of a 1200 x 900 frame at preview_long_edge 800, with a crop, a rotation, a quarter
+    turn and a flip; then a reprint at a new print exposure."""
+    w, h = 1200, 900
+    img = sc.synthetic_image(w, h, 26)
+    delta = dict(BASE, grain_active=False, preview_long_edge=800, **GEOMETRIES["all"])
+    with engine.open(img, delta) as s:
+        a, _ = s.render("live")
+        s.set_params({"print_exposure": 1.3})
+        b, meta2 = s.reprint("live")
+        assert meta2["reprint"] == 1
+    with ref_engine.open(img, delta) as r:
+        want_a, _ = r.render("live")
+        r.set_params({"print_exposure": 1.3})
+        want_b, _ = r.reprint("live")
+    assert a.shape == want_a.shape
+    assert lsb_stats(a, want_a)["max"] <= 1
+    assert lsb_stats(b, want_b)["max"] <= 1
+
+
+def test_live_tier_fp64_gate_fixed_noise(engine, lib, resources):
+    """Grain on the live tier with decode and a rotation against the float64 oracle, the device's own
+    Poisson counts as fixed noise."""
+    w, h = 1100, 700
+    img = encoded(sc.synthetic_image(w, h, 27))
+    delta = dict(BASE, grain_active=True, preview_long_edge=800, input_cctf_decoding=True, **GEOMETRIES["rotate"])
+    with engine.open(img, delta) as s:
+        a, _ = s.render("live")
+        neg, counts = s.develop_debug("live", FIRST_SEED, a.shape[1], a.shape[0])
+    out, neg64 = oracle_render(lib, resources, img, delta, 800, seed=FIRST_SEED, counts=counts)
+    st = lsb_stats(a, out)
+    assert st["frac_gt1"] <= 1e-4, st
+    assert st["max"] <= 64, st
+    np.testing.assert_allclose(neg, neg64, rtol=0, atol=5e-5)
+
+
+def test_preview_long_edge_drops_the_live_tier(engine):
+    img = sc.synthetic_image(1000, 800, 28)
+    with engine.open(img, dict(BASE, grain_active=False, preview_long_edge=900)) as s:
+        a, _ = s.render("live")
+        assert a.shape == (720, 900, 4)
+        _, m = s.reprint("live")
+        assert m["reprint"] == 1
+        s.set_params({"preview_long_edge": 800})  # a new live size: image and negative dropped
+        b, m = s.reprint("live")
+        assert m["reprint"] == 0 and b.shape == (640, 800, 4)
+        s.set_params({"preview_long_edge": 801})  # 801 x 640.8 -> 801 x 640: a new size again
+        _, m = s.reprint("live")
+        assert m["reprint"] == 0
+        _, m = s.reprint("full")
+        assert m["reprint"] == 0
+        _, m = s.reprint("full")
+        assert m["reprint"] == 1
+        s.set_params({"preview_long_edge": 1200})  # the full tier keeps its negative
+        _, m = s.reprint("full")
+        assert m["reprint"] == 1
