@@ -42,6 +42,13 @@ SPK_API spk_status spkx_session_profile(spk_session* session, const char* tier, 
  */
 SPK_API spk_status spkx_session_negative(spk_session* session, const char* tier, float* out, size_t capacity_floats);
 
+/* spkx_session_meter(session, out_json)
+ *   the auto-exposure meter's seven EV values (center_weighted, average, median, balanced, center,
+ *   protect_highlights, protect_shadows) as a JSON object; meters the frame first when no meter is kept.
+ *   SPK_ERR_USER when auto_exposure is off.
+ */
+SPK_API spk_status spkx_session_meter(spk_session* session, char** out_json);
+
 /* spkx_session_tier_image(session, tier, out, capacity_floats, width, height)
  *   the tier's image (the frame downscaled to the tier's long edge, made on first use and kept; the frame
  *   itself when it fits): its size in *width, *height and, when out is not NULL and capacity_floats

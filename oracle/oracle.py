@@ -68,6 +68,7 @@ def lib():
         L.orc_downscale.argtypes = [FP, I32, I32, I32, I32, FP]
         L.orc_prepare.argtypes = [FP, I32, I32, I32, I32, PD, PD, ctypes.POINTER(I32), ctypes.POINTER(I32)]
         L.orc_render64.argtypes = [ctypes.POINTER(OracleSetup), PD, I32, I32, FP, U16, PD]
+        L.orc_meter.argtypes = [PD, I32, I32, PD, PD]
         L.orc_poisson.argtypes = [FP, FP, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32]
         L.orc_poisson.restype = None
         L.orc_lognormal.argtypes = [FP, ctypes.c_uint32, ctypes.c_float, ctypes.c_float, ctypes.c_uint32,
@@ -299,6 +300,20 @@ def prepare(rgb, delta, cctf_mode):
                       1 if delta.get("input_cctf_decoding") else 0, int(cctf_mode), geo, out.ctypes.data_as(PD),
                       ctypes.byref(ow), ctypes.byref(oh))
     return out[: oh.value * ow.value * 3].reshape(oh.value, ow.value, 3)
+
+
+METER_METHODS = ("center_weighted", "average", "median", "balanced", "center", "protect_highlights",
+                 "protect_shadows")
+
+
+def meter(rgb, rgb_to_xyz):
+    """The auto-exposure meter's seven EV values of an image (orc_meter, binary64), by method name."""
+    x = np.ascontiguousarray(rgb, np.float64)
+    h, w, _ = x.shape
+    m = np.ascontiguousarray(np.asarray(rgb_to_xyz, np.float64).reshape(9))
+    out = np.zeros(7, np.float64)
+    lib().orc_meter(x.ctypes.data_as(PD), w, h, m.ctypes.data_as(PD), out.ctypes.data_as(PD))
+    return dict(zip(METER_METHODS, out.tolist()))
 
 
 def gaussian(plane, sigma3):

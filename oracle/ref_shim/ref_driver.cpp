@@ -287,6 +287,24 @@ __attribute__((visibility("default"))) int32_t spkref_print(void* handle, double
 
 __attribute__((visibility("default"))) void spkref_close(void* handle) { delete static_cast<RefSession*>(handle); }
 
+/* spkref_meter(rgb, w, h, rgb_to_xyz, out7): the reference's meter statistics (src/film/meter.cpp:45-120)
+ * of an image, in the order center_weighted, average, median, balanced, center, protect_highlights,
+ * protect_shadows */
+__attribute__((visibility("default"))) int32_t spkref_meter(const float* rgb, uint32_t w, uint32_t h,
+                                                            const double* rgb_to_xyz, double* out) {
+    try {
+        res::Mat3 m{};
+        for (size_t i = 0; i < 9; ++i) m[i] = rgb_to_xyz[i];
+        const film::MeterValues v = film::meter_values(rgb, w, h, m);
+        const double r[7] = {v.center_weighted, v.average, v.median, v.balanced, v.center, v.protect_highlights,
+                             v.protect_shadows};
+        std::memcpy(out, r, sizeof r);
+        return SPK_OK;
+    } catch (const std::exception& ex) {
+        return fail_status(ex);
+    }
+}
+
 /* spkref_downscale(rgb, w, h, long_edge, out, out_w, out_h): the reference's CPU tier downscale
  * (src/session/tiers.cpp:196-227) at a target long edge; out holds w h 3 floats */
 __attribute__((visibility("default"))) int32_t spkref_downscale(const float* rgb, uint32_t w, uint32_t h,

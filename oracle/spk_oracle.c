@@ -727,6 +727,79 @@ int orc_prepare(const float* src, int32_t w, int32_t h, int32_t decode, int32_t 
     return 0;
 }
 
+/* ---- the auto-exposure meter ---- */
+
+/* ascending, NaN last */
+static int cmp_nan_last(const void* pa, const void* pb) {
+    const double a = *(const double*)pa, b = *(const double*)pb;
+    const int na = isnan(a), nb = isnan(b);
+    if (na || nb) return na - nb;
+    return (a > b) - (a < b);
+}
+
+static double meter_legacy(double e) {
+    const double ev = -log2(e);
+    return isfinite(ev) ? ev : 0.0;
+}
+
+static double clamp3(double v, double lo, double hi) {
+    v = v < lo ? lo : v;
+    return hi < v ? hi : v;
+}
+
+int orc_meter(const double* rgb, int32_t sw, int32_t sh, const double m[9], double out[7]) {
+    const double mid = 0.184, floor_y = 0.184 / 4096.0, two_s2 = 2.0 * (0.2 * 0.2);
+    const size_t n = (size_t)sw * sh;
+    for (int i = 0; i < 7; ++i) out[i] = 0.0;
+    if (n == 0) return 0;
+    double* Y = (double*)malloc(n * sizeof(double));
+    double* W = (double*)malloc(n * sizeof(double));
+    double* S = (double*)malloc(n * sizeof(double));
+    const double M = (double)(sw > sh ? sw : sh);
+    for (size_t k = 0; k < n; ++k) {
+        Y[k] = (m[3] * rgb[3 * k] + m[4] * rgb[3 * k + 1]) + m[5] * rgb[3 * k + 2];
+        const double x = ((double)(k % sw) / sw - 0.5) * (sw / M), y = ((double)(k / sw) / sh - 0.5) * (sh / M);
+        W[k] = exp(-(x * x + y * y) / two_s2);
+    }
+    double s = 0.0, swy = 0.0, sw_ = 0.0;
+    for (size_t k = 0; k < n; ++k) {
+        s += Y[k];
+        swy += W[k] * Y[k];
+        sw_ += W[k];
+    }
+    memcpy(S, Y, n * sizeof(double));
+    qsort(S, n, sizeof(double), cmp_nan_last);
+    const double med = (n % 2) ? S[n / 2] : (S[n / 2 - 1] + S[n / 2]) / 2.0;
+    out[0] = meter_legacy((swy / sw_) / mid);
+    out[1] = meter_legacy((s / n) / mid);
+    out[2] = meter_legacy(med / mid);
+    /* y = max(Y, floor) keeps the order (a NaN stays NaN, last) */
+    for (size_t k = 0; k < n; ++k) S[k] = S[k] < floor_y ? floor_y : S[k];
+#define PCT(q) S[(size_t)((uint64_t)(q) * (uint64_t)(n - 1) / 1000u)]
+    const double p1 = PCT(10), p5 = PCT(50), p99 = PCT(990), p995 = PCT(995);
+#undef PCT
+    double sl = 0.0, swl = 0.0, sw2 = 0.0;
+    size_t cnt = 0;
+    for (size_t k = 0; k < n; ++k) {
+        const double y = Y[k] < floor_y ? floor_y : Y[k];
+        if (!(y >= p1 && y <= p99)) continue;
+        const double l = log(y);
+        sl += l;
+        swl += W[k] * l;
+        sw2 += W[k];
+        ++cnt;
+    }
+    const double bal = -log2(exp(sl / (double)cnt) / mid);
+    out[3] = bal;
+    out[4] = -log2(exp(swl / sw2) / mid);
+    out[5] = clamp3(log2(mid * pow(2.0, 2.5) / p995), bal - 3.0, bal);
+    out[6] = clamp3(log2(mid * pow(2.0, -3.5) / p5), bal, bal + 2.0);
+    free(Y);
+    free(W);
+    free(S);
+    return 0;
+}
+
 /* ---- the shared binary32 sampler ---- */
 
 void orc_poisson(const float* lam, float* counts, uint32_t n, uint32_t stream, uint32_t seed) {

@@ -109,6 +109,11 @@ int orc_downscale(const float* src, int32_t w, int32_t h, int32_t ow, int32_t oh
 int orc_prepare(const float* src, int32_t w, int32_t h, int32_t decode, int32_t mode, const double geo[8],
                 double* dst, int32_t* ow, int32_t* oh);
 
+/* The auto-exposure meter (reference src/film/meter.cpp:45-120) of a binary64 image, in binary64:
+ * Y = row 1 of rgb_to_xyz . rgb; out = {center_weighted, average, median, balanced, center,
+ * protect_highlights, protect_shadows}. Returns 0. */
+int orc_meter(const double* rgb, int32_t w, int32_t h, const double rgb_to_xyz[9], double out[7]);
+
 /* orc_render on a binary64 frame (the output of orc_prepare). */
 int orc_render64(const OracleSetup* s, const double* rgb, int32_t w, int32_t h, const float* counts,
                  uint16_t* out_rgba, double* out_negative);

@@ -66,7 +66,12 @@ __global__ void k_expose(const float* __restrict__ rgb, float* __restrict__ hout
                          const __grid_constant__ ExposeArgs q) {
     const uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
     if (gid >= q.n) return;
-    const float r = rgb[3 * size_t(gid)], g = rgb[3 * size_t(gid) + 1], b = rgb[3 * size_t(gid) + 2];
+    float r = rgb[3 * size_t(gid)], g = rgb[3 * size_t(gid) + 1], b = rgb[3 * size_t(gid) + 2];
+    if (q.apply_ae) {  // the auto-exposure scale pass (reference src/film/develop.cpp:132-140), one rounding each
+        r = __fmul_rn(r, q.ae_gain);
+        g = __fmul_rn(g, q.ae_gain);
+        b = __fmul_rn(b, q.ae_gain);
+    }
     const float X = (q.a[0] * r + q.a[1] * g) + q.a[2] * b;
     const float Y = (q.a[3] * r + q.a[4] * g) + q.a[5] * b;
     const float Z = (q.a[6] * r + q.a[7] * g) + q.a[8] * b;

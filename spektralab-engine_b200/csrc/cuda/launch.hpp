@@ -38,6 +38,11 @@ void tier_resample(const float* v, float* dst, const TierResampleArgs& a, cudaSt
 // Input transfer decode and geometry: src (src_w x src_h) -> dst (dst_w x dst_h).
 void prepare(const float* src, float* dst, const PrepareArgs& a, cudaStream_t s);
 
+// The auto-exposure meter's statistics of the meter image into *a.out (13 doubles); a.sel must hold the
+// six ranks with zero prefixes, masks and histograms. a.partial holds meter_partial_doubles() doubles.
+size_t meter_partial_doubles();
+void meter_stats(const MeterArgs& a, cudaStream_t s);
+
 // RGB -> film exposure H (Mitchell bicubic of the spectral table, L x L float4 texels), times the
 // compensation gain.
 void expose(const float* rgb, float* h, const float* table4, const ExposeArgs& a, cudaStream_t s);

@@ -22,6 +22,7 @@
 #include "spektralab.h"
 #include "spektralab_b200.h"
 #include "status.hpp"
+#include "meter.hpp"
 #include "tiers.hpp"
 
 namespace spkb {
@@ -156,10 +157,13 @@ public:
     std::atomic<uint32_t> nodes_done{0};
     uint32_t nodes_total = 0;
     bool done = false;
+    Plane meter_image;                // the frame at the meter's 1600 px long edge, kept
+    std::optional<MeterValues> meter;  // until a field of the meter's key changes
 
     ~Session() {
         // stream-ordered buffers are freed on the stream, so they go before it does
         for (TierState& t : tiers) t = TierState{};
+        meter_image = Plane{};
         source = Plane{};
         pipe = Pipeline{};
         if (stream) {
@@ -213,6 +217,23 @@ public:
             ts.long_edge = std::max(ts.source.w, ts.source.h);
         }
         return ts;
+    }
+    // The auto-exposure EV of the develops, or none when auto_exposure is off (reference
+    // src/session/session.cpp:294-320): the meter runs once, on the live tier's image when that is the
+    // 1600 px downscale already, else on its own downscale, and is kept until a meter-key field changes.
+    std::optional<double> session_ev() {
+        if (!params.b(P::auto_exposure)) return std::nullopt;
+        if (!meter) {
+            if (!meter_image) {
+                const TierState& live = tiers[int(Tier::Live)];
+                if (live.source && params.i(P::preview_long_edge) == int64_t(kMeterLongEdge))
+                    meter_image = live.source;
+                else
+                    meter_image = downscale(pool, stream, source, kMeterLongEdge);
+            }
+            meter = spkb::meter(pool, stream, meter_image, params, pipe.film->input_space);
+        }
+        return meter->ev(params.s(P::auto_exposure_method));
     }
     // rho_tier: the tier image's long edge over the frame's (never L / M: the floor can give L - 1)
     double rho(const TierState& ts) const { return double(ts.long_edge) / double(std::max(source.w, source.h)); }
@@ -380,6 +401,7 @@ Session* open_session(Engine& e, const void* data, bool device_ptr, uint32_t w, 
 void develop_tier(Session& s, Tier t, RenderCtx& ctx) {
     TierState& ts = s.tier_source(t);
     ts.negative = Plane{};
+    ctx.ae_ev = s.session_ev();
     const uint32_t seed = s.params.b(P::grain_active) ? s.seeds.next() : kNoGrainFilmSeed;
     ctx.pitch_um = s.tier_pitch_um(ts);
     s.node();
@@ -893,6 +915,7 @@ std::string session_profile(Session& s, const char* tier_name, bool reprint, uin
             ctx.print_bins = s.print_bins;
             cudaEventRecord(a, s.stream);
             if (!reprint || !ts.negative) {
+                ctx.ae_ev = s.session_ev();
                 ctx.pitch_um = s.tier_pitch_um(ts);
                 const uint32_t seed = s.params.b(P::grain_active) ? s.seeds.next() : kNoGrainFilmSeed;
                 ts.negative = develop(ctx, s.pipe, ts.source, seed, s.hal);
@@ -1107,6 +1130,13 @@ SPK_API spk_status spk_set_params(spk_session* session, const char* delta_text, 
         }
         s.live = LiveParams::from(cand);
         const uint32_t old_live = uint32_t(s.params.i(P::preview_long_edge));
+        // a change to a field of the meter's key re-arms the meter (reference src/session/session.cpp:34-36)
+        constexpr P kMeterKey[] = {P::input_color_space,    P::input_cctf_decoding, P::geometry_crop_x,
+                                   P::geometry_crop_y,      P::geometry_crop_w,     P::geometry_crop_h,
+                                   P::geometry_rotation_deg, P::geometry_quarter_turns, P::geometry_flip_h,
+                                   P::geometry_flip_v};
+        for (P k : kMeterKey)
+            if (json::write(s.params.get(size_t(k))) != json::write(cand.get(size_t(k)))) s.meter.reset();
         s.params = cand;
         s.film = film;
         s.print = print;
@@ -1263,6 +1293,29 @@ SPK_API spk_status spkx_session_profile(spk_session* session, const char* tier, 
     if (!session) return invalid("session is NULL");
     return guarded([&] {
         put_json(out_json, session_profile(*S(session), tier, reprint != 0, steps));
+        return SPK_OK;
+    });
+}
+
+SPK_API spk_status spkx_session_meter(spk_session* session, char** out_json) {
+    last_error::clear();
+    if (!session || !out_json) return invalid("a required pointer is NULL");
+    return guarded([&] {
+        Session& s = *S(session);
+        std::lock_guard<std::mutex> lock(s.m);
+        DeviceGuard dg(s.engine->device);
+        if (!s.params.b(P::auto_exposure)) fail_user("auto_exposure is off in this session");
+        s.session_ev();
+        const MeterValues& m = *s.meter;
+        json::Value r;
+        r["center_weighted"] = m.center_weighted;
+        r["average"] = m.average;
+        r["median"] = m.median;
+        r["balanced"] = m.balanced;
+        r["center"] = m.center;
+        r["protect_highlights"] = m.protect_highlights;
+        r["protect_shadows"] = m.protect_shadows;
+        put_json(out_json, json::write(r));
         return SPK_OK;
     });
 }
@@ -1445,6 +1498,7 @@ json::Value setup_f64(const FilmSetup& f, const PrintSetup& p, const PrintRun& r
     json::Value r;
     r["input_matrix"] = arr(f.input_matrix.data(), 9);
     r["input_cctf_mode"] = int(f.input_space.cctf);
+    r["input_rgb_to_xyz"] = arr(f.input_space.rgb_to_xyz.data(), 9);
     r["gain"] = std::pow(2.0, f.params.f(P::exposure_compensation_ev));
     r["table"] = arr(f.table64.data(), f.table64.size());
     r["curve_x"] = arr(cx.data(), K);
@@ -1657,6 +1711,7 @@ SPK_API spk_status spkx_session_develop_debug(spk_session* session, const char* 
         DeviceGuard dg(s.engine->device);
         TierState& ts = s.tier_source(*t);
         RenderCtx ctx{s.pool, s.stream};
+        ctx.ae_ev = s.session_ev();
         ctx.pitch_um = s.tier_pitch_um(ts);
         const Size2 ns = prepared_size(s.params, ts.source.w, ts.source.h);
         const size_t cbytes = size_t(ns.w) * ns.h * 9 * sizeof(float);
@@ -1685,6 +1740,7 @@ SPK_API spk_status spkx_session_develop_draws(spk_session* session, const char* 
         DeviceGuard dg(s.engine->device);
         TierState& ts = s.tier_source(*t);
         RenderCtx ctx{s.pool, s.stream};
+        ctx.ae_ev = s.session_ev();
         ctx.pitch_um = s.tier_pitch_um(ts);
         const Size2 ns = prepared_size(s.params, ts.source.w, ts.source.h);
         const size_t bytes = size_t(ns.w) * ns.h * 9 * sizeof(float);

@@ -388,7 +388,6 @@ void check_supported(const ParamSet& p) {
     auto refuse = [](const std::string& what) {
         fail_user(what + " is outside this B200 build's render path");
     };
-    if (p.b(P::auto_exposure)) refuse("auto_exposure=true (the meter)");
     if (p.b(P::glare_active) && p.f(P::glare_amount) > 0.0) refuse("glare_active=true (print glare)");
     if (p.f(P::halation_boost_ev) != 0.0) refuse("halation_boost_ev != 0 (highlight boost)");
     if (p.b(P::scanner_white_correction) || p.b(P::scanner_black_correction))
@@ -583,7 +582,12 @@ Plane develop(RenderCtx& ctx, const Pipeline& p, const Plane& tier_source, uint3
     Plane H = make_plane(ctx.pool, w, h);
     {
         Stage st(ctx, "expose");
-        dev::expose(source.data(), H.data(), p.dev.table.as<float>(), expose_args(f, source.pixels()), ctx.stream);
+        ExposeArgs ea = expose_args(f, source.pixels());
+        if (f.params.b(P::auto_exposure) && ctx.ae_ev) {
+            ea.ae_gain = f32(std::pow(2.0, *ctx.ae_ev));
+            ea.apply_ae = 1;
+        }
+        dev::expose(source.data(), H.data(), p.dev.table.as<float>(), ea, ctx.stream);
     }
     if (const double s = film_lens_blur_px(ctx, f); s > 0.0) {
         Stage st(ctx, "lens_blur");
@@ -1025,6 +1029,7 @@ void render_vjp(RenderCtx& ctx, const Pipeline& p, const LiveParams& live, const
     if (dp.grain && (dp.da.mode != 0 || dp.amount != 1.0))
         fail_unsupported("the render's adjoint takes sub-layer grain at full strength (or no grain)");
     if (f.couplers) fail_unsupported("the render's adjoint does not take DIR couplers");
+    if (f.params.b(P::auto_exposure)) fail_unsupported("the render's adjoint does not take the auto-exposure meter");
     if (f.decode || !geometry_identity(f.params))
         fail_unsupported("the render's adjoint does not take the input transfer decode or a geometry");
     Plane G = make_plane(ctx.pool, w, h);

@@ -39,6 +39,7 @@ struct RenderCtx {
     cudaStream_t stream;
     double pitch_um = 0.0;
     double rho_tier = 1.0;
+    std::optional<double> ae_ev = std::nullopt;  // the auto-exposure meter's EV for the develop (none: no scale)
     // optional per-stage timing: events recorded around each stage when set
     struct Timer* timer = nullptr;
     // the print stage: -1 the binary32 print kernel, else a SpectralMode of the spectral-mode kernel at

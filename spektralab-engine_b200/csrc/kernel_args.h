@@ -16,6 +16,8 @@ struct ExposeArgs {
     float a[9];        // input matrix A, row-major
     float gain;        // f32(2^exposure_compensation_ev)
     int32_t apply_gain;
+    float ae_gain;     // f32(2^ev) of the auto-exposure meter, on the RGB before the upsampling
+    int32_t apply_ae;
     uint32_t L;        // table size; the table is L x L float4 texels, [i][j] = (R, G, B, 0)
     uint32_t n;        // pixels
 };
@@ -125,6 +127,39 @@ struct PrepareArgs {
     double ca, sa;          // cos and sin of the rotation
     double ow, oh;          // the output size
     double cx, cy;          // the crop centre in source pixel coordinates
+};
+
+// The auto-exposure meter's device statistics (reference src/film/meter.cpp:45-120). Six order-statistic
+// queries on the ascending luminances (NaN last): the two middle ranks (the same rank twice for an odd
+// count), then the ranks q (n - 1) / 1000 for q = 10, 50, 990, 995.
+#define kMeterQueries 6
+#define kMeterMedLo 0
+#define kMeterMedHi 1
+#define kMeterP10 2
+#define kMeterP50 3
+#define kMeterP990 4
+#define kMeterP995 5
+struct MeterSelect {
+    uint64_t rank[kMeterQueries];    // the rank still to find inside the current prefix
+    uint64_t prefix[kMeterQueries];  // the ordered key's digits found so far
+    uint64_t mask[kMeterQueries];
+    uint32_t hist[kMeterQueries][256];
+    double value[kMeterQueries];     // the selected luminances
+};
+struct MeterOut {
+    // sum Y, sum w Y, sum w; then over the intent range: sum ln y, sum w ln y, sum w, count
+    double sums[7];
+    double select[kMeterQueries];
+};
+struct MeterArgs {
+    const float* rgb;   // the meter image, interleaved RGB
+    uint32_t w, h;
+    uint64_t n;
+    double m0, m1, m2;  // row Y of the input space's RGB -> XYZ matrix
+    uint64_t* key;      // n ordered keys (scratch)
+    double* partial;    // 7 x the launch's blocks (scratch)
+    MeterSelect* sel;
+    MeterOut* out;
 };
 
 // Per-wavelength tables of one spectral integral (already neutralised).

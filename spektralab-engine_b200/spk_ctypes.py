@@ -93,6 +93,7 @@ EXT = {
     "spkx_session_set_halation": (I32, [P, U32, DP, DP, DP]),
     "spkx_session_profile": (I32, [P, C, I32, U32, PS]),
     "spkx_session_negative": (I32, [P, C, FP, ctypes.c_size_t]),
+    "spkx_session_meter": (I32, [P, PS]),
     "spkx_session_tier_image": (I32, [P, C, FP, ctypes.c_size_t, ctypes.POINTER(U32), ctypes.POINTER(U32)]),
     "spkx_session_setup_json": (I32, [P, ctypes.c_double, PS]),
     "spkx_sampler_poisson": (I32, [FP, FP, U32, U32, U32]),
@@ -118,6 +119,7 @@ REF_EXT = {
     "spkref_develop": (I32, [P]),
     "spkref_print": (I32, [P, ctypes.c_double, ctypes.POINTER(ctypes.c_uint16)]),
     "spkref_close": (None, [P]),
+    "spkref_meter": (I32, [FP, U32, U32, DP, DP]),
     "spkref_downscale": (I32, [FP, U32, U32, U32, FP, ctypes.POINTER(U32), ctypes.POINTER(U32)]),
 }
 
@@ -131,6 +133,17 @@ def reference_downscale(ref, rgb, long_edge):
     ref.check(ref.lib.spkref_downscale(img.ctypes.data_as(FP), w, h, long_edge, out.ctypes.data_as(FP),
                                        ctypes.byref(ow), ctypes.byref(oh)))
     return out[: ow.value * oh.value * 3].reshape(oh.value, ow.value, 3)
+
+
+def reference_meter(ref, rgb, rgb_to_xyz):
+    """The reference engine's meter statistics (spkref_meter) of a float32 image, by method name."""
+    img = np.ascontiguousarray(rgb, np.float32)
+    h, w, _ = img.shape
+    m = np.ascontiguousarray(np.asarray(rgb_to_xyz, np.float64).reshape(9))
+    out = np.zeros(7, np.float64)
+    ref.check(ref.lib.spkref_meter(img.ctypes.data_as(FP), w, h, m.ctypes.data_as(DP), out.ctypes.data_as(DP)))
+    names = ("center_weighted", "average", "median", "balanced", "center", "protect_highlights", "protect_shadows")
+    return dict(zip(names, out.tolist()))
 
 
 class SpkError(RuntimeError):
@@ -336,6 +349,12 @@ class Session:
     def profile(self, tier="full", reprint=False, steps=3):
         out = ctypes.c_char_p()
         self.L.check(self.L.lib.spkx_session_profile(self.h, tier.encode(), int(reprint), steps, ctypes.byref(out)))
+        return self.L.take_json(out)
+
+    def meter(self):
+        """spkx_session_meter: the seven auto-exposure EV values."""
+        out = ctypes.c_char_p()
+        self.L.check(self.L.lib.spkx_session_meter(self.h, ctypes.byref(out)))
         return self.L.take_json(out)
 
     def tier_image(self, tier):
