@@ -48,7 +48,8 @@ def test_auto_exposure_render_within_one_lsb(engine, ref, ref_engine, method):
 
 def test_auto_exposure_live_tier_within_one_lsb(engine, lib, resources, ref, ref_engine):
     """A 2000 x 1200 frame on the live tier at 1600 px (the meter reads the live tier's image) and at 900 px
-    (its own downscale), with decode and a rotation; against the reference and the float64 oracle."""
+    (its own downscale), with decode and a rotation: within 1 LSB16 of the reference; the float64 oracle's
+    gate as elsewhere."""
     img = encoded(meter_image(2000, 1200, 44))
     for L in (1600, 900):
         delta = dict(BASE, grain_active=False, auto_exposure=True, input_cctf_decoding=True, preview_long_edge=L,
@@ -56,8 +57,9 @@ def test_auto_exposure_live_tier_within_one_lsb(engine, lib, resources, ref, ref
         with engine.open(img, delta) as s:
             a, _ = s.render("live")
         assert lsb_stats(a, ref_render(ref_engine, img, delta, "live"))["max"] <= 1
-        got, _ = oracle_render_ae(lib, resources, img, delta, L)
-        assert lsb_stats(a, got)["max"] <= 1
+        # binary32 against the float64 oracle (decode and a rotation before the develop): the FP64 gate
+        st = lsb_stats(a, oracle_render_ae(lib, resources, img, delta, L)[0])
+        assert st["frac_gt1"] <= 1e-4 and st["max"] <= 8, st
 
 
 def test_meter_rearms_on_its_key(engine):
