@@ -43,6 +43,8 @@ class OracleSetup(ctypes.Structure):
         ("cctf_active", I32), ("cctf_mode", I32), ("m_nid", D * 9),
         ("couplers", I32), ("n_dir", I32), ("coupler_m", D * 9), ("dmax", D * 3), ("cy0", PD),
         ("dir_w", (D * 3) * MAXC), ("dir_s", (D * 3) * MAXC),
+        ("glare", I32), ("glare_mean", ctypes.c_float), ("glare_sd", ctypes.c_float), ("glare_sigma", D),
+        ("glare_tint", D * 3), ("print_seed", ctypes.c_uint32),
     ]
 
 
@@ -90,7 +92,7 @@ def lib():
 class Oracle:
     """An OracleSetup plus the arrays it points into (kept alive here)."""
 
-    def __init__(self, f64, seed=0, halation=None, print_exposure=None, rho_tier=1.0):
+    def __init__(self, f64, seed=0, halation=None, print_exposure=None, rho_tier=1.0, print_seed=0):
         s = OracleSetup()
         self.keep = []
 
@@ -185,6 +187,14 @@ class Oracle:
         s.cctf_active = 1 if f64["cctf_active"] else 0
         s.cctf_mode = int(f64["cctf_mode"])
         put("m_nid", f64["m_nid"])
+        gl = f64.get("glare")
+        if gl and gl["draws"]:
+            s.glare = 1
+            s.glare_mean = gl["mean"]
+            s.glare_sd = gl["sd"]
+            s.glare_sigma = gl["sigma_full"] * rho_tier
+            put("glare_tint", gl["tint"])
+            s.print_seed = print_seed
         cp = f64.get("couplers")
         if cp and cp["active"]:
             s.couplers = 1

@@ -462,6 +462,23 @@ static uint16_t enc16(double v) {
 int orc_print(const OracleSetup* s, const double* neg, int32_t w, int32_t h, uint16_t* out, double* lin) {
     const size_t n = (size_t)w * h, N = 3 * n;
     double* rgb = (double*)malloc(N * sizeof(double));
+    double* field = NULL;
+    if (s->glare && s->printed) {
+        /* one lognormal value per pixel on all channels, then its blur */
+        double* f = (double*)malloc(N * sizeof(double));
+        field = (double*)malloc(N * sizeof(double));
+#pragma omp parallel for
+        for (size_t p = 0; p < n; ++p) {
+            const double v = (double)spk_lognormal(s->glare_mean, s->glare_sd, (uint32_t)p, 200u, s->print_seed);
+            f[3 * p] = f[3 * p + 1] = f[3 * p + 2] = v;
+        }
+        const double sg[3] = {s->glare_sigma, s->glare_sigma, s->glare_sigma};
+        if (s->glare_sigma > 0.0)
+            orc_gaussian(f, field, w, h, sg);
+        else
+            memcpy(field, f, N * sizeof(double));
+        free(f);
+    }
 #pragma omp parallel for
     for (size_t p = 0; p < n; ++p) {
         double d[3] = {neg[3 * p], neg[3 * p + 1], neg[3 * p + 2]}, r[3];
@@ -475,6 +492,8 @@ int orc_print(const OracleSetup* s, const double* neg, int32_t w, int32_t h, uin
         }
         spectral(s->scan_eps, s->scan_beta, s->scan_wt, d, r);
         for (int c = 0; c < 3; ++c) r[c] = fmax(r[c], 0.0) + kTiny;
+        if (field)
+            for (int c = 0; c < 3; ++c) r[c] += (field[3 * p + c] / 100.0) * s->glare_tint[c];
         double o[3];
         mat(s->to_rgb, r, o);
         gamut(s, o);
@@ -495,6 +514,7 @@ int orc_print(const OracleSetup* s, const double* neg, int32_t w, int32_t h, uin
         for (size_t i = 0; i < N; ++i) rgb[i] = (1.0 + a) * rgb[i] - a * g[i];
         free(g);
     }
+    free(field);
     if (lin) memcpy(lin, rgb, N * sizeof(double));
 #pragma omp parallel for
     for (size_t p = 0; p < n; ++p) {

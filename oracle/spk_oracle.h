@@ -67,6 +67,12 @@ typedef struct {
     double coupler_m[9], dmax[3];
     const double* cy0; /* 3K, channel-major */
     double dir_w[ORC_MAX_COMP][3], dir_s[ORC_MAX_COMP][3];
+    /* print glare (reference src/fx/glare.cpp:27-50): a lognormal field (binary32 mean and sd, stream 200,
+     * the print seed) blurred by glare_sigma and added to the scan's XYZ as (F / 100) tint */
+    int32_t glare;
+    float glare_mean, glare_sd;
+    double glare_sigma, glare_tint[3];
+    uint32_t print_seed;
 } OracleSetup;
 
 /* The whole render of a w x h frame; rgb is 3 floats per pixel (already non-finite-cleaned),

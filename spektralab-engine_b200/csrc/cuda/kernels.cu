@@ -595,6 +595,17 @@ __global__ void k_sampler_poisson(const float* lam, float* out, uint32_t n, uint
     out[i] = spk_poisson(lam[i], i, stream, seed);
 }
 
+// The print glare's field (reference kernels/fx_grain.metal:99-116 with same_all): one lognormal value
+// per pixel, on stream 200 with the print seed, written to the three channels.
+__global__ void k_glare_field(float* out, uint32_t n, float mean, float sd, uint32_t seed) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float v = spk_lognormal(mean, sd, i, 200u, seed);
+    out[3 * size_t(i)] = v;
+    out[3 * size_t(i) + 1] = v;
+    out[3 * size_t(i) + 2] = v;
+}
+
 __global__ void k_sampler_lognormal(float* out, uint32_t n, float mean, float sd, uint32_t stream, uint32_t seed) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -733,6 +744,11 @@ void sampler_poisson(const float* lam, float* out, uint32_t n, uint32_t stream, 
     if (n == 0) return;
     Probe p("sampler_poisson", s);
     k_sampler_poisson<<<div_up(n, 128), 128, 0, s>>>(lam, out, n, stream, seed);
+}
+
+void glare_field(float* out, uint32_t pixels, float mean, float sd, uint32_t seed, cudaStream_t s) {
+    Probe p("glare_field", s);
+    k_glare_field<<<div_up(pixels, 256), 256, 0, s>>>(out, pixels, mean, sd, seed);
 }
 
 void sampler_lognormal(float* out, uint32_t n, float mean, float stddev, uint32_t stream, uint32_t seed,

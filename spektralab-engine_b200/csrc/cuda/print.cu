@@ -63,9 +63,10 @@ __device__ __forceinline__ void print_pair(const PrintArgs& a, const float* __re
 #pragma unroll 1
     for (uint32_t k = 0; k < 2u; ++k) {
         if (k == 1u && !two) break;
-        const float x = fmaxf(k ? X.y : X.x, 0.0f) + kTiny;
-        const float y = fmaxf(k ? Y.y : Y.x, 0.0f) + kTiny;
-        const float z = fmaxf(k ? Z.y : Z.x, 0.0f) + kTiny;
+        float x = fmaxf(k ? X.y : X.x, 0.0f) + kTiny;
+        float y = fmaxf(k ? Y.y : Y.x, 0.0f) + kTiny;
+        float z = fmaxf(k ? Z.y : Z.x, 0.0f) + kTiny;
+        add_glare(a, size_t(p0 + k), x, y, z);
         float r, g, b;
         mat_apply(a.to_rgb, x, y, z, r, g, b);
         gamut(a, r, g, b);

@@ -39,6 +39,16 @@ __device__ __forceinline__ float fsqrt(float x) {
 
 // log10(max(x, 0) + 1e-10) as log2 on the special-function unit times log10 2 (absolute error about
 // 2^-22 on the log-exposure axis)
+// Print glare (reference kernels/fx_glare.metal:12-22): xyz_c + (F / 100) tint_c for the field value F of
+// pixel p, each operation rounded on its own.
+__device__ __forceinline__ void add_glare(const PrintArgs& a, size_t p, float& x, float& y, float& z) {
+    if (!a.glare) return;
+    const float f = __fdiv_rn(a.glare[3 * p], 100.0f);
+    x = __fadd_rn(x, __fmul_rn(f, a.glare_tint[0]));
+    y = __fadd_rn(y, __fmul_rn(f, a.glare_tint[1]));
+    z = __fadd_rn(z, __fmul_rn(f, a.glare_tint[2]));
+}
+
 __device__ __forceinline__ float log10_floor(float x) { return lg2_approx(fmaxf(x, 0.0f) + kTiny) * kLog10Of2; }
 
 __device__ __forceinline__ float paper_lookup(const float* __restrict__ tab, uint32_t K, const AxisGrid& g,

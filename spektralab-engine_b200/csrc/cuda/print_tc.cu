@@ -481,9 +481,10 @@ __global__ void __launch_bounds__(kTcThreads) k_print_spectral(const __grid_cons
         }
         contract<M, NLP, 1>(p, smem, tmem, d, R, g, ok);
         if (valid) {
-            const float x = fmaxf(R[0], 0.0f) + kTiny;
-            const float y = fmaxf(R[1], 0.0f) + kTiny;
-            const float z = fmaxf(R[2], 0.0f) + kTiny;
+            float x = fmaxf(R[0], 0.0f) + kTiny;
+            float y = fmaxf(R[1], 0.0f) + kTiny;
+            float z = fmaxf(R[2], 0.0f) + kTiny;
+            add_glare(a, size_t(px), x, y, z);
             float r, gg, b;
             mat_apply(a.to_rgb, x, y, z, r, gg, b);
             gamut(a, r, gg, b);

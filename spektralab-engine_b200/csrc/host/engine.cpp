@@ -235,6 +235,9 @@ public:
         }
         return meter->ev(params.s(P::auto_exposure_method));
     }
+    // The print seed of a render or reprint: the next draw of the seed sequence when the glare can draw,
+    // even where its stage is skipped (scan_film), else 0 (reference src/session/session.cpp:339-344)
+    uint32_t draw_print_seed() { return pipe.print->glare_draws() ? seeds.next() : 0u; }
     // rho_tier: the tier image's long edge over the frame's (never L / M: the floor can give L - 1)
     double rho(const TierState& ts) const { return double(ts.long_edge) / double(std::max(source.w, source.h)); }
     // the develop's pixel pitch at the tier's long edge
@@ -434,6 +437,7 @@ void render(Session& s, const char* tier_name, bool reprint, spk_result* out) {
             developed = true;
             develop_tier(s, *t, ctx);
         }
+        ctx.print_seed = s.draw_print_seed();
         ctx.pitch_um = ts.pitch_um;
         s.node();
         img = output_acquire(s.engine->device, ts.negative.w, ts.negative.h);
@@ -508,6 +512,7 @@ struct BatchFrame {
     Plane rgb;
     const float* neg = nullptr;
     PrintArgs pa{};
+    Plane glare;             // the print glare's field (empty without glare)
     ScanArgs sa{};
     bool fused = false;      // print and scanner inside the batch graph
     bool reused = false;     // the tier's negative was cached (reprint)
@@ -762,6 +767,7 @@ void render_batch(std::vector<Session*> ss, const char* tier_name, bool reprint,
                 f.developed = true;
                 develop_tier(s, *t, ctx);
             }
+            ctx.print_seed = s.draw_print_seed();
             ctx.pitch_um = ts.pitch_um;
             s.node();
             const uint32_t nw = ts.negative.w, nh = ts.negative.h;
@@ -771,6 +777,8 @@ void render_batch(std::vector<Session*> ss, const char* tier_name, bool reprint,
             f.fused = s.print_mode < 0 && scan_args(s.pipe, ctx.rho_tier, nw, nh, f.img->stride_px, f.sa);
             if (f.fused) {
                 f.pa = print_args(s.pipe, s.live, uint32_t(ts.negative.pixels()));
+                f.glare = glare_plane(ctx, s.pipe, nw, nh);  // on the session's stream, before its ready event
+                f.pa.glare = f.glare ? f.glare.data() : nullptr;
                 f.rgb = make_plane(s.pool, nw, nh);
                 f.ready = e.ready_events[i];
                 cuda_check(cudaEventRecord(f.ready, s.stream), "frame ready");
@@ -921,6 +929,7 @@ std::string session_profile(Session& s, const char* tier_name, bool reprint, uin
                 ts.negative = develop(ctx, s.pipe, ts.source, seed, s.hal);
                 ts.pitch_um = ctx.pitch_um;
             }
+            ctx.print_seed = s.draw_print_seed();
             ctx.pitch_um = ts.pitch_um;
             if (!img) img = output_acquire(s.engine->device, ts.negative.w, ts.negative.h);
             print_scan_encode(ctx, s.pipe, s.live, ts.negative, img);
@@ -1499,6 +1508,18 @@ json::Value setup_f64(const FilmSetup& f, const PrintSetup& p, const PrintRun& r
     r["input_matrix"] = arr(f.input_matrix.data(), 9);
     r["input_cctf_mode"] = int(f.input_space.cctf);
     r["input_rgb_to_xyz"] = arr(f.input_space.rgb_to_xyz.data(), 9);
+    {
+        // the print glare: its binary32 lognormal parameters, the blur at the full tier, the tint
+        const PrintSetup& ps = p;
+        const double pp = ps.glare_percent * ps.glare_amount;
+        json::Value g;
+        g["draws"] = !ps.scanned && ps.glare_draws();
+        g["mean"] = double(f32(pp));
+        g["sd"] = double(f32(ps.glare_roughness * pp));
+        g["sigma_full"] = ps.glare_blur_full * std::sqrt(std::max(ps.glare_amount, 0.0));
+        g["tint"] = arr(ps.glare_tint.data(), 3);
+        r["glare"] = std::move(g);
+    }
     r["gain"] = std::pow(2.0, f.params.f(P::exposure_compensation_ev));
     r["table"] = arr(f.table64.data(), f.table64.size());
     r["curve_x"] = arr(cx.data(), K);

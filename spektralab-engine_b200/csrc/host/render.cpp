@@ -388,7 +388,6 @@ void check_supported(const ParamSet& p) {
     auto refuse = [](const std::string& what) {
         fail_user(what + " is outside this B200 build's render path");
     };
-    if (p.b(P::glare_active) && p.f(P::glare_amount) > 0.0) refuse("glare_active=true (print glare)");
     if (p.f(P::halation_boost_ev) != 0.0) refuse("halation_boost_ev != 0 (highlight boost)");
     if (p.b(P::scanner_white_correction) || p.b(P::scanner_black_correction))
         refuse("scanner white/black correction (levels)");
@@ -739,6 +738,7 @@ PrintArgs print_args(const Pipeline& p, const LiveParams& live, uint32_t pixels)
     a.cam = s.cam_args;
     a.cmax = p.dev.cmax.as<float>();
     a.n = pixels;
+    for (int c = 0; c < 3; ++c) a.glare_tint[c] = f32(p.print->glare_tint[size_t(c)]);
     return a;
 }
 
@@ -779,12 +779,27 @@ bool scan_args(const Pipeline& p, double rho_tier, uint32_t w, uint32_t h, uint3
     return true;
 }
 
+Plane glare_plane(RenderCtx& ctx, const Pipeline& p, uint32_t w, uint32_t h) {
+    const PrintSetup& s = *p.print;
+    if (s.scanned || !s.glare_draws()) return {};
+    const double pp = s.glare_percent * s.glare_amount;
+    Plane f = make_plane(ctx.pool, w, h);
+    dev::glare_field(f.data(), w * h, f32(pp), f32(s.glare_roughness * pp), ctx.print_seed, ctx.stream);
+    if (s.glare_blur_full > 0.0) {
+        const double sg = s.glare_blur_full * ctx.rho_tier * std::sqrt(std::max(s.glare_amount, 0.0));
+        gaussian(ctx, f, f, Vec3{sg, sg, sg});
+    }
+    return f;
+}
+
 namespace {
 // negative -> linear output RGB by the binary32 print kernel, or by the spectral-mode kernel when the
 // context asks for one (its tables and arguments uploaded for the call, its wait status read back)
-void print_stage(RenderCtx& ctx, const Pipeline& p, const LiveParams& live, const Plane& negative, const Plane& rgb) {
+void print_stage(RenderCtx& ctx, const Pipeline& p, const LiveParams& live, const Plane& negative, const Plane& rgb,
+                 const float* glare) {
     const uint32_t n = uint32_t(negative.pixels());
-    const PrintArgs a = print_args(p, live, n);
+    PrintArgs a = print_args(p, live, n);
+    a.glare = glare;
     if (ctx.print_mode < 0) {
         dev::print(negative.data(), rgb.data(), a, ctx.stream);
         return;
@@ -816,7 +831,7 @@ constexpr uint32_t kBandRows = 8 * dev::scan_tile_rows();
 // r1 + r2 rows past its last row, so the print runs that far ahead; the print is per pixel and the scanner
 // per tile, so the bands write what the whole-frame launches write.
 void print_scan_banded(RenderCtx& ctx, const Pipeline& p, const LiveParams& live, const Plane& negative,
-                       const Plane& rgb, OutputImage* img, const ScanArgs& sa) {
+                       const Plane& rgb, OutputImage* img, const ScanArgs& sa, const float* glare) {
     const uint32_t w = negative.w, h = negative.h;
     const uint32_t halo = uint32_t(sa.r1 + sa.r2);
     const uint32_t nb = (h + kBandRows - 1) / kBandRows;
@@ -834,6 +849,7 @@ void print_scan_banded(RenderCtx& ctx, const Pipeline& p, const LiveParams& live
         const uint32_t need = std::min(h, r1 + halo);
         if (need > printed) {
             a.n = (need - printed) * w;
+            a.glare = glare ? glare + size_t(printed) * w * 3 : nullptr;
             dev::print(negative.data() + size_t(printed) * w * 3, rgb.data() + size_t(printed) * w * 3, a, ctx.stream);
             printed = need;
         }
@@ -855,16 +871,22 @@ bool print_scan_encode(RenderCtx& ctx, const Pipeline& p, const LiveParams& live
     const PrintSetup& s = *p.print;
     const uint32_t w = negative.w, h = negative.h;
     Plane rgb = make_plane(ctx.pool, w, h);
+    Plane glare;
+    if (!s.scanned && s.glare_draws()) {
+        Stage st(ctx, "glare");
+        glare = glare_plane(ctx, p, w, h);
+    }
+    const float* gl = glare ? glare.data() : nullptr;
     ScanArgs sa;
     const bool tiled = scan_args(p, ctx.rho_tier, w, h, img->stride_px, sa);
     if (to_host && tiled && ctx.print_mode < 0 && ctx.copy_stream && ctx.band_events && h > kBandRows) {
         Stage st(ctx, "print_scanner");
-        print_scan_banded(ctx, p, live, negative, rgb, img, sa);
+        print_scan_banded(ctx, p, live, negative, rgb, img, sa, gl);
         return true;
     }
     {
         Stage st(ctx, "print");
-        print_stage(ctx, p, live, negative, rgb);
+        print_stage(ctx, p, live, negative, rgb, gl);
     }
     if (tiled) {
         // the scanner's blurs on the FIR branch: one tiled pass from the print output to RGBA16
@@ -1030,6 +1052,7 @@ void render_vjp(RenderCtx& ctx, const Pipeline& p, const LiveParams& live, const
         fail_unsupported("the render's adjoint takes sub-layer grain at full strength (or no grain)");
     if (f.couplers) fail_unsupported("the render's adjoint does not take DIR couplers");
     if (f.params.b(P::auto_exposure)) fail_unsupported("the render's adjoint does not take the auto-exposure meter");
+    if (!p.print->scanned && p.print->glare_draws()) fail_unsupported("the render's adjoint does not take print glare");
     if (f.decode || !geometry_identity(f.params))
         fail_unsupported("the render's adjoint does not take the input transfer decode or a geometry");
     Plane G = make_plane(ctx.pool, w, h);

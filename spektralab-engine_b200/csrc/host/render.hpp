@@ -31,6 +31,13 @@ struct Pipeline {
     DeviceTables dev;
 };
 
+struct RenderCtx;
+// The print glare's field for a w x h print (reference src/fx/glare.cpp:27-50): one lognormal value per
+// pixel (mean percent amount, sd roughness percent amount, stream 200, ctx.print_seed) on all channels,
+// blurred by 0.5 px x rho_tier x sqrt(amount); empty when the glare draws nothing or the negative is
+// scanned directly.
+Plane glare_plane(RenderCtx& ctx, const Pipeline& p, uint32_t w, uint32_t h);
+
 // Upload a pipeline's tables (stream-ordered, then synchronised).
 void upload_tables(Pool& pool, cudaStream_t s, Pipeline& p);
 
@@ -39,7 +46,8 @@ struct RenderCtx {
     cudaStream_t stream;
     double pitch_um = 0.0;
     double rho_tier = 1.0;
-    std::optional<double> ae_ev = std::nullopt;  // the auto-exposure meter's EV for the develop (none: no scale)
+    std::optional<double> ae_ev = std::nullopt;
+    uint32_t print_seed = 0;  // the print glare's seed (0 when the glare draws nothing)  // the auto-exposure meter's EV for the develop (none: no scale)
     // optional per-stage timing: events recorded around each stage when set
     struct Timer* timer = nullptr;
     // the print stage: -1 the binary32 print kernel, else a SpectralMode of the spectral-mode kernel at

@@ -901,6 +901,9 @@ std::shared_ptr<PrintSetup> build_print_setup(const ParamSet& p, const FilmSetup
         narrow(s->scan32.wt, s->scan_wt.data(), 243);
     }
     s->scanner_lens_blur_px = p.f(P::scanner_lens_blur);
+    s->glare = p.b(P::glare_active);
+    s->glare_amount = p.f(P::glare_amount);
+    s->glare_tint = s->view_xyz;  // a printed frame's viewing illuminant (the only case that adds glare)
     {
         auto cat02 = cat_matrix(blob, "CAT02");
         if (!cat02) fail_user("the constants blob lacks colour/cat/CAT02");

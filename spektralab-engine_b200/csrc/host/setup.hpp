@@ -173,6 +173,12 @@ struct PrintSetup {
     float m_nid[9] = {};
     uint32_t cctf_mode = 1;
     double scanner_lens_blur_px = 0.0, unsharp_sigma_full = 0.7, unsharp_amount = 0.7;
+    // print glare (reference src/fx/glare.hpp:13-20): percent 0.03, roughness 0.7, blur 0.5 px at the full
+    // tier, tinted by the viewing illuminant's XYZ at Y = 1
+    bool glare = false;
+    double glare_amount = 1.0, glare_percent = 0.03, glare_roughness = 0.7, glare_blur_full = 0.5;
+    Vec3 glare_tint{};
+    bool glare_draws() const { return glare && glare_percent * glare_amount > 0.0; }
 };
 
 class Cam16Cache {

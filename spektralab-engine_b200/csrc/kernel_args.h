@@ -246,6 +246,10 @@ struct alignas(16) PrintArgs {
     Cam16Args cam;
     const float* cmax;
     uint32_t n;
+    // print glare: the blurred lognormal field (interleaved RGB, equal channels), added to the scan's XYZ
+    // as (F / 100) tint before the output matrix; nullptr without glare
+    const float* glare;
+    float glare_tint[3];
 };
 
 // Scanner unsharp + transfer function + 16-bit encode.
