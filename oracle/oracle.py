@@ -312,6 +312,36 @@ def prepare(rgb, delta, cctf_mode):
     return out[: oh.value * ow.value * 3].reshape(oh.value, ow.value, 3)
 
 
+def print_lut(negative, table, size, lo, hi):
+    """The print-preview table render (reference kernels/print.metal:368-407) restated in numpy binary32:
+    densities (h, w, 3) through the trilinear S x S x S x 3 table (along k, then j, then i), each operation
+    rounded on its own, then the 16-bit encode -> (h, w, 4) uint16."""
+    f32 = np.float32
+    d = np.asarray(negative, f32)
+    T = np.asarray(table, f32).reshape(size, size, size, 3)
+    lo = np.asarray(lo, f32)
+    sc = np.array([np.float32(1.0 / (float(h_) - float(l_))) for l_, h_ in zip(lo, hi)], f32)
+    u = np.minimum(np.maximum((d - lo) * sc, f32(0)), f32(1)) * f32(size - 1)
+    fl = np.floor(u)
+    i0 = fl.astype(np.int64)
+    f = (u - fl).astype(f32)
+    i1 = np.minimum(i0 + 1, size - 1)
+    one = f32(1)
+
+    def lerp(a, b, t):
+        return a * (one - t) + b * t
+
+    idx = [i0, i1]
+    c = [[lerp(T[idx[di][..., 0], idx[dj][..., 1], i0[..., 2]], T[idx[di][..., 0], idx[dj][..., 1], i1[..., 2]],
+               f[..., 2:3]) for dj in (0, 1)] for di in (0, 1)]
+    v = lerp(lerp(c[0][0], c[0][1], f[..., 1:2]), lerp(c[1][0], c[1][1], f[..., 1:2]), f[..., 0:1])
+    out = np.zeros(d.shape[:2] + (4,), np.uint16)
+    vc = np.minimum(np.maximum(v, f32(0)), f32(1))
+    out[..., :3] = np.where(np.isnan(v), 0, np.floor(vc * f32(65535) + f32(0.5))).astype(np.uint16)
+    out[..., 3] = 65535
+    return out
+
+
 METER_METHODS = ("center_weighted", "average", "median", "balanced", "center", "protect_highlights",
                  "protect_shadows")
 

@@ -80,6 +80,9 @@ void print_spectral(const PrintArgs& a, const SpectralTablesN& host_tab, const S
                     const float* neg, float* rgb, uint32_t n, float* contraction, uint32_t* err, cudaStream_t s);
 bool print_spectral_supported(uint32_t nl_pad);
 
+// The print-preview table render: negative densities -> trilinear table -> RGBA16 (row pitch a.stride).
+void print_lut(const float* neg, uint16_t* out, const PrintLutArgs& a, cudaStream_t s);
+
 // The print glare's lognormal field: one value per pixel (stream 200, the print seed) on three channels.
 void glare_field(float* out, uint32_t pixels, float mean, float sd, uint32_t seed, cudaStream_t s);
 

@@ -95,6 +95,9 @@ public:
     // parameters and the resources, so a later open or rebuild with the same parameters reuses them.
     std::mutex pipelines_m;
     std::vector<std::pair<std::string, Pipeline>> pipelines;  // most recent last
+    // print-preview tables in device memory, by print stock (uploaded on first use, kept)
+    std::mutex luts_m;
+    std::map<std::string, DevBuffer> luts;
     static constexpr size_t kPipelineCache = 8;
 
     // Batched renders (spkx_render_batch): one at a time per engine, on their own streams. The plan chosen
@@ -474,6 +477,107 @@ void render(Session& s, const char* tier_name, bool reprint, spk_result* out) {
     out->negative_was_cached = reuse ? 1 : 0;
     std::memset(out->progress_id, 0, sizeof out->progress_id);
     std::strncpy(out->progress_id, s.progress_id.c_str(), sizeof out->progress_id - 1);
+}
+
+// The print-preview table render (reference src/session/session.cpp:503-572): the tier's cached
+// negative (developed and cached first when there is none, which draws the film seed but no print seed)
+// through the stock's trilinear table into RGBA16. A missing table is SPK_ERR_USER before anything runs;
+// the result always reads as a reprint of a cached negative.
+void preview_stock_lut(Session& s, const char* print_stock, const char* tier_name, spk_result* out,
+                       char** out_json) {
+    std::lock_guard<std::mutex> lock(s.m);
+    const auto t0 = std::chrono::steady_clock::now();
+    const std::optional<Tier> t = parse_tier(tier_name ? tier_name : "live");
+    if (!t) fail_invalid(std::string("unknown tier '") + tier_name + "'; expected live, preview or full");
+    const std::string stock = print_stock && *print_stock ? std::string(print_stock) : s.params.s(P::print_stock);
+    const std::shared_ptr<const PrintLut> lut = s.engine->res->print_lut(stock);
+    DeviceGuard dg(s.engine->device);
+    TierState& ts = s.tiers[int(*t)];
+    s.progress_id = "p" + std::to_string(g_next_id++);
+    s.cancel.store(false);
+    s.nodes_done.store(0);
+    s.nodes_total = ts.negative ? 1 : 2;
+    s.done = false;
+    bool developed = false;
+    OutputImage* img = nullptr;
+    double apply_ms = 0.0;
+    try {
+        s.tier_source(*t);
+        RenderCtx ctx{s.pool, s.stream};
+        ctx.rho_tier = s.rho(ts);
+        if (!ts.negative) {
+            developed = true;
+            develop_tier(s, *t, ctx);
+        }
+        s.node();
+        DevBuffer table;
+        {
+            std::lock_guard<std::mutex> g(s.engine->luts_m);
+            DevBuffer& d = s.engine->luts[stock];
+            if (!d) {
+                d = s.pool.persistent(lut->table.size() * sizeof(float));
+                cuda_check(cudaMemcpy(d.ptr(), lut->table.data(), lut->table.size() * sizeof(float),
+                                      cudaMemcpyHostToDevice),
+                           "print table upload");
+            }
+            table = d;
+        }
+        img = output_acquire(s.engine->device, ts.negative.w, ts.negative.h);
+        PrintLutArgs a{};
+        a.lut = table.as<float>();
+        a.size = lut->size;
+        a.w = ts.negative.w;
+        a.h = ts.negative.h;
+        a.stride = img->stride_px;
+        for (int c = 0; c < 3; ++c) {
+            a.lo[c] = lut->lo[c];
+            a.s[c] = f32(1.0 / (double(lut->hi[c]) - double(lut->lo[c])));
+        }
+        const auto ta = std::chrono::steady_clock::now();
+        dev::print_lut(ts.negative.data(), img->dev, a, s.stream);
+        cuda_check(cudaMemcpyAsync(img->host, img->dev, img->bytes, cudaMemcpyDeviceToHost, s.stream), "result copy");
+        cuda_check(cudaStreamSynchronize(s.stream), "print table");
+        cuda_check(cudaGetLastError(), "print table");
+        apply_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - ta).count();
+    } catch (...) {
+        (void)cudaStreamSynchronize(s.stream);
+        if (img) output_release(img);
+        if (developed) ts.negative = Plane{};
+        try {
+            throw;
+        } catch (const Error& e) {
+            if (e.status() == SPK_ERR_CANCELLED || e.status() == SPK_ERR_INVALID_ARG) throw;
+            fail_gpu(e.what());
+        } catch (const std::bad_alloc&) {
+            fail_gpu("out of memory");
+        }
+    }
+    s.done = true;
+    out->rgba16 = img->host;
+    out->texture = img;
+    out->width = img->width;
+    out->height = img->height;
+    out->row_stride_px = img->stride_px;
+    out->elapsed_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    out->reprint = 1;
+    out->negative_was_cached = 1;
+    std::memset(out->progress_id, 0, sizeof out->progress_id);
+    std::strncpy(out->progress_id, s.progress_id.c_str(), sizeof out->progress_id - 1);
+    if (out_json) {
+        json::Value r;
+        r["apply_backend"] = "native-cuda";
+        r["apply_ms"] = apply_ms;
+        r["declared_pairing"] = lut->declared_pairing;
+        r["lut_source"] = "shipped";
+        r["paired_film"] = lut->paired_film;
+        r["print_stock"] = stock;
+        r["tier"] = *t == Tier::Live ? "live" : (*t == Tier::Preview ? "preview" : "full");
+        const std::string& film = s.params.s(P::film_stock);
+        if (film != lut->paired_film)
+            r["warning"] = "the print table for '" + stock + "' was made for '" + lut->paired_film + "', not for '" +
+                           film + "'";
+        put_json(out_json, json::write(r));
+    }
 }
 
 spk_status render_common(spk_session* session, const char* tier, spk_result* out, bool reprint) {
@@ -1213,22 +1317,32 @@ SPK_API spk_status spk_solve(spk_session* session, const char*, char**) {
     return SPK_ERR_UNSUPPORTED;
 }
 
-SPK_API const char* spk_print_lut_catalog(spk_engine*) { return "{}"; }
+SPK_API const char* spk_print_lut_catalog(spk_engine* engine) {
+    return engine ? E(engine)->res->print_lut_catalog().c_str() : "{}";
+}
 
 SPK_API spk_status spk_print_lut_table(spk_engine* engine, const char* print_stock, const float** out_table,
                                        uint32_t* out_size) {
     last_error::clear();
     if (!engine || !print_stock || !out_table || !out_size) return invalid("a required pointer is NULL");
-    last_error::set("print-preview tables are outside this B200 build's render path");
-    return SPK_ERR_UNSUPPORTED;
+    return guarded([&] {
+        // the table lives in the engine's resources for the engine's life
+        const std::shared_ptr<const PrintLut> t = E(engine)->res->print_lut(print_stock);
+        *out_table = t->table.data();
+        *out_size = t->size;
+        return SPK_OK;
+    });
 }
 
-SPK_API spk_status spk_preview_stock_lut(spk_session* session, const char*, const char*, spk_result* out, char**) {
+SPK_API spk_status spk_preview_stock_lut(spk_session* session, const char* print_stock, const char* tier,
+                                         spk_result* out, char** out_json) {
     last_error::clear();
     if (!session || !out) return invalid("a required pointer is NULL");
     std::memset(out, 0, sizeof *out);
-    last_error::set("spk_preview_stock_lut is outside this B200 build's render path");
-    return SPK_ERR_UNSUPPORTED;
+    return guarded([&] {
+        preview_stock_lut(*S(session), print_stock, tier, out, out_json);
+        return SPK_OK;
+    });
 }
 
 SPK_API spk_status spk_output_transform(spk_engine* engine, const char* src, const char* dst, const char*,

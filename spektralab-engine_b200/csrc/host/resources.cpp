@@ -571,7 +571,74 @@ std::shared_ptr<Resources> Resources::load(const std::filesystem::path& dir) {
         }
         if (!r->filters_.is_object()) fail_io("neutral_print_filters.json must be a JSON object");
     }
+    // the print-preview table index (reference src/res/tables.cpp:80-115): optional; a malformed one fails
+    const std::filesystem::path lp = dir / "print_luts.json";
+    if (std::filesystem::exists(lp, ec)) {
+        std::ifstream f(lp, std::ios::binary);
+        std::ostringstream ss;
+        ss << f.rdbuf();
+        try {
+            r->luts_ = json::parse(ss.str());
+        } catch (const json::ParseError& e) {
+            fail_io(std::string("print_luts.json: ") + e.what());
+        }
+        if (!r->luts_.is_object()) fail_io("print_luts.json: not an object");
+        for (const auto& [stock, v] : r->luts_.as_object()) {
+            auto bad = [&](const std::string& m) { fail_io("print_luts.json: '" + stock + "': " + m); };
+            if (!v.is_object()) bad("not an object");
+            const json::Value* pf = v.find("paired_film");
+            if (!pf || !pf->is_string()) bad("missing paired_film");
+            const json::Value* ls = v.find("lut_size");
+            if (!ls || !ls->is_number()) bad("missing lut_size");
+            const double sz = ls->as_number();
+            if (!(sz > 1.0) || sz != std::floor(sz) || sz > 4096.0) bad("lut_size must be an integer > 1");
+        }
+        r->luts_present_ = true;
+        r->lut_text_ = ss.str();
+    }
     return r;
+}
+
+std::shared_ptr<const PrintLut> Resources::print_lut(std::string_view stock) const {
+    {
+        std::lock_guard<std::mutex> g(m_);
+        auto it = lut_cache_.find(stock);
+        if (it != lut_cache_.end()) return it->second;
+    }
+    if (!luts_present_) fail_user("no print-preview table index (print_luts.json) in the resources");
+    const json::Value* v = luts_.find(std::string(stock));
+    if (!v) {
+        std::string list;
+        for (const auto& [k, _] : luts_.as_object()) list += (list.empty() ? "" : ", ") + k;
+        fail_user("no print-preview table for '" + std::string(stock) + "'; available: " + list);
+    }
+    auto t = std::make_shared<PrintLut>();
+    t->stock = std::string(stock);
+    t->paired_film = v->find("paired_film")->as_string();
+    t->size = uint32_t(v->find("lut_size")->as_number());
+    if (const json::Value* d = v->find("declared_pairing"); d && d->is_bool()) t->declared_pairing = d->as_bool();
+    if (const json::Value* d = v->find("output_color_space"); d && d->is_string()) t->output_color_space = d->as_string();
+    if (const json::Value* d = v->find("output_cctf_encoding"); d && d->is_bool()) t->output_cctf_encoding = d->as_bool();
+    const uint32_t S = t->size;
+    const std::string tname = "print_lut/" + std::string(stock), aname = "print_lut_axes/" + std::string(stock);
+    const BlobEntry* te = blob_->find(tname);
+    const BlobEntry* ae = blob_->find(aname);
+    if (!te || te->dtype != 1 || te->ndim != 4 || te->dims[0] != S || te->dims[1] != S || te->dims[2] != S ||
+        te->dims[3] != 3)
+        fail_user("print-preview table '" + tname + "' is missing or has the wrong shape");
+    if (!ae || ae->dtype != 1 || ae->ndim != 2 || ae->dims[0] != 3 || ae->dims[1] != S)
+        fail_user("print-preview axes '" + aname + "' are missing or have the wrong shape");
+    const std::vector<double> tv = blob_->f64(tname), av = blob_->f64(aname);  // binary32 widened exactly
+    t->table.assign(tv.size(), 0.0f);
+    for (size_t i = 0; i < tv.size(); ++i) t->table[i] = float(tv[i]);
+    for (size_t c = 0; c < 3; ++c) {
+        t->lo[c] = float(av[c * S]);
+        t->hi[c] = float(av[c * S + S - 1]);
+        if (!(t->hi[c] > t->lo[c])) fail_user("print-preview axes of '" + std::string(stock) + "' are not increasing");
+    }
+    std::lock_guard<std::mutex> g(m_);
+    lut_cache_[std::string(stock)] = t;
+    return t;
 }
 
 std::shared_ptr<const Profile> Resources::profile(std::string_view id) const {

@@ -111,6 +111,16 @@ bool valid_stock_id(std::string_view id);
 std::shared_ptr<const Profile> load_profile(const std::filesystem::path& dir, std::string_view id);
 
 // ---- the resources folder ----
+// A print-preview table (reference src/res/tables.hpp:48-62): S x S x S x 3 binary32, row-major
+// [i][j][k][ch], over per-channel density axes lo..hi, with its print_luts.json entry.
+struct PrintLut {
+    std::string stock, paired_film, output_color_space;
+    bool declared_pairing = false, output_cctf_encoding = true;
+    uint32_t size = 0;
+    std::vector<float> table;
+    float lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+};
+
 class Resources {
 public:
     static std::shared_ptr<Resources> load(const std::filesystem::path& dir);
@@ -120,11 +130,19 @@ public:
     std::shared_ptr<const Profile> profile(std::string_view id) const;
     // The neutral filter pack for (print, illuminant, film), then the film's base id.
     std::optional<Vec3> neutral_filters(std::string_view print, std::string_view illum, const Profile& film) const;
+    // print_luts.json as read ("{}" when absent), and one stock's table (cached; SPK_ERR_USER when the index,
+    // the entry or its blob tables are missing or malformed).
+    const std::string& print_lut_catalog() const { return lut_text_; }
+    std::shared_ptr<const PrintLut> print_lut(std::string_view stock) const;
 
 private:
     std::filesystem::path dir_;
     std::shared_ptr<const Blob> blob_;
     json::Value filters_;
+    json::Value luts_;
+    bool luts_present_ = false;
+    std::string lut_text_ = "{}";
+    mutable std::map<std::string, std::shared_ptr<const PrintLut>, std::less<>> lut_cache_;
     mutable std::mutex m_;
     mutable std::map<std::string, std::shared_ptr<const Profile>, std::less<>> profiles_;
 };

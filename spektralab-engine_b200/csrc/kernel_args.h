@@ -162,6 +162,15 @@ struct MeterArgs {
     MeterOut* out;
 };
 
+// The print-preview table render (reference kernels/print.metal:368-407): per pixel the negative's
+// densities through a trilinear S x S x S x 3 table, then the 16-bit encode.
+struct PrintLutArgs {
+    const float* lut;   // [i][j][k][ch], row-major
+    uint32_t size;      // S
+    uint32_t w, h, stride;  // output row pitch in pixels
+    float lo[3], s[3];  // axis start and f32(1 / (hi - lo)) per channel
+};
+
 // Per-wavelength tables of one spectral integral (already neutralised).
 struct SpectralTables {
     float eps[SPKB_NL * 3];  // [l][c]

@@ -305,6 +305,20 @@ class Session:
     def render(self, tier="full"):
         return self._render(self.L.lib.spk_render, tier)
 
+    def preview_lut(self, print_stock=None, tier="live"):
+        """spk_preview_stock_lut: (RGBA16 (h, w, 4), meta, reply)."""
+        r = SpkResult()
+        out = ctypes.c_char_p()
+        self.L.check(self.L.lib.spk_preview_stock_lut(self.h, print_stock.encode() if print_stock else None,
+                                                      tier.encode() if tier else None, ctypes.byref(r),
+                                                      ctypes.byref(out)))
+        try:
+            a = np.ctypeslib.as_array(r.rgba16, shape=(r.height, r.row_stride_px, 4))[:, : r.width].copy()
+            meta = {"reprint": r.reprint, "negative_was_cached": r.negative_was_cached}
+        finally:
+            self.L.lib.spk_result_free(ctypes.byref(r))
+        return a, meta, self.L.take_json(out)
+
     def reprint(self, tier="full"):
         return self._render(self.L.lib.spk_reprint, tier)
 

@@ -37,7 +37,8 @@ import sys
 
 import numpy as np
 
-FORMAT_VERSION = "synthetic-resources-v2"
+FORMAT_VERSION = "synthetic-resources-v3"
+LUT_SIZE = 17
 FILM_STOCK = "synthetic_negative_400"
 PAPER_STOCK = "synthetic_paper"
 L_TABLE = 192  # the engine's spectral-upsampling table size (src/film/film_internal.hpp:19)
@@ -293,6 +294,16 @@ def generate(out_dir, seed=0):
             (f"colour/cs/{name}/matrix_RGB_to_XYZ", M),
             (f"colour/cs/{name}/matrix_XYZ_to_RGB", np.linalg.inv(M)),
         ]
+    # a print-preview table for the synthetic paper: densities (three axes 0..3.2) -> a smooth display RGB
+    S = LUT_SIZE
+    ax = np.linspace(0.0, 3.2, S)
+    di, dj, dk = np.meshgrid(ax, ax, ax, indexing="ij")
+    T = np.stack([10.0 ** -(0.9 * di + 0.1 * dj), 10.0 ** -(0.1 * di + 0.8 * dj + 0.1 * dk),
+                  10.0 ** -(0.15 * dj + 0.85 * dk)], axis=-1) ** (1 / 2.2)
+    entries += [
+        (f"print_lut/{PAPER_STOCK}", T.astype(np.float32)),
+        (f"print_lut_axes/{PAPER_STOCK}", np.stack([ax, ax * 1.05, ax * 0.95]).astype(np.float32)),
+    ]
     write_blob(os.path.join(out_dir, "spektralab_constants.bin"), entries)
 
     d55 = daylight_like(5503.0)
@@ -304,6 +315,9 @@ def generate(out_dir, seed=0):
         json.dump(profile_paper(), f)
     with open(os.path.join(out_dir, "neutral_print_filters.json"), "w") as f:
         json.dump({PAPER_STOCK: {"TH-KG3": {FILM_STOCK: [0.0, 10.0, 10.0]}}}, f)
+    with open(os.path.join(out_dir, "print_luts.json"), "w") as f:
+        json.dump({PAPER_STOCK: {"paired_film": FILM_STOCK, "lut_size": LUT_SIZE, "declared_pairing": True,
+                                 "output_color_space": "sRGB", "output_cctf_encoding": True}}, f)
     with open(os.path.join(out_dir, "VERSION"), "w") as f:
         f.write(FORMAT_VERSION + "\n")
     return out_dir
