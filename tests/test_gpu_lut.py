@@ -37,8 +37,8 @@ def test_preview_within_one_lsb_of_reference(lib, engine, ref, ref_engine, tier,
     with ref_engine.open(img, delta) as r:
         want, _, reply2 = r.preview_lut(None, tier)
     assert lsb_stats(got, want)["max"] <= 1
-    assert {k: v for k, v in reply.items() if k not in ("apply_ms", "apply_backend")} == \\
-        {k: v for k, v in reply2.items() if k not in ("apply_ms", "apply_backend")}
+    skip = ("apply_ms", "apply_backend")
+    assert {k: v for k, v in reply.items() if k not in skip} == {k: v for k, v in reply2.items() if k not in skip}
     _, table = table_of(lib, engine, PAPER)
     lut = oracle.print_lut(neg, table, 17, np.float32([0, 0, 0]), np.float32([3.2, 3.2 * 1.05, 3.2 * 0.95]))
     assert lsb_stats(got, lut)["max"] <= 1
