@@ -226,6 +226,9 @@ public:
     // 1600 px downscale already, else on its own downscale, and is kept until a meter-key field changes.
     std::optional<double> session_ev() {
         if (!params.b(P::auto_exposure)) return std::nullopt;
+        return ensure_meter().ev(params.s(P::auto_exposure_method));
+    }
+    const MeterValues& ensure_meter() {
         if (!meter) {
             if (!meter_image) {
                 const TierState& live = tiers[int(Tier::Live)];
@@ -236,7 +239,7 @@ public:
             }
             meter = spkb::meter(pool, stream, meter_image, params, pipe.film->input_space);
         }
-        return meter->ev(params.s(P::auto_exposure_method));
+        return *meter;
     }
     // The print seed of a render or reprint: the next draw of the seed sequence when the glare can draw,
     // even where its stage is skipped (scan_film), else 0 (reference src/session/session.cpp:339-344)
@@ -1168,11 +1171,106 @@ SPK_API const char* spk_memory_report(spk_engine* engine) {
     return e->memory_report.c_str();
 }
 
-SPK_API spk_status spk_warm_up(spk_engine* engine, const char*, const char*, char**) {
+// Warm-up (reference src/session/engine.cpp:331-412): load two profiles, build a private set-up, develop
+// and print a 64 x 64 frame of 0.18 told it is a 1600 px frame, on a private stream and seed sequence.
+// A failing step is reported in the reply and ends the sequence.
+SPK_API spk_status spk_warm_up(spk_engine* engine, const char* film_stock, const char* print_stock, char** out_json) {
     last_error::clear();
     if (!engine) return invalid("engine is NULL");
-    last_error::set("spk_warm_up is outside this B200 build's render path");
-    return SPK_ERR_UNSUPPORTED;
+    return guarded([&] {
+        Engine& e = *E(engine);
+        using clock = std::chrono::steady_clock;
+        auto ms_since = [](clock::time_point t0) {
+            return std::chrono::duration<double, std::milli>(clock::now() - t0).count();
+        };
+        auto r2 = [](double ms) { return std::round(ms * 100.0) / 100.0; };
+        const std::string film_id = film_stock && *film_stock ? film_stock : "kodak_portra_400";
+        const std::string print_id = print_stock && *print_stock ? print_stock : "kodak_portra_endura";
+        const clock::time_point t_all = clock::now();
+        json::Array steps;
+        auto run_step = [&](const char* name, auto&& fn) -> bool {
+            const clock::time_point t0 = clock::now();
+            json::Value st;
+            st["name"] = name;
+            bool ok = true;
+            try {
+                fn();
+            } catch (const std::exception& ex) {
+                ok = false;
+                st["error"] = std::string(ex.what());
+            }
+            st["ok"] = ok;
+            st["ms"] = r2(ms_since(t0));
+            steps.push_back(std::move(st));
+            return ok;
+        };
+        DeviceGuard dg(e.device);
+        ParamSet p;
+        p.set(P::film_stock, film_id);
+        p.set(P::print_stock, print_id);
+        std::shared_ptr<const Profile> fp, pp;
+        Pipeline pl;
+        cudaStream_t stream = nullptr;
+        cuda_check(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "warm-up stream");
+        struct StreamGuard {
+            cudaStream_t s;
+            ~StreamGuard() {
+                cudaStreamSynchronize(s);
+                cudaStreamDestroy(s);
+            }
+        } sg{stream};
+        Pool pool(stream);
+        bool ok = run_step("profiles", [&] {
+            fp = e.res->profile(film_id);
+            pp = e.res->profile(print_id);
+            if (auto pack = e.res->neutral_filters(print_id, p.s(P::enlarger_illuminant), *fp)) {
+                p.set(P::c_filter_neutral, (*pack)[0]);
+                p.set(P::m_filter_neutral, (*pack)[1]);
+                p.set(P::y_filter_neutral, (*pack)[2]);
+            }
+        });
+        if (ok)
+            ok = run_step("pipeline", [&] {
+                check_supported(p);
+                auto fs = build_film_setup(p, fp, *e.res);
+                pl.print = build_print_setup(p, *fs, pp, *e.res, e.cam16, true);
+                pl.film = fs;
+                upload_tables(pool, stream, pl);
+            });
+        if (ok)
+            run_step("kernels", [&] {
+                constexpr uint32_t kSide = 64;
+                Plane src = make_plane(pool, kSide, kSide);
+                const std::vector<float> grey(size_t(kSide) * kSide * 3, 0.18f);
+                cuda_check(cudaMemcpyAsync(src.data(), grey.data(), src.bytes(), cudaMemcpyHostToDevice, stream),
+                           "warm-up frame");
+                RenderCtx ctx{pool, stream};
+                ctx.rho_tier = 1.0;
+                ctx.pitch_um = 1000.0 * p.f(P::film_format_mm) / double(kMeterLongEdge);
+                SeedSequence seeds;  // private: never a session's
+                const uint32_t film_seed = p.b(P::grain_active) ? seeds.next() : kNoGrainFilmSeed;
+                Plane neg = develop(ctx, pl, src, film_seed, std::nullopt);
+                ctx.print_seed = pl.print->glare_draws() ? seeds.next() : 0u;
+                OutputImage* img = output_acquire(e.device, kSide, kSide);
+                try {
+                    print_scan_encode(ctx, pl, LiveParams::from(p), neg, img);
+                    cuda_check(cudaStreamSynchronize(stream), "warm-up");
+                } catch (...) {
+                    output_release(img);
+                    throw;
+                }
+                output_release(img);
+            });
+        json::Value r;
+        r["already_warm"] = false;
+        r["film_stock"] = film_id;
+        r["print_stock"] = print_id;
+        r["render_core"] = "native-cuda";
+        r["steps"] = std::move(steps);
+        r["total_ms"] = r2(ms_since(t_all));
+        put_json(out_json, json::write(r));
+        return SPK_OK;
+    });
 }
 
 SPK_API spk_session* spk_open(spk_engine* engine, const spk_image* input, const char* delta, char** out_json) {
@@ -1310,11 +1408,54 @@ SPK_API void spk_result_free(spk_result* result) {
     result->rgba16 = nullptr;
 }
 
-SPK_API spk_status spk_solve(spk_session* session, const char*, char**) {
+// The solver (reference src/session/session.cpp:450-499): never changes parameters. exposure: the meter
+// (metered now, or the kept one) gives the session method's EV and the four intent EVs; filter_pack: the
+// neutral filter database's row for (paper, enlarger illuminant, film), else the current values.
+SPK_API spk_status spk_solve(spk_session* session, const char* target_in, char** out_json) {
     last_error::clear();
     if (!session) return invalid("session is NULL");
-    last_error::set("spk_solve is outside this B200 build's render path");
-    return SPK_ERR_UNSUPPORTED;
+    return guarded([&] {
+        Session& s = *S(session);
+        const std::string target = target_in && *target_in ? target_in : "both";
+        std::lock_guard<std::mutex> lock(s.m);
+        const bool exposure = target == "exposure" || target == "both";
+        const bool pack = target == "filter_pack" || target == "both";
+        if (!exposure && !pack) fail_user("unknown solve target '" + target + "'; expected exposure, filter_pack or both");
+        json::Value solved = json::Object{};
+        json::Value r;
+        if (exposure) {
+            DeviceGuard dg(s.engine->device);
+            const MeterValues* m = nullptr;
+            try {
+                m = &s.ensure_meter();
+            } catch (const Error& e) {
+                fail_gpu(e.what());  // the meter failed: a render failure
+            }
+            solved["exposure_compensation_ev"] = m->ev(s.params.s(P::auto_exposure_method));
+            json::Value by;
+            by["balanced"] = m->balanced;
+            by["center"] = m->center;
+            by["protect_highlights"] = m->protect_highlights;
+            by["protect_shadows"] = m->protect_shadows;
+            r["exposure_ev_by_method"] = std::move(by);
+        }
+        if (pack) {
+            Vec3 v{s.params.f(P::c_filter_neutral), s.params.f(P::m_filter_neutral), s.params.f(P::y_filter_neutral)};
+            try {
+                if (auto hit = s.engine->res->neutral_filters(s.params.s(P::print_stock),
+                                                              s.params.s(P::enlarger_illuminant), *s.film))
+                    v = *hit;
+            } catch (const std::exception& e) {
+                fail_internal(std::string("filter resolution failed: ") + e.what());
+            }
+            solved["c_filter_neutral"] = v[0];
+            solved["m_filter_neutral"] = v[1];
+            solved["y_filter_neutral"] = v[2];
+        }
+        r["solved_params"] = std::move(solved);
+        put_json(out_json, json::write(r));
+        return SPK_OK;
+    });
 }
 
 SPK_API const char* spk_print_lut_catalog(spk_engine* engine) {
@@ -1345,12 +1486,106 @@ SPK_API spk_status spk_preview_stock_lut(spk_session* session, const char* print
     });
 }
 
-SPK_API spk_status spk_output_transform(spk_engine* engine, const char* src, const char* dst, const char*,
-                                        char**, const float**, uint32_t*) {
+namespace {
+// gamut_compress_json (reference src/print/cam16.cpp:246-277): keys optional; not an object is
+// SPK_ERR_INVALID_ARG, an unknown algorithm SPK_ERR_USER; an array that is not three numbers is ignored
+struct GamutOptions {
+    std::string algorithm = "cam16ucs";
+    std::array<double, 3> knee{0.0, 1.0, 6.0}, lc{0.7, 1.0, 2.2};
+    bool lc_active = true;
+};
+GamutOptions parse_gamut(const char* text) {
+    GamutOptions g;
+    if (!text || !*text) return g;
+    json::Value v;
+    try {
+        v = json::parse(text);
+    } catch (const json::ParseError& e) {
+        fail_invalid(std::string("gamut_compress_json: ") + e.what());
+    }
+    if (!v.is_object()) fail_invalid("gamut_compress_json must be a JSON object");
+    if (const json::Value* a = v.find("algorithm")) {
+        if (!a->is_string() || (a->as_string() != "cam16ucs" && a->as_string() != "off"))
+            fail_user("unknown gamut compression algorithm" + (a->is_string() ? " '" + a->as_string() + "'" : std::string()) +
+                      " (expected cam16ucs or off)");
+        g.algorithm = a->as_string();
+    }
+    auto triple = [&](const char* key, std::array<double, 3>& out) {
+        const json::Value* a = v.find(key);
+        if (!a || !a->is_array() || a->as_array().size() != 3) return;
+        std::array<double, 3> t{};
+        for (size_t i = 0; i < 3; ++i) {
+            if (!a->as_array()[i].is_number()) return;
+            t[i] = a->as_array()[i].as_number();
+        }
+        out = t;
+    };
+    triple("knee", g.knee);
+    triple("lightness_compression", g.lc);
+    if (const json::Value* b = v.find("lightness_compression_active"); b && b->is_bool()) g.lc_active = b->as_bool();
+    return g;
+}
+}  // namespace
+
+// The output transform (reference src/print/cam16.cpp:306-347): a fetch, never a render. The matrix is
+// XYZ -> RGB(dst) . CAT02(white src -> white dst, when the whites differ) . RGB -> XYZ(src); the gamut
+// constants and the C_max table are those of dst, the table engine-owned for the engine's life.
+SPK_API spk_status spk_output_transform(spk_engine* engine, const char* src, const char* dst, const char* gamut_json,
+                                        char** out_json, const float** out_cmax, uint32_t* out_cmax_count) {
     last_error::clear();
-    if (!engine || !src || !dst) return invalid("a required pointer is NULL");
-    last_error::set("spk_output_transform is outside this B200 build's render path");
-    return SPK_ERR_UNSUPPORTED;
+    if (!engine) return invalid("engine is NULL");
+    if (!src) return invalid("src_cs is NULL");
+    if (!dst) return invalid("dst_cs is NULL");
+    if (!out_json || !out_cmax || !out_cmax_count) return invalid("a required output pointer is NULL");
+    return guarded([&] {
+        Engine& e = *E(engine);
+        const GamutOptions g = parse_gamut(gamut_json);
+        auto space = [&](const char* name) {
+            if (!cctf_of(name)) fail_user("unknown colour space '" + std::string(name) + "'");
+            auto cs = colour_space(e.res->blob(), name);
+            if (!cs) fail_user("colour space '" + std::string(name) + "' has no baked matrices or whitepoint");
+            if (cs->whitepoint[1] == 0.0) fail_user("colour space '" + std::string(name) + "' has a whitepoint with y = 0");
+            return *cs;
+        };
+        const ColourSpace sc = space(src), dc = space(dst);
+        auto cat02 = cat_matrix(e.res->blob(), "CAT02");
+        if (!cat02) fail_user("the constants blob has no colour/cat/CAT02");
+        Mat3 m = dc.xyz_to_rgb;
+        if (auto a = von_kries(sc.whitepoint, dc.whitepoint, *cat02, Guard::Target)) m = mat3_mul(m, *a);
+        m = mat3_mul(m, sc.rgb_to_xyz);
+        const std::shared_ptr<const Cam16Tables> t = e.cam16.get(*e.res, dst);
+        const Cam16Constants& c = t->k;
+        auto mat = [](const Mat3& v) {
+            json::Array a;
+            for (double x : v) a.emplace_back(x);
+            return json::Value(std::move(a));
+        };
+        json::Value gc;
+        gc["algorithm"] = g.algorithm;
+        gc["m_to_xyz"] = mat(t->m_to_xyz);
+        gc["m_to_rgb"] = mat(t->m_to_rgb);
+        const double k[22] = {c.F_L, c.N_bb, c.N_cb, c.n, c.z, c.A_w, c.c, c.N_c, 1.0, 110.0, -M_PI,
+                              2.0 * M_PI / 720.0, g.knee[0], g.knee[1], g.knee[2], g.lc_active ? g.lc[0] : 0.0,
+                              g.lc_active ? g.lc[1] : 1.0, g.lc_active ? g.lc[2] : 1.0, c.J_white, c.D_rgb[0],
+                              c.D_rgb[1], c.D_rgb[2]};
+        json::Array ka;
+        for (double v : k) ka.emplace_back(v);
+        gc["k"] = json::Value(std::move(ka));
+        gc["cmax_rows"] = 64;
+        gc["cmax_cols"] = 720;
+        gc["lightness_compression_active"] = g.lc_active;
+        json::Value r;
+        r["source_color_space"] = sc.name;
+        r["target_color_space"] = dc.name;
+        r["source_cctf_mode"] = int(sc.cctf);
+        r["target_cctf_mode"] = int(dc.cctf);
+        r["matrix"] = mat(m);
+        r["gamut_compress"] = std::move(gc);
+        put_json(out_json, json::write(r));
+        *out_cmax = t->cmax32.data();
+        *out_cmax_count = uint32_t(t->cmax32.size());
+        return SPK_OK;
+    });
 }
 
 SPK_API void spk_cancel(spk_session* session, const char* progress_id) {
@@ -1428,8 +1663,7 @@ SPK_API spk_status spkx_session_meter(spk_session* session, char** out_json) {
         std::lock_guard<std::mutex> lock(s.m);
         DeviceGuard dg(s.engine->device);
         if (!s.params.b(P::auto_exposure)) fail_user("auto_exposure is off in this session");
-        s.session_ev();
-        const MeterValues& m = *s.meter;
+        const MeterValues& m = s.ensure_meter();
         json::Value r;
         r["center_weighted"] = m.center_weighted;
         r["average"] = m.average;
