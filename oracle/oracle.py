@@ -45,6 +45,7 @@ class OracleSetup(ctypes.Structure):
         ("dir_w", (D * 3) * MAXC), ("dir_s", (D * 3) * MAXC),
         ("glare", I32), ("glare_mean", ctypes.c_float), ("glare_sd", ctypes.c_float), ("glare_sigma", D),
         ("glare_tint", D * 3), ("print_seed", ctypes.c_uint32),
+        ("boost_ev", D), ("headroom_ev", D),
     ]
 
 
@@ -187,6 +188,8 @@ class Oracle:
         s.cctf_active = 1 if f64["cctf_active"] else 0
         s.cctf_mode = int(f64["cctf_mode"])
         put("m_nid", f64["m_nid"])
+        s.boost_ev = f64.get("boost_ev", 0.0)
+        s.headroom_ev = f64.get("headroom_ev", 0.0)
         gl = f64.get("glare")
         if gl and gl["draws"]:
             s.glare = 1

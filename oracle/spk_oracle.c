@@ -246,11 +246,64 @@ static double grain_value(const OracleSetup* s, double D, int c, uint32_t pixel,
     return G - s->dmin_c[c];
 }
 
+static double smooth01d(double t) {
+    const double u = t < 0.0 ? 0.0 : (t > 1.0 ? 1.0 : t);
+    return u * u * (3.0 - 2.0 * u);
+}
+
+/* the frame maximum of the exposure's values, NaN skipped (reference src/film/geometry.cpp:210-217) */
+static double frame_max(const double* H, size_t N) {
+    double m = -INFINITY;
+    for (size_t i = 0; i < N; ++i)
+        if (H[i] > m) m = H[i];
+    return m;
+}
+
+/* the highlight boost (reference src/film/develop.cpp:32-62) and the back-reflection headroom
+ * (src/fx/halation.cpp:68-86, kernels/fx_halation.metal:18-39), in binary64 */
+static void highlights(const OracleSetup* s, double* H, size_t n) {
+    const size_t N = 3 * n;
+    if (s->boost_ev != 0.0) {
+        const double M = frame_max(H, N);
+        if (M == 0.0) {
+            for (size_t i = 0; i < N; ++i) H[i] *= 0.0;
+        } else {
+            double x0 = 0.184 * pow(2.0, 4.0);
+            x0 = x0 < M ? x0 : M;
+            if (x0 != M) {
+                const double a = pow(28.0, 1.0 - 0.3), q = a * (1.0 - x0 / M);
+                const double k = (pow(2.0, s->boost_ev) - 1.0) / (exp(q) - q - 1.0);
+                for (size_t i = 0; i < N; ++i)
+                    if (H[i] > x0) {
+                        const double z = a * (H[i] - x0) / M;
+                        H[i] += k * M * (exp(z) - z - 1.0);
+                    }
+            }
+        }
+    }
+    if (s->headroom_ev > 0.0) {
+        const double clip = frame_max(H, N);
+        if (clip > 0.0 && isfinite(clip)) {
+            for (size_t p = 0; p < n; ++p) {
+                double* v = H + 3 * p;
+                const double m = fmax(fmax(v[0], v[1]), v[2]);
+                if (!(m > 0.0)) continue;
+                const double lm = log2(m);
+                const double s1 = smooth01d((lm - log2(clip) + 1.0) / 0.75);
+                const double s2 = smooth01d(lm - log2(0.184) - 1.5);
+                const double g = exp2(s->headroom_ev * s1 * s2);
+                for (int c = 0; c < 3; ++c) v[c] *= g;
+            }
+        }
+    }
+}
+
 static int develop_impl(const OracleSetup* s, const float* rgb, const double* rgb64, int32_t w, int32_t h,
                         const float* counts, double* neg) {
     const size_t n = (size_t)w * h, N = 3 * n;
     double* H = (double*)malloc(N * sizeof(double));
     expose(s, rgb, rgb64, H, n);
+    if (s->boost_ev != 0.0 || s->headroom_ev > 0.0) highlights(s, H, n);
     if (s->lens_blur_px > 0.0) {
         double* t = (double*)malloc(N * sizeof(double));
         const double sg[3] = {s->lens_blur_px, s->lens_blur_px, s->lens_blur_px};

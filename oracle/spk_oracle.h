@@ -73,6 +73,9 @@ typedef struct {
     float glare_mean, glare_sd;
     double glare_sigma, glare_tint[3];
     uint32_t print_seed;
+    /* the highlight boost (boost_ev != 0) and the back-reflection headroom (headroom_ev > 0 when it applies),
+     * both on the exposure after the compensation, against the frame maximum */
+    double boost_ev, headroom_ev;
 } OracleSetup;
 
 /* The whole render of a w x h frame; rgb is 3 floats per pixel (already non-finite-cleaned),

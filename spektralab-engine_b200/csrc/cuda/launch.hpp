@@ -43,6 +43,14 @@ void prepare(const float* src, float* dst, const PrepareArgs& a, cudaStream_t s)
 size_t meter_partial_doubles();
 void meter_stats(const MeterArgs& a, cudaStream_t s);
 
+// The frame maximum of n floats (NaN skipped) as an order-preserving integer in *out_ordered, and as a
+// float (plane_max_value); the back-reflection headroom (reading the clip from device memory) and the
+// highlight boost.
+void plane_max(const float* p, size_t n, uint32_t* out_ordered, cudaStream_t s);
+void plane_max_value(const uint32_t* ordered_max, float* out, cudaStream_t s);
+void headroom(float* p, uint32_t pixels, const uint32_t* clip_ordered, float headroom_ev, cudaStream_t s);
+void boost(float* p, size_t n, float x0, float r, float a, float k, cudaStream_t s);
+
 // RGB -> film exposure H (Mitchell bicubic of the spectral table, L x L float4 texels), times the
 // compensation gain.
 void expose(const float* rgb, float* h, const float* table4, const ExposeArgs& a, cudaStream_t s);

@@ -1856,6 +1856,8 @@ json::Value setup_f64(const FilmSetup& f, const PrintSetup& p, const PrintRun& r
     r["input_matrix"] = arr(f.input_matrix.data(), 9);
     r["input_cctf_mode"] = int(f.input_space.cctf);
     r["input_rgb_to_xyz"] = arr(f.input_space.rgb_to_xyz.data(), 9);
+    r["boost_ev"] = f.params.f(P::halation_boost_ev);
+    r["headroom_ev"] = headroom_applies(f.halation) ? f.halation.headroom_ev : 0.0;
     {
         // the print glare: its binary32 lognormal parameters, the blur at the full tier, the tint
         const PrintSetup& ps = p;

@@ -388,7 +388,6 @@ void check_supported(const ParamSet& p) {
     auto refuse = [](const std::string& what) {
         fail_user(what + " is outside this B200 build's render path");
     };
-    if (p.f(P::halation_boost_ev) != 0.0) refuse("halation_boost_ev != 0 (highlight boost)");
     if (p.b(P::scanner_white_correction) || p.b(P::scanner_black_correction))
         refuse("scanner white/black correction (levels)");
     if (p.b(P::extended_dynamic_range)) refuse("extended_dynamic_range=true (EDR tone map)");
@@ -425,8 +424,6 @@ HalationPlan film_halation(const RenderCtx& ctx, const FilmSetup& f, const std::
         }
         return pl;
     }
-    if (f.halation.back_reflection && f.halation.active && f.halation.headroom_ev > 0.0 && f.halation.amount > 0.0)
-        fail_user("the back-reflection halation preset (highlight headroom) is outside this B200 build's render path");
     return halation_plan(f.halation, ctx.pitch_um);
 }
 
@@ -569,6 +566,40 @@ Plane dir_couplers(RenderCtx& ctx, const Pipeline& p, const Plane& H, DevelopArg
 }
 }  // namespace
 
+bool headroom_applies(const HalationParams& h) {
+    return h.active && h.back_reflection && h.headroom_ev > 0.0 && h.amount > 0.0;
+}
+
+namespace {
+// The highlight boost (reference src/film/develop.cpp:32-62): values above x0 = min(0.184 2^4, M) lifted
+// by k M (exp(z) - z - 1), z = a (v - x0) / M, with M the frame maximum (read back: the constants are
+// binary64 functions of it) and k from boost_ev; M = 0 scales the frame by 0.
+void run_boost(RenderCtx& ctx, const Plane& H, double beta_ev) {
+    DevBuffer mx = ctx.pool.acquire(16);
+    uint32_t* ord = mx.as<uint32_t>();
+    float* val = reinterpret_cast<float*>(ord + 1);
+    dev::plane_max(H.data(), 3 * H.pixels(), ord, ctx.stream);
+    dev::plane_max_value(ord, val, ctx.stream);
+    float M = 0.0f;
+    cuda_check(cudaMemcpyAsync(&M, val, sizeof M, cudaMemcpyDeviceToHost, ctx.stream), "frame maximum");
+    cuda_check(cudaStreamSynchronize(ctx.stream), "frame maximum");
+    if (M == 0.0f) {
+        const float zero[3] = {0.0f, 0.0f, 0.0f};
+        dev::lincomb(H.data(), nullptr, H.data(), H.pixels(), zero, zero, ctx.stream);
+        return;
+    }
+    const double Md = double(M);
+    const double x0 = std::min(std::max(0.184 * std::pow(2.0, 4.0), 0.0), Md);
+    if (x0 == Md) return;
+    const double a = std::pow(28.0, 1.0 - 0.3);
+    const double q = a * (1.0 - x0 / Md);
+    const double den = std::exp(q) - q - 1.0;
+    if (!(den > 0.0)) fail_gpu("highlight boost: the frame maximum leaves no range to lift (den <= 0)");
+    const double k = (std::pow(2.0, beta_ev) - 1.0) / den;
+    dev::boost(H.data(), 3 * H.pixels(), f32(x0), f32(1.0 / Md), f32(a), f32(k * Md), ctx.stream);
+}
+}  // namespace
+
 Plane develop(RenderCtx& ctx, const Pipeline& p, const Plane& tier_source, uint32_t film_seed,
               const std::optional<HalationOverride>& hov, float* counts_out, float* lam_out) {
     const FilmSetup& f = *p.film;
@@ -587,6 +618,17 @@ Plane develop(RenderCtx& ctx, const Pipeline& p, const Plane& tier_source, uint3
             ea.apply_ae = 1;
         }
         dev::expose(source.data(), H.data(), p.dev.table.as<float>(), ea, ctx.stream);
+    }
+    if (const double bev = f.params.f(P::halation_boost_ev); bev != 0.0) {
+        Stage st(ctx, "boost");
+        run_boost(ctx, H, bev);
+    }
+    if (headroom_applies(f.halation)) {
+        // the back-reflection halation's highlight headroom, its clip the frame maximum kept on the device
+        Stage st(ctx, "headroom");
+        DevBuffer mx = ctx.pool.acquire(16);
+        dev::plane_max(H.data(), 3 * H.pixels(), mx.as<uint32_t>(), ctx.stream);
+        dev::headroom(H.data(), uint32_t(H.pixels()), mx.as<uint32_t>(), f32(f.halation.headroom_ev), ctx.stream);
     }
     if (const double s = film_lens_blur_px(ctx, f); s > 0.0) {
         Stage st(ctx, "lens_blur");
@@ -1052,6 +1094,8 @@ void render_vjp(RenderCtx& ctx, const Pipeline& p, const LiveParams& live, const
         fail_unsupported("the render's adjoint takes sub-layer grain at full strength (or no grain)");
     if (f.couplers) fail_unsupported("the render's adjoint does not take DIR couplers");
     if (f.params.b(P::auto_exposure)) fail_unsupported("the render's adjoint does not take the auto-exposure meter");
+    if (f.params.f(P::halation_boost_ev) != 0.0 || headroom_applies(f.halation))
+        fail_unsupported("the render's adjoint does not take the highlight boost or headroom");
     if (!p.print->scanned && p.print->glare_draws()) fail_unsupported("the render's adjoint does not take print glare");
     if (f.decode || !geometry_identity(f.params))
         fail_unsupported("the render's adjoint does not take the input transfer decode or a geometry");

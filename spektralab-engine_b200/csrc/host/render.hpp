@@ -32,6 +32,8 @@ struct Pipeline {
 };
 
 struct RenderCtx;
+// Whether the back-reflection halation's highlight headroom runs (reference src/fx/halation.cpp:64-66).
+bool headroom_applies(const HalationParams& h);
 // The print glare's field for a w x h print (reference src/fx/glare.cpp:27-50): one lognormal value per
 // pixel (mean percent amount, sd roughness percent amount, stream 200, ctx.print_seed) on all channels,
 // blurred by 0.5 px x rho_tier x sqrt(amount); empty when the glare draws nothing or the negative is
