@@ -46,6 +46,7 @@ class OracleSetup(ctypes.Structure):
         ("glare", I32), ("glare_mean", ctypes.c_float), ("glare_sd", ctypes.c_float), ("glare_sigma", D),
         ("glare_tint", D * 3), ("print_seed", ctypes.c_uint32),
         ("boost_ev", D), ("headroom_ev", D),
+        ("levels", I32), ("levels_m", D), ("levels_q", D),
     ]
 
 
@@ -190,6 +191,9 @@ class Oracle:
         put("m_nid", f64["m_nid"])
         s.boost_ev = f64.get("boost_ev", 0.0)
         s.headroom_ev = f64.get("headroom_ev", 0.0)
+        lv = f64.get("levels")
+        if lv and lv["active"]:
+            s.levels, s.levels_m, s.levels_q = 1, lv["m"], lv["q"]
         gl = f64.get("glare")
         if gl and gl["draws"]:
             s.glare = 1

@@ -545,6 +545,12 @@ int orc_print(const OracleSetup* s, const double* neg, int32_t w, int32_t h, uin
         }
         spectral(s->scan_eps, s->scan_beta, s->scan_wt, d, r);
         for (int c = 0; c < 3; ++c) r[c] = fmax(r[c], 0.0) + kTiny;
+        if (s->levels) {
+            double Yp = s->levels_m * r[1] + s->levels_q;
+            Yp = Yp < 0.0 ? 0.0 : (Yp > 1.0 ? 1.0 : Yp);
+            const double sc = Yp / (r[1] + kTiny);
+            for (int c = 0; c < 3; ++c) r[c] *= sc;
+        }
         if (field)
             for (int c = 0; c < 3; ++c) r[c] += (field[3 * p + c] / 100.0) * s->glare_tint[c];
         double o[3];

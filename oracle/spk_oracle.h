@@ -76,6 +76,9 @@ typedef struct {
     /* the highlight boost (boost_ev != 0) and the back-reflection headroom (headroom_ev > 0 when it applies),
      * both on the exposure after the compensation, against the frame maximum */
     double boost_ev, headroom_ev;
+    /* scanner levels on the scan's XYZ before the glare: Y' = clamp(m Y + q, 0, 1), XYZ times Y' / (Y + 1e-10) */
+    int32_t levels;
+    double levels_m, levels_q;
 } OracleSetup;
 
 /* The whole render of a w x h frame; rgb is 3 floats per pixel (already non-finite-cleaned),

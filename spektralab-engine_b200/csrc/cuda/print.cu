@@ -66,6 +66,7 @@ __device__ __forceinline__ void print_pair(const PrintArgs& a, const float* __re
         float x = fmaxf(k ? X.y : X.x, 0.0f) + kTiny;
         float y = fmaxf(k ? Y.y : Y.x, 0.0f) + kTiny;
         float z = fmaxf(k ? Z.y : Z.x, 0.0f) + kTiny;
+        apply_levels(a, x, y, z);
         add_glare(a, size_t(p0 + k), x, y, z);
         float r, g, b;
         mat_apply(a.to_rgb, x, y, z, r, g, b);

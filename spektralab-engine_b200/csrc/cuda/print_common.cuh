@@ -39,6 +39,16 @@ __device__ __forceinline__ float fsqrt(float x) {
 
 // log10(max(x, 0) + 1e-10) as log2 on the special-function unit times log10 2 (absolute error about
 // 2^-22 on the log-exposure axis)
+// Scanner levels (reference kernels/print.metal:234-246), each operation rounded on its own.
+__device__ __forceinline__ void apply_levels(const PrintArgs& a, float& x, float& y, float& z) {
+    if (!a.levels) return;
+    const float Yp = fminf(fmaxf(__fadd_rn(__fmul_rn(a.levels_m, y), a.levels_q), 0.0f), 1.0f);
+    const float s = __fdiv_rn(Yp, __fadd_rn(y, kTiny));
+    x = __fmul_rn(s, x);
+    y = __fmul_rn(s, y);
+    z = __fmul_rn(s, z);
+}
+
 // Print glare (reference kernels/fx_glare.metal:12-22): xyz_c + (F / 100) tint_c for the field value F of
 // pixel p, each operation rounded on its own.
 __device__ __forceinline__ void add_glare(const PrintArgs& a, size_t p, float& x, float& y, float& z) {

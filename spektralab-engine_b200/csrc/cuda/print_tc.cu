@@ -484,6 +484,7 @@ __global__ void __launch_bounds__(kTcThreads) k_print_spectral(const __grid_cons
             float x = fmaxf(R[0], 0.0f) + kTiny;
             float y = fmaxf(R[1], 0.0f) + kTiny;
             float z = fmaxf(R[2], 0.0f) + kTiny;
+            apply_levels(a, x, y, z);
             add_glare(a, size_t(px), x, y, z);
             float r, gg, b;
             mat_apply(a.to_rgb, x, y, z, r, gg, b);

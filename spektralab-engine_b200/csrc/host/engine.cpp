@@ -1857,6 +1857,13 @@ json::Value setup_f64(const FilmSetup& f, const PrintSetup& p, const PrintRun& r
     r["input_cctf_mode"] = int(f.input_space.cctf);
     r["input_rgb_to_xyz"] = arr(f.input_space.rgb_to_xyz.data(), 9);
     r["boost_ev"] = f.params.f(P::halation_boost_ev);
+    {
+        json::Value lv;
+        lv["active"] = run.levels;
+        lv["m"] = run.m;
+        lv["q"] = run.q;
+        r["levels"] = std::move(lv);
+    }
     r["headroom_ev"] = headroom_applies(f.halation) ? f.halation.headroom_ev : 0.0;
     {
         // the print glare: its binary32 lognormal parameters, the blur at the full tier, the tint
@@ -1944,7 +1951,7 @@ json::Value setup_f64(const FilmSetup& f, const PrintSetup& p, const PrintRun& r
     r["enl_wt"] = arr(run.w_n.data(), 243);
     r["enl_g"] = arr(run.g.data(), 3);
     r["enl_o"] = arr(run.o.data(), 3);
-    r["k_gain"] = live.print_exposure;
+    r["k_gain"] = live.print_exposure * run.kappa_bw;  // the levels' exposure correction included
     r["scan_eps"] = arr(p.scan_eps.data(), 243);
     r["scan_beta"] = arr(p.scan_beta.data(), 81);
     r["scan_wt"] = arr(p.scan_wt.data(), 243);

@@ -388,8 +388,6 @@ void check_supported(const ParamSet& p) {
     auto refuse = [](const std::string& what) {
         fail_user(what + " is outside this B200 build's render path");
     };
-    if (p.b(P::scanner_white_correction) || p.b(P::scanner_black_correction))
-        refuse("scanner white/black correction (levels)");
     if (p.b(P::extended_dynamic_range)) refuse("extended_dynamic_range=true (EDR tone map)");
 }
 
@@ -781,6 +779,9 @@ PrintArgs print_args(const Pipeline& p, const LiveParams& live, uint32_t pixels)
     a.cmax = p.dev.cmax.as<float>();
     a.n = pixels;
     for (int c = 0; c < 3; ++c) a.glare_tint[c] = f32(p.print->glare_tint[size_t(c)]);
+    a.levels = r.levels ? 1 : 0;
+    a.levels_m = f32(r.m);
+    a.levels_q = f32(r.q);
     return a;
 }
 

@@ -901,6 +901,35 @@ std::shared_ptr<PrintSetup> build_print_setup(const ParamSet& p, const FilmSetup
         narrow(s->scan32.wt, s->scan_wt.data(), 243);
     }
     s->scanner_lens_blur_px = p.f(P::scanner_lens_blur);
+    s->levels_black = p.b(P::scanner_black_correction);
+    s->levels_white = p.b(P::scanner_white_correction);
+    s->levels_B = 0.01 / 12.92;
+    s->levels_W = std::pow((0.98 + 0.055) / 1.055, 2.4);
+    s->film_positive = film.positive();
+    s->paper_positive = paper.positive();
+    for (size_t c = 0; c < 3; ++c) {  // the film's white density: the density curve's largest value (NaN skipped)
+        double m = std::numeric_limits<double>::quiet_NaN();
+        for (size_t k = 0; k < film.density_curves.rows; ++k) {
+            const double v = film.density_curves(k, c);
+            if (!std::isnan(v) && (std::isnan(m) || v > m)) m = v;
+        }
+        s->film_white_density[c] = m;
+    }
+    if (!s->scanned) {  // the paper's mean curve and mean base (NaN skipped)
+        auto nanmean = [](const double* v, size_t n, size_t stride) {
+            double sum = 0.0;
+            size_t k = 0;
+            for (size_t i = 0; i < n; ++i)
+                if (!std::isnan(v[i * stride])) {
+                    sum += v[i * stride];
+                    ++k;
+                }
+            return k ? sum / double(k) : std::numeric_limits<double>::quiet_NaN();
+        };
+        s->paper_mean_curve.resize(paper.K());
+        for (size_t i = 0; i < paper.K(); ++i) s->paper_mean_curve[i] = nanmean(&paper.density_curves.v[3 * i], 3, 1);
+        s->paper_mean_base = nanmean(paper.base_density.data(), paper.base_density.size(), 1);
+    }
     s->glare = p.b(P::glare_active);
     s->glare_amount = p.f(P::glare_amount);
     s->glare_tint = s->view_xyz;  // a printed frame's viewing illuminant (the only case that adds glare)
@@ -974,6 +1003,40 @@ std::shared_ptr<PrintSetup> build_print_setup(const ParamSet& p, const FilmSetup
     return s;
 }
 
+namespace {
+// The Y that a film density triple d prints to (reference src/print/setup.cpp:281-314): the enlarger
+// integral, the paper's log exposure, its density curves, then the scan integral's Y with the narrowed
+// scan tables; max(y, 0) + 1e-10.
+double reference_y(const PrintSetup& s, const PrintRun& r, const Vec3& d) {
+    constexpr double kLog2Of10 = 3.32192809488736234787;
+    const Profile& paper = *s.paper;
+    Vec3 ell{};
+    {
+        Vec3 R{};
+        for (size_t l = 0; l < 81; ++l) {
+            const double D = r.beta_n[l] + ((d[0] * r.eps_n[3 * l] + d[1] * r.eps_n[3 * l + 1]) + d[2] * r.eps_n[3 * l + 2]);
+            const double T = std::exp2(-D * kLog2Of10);
+            for (size_t c = 0; c < 3; ++c) R[c] += T * r.w_n[3 * l + c];
+        }
+        for (size_t c = 0; c < 3; ++c) ell[c] = std::log10(std::max(R[c] * r.g[c] + r.o[c], 0.0) + 1e-10);
+    }
+    Vec3 Dp{};
+    for (size_t c = 0; c < 3; ++c) {
+        std::vector<double> curve(paper.density_curves.rows);
+        for (size_t i = 0; i < curve.size(); ++i) curve[i] = paper.density_curves(i, c);
+        Dp[c] = interp(ell[c], paper.log_exposure, curve);
+    }
+    const SpectralTables& a = s.scan32;
+    double y = 0.0;
+    for (size_t l = 0; l < 81; ++l) {
+        const double D = ((Dp[0] * double(a.eps[3 * l]) + Dp[1] * double(a.eps[3 * l + 1])) + Dp[2] * double(a.eps[3 * l + 2])) +
+                         double(a.beta[l]);
+        y += std::exp2(-D * kLog2Of10) * double(a.wt[3 * l + 1]);
+    }
+    return std::max(y, 0.0) + 1e-10;
+}
+}  // namespace
+
 PrintRun compute_run(const PrintSetup& s, const LiveParams& live) {
     PrintRun r;
     if (!s.scanned) {
@@ -999,7 +1062,29 @@ PrintRun compute_run(const PrintSetup& s, const LiveParams& live) {
             for (size_t c = 0; c < 3; ++c) r.o[c] = live.preflash_exposure * sum[c];
         }
     }
-    r.k_gain = f32(live.print_exposure * 1.0);
+    // scanner levels (reference src/print/setup.cpp:371-390): the print's Y of the film's black and
+    // white densities, the line through the targets, and the exposure correction that keeps mid grey
+    r.levels = s.levels_active();
+    if (r.levels) {
+        if (!s.scanned && !s.paper_positive) {
+            r.y_k = reference_y(s, r, {-0.03, -0.03, -0.03});
+            r.y_w = reference_y(s, r, s.film_white_density);
+        }
+        double B = s.levels_B, W = s.levels_W;
+        if (s.levels_black && !s.levels_white) W = r.y_w;
+        if (s.levels_white && !s.levels_black) B = r.y_k;
+        r.m = (W - B) / (r.y_w - r.y_k + 1e-10);
+        r.q = B - r.m * r.y_k;
+        if (!s.scanned && !s.paper_positive) {
+            const Profile& paper = *s.paper;
+            const double mid = 0.184;
+            const double g_star = (mid - r.q) / r.m;
+            const double e_star = interp(-std::log10(g_star) - s.paper_mean_base, s.paper_mean_curve, paper.log_exposure);
+            const double e_0 = interp(-std::log10(mid) - s.paper_mean_base, s.paper_mean_curve, paper.log_exposure);
+            r.kappa_bw = std::pow(10.0, e_star - e_0);
+        }
+    }
+    r.k_gain = f32(live.print_exposure * r.kappa_bw);
     narrow(r.enl32.eps, r.eps_n.data(), 243);
     narrow(r.enl32.beta, r.beta_n.data(), 81);
     narrow(r.enl32.wt, r.w_n.data(), 243);

@@ -179,6 +179,17 @@ struct PrintSetup {
     double glare_amount = 1.0, glare_percent = 0.03, glare_roughness = 0.7, glare_blur_full = 0.5;
     Vec3 glare_tint{};
     bool glare_draws() const { return glare && glare_percent * glare_amount > 0.0; }
+    // scanner levels (reference src/print/build.cpp:152-155, src/print/setup.cpp:262-270): black and
+    // white targets B and W, the film's white density, the paper's mean curve and base for the exposure
+    // correction; a directly scanned negative passes through
+    bool levels_black = false, levels_white = false, film_positive = false, paper_positive = false;
+    double levels_B = 0.0, levels_W = 0.0, paper_mean_base = 0.0;
+    Vec3 film_white_density{};
+    std::vector<double> paper_mean_curve;
+    bool levels_active() const {
+        if (!levels_black && !levels_white) return false;
+        return scanned ? film_positive : true;
+    }
 };
 
 class Cam16Cache {
@@ -202,6 +213,8 @@ struct PrintRun {
     Vec3 g{}, o{};
     float k_gain = 1.0f;
     SpectralTables enl32{};
+    bool levels = false;
+    double m = 1.0, q = 0.0, y_k = 0.0, y_w = 1.0, kappa_bw = 1.0;
 };
 PrintRun compute_run(const PrintSetup& s, const LiveParams& live);
 

@@ -259,6 +259,10 @@ struct alignas(16) PrintArgs {
     // as (F / 100) tint before the output matrix; nullptr without glare
     const float* glare;
     float glare_tint[3];
+    // scanner levels (reference kernels/print.metal:234-246): Y' = clamp(m Y + q, 0, 1), XYZ times
+    // Y' / (Y + 1e-10), before the glare; levels = 0: none
+    int32_t levels;
+    float levels_m, levels_q;
 };
 
 // Scanner unsharp + transfer function + 16-bit encode.

@@ -68,7 +68,7 @@ def test_unknown_tier_and_result_zeroed(engine, lib):
 
 def test_outside_render_path_is_refused(engine):
     img = sc.synthetic_image(8, 8, 0)
-    for extra in ({"extended_dynamic_range": True}, {"scanner_white_correction": True}):
+    for extra in ({"extended_dynamic_range": True},):
         with pytest.raises(sc.SpkError) as e:
             engine.open(img, dict(BASE, **extra))
         assert e.value.status == sc.SPK_ERR_USER and "outside this B200 build" in str(e.value)
