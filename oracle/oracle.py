@@ -47,6 +47,8 @@ class OracleSetup(ctypes.Structure):
         ("glare_tint", D * 3), ("print_seed", ctypes.c_uint32),
         ("boost_ev", D), ("headroom_ev", D),
         ("levels", I32), ("levels_m", D), ("levels_q", D),
+        ("edr", I32), ("edr_n", I32), ("edr_r_y", D * 3), ("edr_lo", D), ("edr_hi", D), ("edr_toe", D),
+        ("edr_shoulder", D), ("edr_tab", PD),
     ]
 
 
@@ -191,6 +193,12 @@ class Oracle:
         put("m_nid", f64["m_nid"])
         s.boost_ev = f64.get("boost_ev", 0.0)
         s.headroom_ev = f64.get("headroom_ev", 0.0)
+        ed = f64.get("edr")
+        if ed and ed["active"]:
+            s.edr, s.edr_n = 1, len(ed["table"])
+            put("edr_r_y", ed["r_y"])
+            s.edr_lo, s.edr_hi, s.edr_toe, s.edr_shoulder = ed["lo"], ed["hi"], ed["toe"], ed["shoulder"]
+            s.edr_tab = buf(ed["table"])
         lv = f64.get("levels")
         if lv and lv["active"]:
             s.levels, s.levels_m, s.levels_q = 1, lv["m"], lv["q"]

@@ -574,6 +574,25 @@ int orc_print(const OracleSetup* s, const double* neg, int32_t w, int32_t h, uin
         free(g);
     }
     free(field);
+    if (s->edr && s->printed) {
+#pragma omp parallel for
+        for (size_t p = 0; p < n; ++p) {
+            double* v = rgb + 3 * p;
+            double y = (s->edr_r_y[0] * v[0] + s->edr_r_y[1] * v[1]) + s->edr_r_y[2] * v[2];
+            y = y > 0.0 ? y : 0.0;
+            double yp = y;
+            if (y > 0.0 && (y < s->edr_toe || y > s->edr_shoulder)) {
+                const int N = s->edr_n > 2 ? s->edr_n : 2;
+                double u = (log2(y) - s->edr_lo) / (s->edr_hi - s->edr_lo);
+                u = (u < 0.0 ? 0.0 : (u > 1.0 ? 1.0 : u)) * (N - 1);
+                int i0 = (int)floor(u);
+                i0 = i0 < N - 2 ? i0 : N - 2;
+                const double t = u - i0;
+                yp = exp2((1.0 - t) * s->edr_tab[i0] + t * s->edr_tab[i0 + 1]);
+            }
+            for (int c = 0; c < 3; ++c) v[c] = v[c] * yp / (y + kTiny);
+        }
+    }
     if (lin) memcpy(lin, rgb, N * sizeof(double));
 #pragma omp parallel for
     for (size_t p = 0; p < n; ++p) {

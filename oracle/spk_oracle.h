@@ -79,6 +79,11 @@ typedef struct {
     /* scanner levels on the scan's XYZ before the glare: Y' = clamp(m Y + q, 0, 1), XYZ times Y' / (Y + 1e-10) */
     int32_t levels;
     double levels_m, levels_q;
+    /* the EDR tone map after the scanner: y = max(r_y . rgb, 0); outside [toe, shoulder] y' = 2^(the target
+     * curve at the clamped (log2 y - lo) / (hi - lo)); rgb times y' / (y + 1e-10) */
+    int32_t edr, edr_n;
+    double edr_r_y[3], edr_lo, edr_hi, edr_toe, edr_shoulder;
+    const double* edr_tab;
 } OracleSetup;
 
 /* The whole render of a w x h frame; rgb is 3 floats per pixel (already non-finite-cleaned),

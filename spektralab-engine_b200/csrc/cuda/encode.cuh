@@ -43,6 +43,29 @@ __device__ __forceinline__ float cctf_encode(float v, uint32_t mode) {
 }
 
 // floor(clamp(v, 0, 1) 65535 + 0.5); NaN -> 0
+// The EDR tone map (reference kernels/print.metal:319-347): y = max(r_y . rgb, 0); outside [toe, shoulder]
+// y' is 2 to the power of the target curve interpolated at the clamped log2 y; rgb times y' / (y + 1e-10).
+// Each operation rounded on its own.
+__device__ __forceinline__ void edr_tone(const EncodeArgs& e, float& r, float& g, float& b) {
+    if (!e.edr) return;
+    const float y = fmaxf(__fadd_rn(__fadd_rn(__fmul_rn(e.edr_r_y[0], r), __fmul_rn(e.edr_r_y[1], g)),
+                                    __fmul_rn(e.edr_r_y[2], b)),
+                          0.0f);
+    float yp = y;
+    if (y > 0.0f && (y < e.edr_toe || y > e.edr_shoulder)) {
+        const uint32_t N = e.edr_n > 2u ? e.edr_n : 2u;
+        const float u = __fmul_rn(fminf(fmaxf(__fdiv_rn(__fsub_rn(log2f(y), e.edr_lo), e.edr_span), 0.0f), 1.0f),
+                                  float(N - 1));
+        const uint32_t i0 = min(uint32_t(floorf(u)), N - 2);
+        const float t = __fsub_rn(u, float(i0));
+        yp = exp2f(__fadd_rn(__fmul_rn(__fsub_rn(1.0f, t), e.edr_tab[i0]), __fmul_rn(t, e.edr_tab[i0 + 1])));
+    }
+    const float den = __fadd_rn(y, 1e-10f);
+    r = __fdiv_rn(__fmul_rn(r, yp), den);
+    g = __fdiv_rn(__fmul_rn(g, yp), den);
+    b = __fdiv_rn(__fmul_rn(b, yp), den);
+}
+
 __device__ __forceinline__ uint16_t encode16(float v) {
     if (isnan(v)) return 0;
     const float c = fminf(fmaxf(v, 0.0f), 1.0f);

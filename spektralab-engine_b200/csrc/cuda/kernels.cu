@@ -552,6 +552,7 @@ __global__ void k_encode(const float* __restrict__ rgb, const float* __restrict_
         v1 = e.lincomb_a * v1 + e.lincomb_b * gpl[i + 1];
         v2 = e.lincomb_a * v2 + e.lincomb_b * gpl[i + 2];
     }
+    edr_tone(e, v0, v1, v2);
     if (e.cctf_active) {
         float m0, m1, m2;
         mat_apply(e.m_nid, v0, v1, v2, m0, m1, m2);

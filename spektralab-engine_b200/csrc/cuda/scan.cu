@@ -140,6 +140,7 @@ __device__ __forceinline__ void scan_tile(const ScanArgs& a, const float* __rest
             v1 = e.lincomb_a * v1 + e.lincomb_b * g1;
             v2 = e.lincomb_a * v2 + e.lincomb_b * g2;
         }
+        edr_tone(e, v0, v1, v2);
         if (e.cctf_active) {
             float m0, m1, m2;
             mat_apply(e.m_nid, v0, v1, v2, m0, m1, m2);

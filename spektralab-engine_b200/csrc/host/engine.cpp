@@ -1858,6 +1858,19 @@ json::Value setup_f64(const FilmSetup& f, const PrintSetup& p, const PrintRun& r
     r["input_rgb_to_xyz"] = arr(f.input_space.rgb_to_xyz.data(), 9);
     r["boost_ev"] = f.params.f(P::halation_boost_ev);
     {
+        json::Value ed;
+        ed["active"] = p.edr && !p.scanned;
+        ed["r_y"] = arr(p.out_cs.rgb_to_xyz.data() + 3, 3);
+        ed["lo"] = p.edr_lo;
+        ed["hi"] = p.edr_hi;
+        ed["toe"] = p.edr_toe;
+        ed["shoulder"] = p.edr_shoulder;
+        std::vector<double> t;
+        if (p.edr) t = p.paper->edr->target;
+        ed["table"] = arr(t.data(), t.size());
+        r["edr"] = std::move(ed);
+    }
+    {
         json::Value lv;
         lv["active"] = run.levels;
         lv["m"] = run.m;

@@ -47,6 +47,7 @@ void upload_tables(Pool& pool, cudaStream_t s, Pipeline& p) {
     const PrintSetup& pr = *p.print;
     if (!pr.paper_tab.empty()) upload(pool, s, p.dev.paper, pr.paper_tab.data(), pr.paper_tab.size() * sizeof(float));
     upload(pool, s, p.dev.cmax, pr.cam->cmax32.data(), pr.cam->cmax32.size() * sizeof(float));
+    if (pr.edr) upload(pool, s, p.dev.edr, pr.edr_tab.data(), pr.edr_tab.size() * sizeof(float));
     cuda_check(cudaStreamSynchronize(s), "table upload");
 }
 
@@ -384,11 +385,8 @@ bool iir_mixture_mix(RenderCtx& ctx, const Plane& raw, const std::vector<Mixture
 
 }  // namespace
 
-void check_supported(const ParamSet& p) {
-    auto refuse = [](const std::string& what) {
-        fail_user(what + " is outside this B200 build's render path");
-    };
-    if (p.b(P::extended_dynamic_range)) refuse("extended_dynamic_range=true (EDR tone map)");
+void check_supported(const ParamSet&) {
+    // every field of the reference's parameter schema has its stage in this build: nothing is refused
 }
 
 namespace {
@@ -786,12 +784,23 @@ PrintArgs print_args(const Pipeline& p, const LiveParams& live, uint32_t pixels)
 }
 
 namespace {
-EncodeArgs encode_args(const PrintSetup& s, uint32_t stride_px) {
+EncodeArgs encode_args(const Pipeline& p, uint32_t stride_px) {
+    const PrintSetup& s = *p.print;
     EncodeArgs e{};
     std::memcpy(e.m_nid, s.m_nid, sizeof e.m_nid);
     e.cctf_active = s.cctf ? 1 : 0;
     e.cctf_mode = s.cctf_mode;
     e.stride = stride_px;
+    if (s.edr && !s.scanned) {  // the EDR tone map of a printed frame (reference src/print/run.cpp:177-180)
+        e.edr = 1;
+        e.edr_n = uint32_t(s.edr_tab.size());
+        for (int c = 0; c < 3; ++c) e.edr_r_y[c] = f32(s.out_cs.rgb_to_xyz[size_t(3 + c)]);
+        e.edr_lo = f32(s.edr_lo);
+        e.edr_span = f32(s.edr_hi - s.edr_lo);
+        e.edr_toe = f32(s.edr_toe);
+        e.edr_shoulder = f32(s.edr_shoulder);
+        e.edr_tab = p.dev.edr.as<float>();
+    }
     return e;
 }
 }  // namespace
@@ -815,7 +824,7 @@ bool scan_args(const Pipeline& p, double rho_tier, uint32_t w, uint32_t h, uint3
     if (sa.r1 == 0) sa.t1[0] = 1.0f;
     if (sa.r2 == 0) sa.t2[0] = 1.0f;
     if (!dev::scan_encode_fits(w, h, sa.r1, sa.r2)) return false;
-    sa.e = encode_args(s, stride_px);
+    sa.e = encode_args(p, stride_px);
     sa.e.unsharp = unsharp ? 1 : 0;
     sa.e.lincomb_a = f32(1.0 + am);
     sa.e.lincomb_b = f32(-am);
@@ -937,7 +946,7 @@ bool print_scan_encode(RenderCtx& ctx, const Pipeline& p, const LiveParams& live
         dev::scan_encode(rgb.data(), img->dev, w, h, sa, ctx.stream);
         return false;
     }
-    EncodeArgs e = encode_args(s, img->stride_px);
+    EncodeArgs e = encode_args(p, img->stride_px);
     Plane gpl;
     {
         Stage st(ctx, "scanner");
@@ -1095,6 +1104,7 @@ void render_vjp(RenderCtx& ctx, const Pipeline& p, const LiveParams& live, const
         fail_unsupported("the render's adjoint takes sub-layer grain at full strength (or no grain)");
     if (f.couplers) fail_unsupported("the render's adjoint does not take DIR couplers");
     if (f.params.b(P::auto_exposure)) fail_unsupported("the render's adjoint does not take the auto-exposure meter");
+    if (p.print->edr && !p.print->scanned) fail_unsupported("the render's adjoint does not take the EDR tone map");
     if (f.params.f(P::halation_boost_ev) != 0.0 || headroom_applies(f.halation))
         fail_unsupported("the render's adjoint does not take the highlight boost or headroom");
     if (!p.print->scanned && p.print->glare_draws()) fail_unsupported("the render's adjoint does not take print glare");

@@ -23,6 +23,7 @@ struct DeviceTables {
     DevBuffer gaxis, ginv, glayers;
     DevBuffer paper;              // x[K] | r[K] | y[K][3]
     DevBuffer cmax;               // 64 x 720
+    DevBuffer edr;                // the EDR tone map's target_log2_y (binary32), when EDR is on
 };
 
 struct Pipeline {

@@ -463,6 +463,32 @@ void read_data(const json::Value& data, Profile& p, const Ctx& c) {
             p.layers.insert(p.layers.end(), m.v.begin(), m.v.end());
         }
     }
+    if (const json::Value* v = data.find("edr_tone_map")) {
+        // validated as the reference does (src/res/profile.cpp:113-141)
+        if (!v->is_object()) c.bad("'edr_tone_map' must be an object");
+        const json::Value* ver = v->find("version");
+        if (!ver || !ver->is_number() || ver->as_number() != 1.0) c.bad("edr_tone_map.version must be 1");
+        const json::Value* dom = v->find("domain_log2_y");
+        if (!dom) c.bad("edr_tone_map.domain_log2_y is missing");
+        const std::vector<double> d = vec(*dom, 2, c, "edr_tone_map.domain_log2_y");
+        Profile::Edr e;
+        e.lo = d[0];
+        e.hi = d[1];
+        if (!(e.hi > e.lo)) c.bad("edr_tone_map.domain_log2_y needs hi > lo");
+        const json::Value* toe = v->find("toe_y");
+        const json::Value* sh = v->find("shoulder_y");
+        if (!toe || !toe->is_number() || !(toe->as_number() > 0)) c.bad("edr_tone_map.toe_y must be > 0");
+        if (!sh || !sh->is_number() || !(sh->as_number() > toe->as_number())) c.bad("edr_tone_map.shoulder_y must be > toe_y");
+        e.toe = toe->as_number();
+        e.shoulder = sh->as_number();
+        const json::Value* t = v->find("target_log2_y");
+        if (!t) c.bad("edr_tone_map.target_log2_y is missing");
+        e.target = vec(*t, 0, c, "edr_tone_map.target_log2_y");
+        if (e.target.size() < 2) c.bad("edr_tone_map.target_log2_y needs at least 2 values");
+        for (double x : e.target)
+            if (!std::isfinite(x)) c.bad("edr_tone_map.target_log2_y must be finite");
+        p.edr = std::move(e);
+    }
     if (const json::Value* v = data.find("density_curves_model")) {
         if (!v->is_object()) c.bad("density_curves_model must be an object");
         if (const json::Value* t = v->find("model_type"); t && t->is_string()) p.model_type = t->as_string();

@@ -101,6 +101,13 @@ struct Profile {
     std::string model_type = "cdfs";
     Mat centers, amplitudes, sigmas;       // channels x layers
     std::vector<double> window;            // 0, 4 or 8 values
+    // the EDR tone map of a paper (reference src/res/profile.hpp:69-76): log2 Y domain, toe and shoulder
+    // luminances, the target curve in log2 Y
+    struct Edr {
+        double lo = 0.0, hi = 0.0, toe = 0.0, shoulder = 0.0;
+        std::vector<double> target;
+    };
+    std::optional<Edr> edr;
     // derived at load
     std::array<double, 3> dmin{}, dmax{};
     Mat normalized;                        // K x 3: density - dmin

@@ -930,6 +930,16 @@ std::shared_ptr<PrintSetup> build_print_setup(const ParamSet& p, const FilmSetup
         for (size_t i = 0; i < paper.K(); ++i) s->paper_mean_curve[i] = nanmean(&paper.density_curves.v[3 * i], 3, 1);
         s->paper_mean_base = nanmean(paper.base_density.data(), paper.base_density.size(), 1);
     }
+    s->edr = p.b(P::extended_dynamic_range);
+    if (s->edr) {
+        if (!paper.edr) fail_user("extended_dynamic_range: print profile '" + paper.id + "' has no valid edr_tone_map");
+        s->edr_lo = paper.edr->lo;
+        s->edr_hi = paper.edr->hi;
+        s->edr_toe = paper.edr->toe;
+        s->edr_shoulder = paper.edr->shoulder;
+        s->edr_tab.resize(paper.edr->target.size());
+        for (size_t i = 0; i < s->edr_tab.size(); ++i) s->edr_tab[i] = f32(paper.edr->target[i]);
+    }
     s->glare = p.b(P::glare_active);
     s->glare_amount = p.f(P::glare_amount);
     s->glare_tint = s->view_xyz;  // a printed frame's viewing illuminant (the only case that adds glare)

@@ -186,6 +186,10 @@ struct PrintSetup {
     double levels_B = 0.0, levels_W = 0.0, paper_mean_base = 0.0;
     Vec3 film_white_density{};
     std::vector<double> paper_mean_curve;
+    // the EDR tone map (reference src/print/build.cpp:83-85, :210-222), from the paper profile
+    bool edr = false;
+    double edr_lo = 0.0, edr_hi = 0.0, edr_toe = 0.0, edr_shoulder = 0.0;
+    std::vector<float> edr_tab;
     bool levels_active() const {
         if (!levels_black && !levels_white) return false;
         return scanned ? film_positive : true;

@@ -273,6 +273,13 @@ struct EncodeArgs {
     uint32_t stride;      // output row pitch in pixels
     float lincomb_a, lincomb_b;  // out = a x + b g (unsharp), applied when unsharp != 0
     int32_t unsharp;
+    // the EDR tone map on luminance (reference kernels/print.metal:319-347), after the unsharp mask and
+    // before the output matrix; edr = 0: none
+    int32_t edr;
+    uint32_t edr_n;             // target_log2_y points
+    float edr_r_y[3];           // row Y of the output space's RGB -> XYZ
+    float edr_lo, edr_span, edr_toe, edr_shoulder;
+    const float* edr_tab;       // target_log2_y, binary32
 };
 
 // The scanner's two FIR blurs, the unsharp combine and the encode in one tiled pass

@@ -66,12 +66,15 @@ def test_unknown_tier_and_result_zeroed(engine, lib):
         assert a.shape == (3, 3400, 4) and meta["row_stride_px"] % 32 == 0
 
 
-def test_outside_render_path_is_refused(engine):
-    img = sc.synthetic_image(8, 8, 0)
-    for extra in ({"extended_dynamic_range": True},):
-        with pytest.raises(sc.SpkError) as e:
-            engine.open(img, dict(BASE, **extra))
-        assert e.value.status == sc.SPK_ERR_USER and "outside this B200 build" in str(e.value)
+def test_every_parameter_renders(engine):
+    """No parameter of the schema is refused at open: every stage of the reference's render path is here."""
+    img = sc.synthetic_image(32, 24, 0)
+    for extra in ({"auto_exposure": True}, {"glare_active": True}, {"halation_boost_ev": 1.0},
+                  {"scanner_white_correction": True}, {"extended_dynamic_range": True},
+                  {"antihalation_removed": True}, {"geometry_flip_h": True}, {"input_cctf_decoding": True}):
+        with engine.open(img, dict(BASE, **extra)) as s:
+            a, _ = s.render("full")
+            assert (a[..., 3] == 65535).all()
 
 
 def test_couplers_have_no_adjoint(engine):
@@ -88,7 +91,7 @@ def test_couplers_have_no_adjoint(engine):
 def test_geometry_and_decode_have_no_adjoint(engine):
     img = sc.synthetic_image(16, 12, 0)
     for extra in ({"geometry_flip_h": True}, {"input_cctf_decoding": True}, {"auto_exposure": True},
-                  {"glare_active": True}, {"halation_boost_ev": 1.0}):
+                  {"glare_active": True}, {"halation_boost_ev": 1.0}, {"extended_dynamic_range": True}):
         with engine.open(img, dict(BASE, grain_active=False, **extra)) as s:
             with pytest.raises(sc.SpkError) as e:
                 s.render_vjp(np.ones((12, 16, 3), np.float32), 1)
