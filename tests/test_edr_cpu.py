@@ -20,9 +20,11 @@ def test_edr_against_reference(lib, resources, ref, ref_engine, extra):
     f64 = setup_f64(lib, resources, delta, 35000.0 / max(w, h))["f64"]
     assert f64["edr"]["active"]
     got, _ = oracle.Oracle(f64).render(img)
-    # binary64 against binary32: where a saturated colour's luminance y is small next to its channels, the
-    # tone map's y' / y amplifies the rounding of y; the float64 gate as elsewhere
-    st = lsb_stats(got, want)
-    assert st["frac_gt1"] <= 2e-4 and st["max"] <= 128, st
+    # within 1 LSB16 where the reference's channels are all away from the ends of the encode range; in
+    # saturated colours the tone map's y' / y amplifies the rounding of a small luminance y
+    d = np.abs(got.astype(np.int64) - want.astype(np.int64))[..., :3].max(-1)
+    inside = ((want[..., :3] >= 4096) & (want[..., :3] <= 61439)).all(-1)
+    assert d[inside].max(initial=0) <= 1
+    assert (d > 1).mean() <= 2e-3
     plain = ref_render(ref_engine, img, dict(delta, extended_dynamic_range=False), "full")
     assert lsb_stats(plain, want)["max"] > 1  # the tone map shows
