@@ -37,7 +37,7 @@ import sys
 
 import numpy as np
 
-FORMAT_VERSION = "synthetic-resources-v4"
+FORMAT_VERSION = "synthetic-resources-v5"
 LUT_SIZE = 17
 FILM_STOCK = "synthetic_negative_400"
 PAPER_STOCK = "synthetic_paper"
@@ -229,10 +229,12 @@ def profile_paper():
             "density_curves": curves.tolist(),
             "density_curves_model": {"model_type": "cdfs", "centers": centers.tolist(),
                                      "amplitudes": amplitudes.tolist(), "sigmas": sigmas.tolist()},
-            # an EDR tone map: a soft toe and a shoulder rolled off above diffuse white, in log2 Y
-            "edr_tone_map": {"version": 1, "domain_log2_y": [-14.0, 3.0], "toe_y": 0.004, "shoulder_y": 0.8,
-                             "target_log2_y": (np.linspace(-14.0, 3.0, 35) * 0.9 + 0.25 * np.tanh(
-                                 np.linspace(-3.0, 3.0, 35))).tolist()},
+            # an EDR tone map: identity between toe (2^-8) and shoulder (2^-0.5), both on knots of the 0.5-step
+            # table, shadows lifted (slope 0.8) and highlights compressed (slope 0.5) outside, in log2 Y
+            "edr_tone_map": {"version": 1, "domain_log2_y": [-14.0, 3.0], "toe_y": 2.0 ** -8, "shoulder_y": 2.0 ** -0.5,
+                             "target_log2_y": [x if -8.0 <= x <= -0.5 else
+                                               (-8.0 + 0.8 * (x + 8.0) if x < -8.0 else -0.5 + 0.5 * (x + 0.5))
+                                               for x in np.linspace(-14.0, 3.0, 35).tolist()]},
         },
     }
 
