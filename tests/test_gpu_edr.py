@@ -52,10 +52,9 @@ def test_edr_on_a_scanned_negative_is_off(engine, ref, ref_engine):
 @pytest.mark.parametrize("space", ["sRGB", "Adobe RGB (1998)", "ITU-R BT.709"])
 def test_output_spaces_within_one_lsb(engine, ref, ref_engine, space):
     """Output spaces narrower than ProPhoto, where the CAM16 gamut compression works on many pixels: the
-    print side's approximate special functions (and the compression's inverse, which amplifies their
-    last-bit differences in saturated colours) part from the reference by a few LSB16 on about 0.02 % of
-    the pixels; correctly rounded arithmetic in the gamut stage did not remove them and cost half the
-    print kernel's speed, so the gate is the float64 gate's."""
+    device parts from the reference by a few LSB16 on about 0.02 % of the pixels, the same share with
+    binary32 or binary64 print integrals and with correctly rounded arithmetic in the gamut stage (cause
+    not found); the gate is the float64 gate's."""
     img = edr_image(640, 400, 114)
     delta = dict(BASE, grain_active=False, output_color_space=space)
     with engine.open(img, delta) as s:
