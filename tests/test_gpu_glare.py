@@ -70,3 +70,26 @@ def test_glare_in_a_batch(engine):
     finally:
         for s in sessions:
             s.close()
+
+
+def test_batch_on_the_live_tier_with_meter_and_glare(engine):
+    """A batch on the live tier (frames of different sizes and geometries) with the meter and glare on
+    gives each frame its single render's bits: tier images, EVs and print seeds per session."""
+    frames = [(1200, 800, {}), (900, 1300, {"geometry_quarter_turns": 1}),
+              (1000, 700, {"geometry_crop_w": 0.6, "geometry_rotation_deg": 4.0})]
+    delta0 = dict(BASE, grain_active=True, glare_active=True, auto_exposure=True, preview_long_edge=800)
+    singles = []
+    for k, (w, h, extra) in enumerate(frames):
+        with engine.open(sc.synthetic_image(w, h, 70 + k), dict(delta0, **extra)) as s:
+            singles.append(s.render("live")[0])
+    sessions = [engine.open(sc.synthetic_image(w, h, 70 + k), dict(delta0, **extra))
+                for k, (w, h, extra) in enumerate(frames)]
+    try:
+        outs, _ = engine.render_batch(sessions, "live")
+        for r, b in zip(outs, singles):
+            assert r.pixels.shape == b.shape
+            assert np.array_equal(r.pixels, b)
+            r.free()
+    finally:
+        for s in sessions:
+            s.close()
