@@ -837,11 +837,12 @@ Plane glare_plane(RenderCtx& ctx, const Pipeline& p, uint32_t w, uint32_t h) {
     const double pp = s.glare_percent * s.glare_amount;
     Plane f = make_plane(ctx.pool, w, h);
     dev::glare_field(f.data(), w * h, f32(pp), f32(s.glare_roughness * pp), ctx.print_seed, ctx.stream);
-    if (s.glare_blur_full > 0.0) {
-        const double sg = s.glare_blur_full * ctx.rho_tier * std::sqrt(std::max(s.glare_amount, 0.0));
-        gaussian(ctx, f, f, Vec3{sg, sg, sg});
-    }
-    return f;
+    if (!(s.glare_blur_full > 0.0)) return f;
+    // blurred out of place: the tiled FIR then writes its result once, with no copy back
+    const double sg = s.glare_blur_full * ctx.rho_tier * std::sqrt(std::max(s.glare_amount, 0.0));
+    Plane blurred = make_plane(ctx.pool, w, h);
+    gaussian(ctx, f, blurred, Vec3{sg, sg, sg});
+    return blurred;
 }
 
 namespace {
