@@ -1,9 +1,11 @@
 // The binary64 set-up of the render path: everything the kernels need that does not depend on a
 // pixel, computed on the host once per pipeline build (film, print) or once per print (compute_run)
-// and narrowed once to binary32. Formulas and their operation order follow the reference's set-up
-// (src/film/setup.cpp, src/print/setup.cpp, src/print/build.cpp, src/print/cam16.cpp,
+// and narrowed once to binary32. The floating-point expressions keep the operation order of the
+// reference's set-up (src/film/setup.cpp, src/print/setup.cpp, src/print/build.cpp, src/print/cam16.cpp,
 // src/fx/gaussian.cpp, src/fx/halation.cpp, src/fx/grain.cpp), so the narrowed constants equal the
-// reference's bit for bit.
+// reference's bit for bit. Implemented in film_setup.cpp (blurs, grain, curves, couplers, the film
+// set-up), upsampling.cpp (the spectral upsampling table), halation_setup.cpp, cam16.cpp and
+// print_setup.cpp.
 #pragma once
 
 #include <array>
@@ -116,6 +118,12 @@ struct FilmSetup {
 };
 std::shared_ptr<FilmSetup> build_film_setup(const ParamSet& p, std::shared_ptr<const Profile> film,
                                             const Resources& res);
+// The L x L x 3 spectral upsampling table (upsampling.cpp; reference src/film/setup.cpp:133-257): the layer
+// sensitivities sens (bin-major, shaped by the stock's adaptation window under `light`) contracted with
+// every grid node's spectrum, read back at the node's gamut-compressed chromaticity.
+std::vector<double> spectral_upsampling_table(const Blob& blob, const std::array<double, 243>& sens,
+                                              const std::vector<double>& window, const Spectrum& light,
+                                              uint32_t* L_out);
 
 // ---- CAM16-UCS (reference src/print/cam16.cpp) ----
 struct Cam16Constants {
