@@ -14,9 +14,10 @@ reprint of the device-resident negative at print_exposure 1.2.
                 (host->device copy), spk_render, spk_set_params, spk_reprint, each result copied to
                 pinned host memory, wall clock
   roofline      the dominant kernel: algorithmic bytes per launch / its mean CUDA-event duration
-  cpu_baseline  the reference engine's own code (oracle/_ref) on this host's cores, one quarter-frame
-                render + reprint at the same pixel pitch, scaled to 4K frames/s
-  --impl reference  the reference engine alone on the host cores, same workload and metric
+  cpu_baseline  the reference engine's own code (oracle/_ref) on this host's cores: three full 4K render
+                + reprint steps, with the OpenMP thread count and the host's cores
+  --impl reference  the reference engine alone on the host cores, same workload, metric and film format
+                (from the reference's own grain set-up); the B200 library is not loaded
 """
 
 from __future__ import annotations
@@ -71,15 +72,20 @@ def workload_name():
     return "4K full render + reprint" if (W, H) == (3840, 2160) else f"{W}x{H} full render + reprint"
 
 
+def film_format_from_counts(counts, p0, long_edge):
+    """film_format_mm giving a mean of TARGET_GRAINS grains per sub-layer and pixel, from the grain counts
+    of a set-up at pixel pitch p0 (counts scale with the square of the pixel pitch), rounded to 0.1 um of
+    film so that both arms open the same parameter set."""
+    p = p0 * (TARGET_GRAINS / float(np.mean(counts))) ** 0.5
+    return round(p * long_edge / 1000.0, 4)
+
+
 def film_format_for_grains(lib, resources, long_edge):
-    """film_format_mm giving a mean of TARGET_GRAINS grains per sub-layer and pixel (counts scale with
-    the square of the pixel pitch)."""
+    """The film format of the workload from this library's set-up."""
     p0 = 10.0
     out = ctypes.c_char_p()
     lib.check(lib.lib.spkx_setup_json(resources.encode(), json.dumps(BASE).encode(), p0, ctypes.byref(out)))
-    counts = lib.take_json(out)["f64"]["grain_count"]
-    p = p0 * (TARGET_GRAINS / float(np.mean(counts))) ** 0.5
-    return p * long_edge / 1000.0
+    return film_format_from_counts(lib.take_json(out)["f64"]["grain_count"], p0, long_edge)
 
 
 def hbm_peak():
@@ -194,54 +200,84 @@ def replica_throughput(world, steps, dev_ms_max):
     return world * steps / (dev_ms_max / 1000.0)
 
 
-def cpu_reference_sample(resources, film_format_mm, steps=1):
-    """The reference engine on this host's cores: a 1920 x 1080 quadrant of the workload at the same
-    pixel pitch (film format halved), render + reprint; returns (4K frames/s, seconds, cores)."""
+def host_threads():
+    """(OpenMP threads the reference engine's parallel loops use, host cores this process may run on)."""
+    try:
+        omp = int(ctypes.CDLL("libgomp.so.1").omp_get_max_threads())
+    except (OSError, AttributeError):
+        omp = None
+    try:
+        nproc = len(os.sched_getaffinity(0))
+    except AttributeError:
+        nproc = os.cpu_count()
+    return omp, nproc
+
+
+def cpu_reference_run(resources, steps, warmup):
+    """The reference engine alone (oracle/_ref: its own stage code and kernels built for the CPU, OpenMP over
+    each kernel's grid) on the full workload: open the 3840 x 2160 frame with the workload's parameters,
+    then per step a render (develop + print at print_exposure 1.0) and a reprint of its negative at 1.2.
+    The film format comes from the reference's own grain set-up; nothing of the B200 library is loaded.
+    Returns (frames/s, seconds per step, OpenMP threads, host cores, film format)."""
     ref = sc.load_reference()
     eng = ref.engine(resources)
-    w, h = W // 2, H // 2
-    img = np.ascontiguousarray(sc.synthetic_image(W, H, 0)[:h, :w])
-    delta = dict(BASE, film_format_mm=film_format_mm / 2.0)
+    p0 = 10.0
+    out = ctypes.c_char_p()
+    ref.check(ref.lib.spkref_setup_json(eng.h, json.dumps(BASE).encode(), p0, ctypes.byref(out)))
+    ff = film_format_from_counts(ref.take_json(out)["grain_count"], p0, W)
+    img = sc.synthetic_image(W, H, 0)
+    delta = dict(BASE, film_format_mm=ff)
     comps, strength = HALATION
     wts = (ctypes.c_double * 6)(*[float(v) for c in comps for v in c[0]])
     sig = (ctypes.c_double * 6)(*[float(v) for c in comps for v in c[1]])
     st = (ctypes.c_double * 3)(*strength)
-    s = ref.lib.spkref_open(eng.h, img.ctypes.data_as(sc.FP), w, h, json.dumps(delta).encode(), 2, wts, sig, st)
+    s = ref.lib.spkref_open(eng.h, img.ctypes.data_as(sc.FP), W, H, json.dumps(delta).encode(), 2, wts, sig, st)
     if not s:
         raise RuntimeError(ref.last_error())
-    out = np.zeros((h, w, 4), np.uint16)
+    rgba = np.zeros((H, W, 4), np.uint16)
+    rp = rgba.ctypes.data_as(ctypes.POINTER(ctypes.c_uint16))
     times = []
-    for _ in range(steps):
+    for i in range(warmup + steps):
         t0 = time.perf_counter()
         ref.check(ref.lib.spkref_develop(s))
-        ref.check(ref.lib.spkref_print(s, 1.0, out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint16))))
-        ref.check(ref.lib.spkref_print(s, 1.2, out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint16))))
-        times.append(time.perf_counter() - t0)
+        ref.check(ref.lib.spkref_print(s, 1.0, rp))
+        ref.check(ref.lib.spkref_print(s, 1.2, rp))
+        if i >= warmup:
+            times.append(time.perf_counter() - t0)
     ref.lib.spkref_close(s)
     eng.close()
+    omp, nproc = host_threads()
     t = sum(times) / len(times)
-    return 1.0 / (4.0 * t), times, os.cpu_count()
+    return 1.0 / t, t, omp, nproc, ff
 
 
 def run_reference(args):
+    """--impl reference: the reference engine's CPU build on this host's cores, the same 4K render + reprint
+    workload, metric and units as the B200 arm; rank 0 alone (the other ranks exit without work)."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
     resources = synth_resources.ensure(sc.RESOURCES)
-    lib = sc.load()
-    ff = film_format_for_grains(lib, resources, W)
-    if args.warmup > 0:
-        cpu_reference_sample(resources, ff, steps=1)  # warm-up: set-up caches, page faults
-    fps, times, cores = cpu_reference_sample(resources, ff, steps=max(args.steps, 1))
-    sample = f"{args.steps} x (1920x1080 quadrant render + reprint at the 4K pitch), scaled x4 to 3840x2160"
-    line = {"impl": "reference", "metric": METRIC, "value": fps, "unit": UNIT, "n_gpus": 0, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1000.0 * 4.0 * sum(times) / len(times), "higher_is_better": True,
+    steps = max(args.steps, 1)
+    fps, t, omp, nproc, ff = cpu_reference_run(resources, steps, args.warmup)
+    sample = (f"{steps} full {W}x{H} render + reprint steps (print_exposure 1.0 then 1.2), after {args.warmup} "
+              f"untimed; {omp} OpenMP threads on {nproc} host cores")
+    line = {"impl": "reference", "metric": METRIC, "value": fps, "unit": UNIT, "n_gpus": 0, "steps": steps,
+            "warmup": args.warmup, "ms_per_step": 1000.0 * t, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": workload_name(), "width": W, "height": H},
-            "cpu_baseline": {"value": fps, "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample},
+            "config": workload_config(ff, 1),
+            "cpu_baseline": {"value": fps, "unit": UNIT, "cores": omp, "nproc": nproc, "kind": "reference",
+                             "sample": sample},
             "e2e": {"value": fps, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
+
+
+def workload_config(ff, world):
+    return {"workload": workload_name(), "width": W, "height": H, "halation_sigma_px": [20, 120],
+            "halation_weight": 0.03, "scanner_lens_blur_px": 1.5, "grains_per_px": TARGET_GRAINS,
+            "film_format_mm": ff, "parallelism": f"replicas{world}",
+            "l2": "flushed (256 MiB write) before each step"}
 
 
 def run_e2e(args, eng, img, delta, pg, dev, world):
@@ -660,19 +696,16 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline and os.path.exists(sc.REF_PATH):
-        fps, times, cores = cpu_reference_sample(resources, ff, steps=1)
-        cpu = {"value": fps, "unit": UNIT, "cores": cores, "kind": "reference",
-               "sample": "one 1920x1080 quadrant render + reprint at the 4K pixel pitch, scaled x4 "
-                         f"({times[0]:.2f} s on {cores} host threads)"}
+        fps, t, omp, nproc, _ = cpu_reference_run(resources, steps=3, warmup=1)
+        cpu = {"value": fps, "unit": UNIT, "cores": omp, "nproc": nproc, "kind": "reference",
+               "sample": f"3 full {W}x{H} render + reprint steps after 1 untimed ({t:.2f} s per step), "
+                         f"{omp} OpenMP threads on {nproc} host cores"}
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": dev_ms_max / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": {"workload": workload_name(), "width": W, "height": H,
-                           "halation_sigma_px": [20, 120], "halation_weight": 0.03, "scanner_lens_blur_px": 1.5,
-                           "grains_per_px": TARGET_GRAINS, "film_format_mm": round(ff, 4),
-                           "parallelism": f"replicas{world}", "l2": "flushed (256 MiB write) before each step"},
+                "config": workload_config(ff, world),
                 "render_ms": render_ms, "reprint_ms": reprint_ms,
                 "render_fps": 1000.0 / render_ms, "reprint_fps": 1000.0 / reprint_ms,
                 "wall_s_timed": wall, "stage_ms": stage_ms, "kernels": table,
