@@ -100,6 +100,13 @@ SPK_API spk_status spkx_sampler_lognormal(float* out, uint32_t n, float mean, fl
 /* Philox4x32-10 of n (counter[4], key[2]) pairs into out[4n] */
 SPK_API spk_status spkx_philox(const uint32_t* counters, const uint32_t* keys, uint32_t* out, uint32_t n);
 
+/* Test hook of the failure path (no counterpart in the reference engine): the SM clocks a stage wait of
+ * the tensor-core print kernel may take before it gives up (0: the normal limit, about 2 s). With a limit
+ * of a few clocks a wait runs out at once; the kernel then stops issuing work, drains the MMAs it issued
+ * under the normal limit, frees its tensor memory and flags the failure, and the render returns
+ * SPK_ERR_GPU with the context still usable. Process-wide; set it back to 0 afterwards. */
+SPK_API spk_status spkx_test_set_tc_wait_limit(int64_t cycles);
+
 /* the Gaussian blur of a w x h RGB float plane (3 floats per pixel) with per-channel sigma in pixels,
  * by the engine's FIR / recursive branch rule */
 SPK_API spk_status spkx_gaussian(const float* in, float* out, uint32_t w, uint32_t h, const double* sigma3);
@@ -187,10 +194,12 @@ SPK_API spk_status spk_render_vjp(spk_session* session, const char* tier, uint32
  *   stream and the call returns without waiting. It allocates nothing: the intermediate planes live in a
  *   fixed 16 MiB array compiled into the library, so w * h must not exceed 699,050 pixels (2^21 floats
  *   per plane); larger frames are refused with SPK_ERR_INVALID_ARG. Every GPU that loads the library
- *   keeps the array until the process exits. The first call on each device (with that device current)
- *   looks up the array's device address; make it before any stream capture. All calls on a device share
- *   the one array and leave their data in it, so calls whose work overlaps on the GPU race: order them on
- *   one stream, or wait for one before starting the next on another.
+ *   keeps the array until the process exits. The first call in each CUDA context (the device's primary
+ *   context, or a driver context the host made current) looks up the array's address in that context and
+ *   keeps it for later calls in the same context (keyed by the driver's context id, so a new context or a
+ *   reset device gets a fresh lookup); make that first call before any stream capture. All calls in a
+ *   context share the one array and leave their data in it, so calls whose work overlaps on the GPU race:
+ *   order them on one stream, or wait for one before starting the next on another.
  */
 SPK_API spk_status spkx_gaussian_noalloc(const float* in, float* out, uint32_t w, uint32_t h, const double* sigma3,
                                          void* stream);

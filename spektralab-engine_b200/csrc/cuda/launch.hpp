@@ -87,6 +87,8 @@ void print(const float* neg, float* rgb, const PrintArgs& a, cudaStream_t s);
 void print_spectral(const PrintArgs& a, const SpectralTablesN& host_tab, const SpectralTablesN* tab, int mode,
                     const float* neg, float* rgb, uint32_t n, float* contraction, uint32_t* err, cudaStream_t s);
 bool print_spectral_supported(uint32_t nl_pad);
+// The limit of the spectral-mode kernel's stage waits in SM clocks (0: the normal limit); a test hook.
+void set_tc_wait_limit(long long cycles);
 
 // The print-preview table render: negative densities -> trilinear table -> RGBA16 (row pitch a.stride).
 void print_lut(const float* neg, uint16_t* out, const PrintLutArgs& a, cudaStream_t s);

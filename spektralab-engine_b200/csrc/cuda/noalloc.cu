@@ -9,16 +9,21 @@
 // The scratch is a file-scope __device__ array of two planes of kMaxFloats floats each (16 MiB in all),
 // so a frame of at most kMaxFloats / 3 pixels (699,050, e.g. 1024 x 682). Every GPU that loads the
 // library holds the array until the process exits. Host code cannot use the array's name as a device
-// address (it is a host-side stand-in), so the first call on each device, with that device current,
-// looks the address up with cudaGetSymbolAddress and keeps it for later calls; make that first call
-// before any stream capture. Every call on a device shares the array, which keeps whatever the last
-// call left in it: calls whose work overlaps on the GPU (different streams, or a later call before an
-// earlier one's work has finished on another stream) race on it. Nothing has to start at zero: each
-// pass writes every scratch element it later reads.
+// address (it is a host-side stand-in), so the first call in each CUDA context, with that context current,
+// looks the address up with cudaGetSymbolAddress and keeps it for later calls in the same context; make
+// that first call before any stream capture. The address belongs to the context it was looked up in: a
+// host that makes its own driver contexts current, or resets the device, gets a fresh lookup for each new
+// context (the cache is keyed by the driver's unique context id). Every call in a context shares the
+// array, which keeps whatever the last call left in it: calls whose work overlaps on the GPU (different
+// streams, or a later call before an earlier one's work has finished on another stream) race on it.
+// Nothing has to start at zero: each pass writes every scratch element it later reads.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <mutex>
 #include <string>
+#include <utility>
+#include <vector>
 
 #include "../host/blur_plan.h"
 #include "../host/status.hpp"
@@ -29,26 +34,55 @@ namespace spkb::dev {
 namespace {
 
 constexpr size_t kMaxFloats = size_t(1) << 21;  // one plane: 2,097,152 floats (8 MiB)
-constexpr int kMaxDevices = 64;
-
 __device__ __align__(256) float g_scratch[2 * kMaxFloats];
 
-std::mutex g_mutex;
-float* g_address[kMaxDevices] = {};
+using CtxGetCurrent = CUresult (*)(CUcontext*);
+using CtxGetId = CUresult (*)(CUcontext, unsigned long long*);
 
-// The device address of g_scratch on the current device, looked up once per device.
-float* scratch_address(int device, cudaError_t* err) {
-    std::lock_guard<std::mutex> lock(g_mutex);
-    if (!g_address[device]) {
-        void* p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_scratch);
-        if (e != cudaSuccess) {
-            *err = e;
+std::mutex g_mutex;
+CtxGetCurrent g_get_current = nullptr;
+CtxGetId g_get_id = nullptr;
+std::vector<std::pair<unsigned long long, float*>> g_address;  // (driver context id, address of g_scratch)
+
+// The driver's id of the current context (0 when none is current or the driver cannot say).
+unsigned long long current_context_id() {
+    CUcontext ctx = nullptr;
+    unsigned long long id = 0;
+    if (g_get_current(&ctx) != CUDA_SUCCESS || !ctx || g_get_id(ctx, &id) != CUDA_SUCCESS) return 0;
+    return id;
+}
+
+// The device address of g_scratch in the current context, looked up once per context. The caller holds
+// g_mutex.
+float* scratch_address(cudaError_t* err) {
+    if (!g_get_current || !g_get_id) {
+        void* f0 = nullptr;
+        void* f1 = nullptr;
+        cudaDriverEntryPointQueryResult q0{}, q1{};
+        *err = cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f0, 12000, cudaEnableDefault, &q0);
+        if (*err == cudaSuccess)
+            *err = cudaGetDriverEntryPointByVersion("cuCtxGetId", &f1, 12000, cudaEnableDefault, &q1);
+        if (*err != cudaSuccess || !f0 || !f1) {
+            if (*err == cudaSuccess) *err = cudaErrorNotSupported;
             return nullptr;
         }
-        g_address[device] = static_cast<float*>(p);
+        g_get_current = reinterpret_cast<CtxGetCurrent>(f0);
+        g_get_id = reinterpret_cast<CtxGetId>(f1);
     }
-    return g_address[device];
+    unsigned long long id = current_context_id();
+    for (const auto& [ctx, p] : g_address)
+        if (id != 0 && ctx == id) return p;
+    void* p = nullptr;
+    *err = cudaGetSymbolAddress(&p, g_scratch);  // makes the device's primary context current if none is
+    if (*err != cudaSuccess) return nullptr;
+    if (id == 0) id = current_context_id();
+    if (id == 0) {
+        *err = cudaErrorDeviceUninitialized;
+        return nullptr;
+    }
+    if (g_address.size() >= 256) g_address.clear();  // a host that cycles through contexts: forget the old
+    g_address.emplace_back(id, static_cast<float*>(p));
+    return static_cast<float*>(p);
 }
 
 }  // namespace
@@ -75,15 +109,15 @@ extern "C" SPK_API spk_status spkx_gaussian_noalloc(const float* in, float* out,
                         " pixels)");
         return SPK_ERR_INVALID_ARG;
     }
-    int device = 0;
-    cudaError_t e = cudaGetDevice(&device);
-    if (e != cudaSuccess || device < 0 || device >= dev::kMaxDevices) {
-        last_error::set("spkx_gaussian_noalloc: no usable current CUDA device");
-        return SPK_ERR_GPU;
+    cudaError_t e = cudaSuccess;
+    float* s0 = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(dev::g_mutex);
+        s0 = dev::scratch_address(&e);
     }
-    float* s0 = dev::scratch_address(device, &e);
     if (!s0) {
-        last_error::set(std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+        last_error::set(std::string("spkx_gaussian_noalloc: no scratch address in the current CUDA context: ") +
+                        cudaGetErrorString(e));
         return SPK_ERR_GPU;
     }
     float* s1 = s0 + dev::kMaxFloats;

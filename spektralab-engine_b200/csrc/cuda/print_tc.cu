@@ -20,9 +20,11 @@
 // wavelengths the output equals k_print's bit for bit); F64 evaluates both integrals in binary64 from the
 // binary64 tables.
 //
-// Every mbarrier wait gives up after 4e9 SM clocks (about 2 s); the thread then skips its remaining waits, the
-// CTA leaves its tile loop at the next tile boundary, waits (also bounded) for its own MMAs, frees its
-// tensor memory and sets *err.
+// Every mbarrier wait gives up after 4e9 SM clocks (about 2 s; a test hook can shorten the stage waits'
+// limit to a few clocks so that one runs out). A wait that gives up is made known to the whole CTA at the
+// chunk's barrier; from then on the CTA forms no operands, issues no MMAs and reads no tensor memory, leaves
+// its tile loop at the tile's end, waits for the MMAs it already issued (bounded by the full limit, never
+// the shortened one), frees its tensor memory and sets *err.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -102,6 +104,7 @@ struct alignas(16) SpectralParams {
     float* rgb;
     float* contraction;
     uint32_t* err;
+    long long wait_limit;  // SM clocks a stage wait may take before it gives up
     uint32_t n, nl;
 };
 
@@ -124,14 +127,14 @@ __device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
     return done != 0;
 }
 
-// Waits for the completion of the barrier's phase of the given parity; false after kWaitCycles SM clocks
-// (about 2 s at the B200's clocks). The clock is read only once the phase was found incomplete.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+// Waits for the completion of the barrier's phase of the given parity; false after `limit` SM clocks
+// (kWaitCycles: about 2 s at the B200's clocks). The clock is read only once the phase was found incomplete.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, long long limit) {
     if (mbar_try(bar, parity)) return true;
     const long long t0 = clock64();
     for (;;) {
         if (mbar_try(bar, parity)) return true;
-        if (clock64() - t0 > kWaitCycles) return false;
+        if (clock64() - t0 > limit) return false;
     }
 }
 
@@ -304,7 +307,8 @@ __device__ __forceinline__ void issue(uint32_t tmem, uint32_t a_saddr, uint32_t 
 }
 
 // One integral on the tensor cores for the CTA's 128 pixels. g counts the CTA's chunks (stage and
-// barrier phase); ok turns false at a wait that gave up, after which this thread waits no more.
+// barrier phase); ok, the same in every thread of the CTA, turns false once any thread's wait gave up:
+// from then on nothing is produced, issued, waited for or read from tensor memory (R is 0).
 template <int M, int NLP, uint32_t PASS>
 __device__ __forceinline__ void contract_tc(const SpectralParams<NLP>& p, unsigned char* smem, uint32_t tmem,
                                             const float d[3], float R[3], uint32_t& g, bool& ok) {
@@ -321,20 +325,26 @@ __device__ __forceinline__ void contract_tc(const SpectralParams<NLP>& p, unsign
         const uint32_t st = g % kStages;
         unsigned char* A = smem + L.a + st * stage_bytes(M);
         // the MMAs of chunk g - kStages read this stage
-        if (g >= kStages && ok) ok = mbar_wait(bar0 + 8 * st, ((g / kStages) - 1) & 1u);
-        produce<M, NLP, PASS>(p, reinterpret_cast<const float*>(smem + L.e), j, D0, D1, D2, A, tid);
+        bool mine = ok;
+        if (g >= kStages && mine) mine = mbar_wait(bar0 + 8 * st, ((g / kStages) - 1) & 1u, p.wait_limit);
+        if (mine) produce<M, NLP, PASS>(p, reinterpret_cast<const float*>(smem + L.e), j, D0, D1, D2, A, tid);
         fence_async_smem();
         tc_fence_before();
-        __syncthreads();
-        if (tid == 0) {
+        ok = __syncthreads_or(mine ? 0 : 1) == 0;
+        if (tid == 0 && ok) {
             tc_fence_after();
             issue<M, NLP>(tmem, smem_addr(A), b_saddr, j);
             mma_commit(bar0 + 8 * st);
         }
     }
     const uint32_t last = g - 1;
-    if (ok) ok = mbar_wait(bar0 + 8 * (last % kStages), (last / kStages) & 1u);
-    __syncwarp();  // tcgen05.ld is warp-collective: the warp reconverges after the per-thread waits
+    bool mine = ok;
+    if (mine) mine = mbar_wait(bar0 + 8 * (last % kStages), (last / kStages) & 1u, p.wait_limit);
+    ok = __syncthreads_or(mine ? 0 : 1) == 0;  // uniform: tcgen05.ld is warp-collective
+    if (!ok) {
+        R[0] = R[1] = R[2] = 0.0f;
+        return;
+    }
     tc_fence_after();
     float v[8];
     tmem_ld8(tmem + ((32u * (tid / 32u)) << 16), v);
@@ -505,7 +515,7 @@ __global__ void __launch_bounds__(kTcThreads) k_print_spectral(const __grid_cons
         bool done = true;
         if (tid == 0) {
             mma_commit(bar_end);
-            done = mbar_wait(bar_end, 0);
+            done = mbar_wait(bar_end, 0, kWaitCycles);  // every issued MMA ends before the tensor memory is freed
         }
         const int failed = __syncthreads_or((ok && done) ? 0 : 1);
         if (tid < 32) {
@@ -515,6 +525,8 @@ __global__ void __launch_bounds__(kTcThreads) k_print_spectral(const __grid_cons
         if (tid == 0 && failed) atomicOr(p.err, 1u);
     }
 }
+
+long long g_wait_limit = 0;  // spkx_test_set_tc_wait_limit: 0 the full limit
 
 template <int M, int NLP>
 void launch_spectral(const PrintArgs& a, const SpectralTablesN& host_tab, const SpectralTablesN* tab, const float* neg,
@@ -537,6 +549,7 @@ void launch_spectral(const PrintArgs& a, const SpectralTablesN& host_tab, const 
     prm->rgb = rgb;
     prm->contraction = contraction;
     prm->err = err;
+    prm->wait_limit = g_wait_limit > 0 ? g_wait_limit : kWaitCycles;
     prm->n = n;
     prm->nl = host_tab.nl;
     int dev = 0, sms = 0, per_sm = 0;
@@ -567,6 +580,8 @@ void launch_mode(const PrintArgs& a, const SpectralTablesN& host_tab, const Spec
 }  // namespace
 
 bool print_spectral_supported(uint32_t nl_pad) { return nl_pad == 96 || nl_pad == SPKB_NL_MAX; }
+
+void set_tc_wait_limit(long long cycles) { g_wait_limit = cycles; }
 
 void print_spectral(const PrintArgs& a, const SpectralTablesN& host_tab, const SpectralTablesN* tab, int mode,
                     const float* neg, float* rgb, uint32_t n, float* contraction, uint32_t* err, cudaStream_t s) {

@@ -1,5 +1,6 @@
 #include "device.hpp"
 
+#include <atomic>
 #include <cstdint>
 #include <vector>
 
@@ -17,6 +18,12 @@ struct PoolState {
     size_t live = 0;
 };
 
+namespace {
+// process-wide allocation counters behind the memory report
+std::atomic<uint64_t> g_scratch_allocations{0}, g_scratch_live{0}, g_persistent_allocations{0};
+std::atomic<uint64_t> g_persistent_live{0}, g_persistent_bytes{0};
+}  // namespace
+
 struct DevBuffer::Impl {
     void* p = nullptr;
     size_t size = 0;
@@ -27,7 +34,10 @@ struct DevBuffer::Impl {
             std::lock_guard<std::mutex> g(pool->m);
             cudaFreeAsync(p, pool->stream);
             pool->live -= size;
+            g_scratch_live.fetch_sub(1);
         } else {
+            g_persistent_live.fetch_sub(1);
+            g_persistent_bytes.fetch_sub(size);
             cudaFree(p);
         }
     }
@@ -61,6 +71,8 @@ DevBuffer Pool::acquire(size_t bytes) {
         std::lock_guard<std::mutex> g(s_->m);
         s_->live += bytes;
     }
+    g_scratch_allocations.fetch_add(1);
+    g_scratch_live.fetch_add(1);
     auto impl = std::make_shared<DevBuffer::Impl>();
     impl->p = p;
     impl->size = bytes;
@@ -81,6 +93,9 @@ DevBuffer Pool::persistent(size_t bytes) {
         device_pool_trim(dev);
         cuda_check(cudaMalloc(&p, bytes), "cudaMalloc (persistent)");
     }
+    g_persistent_allocations.fetch_add(1);
+    g_persistent_live.fetch_add(1);
+    g_persistent_bytes.fetch_add(bytes);
     auto impl = std::make_shared<DevBuffer::Impl>();
     impl->p = p;
     impl->size = bytes;
@@ -107,6 +122,30 @@ size_t device_pool_reserved(int device) {
     uint64_t v = 0;
     cudaMemPoolGetAttribute(mp, cudaMemPoolAttrReservedMemCurrent, &v);
     return size_t(v);
+}
+
+DeviceMemory device_memory(int device) {
+    DeviceMemory m;
+    cudaMemPool_t mp = nullptr;
+    if (cudaDeviceGetDefaultMemPool(&mp, device) == cudaSuccess) {
+        uint64_t v = 0;
+        if (cudaMemPoolGetAttribute(mp, cudaMemPoolAttrReservedMemCurrent, &v) == cudaSuccess) m.reserved = v;
+        if (cudaMemPoolGetAttribute(mp, cudaMemPoolAttrUsedMemCurrent, &v) == cudaSuccess) m.used = v;
+        if (cudaMemPoolGetAttribute(mp, cudaMemPoolAttrUsedMemHigh, &v) == cudaSuccess) m.used_high = v;
+    }
+    m.scratch_allocations = g_scratch_allocations.load();
+    m.scratch_live = g_scratch_live.load();
+    m.persistent_allocations = g_persistent_allocations.load();
+    m.persistent_live = g_persistent_live.load();
+    m.persistent_bytes = g_persistent_bytes.load();
+    return m;
+}
+
+void device_pool_begin_frame(int device) {
+    cudaMemPool_t mp = nullptr;
+    if (cudaDeviceGetDefaultMemPool(&mp, device) != cudaSuccess) return;
+    uint64_t zero = 0;
+    (void)cudaMemPoolSetAttribute(mp, cudaMemPoolAttrUsedMemHigh, &zero);
 }
 
 size_t device_pool_trim(int device) {

@@ -59,6 +59,17 @@ void configure_device_pool(int device);
 size_t device_pool_trim(int device);          // returns the cached bytes released to the driver
 size_t device_pool_reserved(int device);
 
+// The figures behind the memory report: the device pool's reserved and used bytes and its used high-water
+// mark (cudaMemPoolAttr*), and this process's scratch and persistent allocation counters.
+struct DeviceMemory {
+    uint64_t reserved = 0, used = 0, used_high = 0;
+    uint64_t scratch_allocations = 0, scratch_live = 0;
+    uint64_t persistent_allocations = 0, persistent_live = 0, persistent_bytes = 0;
+};
+DeviceMemory device_memory(int device);
+// A render begins: the pool's used high-water mark starts again from the bytes in use.
+void device_pool_begin_frame(int device);
+
 struct Plane {
     DevBuffer buf;
     uint32_t w = 0, h = 0;

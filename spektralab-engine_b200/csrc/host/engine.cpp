@@ -133,6 +133,75 @@ struct TierState {
     uint32_t long_edge = 0;  // of the tier's image
     Plane negative;
     double pitch_um = 0.0;
+    std::optional<double> applied_ev;  // the auto-exposure EV the negative was developed with
+};
+
+// The effect variants of the desktop device, the one this build serves (reference src/core/render.hpp:40-44)
+constexpr const char* kEffectVersions =
+    "halation=reference;grain=reference;glare=reference;print_spatial=reference;dir_couplers=reference";
+
+// A session's progress record (reference src/session/progress.cpp): the current render's id, its node
+// total and the nodes passed, the last node's label, done, the applied EV and the cancel flag. It has its
+// own small lock, apart from the session's, so spk_progress and spk_cancel answer while a render runs.
+class ProgressRecord final : public ProgressSink {
+public:
+    // a render-type call starts: new id, node total, stage "queued"; the cancel flag is cleared
+    void reset(std::string id, uint32_t total) {
+        std::lock_guard<std::mutex> g(m_);
+        id_ = std::move(id);
+        total_ = total;
+        fired_ = 0;
+        stage_ = "queued";
+        done_ = false;
+        ev_.reset();
+        cancelled_.store(false);
+    }
+    void add_nodes(uint32_t n) {
+        std::lock_guard<std::mutex> g(m_);
+        total_ += n;
+    }
+    // between stages: a set cancel flag ends the render with SPK_ERR_CANCELLED; else the label is recorded
+    void node(const char* label) override {
+        if (cancelled_.load(std::memory_order_relaxed)) fail_cancelled();
+        std::lock_guard<std::mutex> g(m_);
+        stage_ = label;
+        ++fired_;
+    }
+    void finish(bool done, std::optional<double> ev) {
+        std::lock_guard<std::mutex> g(m_);
+        done_ = done;
+        ev_ = ev;
+    }
+    // spk_cancel: a NULL id, or the current one, cancels the current render
+    void cancel(const char* id) {
+        std::lock_guard<std::mutex> g(m_);
+        if (!id || id_ == id) cancelled_.store(true);
+    }
+    // the spk_progress reply; an id that is given and is not the current one is SPK_ERR_USER
+    json::Value snapshot(const char* id) const {
+        std::lock_guard<std::mutex> g(m_);
+        if (id && *id && id_ != id) fail_user("unknown progress id '" + std::string(id) + "'");
+        json::Value r;
+        r["auto_exposure_ev"] = ev_ ? json::Value(*ev_) : json::Value(nullptr);
+        r["cancelled"] = cancelled_.load();
+        r["done"] = done_;
+        r["effect_versions"] = std::string(kEffectVersions);
+        r["memory_pressure_critical"] = false;  // no memory-pressure source on this device
+        r["node_times"] = json::Object{};
+        r["pct"] = done_ ? 100.0 : total_ ? 100.0 * std::min(fired_, total_) / double(total_) : 0.0;
+        r["progress_id"] = id_;
+        r["stage"] = stage_;
+        return r;
+    }
+
+private:
+    mutable std::mutex m_;
+    std::atomic<bool> cancelled_{false};
+    std::string id_;
+    std::string stage_ = "queued";
+    uint32_t fired_ = 0, total_ = 0;
+    bool done_ = false;
+    std::optional<double> ev_;
 };
 
 class Session {
@@ -155,11 +224,7 @@ public:
     std::optional<HalationOverride> hal;
     int print_mode = -1;  // spkx_session_set_print_mode: -1 the binary32 print kernel, else a SpectralMode
     uint32_t print_bins = SPKB_NL;
-    std::atomic<bool> cancel{false};
-    std::string progress_id;
-    std::atomic<uint32_t> nodes_done{0};
-    uint32_t nodes_total = 0;
-    bool done = false;
+    ProgressRecord progress;
     Plane meter_image;                // the frame at the meter's 1600 px long edge, kept
     std::optional<MeterValues> meter;  // until a field of the meter's key changes
 
@@ -251,9 +316,15 @@ public:
         return 1000.0 * params.f(P::film_format_mm) / double(ts.long_edge);
     }
 
-    void node() {
-        if (cancel.load(std::memory_order_relaxed)) fail_cancelled();
-        nodes_done.fetch_add(1, std::memory_order_relaxed);
+    // a render-type call starts: a new progress id and the node total of its develop (unless the negative
+    // is reused) and print
+    std::string begin_progress(bool develops, bool prints = true) {
+        uint32_t total = 0;
+        if (develops && pipe.film) total += film_node_count(*pipe.film);
+        if (prints && pipe.print) total += print_node_count(*pipe.print);
+        std::string pid = "p" + std::to_string(g_next_id++);
+        progress.reset(pid, total);
+        return pid;
     }
 };
 
@@ -413,9 +484,10 @@ void develop_tier(Session& s, Tier t, RenderCtx& ctx) {
     ctx.ae_ev = s.session_ev();
     const uint32_t seed = s.params.b(P::grain_active) ? s.seeds.next() : kNoGrainFilmSeed;
     ctx.pitch_um = s.tier_pitch_um(ts);
-    s.node();
+    ts.applied_ev.reset();
     ts.negative = develop(ctx, s.pipe, ts.source, seed, s.hal);
     ts.pitch_um = ctx.pitch_um;
+    ts.applied_ev = ctx.ae_ev;
 }
 
 void render(Session& s, const char* tier_name, bool reprint, spk_result* out) {
@@ -426,16 +498,14 @@ void render(Session& s, const char* tier_name, bool reprint, spk_result* out) {
     DeviceGuard dg(s.engine->device);
     TierState& ts = s.tiers[int(*t)];
     const bool reuse = reprint && static_cast<bool>(ts.negative);
-    s.progress_id = "p" + std::to_string(g_next_id++);
-    s.cancel.store(false);
-    s.nodes_done.store(0);
-    s.nodes_total = reuse ? 1 : 2;
-    s.done = false;
+    const std::string pid = s.begin_progress(!reuse);
+    device_pool_begin_frame(s.engine->device);
     bool developed = false;
     OutputImage* img = nullptr;
     try {
         s.tier_source(*t);  // a failed downscale is a render failure (SPK_ERR_GPU), as in the reference
         RenderCtx ctx{s.pool, s.stream};
+        ctx.progress = &s.progress;
         ctx.rho_tier = s.rho(ts);
         ctx.print_mode = s.print_mode;
         ctx.print_bins = s.print_bins;
@@ -445,7 +515,6 @@ void render(Session& s, const char* tier_name, bool reprint, spk_result* out) {
         }
         ctx.print_seed = s.draw_print_seed();
         ctx.pitch_um = ts.pitch_um;
-        s.node();
         img = output_acquire(s.engine->device, ts.negative.w, ts.negative.h);
         ctx.copy_stream = s.copy_stream;
         ctx.band_events = &s.band_events;
@@ -459,7 +528,11 @@ void render(Session& s, const char* tier_name, bool reprint, spk_result* out) {
         (void)cudaStreamSynchronize(s.copy_stream);
         (void)cudaStreamSynchronize(s.stream);
         if (img) output_release(img);
-        if (developed) ts.negative = Plane{};
+        if (developed) {  // a cancelled or failed render caches no negative of its own; a reused one stays
+            ts.negative = Plane{};
+            ts.applied_ev.reset();
+        }
+        s.progress.finish(false, std::nullopt);
         try {
             throw;
         } catch (const Error& e) {
@@ -469,7 +542,7 @@ void render(Session& s, const char* tier_name, bool reprint, spk_result* out) {
             fail_gpu("out of memory");
         }
     }
-    s.done = true;
+    s.progress.finish(true, ts.applied_ev);
     out->rgba16 = img->host;
     out->texture = img;
     out->width = img->width;
@@ -479,7 +552,7 @@ void render(Session& s, const char* tier_name, bool reprint, spk_result* out) {
     out->reprint = reuse ? 1 : 0;
     out->negative_was_cached = reuse ? 1 : 0;
     std::memset(out->progress_id, 0, sizeof out->progress_id);
-    std::strncpy(out->progress_id, s.progress_id.c_str(), sizeof out->progress_id - 1);
+    std::strncpy(out->progress_id, pid.c_str(), sizeof out->progress_id - 1);
 }
 
 // The print-preview table render (reference src/session/session.cpp:503-572): the tier's cached
@@ -496,23 +569,21 @@ void preview_stock_lut(Session& s, const char* print_stock, const char* tier_nam
     const std::shared_ptr<const PrintLut> lut = s.engine->res->print_lut(stock);
     DeviceGuard dg(s.engine->device);
     TierState& ts = s.tiers[int(*t)];
-    s.progress_id = "p" + std::to_string(g_next_id++);
-    s.cancel.store(false);
-    s.nodes_done.store(0);
-    s.nodes_total = ts.negative ? 1 : 2;
-    s.done = false;
+    const std::string pid = s.begin_progress(!ts.negative, false);  // the table pass is one more node
+    s.progress.add_nodes(1);
     bool developed = false;
     OutputImage* img = nullptr;
     double apply_ms = 0.0;
     try {
         s.tier_source(*t);
         RenderCtx ctx{s.pool, s.stream};
+        ctx.progress = &s.progress;
         ctx.rho_tier = s.rho(ts);
         if (!ts.negative) {
             developed = true;
             develop_tier(s, *t, ctx);
         }
-        s.node();
+        ctx.node("printing.preview_lut");
         DevBuffer table;
         {
             std::lock_guard<std::mutex> g(s.engine->luts_m);
@@ -545,7 +616,11 @@ void preview_stock_lut(Session& s, const char* print_stock, const char* tier_nam
     } catch (...) {
         (void)cudaStreamSynchronize(s.stream);
         if (img) output_release(img);
-        if (developed) ts.negative = Plane{};
+        if (developed) {  // a cancelled or failed render caches no negative of its own; a reused one stays
+            ts.negative = Plane{};
+            ts.applied_ev.reset();
+        }
+        s.progress.finish(false, std::nullopt);
         try {
             throw;
         } catch (const Error& e) {
@@ -555,7 +630,7 @@ void preview_stock_lut(Session& s, const char* print_stock, const char* tier_nam
             fail_gpu("out of memory");
         }
     }
-    s.done = true;
+    s.progress.finish(true, ts.applied_ev);
     out->rgba16 = img->host;
     out->texture = img;
     out->width = img->width;
@@ -565,7 +640,7 @@ void preview_stock_lut(Session& s, const char* print_stock, const char* tier_nam
     out->reprint = 1;
     out->negative_was_cached = 1;
     std::memset(out->progress_id, 0, sizeof out->progress_id);
-    std::strncpy(out->progress_id, s.progress_id.c_str(), sizeof out->progress_id - 1);
+    std::strncpy(out->progress_id, pid.c_str(), sizeof out->progress_id - 1);
     if (out_json) {
         json::Value r;
         r["apply_backend"] = "native-cuda";
@@ -625,6 +700,7 @@ struct BatchFrame {
     bool reused = false;     // the tier's negative was cached (reprint)
     bool developed = false;  // the tier's negative was made by this batch
     cudaEvent_t ready = nullptr;  // the engine's ready event of the frame's slot
+    std::string pid;              // the frame's progress id
 };
 
 const char* const kBatchPlans[] = {"frames:4", "frames:16", "persistent:2048:592", "persistent:8192:1184"};
@@ -860,13 +936,10 @@ void render_batch(std::vector<Session*> ss, const char* tier_name, bool reprint,
             f.s = &s;
             TierState& ts = s.tiers[int(*t)];
             f.reused = reprint && static_cast<bool>(ts.negative);
-            s.progress_id = "p" + std::to_string(g_next_id++);
-            s.cancel.store(false);
-            s.nodes_done.store(0);
-            s.nodes_total = f.reused ? 1 : 2;
-            s.done = false;
+            f.pid = s.begin_progress(!f.reused);
             s.tier_source(*t);
             RenderCtx ctx{s.pool, s.stream};
+            ctx.progress = &s.progress;
             ctx.rho_tier = s.rho(ts);
             ctx.print_mode = s.print_mode;
             ctx.print_bins = s.print_bins;
@@ -876,13 +949,13 @@ void render_batch(std::vector<Session*> ss, const char* tier_name, bool reprint,
             }
             ctx.print_seed = s.draw_print_seed();
             ctx.pitch_um = ts.pitch_um;
-            s.node();
             const uint32_t nw = ts.negative.w, nh = ts.negative.h;
             f.img = output_acquire(e.device, nw, nh);
             f.neg = ts.negative.data();
             // a session on the spectral-mode print kernel stays on its own stream
             f.fused = s.print_mode < 0 && scan_args(s.pipe, ctx.rho_tier, nw, nh, f.img->stride_px, f.sa);
             if (f.fused) {
+                print_nodes(ctx, *s.pipe.print);
                 f.pa = print_args(s.pipe, s.live, uint32_t(ts.negative.pixels()));
                 f.glare = glare_plane(ctx, s.pipe, nw, nh);  // on the session's stream, before its ready event
                 f.pa.glare = f.glare ? f.glare.data() : nullptr;
@@ -956,7 +1029,11 @@ void render_batch(std::vector<Session*> ss, const char* tier_name, bool reprint,
             if (f.s) (void)cudaStreamSynchronize(f.s->stream);
             if (f.img) output_release(f.img);
             f.img = nullptr;
-            if (f.developed) f.s->tiers[int(*t)].negative = Plane{};
+            if (f.s) f.s->progress.finish(false, std::nullopt);
+            if (f.developed) {
+                f.s->tiers[int(*t)].negative = Plane{};
+                f.s->tiers[int(*t)].applied_ev.reset();
+            }
         }
         try {
             throw;
@@ -972,7 +1049,7 @@ void render_batch(std::vector<Session*> ss, const char* tier_name, bool reprint,
     for (size_t i = 0; i < n; ++i) {
         BatchFrame& f = fr[i];
         Session& s = *f.s;
-        s.done = true;
+        s.progress.finish(true, s.tiers[int(*t)].applied_ev);
         spk_result& o = out[i];
         o.rgba16 = f.img->host;
         o.texture = f.img;
@@ -983,7 +1060,7 @@ void render_batch(std::vector<Session*> ss, const char* tier_name, bool reprint,
         o.reprint = f.reused ? 1 : 0;
         o.negative_was_cached = f.reused ? 1 : 0;
         std::memset(o.progress_id, 0, sizeof o.progress_id);
-        std::strncpy(o.progress_id, s.progress_id.c_str(), sizeof o.progress_id - 1);
+        std::strncpy(o.progress_id, f.pid.c_str(), sizeof o.progress_id - 1);
         dms.push_back(json::Value(done_ms[i]));
     }
     r["plan"] = plan.empty() ? std::string("none") : plan;
@@ -1149,24 +1226,97 @@ SPK_API const char* spk_capabilities(spk_engine* engine) {
 
 SPK_API const char* spk_params_schema(spk_engine* engine) { return engine ? schema_json().c_str() : ""; }
 
+// The memory report in the reference's shape (src/session/engine.cpp:246-319): {total_bytes, pool,
+// persistent, pressure}. Here "pool" is the per-frame scratch of CUDA's stream-ordered device pool, and
+// "persistent" what outlives a render: the cudaMalloc'd tables (the engine's cached pipelines, output
+// images excluded) plus each session's frame, tier images and cached negatives, which live in the same
+// device pool but are held from render to render. total_bytes = pool.total_bytes + persistent.bytes. The
+// stream-ordered pool reuses freed memory in stream order, so nothing is pending and its free blocks are
+// not counted as buffers; no memory-pressure monitor or idle trim runs on this device.
 SPK_API const char* spk_memory_report(spk_engine* engine) {
     if (!engine) return "";
     Engine* e = E(engine);
     std::lock_guard<std::mutex> g(e->m);
-    size_t live = 0, negs = 0, tiers = 0;
+    const DeviceMemory dm = device_memory(e->device);
+    uint64_t held = 0, held_buffers = 0, src = 0, neg = 0, nneg = 0;
+    json::Array per;
     for (Session* s : e->sessions) {
-        live += s->pool.live_bytes();
+        uint64_t s_src = s->source ? s->source.bytes() : 0, s_neg = 0, s_n = 0, s_held = s_src;
+        held_buffers += s->source ? 1 : 0;
         for (const TierState& t : s->tiers) {
-            negs += t.negative ? t.negative.bytes() : 0;
-            if (t.source && t.source.data() != s->source.data()) tiers += t.source.bytes();
+            if (t.negative) {
+                s_neg += t.negative.bytes();
+                ++s_n;
+                ++held_buffers;
+            }
+            if (t.source && t.source.data() != s->source.data()) {
+                s_held += t.source.bytes();
+                ++held_buffers;
+            }
         }
+        if (s->meter_image && s->meter_image.data() != s->tiers[int(Tier::Live)].source.data()) {
+            s_held += s->meter_image.bytes();
+            ++held_buffers;
+        }
+        s_held += s_neg;
+        json::Value r;
+        r["session_id"] = s->id;
+        r["source_bytes"] = double(s_src);
+        r["cached_negative_bytes"] = double(s_neg);
+        r["negatives"] = double(s_n);
+        per.push_back(std::move(r));
+        src += s_src;
+        neg += s_neg;
+        nneg += s_n;
+        held += s_held;
     }
+    auto minus = [](uint64_t a, uint64_t b) { return a > b ? a - b : uint64_t(0); };
+    const uint64_t pool_total = minus(dm.reserved, held), pool_live = minus(dm.used, held);
+    const uint64_t live_buffers = minus(dm.scratch_live, held_buffers);
+    json::Value audit;
+    audit["allocations"] = double(dm.scratch_allocations);
+    audit["reuses"] = 0.0;  // the device pool's own reuse is not observable
+    audit["persistent_allocations"] = double(dm.persistent_allocations);
+    audit["reuse_bytes_requested"] = 0.0;
+    audit["reuse_bytes_taken"] = 0.0;
+    audit["reuse_max_taken"] = 0.0;
+    audit["reuse_max_taken_for_request"] = 0.0;
+    audit["pending_held"] = 0.0;
+    audit["live_underflows"] = 0.0;
+    audit["over_releases"] = 0.0;
+    audit["reclaim_while_encoding"] = 0.0;
+    json::Value pool;
+    pool["total_bytes"] = double(pool_total);
+    pool["live_bytes"] = double(pool_live);
+    pool["free_bytes"] = double(minus(dm.reserved, dm.used));
+    pool["pending_bytes"] = 0.0;
+    pool["buffers"] = double(live_buffers);
+    pool["live_buffers"] = double(live_buffers);
+    pool["free_buffers"] = 0.0;
+    pool["pending_buffers"] = 0.0;
+    pool["frame_high_water_bytes"] = double(minus(dm.used_high, held));
+    pool["audit"] = std::move(audit);
+    json::Value pers;
+    pers["bytes"] = double(dm.persistent_bytes + held);
+    pers["buffers"] = double(dm.persistent_live + held_buffers);
+    pers["file_backed_bytes"] = 0.0;
+    pers["file_backed_buffers"] = 0.0;
+    pers["source_bytes"] = double(src);
+    pers["cached_negative_bytes"] = double(neg);
+    pers["negatives"] = double(nneg);
+    pers["sessions"] = std::move(per);
+    json::Value pr;
+    pr["monitor"] = false;
+    pr["warn_events"] = 0.0;
+    pr["critical_events"] = 0.0;
+    pr["critical_pending"] = false;
+    pr["idle_trim_seconds"] = 0.0;
+    pr["idle_trims"] = 0.0;
     json::Value r;
-    r["pool_live_bytes"] = double(live);
-    r["pool_reserved_bytes"] = double(device_pool_reserved(e->device));
-    r["cached_negative_bytes"] = double(negs);
-    r["tier_image_bytes"] = double(tiers);
-    r["sessions"] = unsigned(e->sessions.size());
+    r["total_bytes"] = double(pool_total + dm.persistent_bytes + held);
+    r["pool"] = std::move(pool);
+    r["persistent"] = std::move(pers);
+    r["pressure"] = std::move(pr);
     e->memory_report = json::write(r);
     return e->memory_report.c_str();
 }
@@ -1590,21 +1740,13 @@ SPK_API spk_status spk_output_transform(spk_engine* engine, const char* src, con
 
 SPK_API void spk_cancel(spk_session* session, const char* progress_id) {
     if (!session) return;
-    Session* s = S(session);
-    (void)progress_id;
-    s->cancel.store(true);
+    S(session)->progress.cancel(progress_id);
 }
 
 SPK_API spk_status spk_progress(spk_session* session, const char* progress_id, char** out_json) {
     if (!session) return invalid("session is NULL");
     return guarded([&] {
-        Session& s = *S(session);
-        json::Value r;
-        r["progress_id"] = s.progress_id;
-        r["nodes_done"] = unsigned(s.nodes_done.load());
-        r["nodes_total"] = s.nodes_total;
-        r["done"] = s.done;
-        if (progress_id && *progress_id && s.progress_id != progress_id) fail_user("unknown progress id");
+        const json::Value r = S(session)->progress.snapshot(progress_id);
         put_json(out_json, json::write(r));
         return SPK_OK;
     });
@@ -2277,6 +2419,13 @@ SPK_API spk_status spkx_philox(const uint32_t* counters, const uint32_t* keys, u
         cuda_check(cudaMemcpyAsync(out, dout.p, n * 16ull, cudaMemcpyDeviceToHost, s), "copy");
         cuda_check(cudaStreamSynchronize(s), "philox");
     });
+}
+
+SPK_API spk_status spkx_test_set_tc_wait_limit(int64_t cycles) {
+    last_error::clear();
+    if (cycles < 0) return invalid("a wait limit is a count of SM clocks, 0 or more");
+    dev::set_tc_wait_limit(cycles);
+    return SPK_OK;
 }
 
 SPK_API spk_status spkx_gaussian(const float* in, float* out, uint32_t w, uint32_t h, const double* sigma3) {

@@ -600,12 +600,17 @@ Plane develop(RenderCtx& ctx, const Pipeline& p, const Plane& tier_source, uint3
               const std::optional<HalationOverride>& hov, float* counts_out, float* lam_out) {
     const FilmSetup& f = *p.film;
     Plane source = tier_source;
+    if (f.decode) ctx.node("preprocess.decode");
+    if (!geometry_identity(f.params)) ctx.node("preprocess.geometry");
     if (f.decode || !geometry_identity(f.params)) {
         Stage st(ctx, "prepare");
         source = prepare_source(ctx.pool, ctx.stream, tier_source, f.params, f.decode, uint32_t(f.input_space.cctf));
     }
     const uint32_t w = source.w, h = source.h;
     Plane H = make_plane(ctx.pool, w, h);
+    if (f.params.b(P::auto_exposure)) ctx.node("filming.auto_exposure");
+    ctx.node("filming.upsample");
+    ctx.node("filming.exposure_compensation");
     {
         Stage st(ctx, "expose");
         ExposeArgs ea = expose_args(f, source.pixels());
@@ -616,16 +621,19 @@ Plane develop(RenderCtx& ctx, const Pipeline& p, const Plane& tier_source, uint3
         dev::expose(source.data(), H.data(), p.dev.table.as<float>(), ea, ctx.stream);
     }
     if (const double bev = f.params.f(P::halation_boost_ev); bev != 0.0) {
+        ctx.node("filming.boost");
         Stage st(ctx, "boost");
         run_boost(ctx, H, bev);
     }
     if (headroom_applies(f.halation)) {
         // the back-reflection halation's highlight headroom, its clip the frame maximum kept on the device
+        ctx.node("filming.headroom");
         Stage st(ctx, "headroom");
         DevBuffer mx = ctx.pool.acquire(16);
         dev::plane_max(H.data(), 3 * H.pixels(), mx.as<uint32_t>(), ctx.stream);
         dev::headroom(H.data(), uint32_t(H.pixels()), mx.as<uint32_t>(), f32(f.halation.headroom_ev), ctx.stream);
     }
+    if (f.params.f(P::lens_blur_um) > 0.0) ctx.node("filming.lens_blur");
     if (const double s = film_lens_blur_px(ctx, f); s > 0.0) {
         Stage st(ctx, "lens_blur");
         Plane Hb = make_plane(ctx.pool, w, h);
@@ -635,11 +643,16 @@ Plane develop(RenderCtx& ctx, const Pipeline& p, const Plane& tier_source, uint3
     {
         const HalationPlan pl = film_halation(ctx, f, hov);
         if (pl.scatter || pl.bounce) {
+            ctx.node("filming.halation");
             Stage st(ctx, "halation");
             apply_halation(ctx, pl, H);
         }
     }
     DevelopPlan dp = develop_plan(ctx, p, w, film_seed, counts_out, lam_out);
+    ctx.node("filming.log");  // log, curves, couplers and grain are fused into the develop launches
+    ctx.node("filming.curves");
+    if (f.couplers) ctx.node("filming.couplers");
+    if (f.grain) ctx.node("filming.grain");
     Plane chi;
     if (f.couplers) {
         Stage st(ctx, "couplers");
@@ -919,9 +932,62 @@ void print_scan_banded(RenderCtx& ctx, const Pipeline& p, const LiveParams& live
 }
 }  // namespace
 
+uint32_t film_node_count(const FilmSetup& f) {
+    uint32_t n = 4;  // upsample, exposure compensation, log and curves
+    if (f.decode) ++n;
+    if (!geometry_identity(f.params)) ++n;
+    if (f.params.b(P::auto_exposure)) ++n;
+    if (f.params.f(P::halation_boost_ev) != 0.0) ++n;
+    if (headroom_applies(f.halation)) ++n;
+    if (f.params.f(P::lens_blur_um) > 0.0) ++n;
+    if (f.halation.active) ++n;
+    if (f.couplers) ++n;
+    if (f.grain) ++n;
+    return n;
+}
+
+uint32_t print_node_count(const PrintSetup& s) {
+    const bool printed = !s.scanned;
+    uint32_t n = 5;  // scan, to_rgb, gamut, scanner and encode (the desktop variant keeps the scanner)
+    if (printed) n += 3;
+    if (s.levels_active()) ++n;
+    if (printed && s.glare_draws()) ++n;
+    if (printed && s.edr) ++n;
+    return n;
+}
+
+namespace {
+// labels before the print launch: enlarger, gain, paper, scan, levels, glare, to_rgb, gamut
+void print_nodes_head(RenderCtx& ctx, const PrintSetup& s) {
+    const bool printed = !s.scanned;
+    if (printed) {
+        ctx.node("printing.enlarger");
+        ctx.node("printing.gain");
+        ctx.node("printing.paper");
+    }
+    ctx.node("scanning.scan");
+    if (s.levels_active()) ctx.node("scanning.levels");
+    if (printed && s.glare_draws()) ctx.node("scanning.glare");
+    ctx.node("scanning.to_rgb");
+    ctx.node("scanning.gamut");
+}
+// labels before the scanner launch: scanner, EDR, encode
+void print_nodes_tail(RenderCtx& ctx, const PrintSetup& s) {
+    ctx.node("scanning.scanner");
+    if (!s.scanned && s.edr) ctx.node("scanning.edr");
+    ctx.node("scanning.encode");
+}
+}  // namespace
+
+void print_nodes(RenderCtx& ctx, const PrintSetup& s) {
+    print_nodes_head(ctx, s);
+    print_nodes_tail(ctx, s);
+}
+
 bool print_scan_encode(RenderCtx& ctx, const Pipeline& p, const LiveParams& live, const Plane& negative,
                        OutputImage* img, bool to_host) {
     const PrintSetup& s = *p.print;
+    print_nodes_head(ctx, s);
     const uint32_t w = negative.w, h = negative.h;
     Plane rgb = make_plane(ctx.pool, w, h);
     Plane glare;
@@ -933,6 +999,7 @@ bool print_scan_encode(RenderCtx& ctx, const Pipeline& p, const LiveParams& live
     ScanArgs sa;
     const bool tiled = scan_args(p, ctx.rho_tier, w, h, img->stride_px, sa);
     if (to_host && tiled && ctx.print_mode < 0 && ctx.copy_stream && ctx.band_events && h > kBandRows) {
+        print_nodes_tail(ctx, s);
         Stage st(ctx, "print_scanner");
         print_scan_banded(ctx, p, live, negative, rgb, img, sa, gl);
         return true;
@@ -941,6 +1008,7 @@ bool print_scan_encode(RenderCtx& ctx, const Pipeline& p, const LiveParams& live
         Stage st(ctx, "print");
         print_stage(ctx, p, live, negative, rgb, gl);
     }
+    print_nodes_tail(ctx, s);
     if (tiled) {
         // the scanner's blurs on the FIR branch: one tiled pass from the print output to RGBA16
         Stage st(ctx, "scanner");

@@ -44,9 +44,29 @@ Plane glare_plane(RenderCtx& ctx, const Pipeline& p, uint32_t w, uint32_t h);
 // Upload a pipeline's tables (stream-ordered, then synchronised).
 void upload_tables(Pool& pool, cudaStream_t s, Pipeline& p);
 
+// Receives the render's progress nodes: one call per stage of the reference's pipeline, with its label
+// (reference src/core/render.hpp:52-84), before the stage's work is enqueued. The session's record checks
+// its cancel flag there and throws SPK_ERR_CANCELLED.
+class ProgressSink {
+public:
+    virtual void node(const char* label) = 0;
+
+protected:
+    ~ProgressSink() = default;
+};
+
+// The node() calls a develop and a print make (reference src/film/develop.cpp:64-78,
+// src/print/run.cpp:89-99): the totals behind the progress percentage.
+uint32_t film_node_count(const FilmSetup& f);
+uint32_t print_node_count(const PrintSetup& s);
+
 struct RenderCtx {
     Pool& pool;
     cudaStream_t stream;
+    ProgressSink* progress = nullptr;  // null: no progress, not cancellable (warm-up, adjoint, hooks)
+    void node(const char* label) const {
+        if (progress) progress->node(label);
+    }
     double pitch_um = 0.0;
     double rho_tier = 1.0;
     std::optional<double> ae_ev = std::nullopt;
@@ -101,6 +121,9 @@ bool scan_args(const Pipeline& p, double rho_tier, uint32_t w, uint32_t h, uint3
 // (the stream then orders after the copies); false: no host copy was made.
 bool print_scan_encode(RenderCtx& ctx, const Pipeline& p, const LiveParams& live, const Plane& negative,
                        OutputImage* img, bool to_host = false);
+// The print side's progress nodes for a print that runs as one fused launch chain (the batch plans):
+// every label of print_node_count, in order.
+void print_nodes(RenderCtx& ctx, const PrintSetup& s);
 
 // The adjoint of the render. The differentiated output y is the scanned linear RGB (print, scanner lens
 // blur and unsharp mask; before the output transfer function and the 16-bit encode) of the source frame,

@@ -108,6 +108,7 @@ EXT = {
     "spkx_engine_batch_plan": (I32, [P, C]),
     "spkx_session_set_print_mode": (I32, [P, C, U32]),
     "spkx_print_negative": (I32, [P, P, U32, U32, P, U32, P, ctypes.POINTER(ctypes.c_double)]),
+    "spkx_test_set_tc_wait_limit": (I32, [ctypes.c_int64]),
 }
 
 REF_EXT = {

@@ -66,9 +66,34 @@ def setup_f64(lib, resources, delta, pitch):
     return lib.take_json(out)
 
 
-def lsb_stats(a, b):
+def lsb_stats(a, b, label=None):
+    """|a - b| of the colour channels of two RGBA16 images in LSB16: max, mean, share and count above 1
+    (recorded under the label, or the running test's id, when SPK_TEST_STATS is set)."""
     d = np.abs(a.astype(np.int64) - b.astype(np.int64))[..., :3]
-    return {"max": int(d.max()), "mean": float(d.mean()), "frac_gt1": float((d > 1).mean())}
+    st = {"max": int(d.max()), "mean": float(d.mean()), "frac_gt1": float((d > 1).mean()),
+          "n_gt1": int((d > 1).sum()), "n": int(d.size)}
+    record(label or os.environ.get("PYTEST_CURRENT_TEST", "?").split(" ")[0], st)
+    return st
+
+
+def record(label, stats):
+    """Append a gate's measured figures to the JSON-lines file named by SPK_TEST_STATS (when set), so that a
+    run of the suite leaves the maxima behind, not only a pass."""
+    path = os.environ.get("SPK_TEST_STATS")
+    if path:
+        with open(path, "a") as f:
+            f.write(json.dumps({"gate": label, **stats}) + "\n")
+
+
+def lsb_gate(got, want, label, max_lsb=1, max_over=0):
+    """RGBA16 agreement: alpha equal, and every colour channel within max_lsb LSB16 of want except at most
+    max_over of them (which stay within 64). The message carries the maximum and the count above 1."""
+    st = lsb_stats(got, want, label)
+    d = np.abs(got.astype(np.int64) - want.astype(np.int64))[..., :3]
+    st["n_over"] = int((d > max_lsb).sum())
+    assert (got[..., 3] == want[..., 3]).all(), (label, "alpha differs")
+    assert st["n_over"] <= max_over and (st["n_over"] == 0 or st["max"] <= 64), (label, st)
+    return st
 
 
 def golden(name):
