@@ -53,7 +53,10 @@ void boost(float* p, size_t n, float x0, float r, float a, float k, cudaStream_t
 
 // RGB -> film exposure H (Mitchell bicubic of the spectral table, L x L float4 texels), times the
 // compensation gain.
-void expose(const float* rgb, float* h, const float* table4, const ExposeArgs& a, cudaStream_t s);
+// patches (may be null): the table as 4 x 4 patches (kPatchFloats floats per base pair, (L - 1)^2 pairs),
+// read by the vectorised kernel when both planes are 16-byte aligned; else the texel kernel reads table4.
+void expose(const float* rgb, float* h, const float* table4, const float* patches, const ExposeArgs& a,
+            cudaStream_t s);
 
 // Separable FIR: vertical pass in -> out (no accumulation).
 void fir_v(const float* in, float* out, uint32_t w, uint32_t h, const FirTaps& t, cudaStream_t s);

@@ -32,6 +32,21 @@ void upload_tables(Pool& pool, cudaStream_t s, Pipeline& p) {
         for (size_t i = 0; i < texels; ++i)
             for (size_t c = 0; c < 3; ++c) t4[4 * i + c] = f.table32[3 * i + c];
         upload(pool, s, p.dev.table, t4.data(), t4.size() * sizeof(float));
+        // the 4 x 4 patch of every base pair (ba, bb): rows and columns base - 1 .. base + 2, reflected at
+        // the table's edges as the bicubic's taps are
+        const int L = int(f.L);
+        auto reflect = [L](int i) { return i < 0 ? -i : (i >= L ? 2 * (L - 1) - i : i); };
+        std::vector<float> pt(size_t(L - 1) * size_t(L - 1) * kPatchFloats);
+        for (int ba = 0; ba < L - 1; ++ba)
+            for (int bb = 0; bb < L - 1; ++bb) {
+                float* o = pt.data() + (size_t(ba) * size_t(L - 1) + size_t(bb)) * kPatchFloats;
+                for (int i = 0; i < 4; ++i)
+                    for (int j = 0; j < 4; ++j)
+                        for (int c = 0; c < 3; ++c)
+                            o[3 * (4 * i + j) + c] =
+                                f.table32[3 * (size_t(reflect(ba - 1 + i)) * size_t(L) + size_t(reflect(bb - 1 + j))) + c];
+            }
+        upload(pool, s, p.dev.patches, pt.data(), pt.size() * sizeof(float));
     }
     std::vector<float> c(8 * size_t(f.K));
     std::memcpy(c.data(), f.cx.data(), f.K * sizeof(float));
@@ -618,7 +633,7 @@ Plane develop(RenderCtx& ctx, const Pipeline& p, const Plane& tier_source, uint3
             ea.ae_gain = f32(std::pow(2.0, *ctx.ae_ev));
             ea.apply_ae = 1;
         }
-        dev::expose(source.data(), H.data(), p.dev.table.as<float>(), ea, ctx.stream);
+        dev::expose(source.data(), H.data(), p.dev.table.as<float>(), p.dev.patches.as<float>(), ea, ctx.stream);
     }
     if (const double bev = f.params.f(P::halation_boost_ev); bev != 0.0) {
         ctx.node("filming.boost");
@@ -1143,7 +1158,7 @@ void render_vjp(RenderCtx& ctx, const Pipeline& p, const LiveParams& live, const
     // ---- forward, keeping what the adjoint needs ----
     Plane H0 = make_plane(ctx.pool, w, h);
     const ExposeArgs ea = expose_args(f, n);
-    dev::expose(source.data(), H0.data(), p.dev.table.as<float>(), ea, ctx.stream);
+    dev::expose(source.data(), H0.data(), p.dev.table.as<float>(), p.dev.patches.as<float>(), ea, ctx.stream);
     const double s_lens = film_lens_blur_px(ctx, f);
     Plane H1 = H0;
     if (s_lens > 0.0) {

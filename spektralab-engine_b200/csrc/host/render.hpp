@@ -19,6 +19,7 @@ namespace spkb {
 // A film/print set-up pair with its device tables, built once per pipeline.
 struct DeviceTables {
     DevBuffer table;              // L x L spectral table, float4 texels (R, G, B, 0)
+    DevBuffer patches;            // the same as (L - 1)^2 patches of 4 x 4 RGB texels (kPatchFloats each)
     DevBuffer curves;             // x[K] | inv[K] | y[3K] | y0[3K] (the DIR couplers' pre-inverted curve)
     DevBuffer gaxis, ginv, glayers;
     DevBuffer paper;              // x[K] | r[K] | y[K][3]

@@ -21,6 +21,8 @@ struct ExposeArgs {
     uint32_t L;        // table size; the table is L x L float4 texels, [i][j] = (R, G, B, 0)
     uint32_t n;        // pixels
 };
+// floats of one 4 x 4 patch of the spectral table (16 RGB texels)
+#define kPatchFloats 48u
 
 // One separable FIR Gaussian: taps -r..r per channel (a channel without a FIR blur holds the delta).
 struct FirTaps {
