@@ -323,6 +323,75 @@ __device__ __forceinline__ void iir_line(const float* src, float* work, float* d
     }
 }
 
+// The same line with its tangent along sigma (forward mode): the coefficients' derivatives dq (the same
+// layout as q) and the input's tangent src_dot (nullptr: zero) give the output's tangent
+//   forward:  w'[i] = dB x[i] + B x'[i] + sum_j (dB_j w[i-j] + B_j w'[i-j]), w'[-1..-3] = x'[0]
+//   backward: y'[i] = dB u[i] + B u'[i] + sum_j (dB_j y[i+j] + B_j y'[i+j]), y'[n..n+2] = u'[n-1]
+// with u = the forward pass rounded to binary32 (its tangent is not rounded). Work planes: the forward
+// pass's value and tangent.
+__device__ __forceinline__ void iir_line_tangent(const float* src, const float* src_dot, float* work, float* work_dot,
+                                                 float* dst, float* dst_dot, size_t base, size_t stride, uint32_t n,
+                                                 const IirCoefs& q, const IirCoefs& dq, int c) {
+    const double B = q.B[c], B1 = q.B1[c], B2 = q.B2[c], B3 = q.B3[c];
+    const double dB = dq.B[c], dB1 = dq.B1[c], dB2 = dq.B2[c], dB3 = dq.B3[c];
+    double w1 = double(src[base]), w2 = w1, w3 = w1;
+    double t1 = src_dot ? double(src_dot[base]) : 0.0, t2 = t1, t3 = t1;
+    for (uint32_t i = 0; i < n; ++i) {
+        const size_t o = base + i * stride;
+        const double x = double(src[o]), xd = src_dot ? double(src_dot[o]) : 0.0;
+        const double v = ((B * x + B1 * w1) + B2 * w2) + B3 * w3;
+        const double vd = dB * x + B * xd + (dB1 * w1 + B1 * t1) + (dB2 * w2 + B2 * t2) + (dB3 * w3 + B3 * t3);
+        w3 = w2;
+        w2 = w1;
+        w1 = v;
+        t3 = t2;
+        t2 = t1;
+        t1 = vd;
+        work[o] = float(v);
+        work_dot[o] = float(vd);
+    }
+    const size_t last = base + size_t(n - 1) * stride;
+    double y1 = double(work[last]), y2 = y1, y3 = y1;
+    double s1 = double(work_dot[last]), s2 = s1, s3 = s1;
+    for (uint32_t k = n; k-- > 0;) {
+        const size_t o = base + k * stride;
+        const double u = double(work[o]), ud = double(work_dot[o]);
+        const double v = ((B * u + B1 * y1) + B2 * y2) + B3 * y3;
+        const double vd = dB * u + B * ud + (dB1 * y1 + B1 * s1) + (dB2 * y2 + B2 * s2) + (dB3 * y3 + B3 * s3);
+        y3 = y2;
+        y2 = y1;
+        y1 = v;
+        s3 = s2;
+        s2 = s1;
+        s1 = vd;
+        dst[o] = float(v);
+        dst_dot[o] = float(vd);
+    }
+}
+
+// the blur's tangent along sigma, one thread per line: rows (vertical = 0) or columns (vertical = 1); a
+// channel outside q.mask passes its value and tangent through
+__global__ void k_iir_tangent(const float* __restrict__ in, const float* in_dot, float* work, float* work_dot,
+                              float* out, float* out_dot, uint32_t w, uint32_t h, int vertical,
+                              const __grid_constant__ IirCoefs q, const __grid_constant__ IirCoefs dq) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t lines = vertical ? 3u * w : 3u * h;
+    if (t >= lines) return;
+    const uint32_t c = t % 3u;
+    const size_t base = vertical ? size_t(t) : 3 * size_t(t / 3u) * w + c;
+    const size_t stride = vertical ? 3 * size_t(w) : 3;
+    const uint32_t n = vertical ? h : w;
+    if (((q.mask >> c) & 1u) == 0u) {
+        for (uint32_t i = 0; i < n; ++i) {
+            const size_t o = base + i * stride;
+            out[o] = in[o];
+            out_dot[o] = in_dot ? in_dot[o] : 0.0f;
+        }
+        return;
+    }
+    iir_line_tangent(in, in_dot, work, work_dot, out, out_dot, base, stride, n, q, dq, int(c));
+}
+
 __global__ void k_iir_h(const float* __restrict__ in, float* out, uint32_t w, uint32_t h,
                         const __grid_constant__ IirCoefs q) {
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -495,6 +564,25 @@ struct DeferredDraw {
 };
 // kinds: 0 product method (lam < 10 or NaN); 1 attempt 0 needs the full test; 2 attempt 0 rejected
 
+// log(k!) for k = 0 .. kLgammaTable - 1, each the sampler's own spk_lgamma_k(k + 1) computed by this
+// device once per process (k_lgamma_table): the full test's largest single cost, a table read instead.
+constexpr uint32_t kLgammaTable = 4096;
+__device__ float g_lgamma[kLgammaTable];
+
+__global__ void k_lgamma_table() {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < kLgammaTable) g_lgamma[k] = spk_lgamma_k(SPK_ADD(float(k), 1.0f));
+}
+
+// spk_ptrs_test with log(k!) from the table while k is in it (k >= 0 and integral here)
+__device__ __forceinline__ int ptrs_test_table(const spk_ptrs* p, float V, float k, float us) {
+    const float L = SPK_SUB(SPK_ADD(spk_logf(V), p->loginvalpha),
+                            spk_logf(SPK_ADD(SPK_DIV(p->a, SPK_MUL(us, us)), p->b)));
+    const float lg = k < float(kLgammaTable) ? g_lgamma[int(k)] : spk_lgamma_k(SPK_ADD(k, 1.0f));
+    const float Rt = SPK_SUB(SPK_ADD(-p->lam, SPK_MUL(k, p->loglam)), lg);
+    return L <= Rt;
+}
+
 // The rest of a deferred draw: attempt 0's pending full test (kind 1), then attempts 1..63 exactly as
 // spk_ptrs_from runs them, with one copy of the test, the squeeze and the generator in the loop. The
 // test's own constants (log lam, 1 / alpha) are formed here, for the draws that reach it.
@@ -520,7 +608,7 @@ __device__ __forceinline__ void finish_draw(const DeferredDraw& d, uint32_t seed
         int state = kind == 1u ? SPK_PTRS_TEST : SPK_PTRS_REJECT;
         for (int it = 1;; ++it) {
             // state: the outcome of attempt it - 1's squeeze
-            if (state == SPK_PTRS_ACCEPT || (state == SPK_PTRS_TEST && spk_ptrs_test(&p, V, k, us))) {
+            if (state == SPK_PTRS_ACCEPT || (state == SPK_PTRS_TEST && ptrs_test_table(&p, V, k, us))) {
                 value = k;
                 break;
             }
@@ -782,6 +870,15 @@ void expose(const float* rgb, float* h, const float* table4, const float* patche
     k_expose<<<div_up(a.n, 256), 256, 0, s>>>(rgb, h, reinterpret_cast<const float4*>(table4), a);
 }
 
+void iir_tangent(const float* in, const float* in_dot, float* work, float* work_dot, float* out, float* out_dot,
+                 uint32_t w, uint32_t h, bool vertical, const IirCoefs& c, const IirCoefs& dc, cudaStream_t s) {
+    const uint32_t lines = vertical ? 3u * w : 3u * h;
+    if (lines == 0) return;
+    Probe p("iir_tangent", s);
+    k_iir_tangent<<<div_up(lines, 128), 128, 0, s>>>(in, in_dot, work, work_dot, out, out_dot, w, h, vertical ? 1 : 0,
+                                                     c, dc);
+}
+
 void fir_v(const float* in, float* out, uint32_t w, uint32_t h, const FirTaps& t, cudaStream_t s) {
     const dim3 b(32, 8), g(div_up(w, 32), div_up(h, 8));
     Probe p("fir_v", s);
@@ -820,9 +917,22 @@ void copy(const float* x, float* out, size_t pixels, cudaStream_t s) {
     k_copy<<<unsigned((n + 255) / 256), 256, 0, s>>>(x, out, n);
 }
 
+void develop_prepare(cudaStream_t s) {
+    static std::mutex m;
+    static bool done[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return;
+    std::lock_guard<std::mutex> g(m);
+    if (done[dev]) return;
+    k_lgamma_table<<<div_up(kLgammaTable, 256), 256, 0, s>>>();
+    // once written and waited for, every later launch on any stream reads the table
+    if (cudaStreamSynchronize(s) == cudaSuccess && cudaGetLastError() == cudaSuccess) done[dev] = true;
+}
+
 void develop(const float* exposure, float* out, const DevelopArgs& a, uint32_t w, uint32_t h, cudaStream_t s) {
     if (uint64_t(w) * h == 0) return;
     if (a.grain && a.mode == 0) {
+        develop_prepare(s);
         const uint32_t bx = div_up(w, kDrawWarps * 32);
         Probe p("develop_layers", s);
         k_develop_layers<<<bx * h, kDrawWarps * 32, 0, s>>>(exposure, out, w, bx, a);

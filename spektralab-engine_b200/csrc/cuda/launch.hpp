@@ -69,6 +69,10 @@ void iir_h(const float* in, float* out, uint32_t w, uint32_t h, const IirCoefs& 
 // pass; out := y, 0 + w y or acc + w y.
 void iir_v(float* work, float* out, const float* acc, uint32_t w, uint32_t h, const IirCoefs& c, int mode,
            const float weight[3], cudaStream_t s);
+// The recursive Gaussian of one direction with its tangent along sigma (the adjoint's sigma gradient):
+// (in, in_dot) -> (out, out_dot), dc the coefficients' derivatives; work planes hold the forward pass.
+void iir_tangent(const float* in, const float* in_dot, float* work, float* work_dot, float* out, float* out_dot,
+                 uint32_t w, uint32_t h, bool vertical, const IirCoefs& c, const IirCoefs& dc, cudaStream_t s);
 // out = a x + b y per channel (y reads as 0 when y == nullptr).
 void lincomb(const float* x, const float* y, float* out, size_t pixels, const float a[3], const float b[3],
              cudaStream_t s);
@@ -79,6 +83,9 @@ void coupler_source(const float* exposure, float* chi, const CouplerArgs& a, cud
 
 // log10 exposure -> density curves -> grain draw (grain mode) or density (no grain).
 void develop(const float* exposure, float* out, const DevelopArgs& a, uint32_t w, uint32_t h, cudaStream_t s);
+// The grain's log(k!) table on the current device (once per process; waits for it on s). The engine calls
+// it at creation; develop calls it too, before its first grain launch on a device.
+void develop_prepare(cudaStream_t s);
 
 // negative density -> linear output RGB (enlarger, gain, paper, scan, XYZ -> RGB, CAM16 gamut).
 void print(const float* neg, float* rgb, const PrintArgs& a, cudaStream_t s);

@@ -27,52 +27,91 @@ namespace {
 
 constexpr uint32_t kPrintThreads = 128;
 
+// Every kPolyEvery-th wavelength (l % kPolyEvery == kPolyEvery - 1) takes its 2^e from the FMA-pipe
+// polynomial (exp2_poly2) instead of the special-function unit; 0: none. The split balances the two pipes.
+#ifndef SPKB_PRINT_POLY_EVERY
+#define SPKB_PRINT_POLY_EVERY 0
+#endif
+constexpr int kPolyEvery = SPKB_PRINT_POLY_EVERY;
+
+// Packed pixel pairs per thread (two pixels each): the constant-bank table operands of a wavelength are
+// shared by all of them.
+#ifndef SPKB_PRINT_PAIRS
+#define SPKB_PRINT_PAIRS 1
+#endif
+constexpr uint32_t kPairs = SPKB_PRINT_PAIRS;
+
 __device__ __forceinline__ float2 dup(const F32Pair& p) { return make_float2(p.x, p.y); }
 
-// R_k for a pair of pixels: sum over l of 2^(e(l)) w_k(l), ascending l
-__device__ __forceinline__ void spectral2(const SpectralPairs& t, float2 d0, float2 d1, float2 d2, float2& r0,
-                                          float2& r1, float2& r2) {
-    r0 = r1 = r2 = make_float2(0.0f, 0.0f);
+// R_k for NP pairs of pixels: sum over l of 2^(e(l)) w_k(l), ascending l. Each table pair, read once per
+// wavelength, serves every pair of pixels. Every kPolyEvery-th wavelength takes 2^e from the FMA-pipe
+// polynomial (the loop is unrolled, so the choice is made at compile time).
+template <int NP>
+__device__ __forceinline__ void spectral(const SpectralPairs& t, const float2 (&d)[NP][3], float2 (&r)[NP][3]) {
+#pragma unroll
+    for (int i = 0; i < NP; ++i) r[i][0] = r[i][1] = r[i][2] = make_float2(0.0f, 0.0f);
 #pragma unroll
     for (int l = 0; l < SPKB_NL; ++l) {
-        const float2 e =
-            __ffma2_rn(d2, dup(t.e[3 * l + 2]), __ffma2_rn(d1, dup(t.e[3 * l + 1]), __fmul2_rn(d0, dup(t.e[3 * l]))));
-        const float2 T = make_float2(ex2_ftz(e.x), ex2_ftz(e.y));
-        r0 = __ffma2_rn(T, dup(t.w[3 * l]), r0);
-        r1 = __ffma2_rn(T, dup(t.w[3 * l + 1]), r1);
-        r2 = __ffma2_rn(T, dup(t.w[3 * l + 2]), r2);
+        const float2 e0 = dup(t.e[3 * l]), e1 = dup(t.e[3 * l + 1]), e2 = dup(t.e[3 * l + 2]);
+        const float2 w0 = dup(t.w[3 * l]), w1 = dup(t.w[3 * l + 1]), w2 = dup(t.w[3 * l + 2]);
+        const bool poly = kPolyEvery > 0 && l % kPolyEvery == kPolyEvery - 1;
+#pragma unroll
+        for (int i = 0; i < NP; ++i) {
+            const float2 e = __ffma2_rn(d[i][2], e2, __ffma2_rn(d[i][1], e1, __fmul2_rn(d[i][0], e0)));
+            const float2 T = poly ? exp2_poly2(e) : make_float2(ex2_ftz(e.x), ex2_ftz(e.y));
+            r[i][0] = __ffma2_rn(T, w0, r[i][0]);
+            r[i][1] = __ffma2_rn(T, w1, r[i][1]);
+            r[i][2] = __ffma2_rn(T, w2, r[i][2]);
+        }
     }
 }
 
-// pixels p0 and p0 + 1 (when p0 + 1 < n) of one frame
-__device__ __forceinline__ void print_pair(const PrintArgs& a, const float* __restrict__ neg, float* __restrict__ rgb,
-                                           uint32_t p0, uint32_t n) {
-    const bool two = p0 + 1 < n;
-    const float* s0 = neg + 3 * size_t(p0);
-    const float* s1 = two ? s0 + 3 : s0;
-    float2 d0 = make_float2(s0[0], s1[0]), d1 = make_float2(s0[1], s1[1]), d2 = make_float2(s0[2], s1[2]);
-    if (a.printed) {
-        float2 r0, r1, r2;
-        spectral2(a.enl, d0, d1, d2, r0, r1, r2);
-        d0 = make_float2(print_density(a, 0, r0.x), print_density(a, 0, r0.y));
-        d1 = make_float2(print_density(a, 1, r1.x), print_density(a, 1, r1.y));
-        d2 = make_float2(print_density(a, 2, r2.x), print_density(a, 2, r2.y));
+// Pixels p0 .. p0 + 2 kPairs - 1 of one frame (those below n): the spectral integrals on kPairs packed
+// pairs, the rest one pixel after the other.
+__device__ __forceinline__ void print_group(const PrintArgs& a, const float* __restrict__ neg, float* __restrict__ rgb,
+                                            uint32_t p0, uint32_t n) {
+    constexpr int NP = kPairs;
+    float2 d[NP][3];
+#pragma unroll
+    for (int i = 0; i < NP; ++i) {
+        const float* s0 = neg + 3 * size_t(min(p0 + 2 * i, n - 1));
+        const float* s1 = neg + 3 * size_t(min(p0 + 2 * i + 1, n - 1));
+#pragma unroll
+        for (int c = 0; c < 3; ++c) d[i][c] = make_float2(s0[c], s1[c]);
     }
-    float2 X, Y, Z;
-    spectral2(a.scan, d0, d1, d2, X, Y, Z);
+    float2 r[NP][3];
+    if (a.printed) {
+        spectral<NP>(a.enl, d, r);
+#pragma unroll
+        for (int i = 0; i < NP; ++i)
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+                d[i][c] = make_float2(print_density(a, c, r[i][c].x), print_density(a, c, r[i][c].y));
+    }
+    spectral<NP>(a.scan, d, r);
 #pragma unroll 1
-    for (uint32_t k = 0; k < 2u; ++k) {
-        if (k == 1u && !two) break;
-        float x = fmaxf(k ? X.y : X.x, 0.0f) + kTiny;
-        float y = fmaxf(k ? Y.y : Y.x, 0.0f) + kTiny;
-        float z = fmaxf(k ? Z.y : Z.x, 0.0f) + kTiny;
+    for (uint32_t k = 0; k < uint32_t(2 * NP); ++k) {
+        if (p0 + k >= n) break;
+        const uint32_t i = k / 2u;
+        const bool hi = (k & 1u) != 0u;
+        float x = 0.0f, y = 0.0f, z = 0.0f;
+#pragma unroll
+        for (int j = 0; j < NP; ++j)
+            if (uint32_t(j) == i) {
+                x = hi ? r[j][0].y : r[j][0].x;
+                y = hi ? r[j][1].y : r[j][1].x;
+                z = hi ? r[j][2].y : r[j][2].x;
+            }
+        x = fmaxf(x, 0.0f) + kTiny;
+        y = fmaxf(y, 0.0f) + kTiny;
+        z = fmaxf(z, 0.0f) + kTiny;
         apply_levels(a, x, y, z);
         add_glare(a, size_t(p0 + k), x, y, z);
-        float r, g, b;
-        mat_apply(a.to_rgb, x, y, z, r, g, b);
-        gamut(a, r, g, b);
+        float rr, g, b;
+        mat_apply(a.to_rgb, x, y, z, rr, g, b);
+        gamut(a, rr, g, b);
         float* o = rgb + 3 * size_t(p0 + k);
-        o[0] = r;
+        o[0] = rr;
         o[1] = g;
         o[2] = b;
     }
@@ -80,9 +119,9 @@ __device__ __forceinline__ void print_pair(const PrintArgs& a, const float* __re
 
 __global__ void __launch_bounds__(kPrintThreads) k_print(const float* __restrict__ neg, float* __restrict__ rgb,
                                                          const __grid_constant__ PrintArgs a) {
-    const uint32_t p0 = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
+    const uint32_t p0 = 2 * kPairs * (blockIdx.x * blockDim.x + threadIdx.x);
     if (p0 >= a.n) return;
-    print_pair(a, neg, rgb, p0, a.n);
+    print_group(a, neg, rgb, p0, a.n);
 }
 
 // The print stage of many frames in one persistent launch. Work item i covers `item_px` pixels of frame
@@ -112,8 +151,9 @@ __global__ void __launch_bounds__(kPrintThreads) k_print_batch(const BatchPrintF
             cur = f;
         }
         const uint32_t first = item_first[it];
-        for (uint32_t p0 = first + 2 * threadIdx.x; p0 < min(first + item_px, sa.n); p0 += 2 * blockDim.x)
-            print_pair(sa, s_neg, s_rgb, p0, sa.n);
+        for (uint32_t p0 = first + 2 * kPairs * threadIdx.x; p0 < min(first + item_px, sa.n);
+             p0 += 2 * kPairs * blockDim.x)
+            print_group(sa, s_neg, s_rgb, p0, sa.n);
     }
 }
 
@@ -121,7 +161,7 @@ __global__ void __launch_bounds__(kPrintThreads) k_print_batch(const BatchPrintF
 
 void print(const float* neg, float* rgb, const PrintArgs& a, cudaStream_t s) {
     if (a.n == 0) return;
-    const uint32_t threads = (a.n + 1) / 2;
+    const uint32_t threads = (a.n + 2 * kPairs - 1) / (2 * kPairs);
     Probe p("print", s);
     k_print<<<(threads + kPrintThreads - 1) / kPrintThreads, kPrintThreads, 0, s>>>(neg, rgb, a);
 }

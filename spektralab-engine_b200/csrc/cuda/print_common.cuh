@@ -24,6 +24,32 @@ __device__ __forceinline__ float ex2_ftz(float x) {
     asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
     return y;
 }
+// 2^x for a pair of binary32 values on the FMA pipe: a stand-in for ex2.approx on part of the print's
+// wavelengths, where the special-function unit is the busiest pipe. Method: Cody and Waite's argument
+// reduction x = j + r with j = rint(x) from the 1.5 * 2^23 addition and r = x - j in [-1/2, 1/2] (both
+// exact); 2^r by the degree-6 polynomial of least maximum relative error on [-1/2, 1/2] (Remez exchange,
+// coefficients rounded to binary32; with the binary32 Horner steps the relative error stays below 8e-8,
+// under ex2.approx's); 2^j added to the result's exponent field. x is clamped to [-126, 126] first, so the
+// result is a normal number (the print's exponents lie in [-60, 0]).
+__device__ __forceinline__ float2 exp2_poly2(float2 x) {
+    constexpr float kShift = 12582912.0f;  // 1.5 * 2^23: x + kShift rounds x to an integer in its low bits
+    x.x = fminf(fmaxf(x.x, -126.0f), 126.0f);
+    x.y = fminf(fmaxf(x.y, -126.0f), 126.0f);
+    const float2 t = __fadd2_rn(x, make_float2(kShift, kShift));
+    const float2 j = __fadd2_rn(t, make_float2(-kShift, -kShift));
+    const float2 r = __ffma2_rn(j, make_float2(-1.0f, -1.0f), x);
+    float2 p = make_float2(0x1.41d334p-13f, 0x1.41d334p-13f);
+    p = __ffma2_rn(p, r, make_float2(0x1.5f456ap-10f, 0x1.5f456ap-10f));
+    p = __ffma2_rn(p, r, make_float2(0x1.3b2dbcp-7f, 0x1.3b2dbcp-7f));
+    p = __ffma2_rn(p, r, make_float2(0x1.c6aed4p-5f, 0x1.c6aed4p-5f));
+    p = __ffma2_rn(p, r, make_float2(0x1.ebfbdap-3f, 0x1.ebfbdap-3f));
+    p = __ffma2_rn(p, r, make_float2(0x1.62e430p-1f, 0x1.62e430p-1f));
+    p = __ffma2_rn(p, r, make_float2(1.0f, 1.0f));
+    // the low bits of t hold j in two's complement; shifted to the exponent field they scale p by 2^j
+    return make_float2(__int_as_float(__float_as_int(p.x) + (__float_as_int(t.x) << 23)),
+                       __int_as_float(__float_as_int(p.y) + (__float_as_int(t.y) << 23)));
+}
+
 __device__ __forceinline__ float lg2_approx(float x) {
     float y;
     asm("lg2.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
@@ -78,6 +104,11 @@ __device__ __forceinline__ float paper_lookup(const float* __restrict__ tab, uin
 // host, or folded by the compiler): as accurate as the approximate divide and no special-function op.
 #define RCP(x) (1.0f / (x))
 
+// 1: the gamut stage's cos, sin, log and exp on the special-function unit (__sincosf, __logf, __expf)
+#ifndef SPKB_GAMUT_FAST
+#define SPKB_GAMUT_FAST 0
+#endif
+
 __device__ __forceinline__ float knee(float d, float tau, float lim, float p, float inv_span, float inv_p) {
     if (d <= tau) return d;
     const float x = (d - tau) * inv_span;
@@ -105,7 +136,14 @@ __device__ __forceinline__ void gamut(const PrintArgs& pa, float& r, float& g, f
     const float a = (ra - (12.0f * ga) * RCP(11.0f)) + ba * RCP(11.0f);
     const float bb = ((ra + ga) - 2.0f * ba) * RCP(9.0f);
     const float h = atan2f(bb, a);
+#if SPKB_GAMUT_FAST
+    // cos(h + 2) from the special-function sine and cosine of h in [-pi, pi]
+    float sh_h, ch_h;
+    __sincosf(h, &sh_h, &ch_h);
+    const float et = 0.25f * ((ch_h * -0.41614683654714241f - sh_h * 0.90929742682568170f) + 3.8f);
+#else
     const float et = 0.25f * (cosf(h + 2.0f) + 3.8f);
+#endif
     const float A = (((2.0f * ra + ga) + ba * RCP(20.0f)) - 0.305f) * q.n_bb;
     const float ratio = A * q.inv_a_w;
     const float J = (100.0f * sgnf(ratio)) * powm(fabsf(ratio), cz);
@@ -114,7 +152,11 @@ __device__ __forceinline__ void gamut(const PrintArgs& pa, float& r, float& g, f
                                 : 0.0f;
     const float C = t > 0.0f ? (powm(t, 0.9f) * fsqrt(fabsf(J) * RCP(100.0f))) * chroma_k : 0.0f;
     const float M = C * f_l_qrt;
+#if SPKB_GAMUT_FAST
+    const float Mp = __logf(1.0f + 0.0228f * M) * RCP(0.0228f);
+#else
     const float Mp = logf(1.0f + 0.0228f * M) * RCP(0.0228f);
+#endif
     float Jp = fdiv(1.7f * J, 1.0f + 0.007f * J);
     if (q.lc_active != 0u) {
         float Ln = Jp * q.inv_j_white;
@@ -144,7 +186,11 @@ __device__ __forceinline__ void gamut(const PrintArgs& pa, float& r, float& g, f
     if (dch > 0.0f) dch = knee(dch, q.knee[0], q.knee[1], q.knee[2], q.knee_inv_span, q.knee_inv_p);
     const float Mn = dch * cs;
     // guarded inverse
+#if SPKB_GAMUT_FAST
+    const float Mi = (__expf(0.0228f * Mn) - 1.0f) * RCP(0.0228f);
+#else
     const float Mi = (expf(0.0228f * Mn) - 1.0f) * RCP(0.0228f);
+#endif
     const float Ji = fdiv(Jp, 1.7f - 0.007f * Jp);
     const float Ci = Mi * q.inv_f_l_qrt;
     const float Ai = (q.a_w * sgnf(Ji)) * powm(fabsf(Ji * RCP(100.0f)), inv_cz);
@@ -155,8 +201,12 @@ __device__ __forceinline__ void gamut(const PrintArgs& pa, float& r, float& g, f
     float ai = 0.0f, bi = 0.0f;
     if (ti != 0.0f) {
         const float p1 = fdiv((((50000.0f / 13.0f) * q.n_c) * q.n_cb) * et, ti);
+#if SPKB_GAMUT_FAST
+        const float sh = sh_h, ch = ch_h;
+#else
         float sh, ch;
         sincosf(h, &sh, &ch);
+#endif
         if (fabsf(sh) >= fabsf(ch)) {
             const float rs = fdiv(1.0f, sh);
             const float p4 = p1 * rs;

@@ -399,6 +399,7 @@ spk_engine* create(const char* dir, void* device, int32_t type) noexcept {
         if (dev < 0 || dev >= n) fail_gpu("CUDA device ordinal out of range");
         DeviceGuard g(dev);
         configure_device_pool(dev);
+        dev::develop_prepare(nullptr);
         auto e = std::make_unique<Engine>();
         e->device = dev;
         e->res = Resources::load(dir);

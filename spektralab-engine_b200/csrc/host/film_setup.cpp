@@ -52,6 +52,47 @@ IirCoefficients iir_coefficients(double sigma) {
     return c;
 }
 
+IirCoefficients iir_coefficients_dsigma(double sigma) {
+    // q(sigma) and dq/dsigma in the regime iir_coefficients uses
+    double q, dq;
+    if (sigma >= 2.5) {
+        q = 0.98711 * sigma - 0.96330;
+        dq = 0.98711;
+    } else {
+        const double r = std::sqrt(1.0 - 0.26891 * sigma);
+        q = 3.97156 - 4.14554 * r;
+        dq = 4.14554 * 0.26891 / (2.0 * r);
+    }
+    const double q2 = q * q, q3 = q2 * q;
+    const double b0 = ((1.57825 + 2.44413 * q) + 1.4281 * q2) + 0.422205 * q3;
+    const double b1 = (2.44413 * q + 2.85619 * q2) + 1.26661 * q3;
+    const double b2 = -(1.4281 * q2 + 1.26661 * q3);
+    const double b3 = 0.422205 * q3;
+    const double d0 = 2.44413 + 2.0 * 1.4281 * q + 3.0 * 0.422205 * q2;  // db_i / dq
+    const double d1 = 2.44413 + 2.0 * 2.85619 * q + 3.0 * 1.26661 * q2;
+    const double d2 = -(2.0 * 1.4281 * q + 3.0 * 1.26661 * q2);
+    const double d3 = 3.0 * 0.422205 * q2;
+    auto ratio = [&](double b, double d) { return (d * b0 - b * d0) / (b0 * b0) * dq; };  // d(b / b0) / dsigma
+    IirCoefficients c;
+    c.B1 = ratio(b1, d1);
+    c.B2 = ratio(b2, d2);
+    c.B3 = ratio(b3, d3);
+    c.B = -((c.B1 + c.B2) + c.B3);
+    return c;
+}
+
+std::vector<double> gaussian_kernel_dsigma(double sigma, double truncate) {
+    const std::vector<double> w = gaussian_kernel(sigma, truncate);
+    const int radius = int(w.size() / 2);
+    double second = 0.0;  // sum_j w_j j^2
+    for (int k = -radius; k <= radius; ++k) second += w[size_t(k + radius)] * double(k) * double(k);
+    const double s3 = sigma * sigma * sigma;
+    std::vector<double> d(w.size());
+    for (int k = -radius; k <= radius; ++k)
+        d[size_t(k + radius)] = w[size_t(k + radius)] * (double(k) * double(k) - second) / s3;
+    return d;
+}
+
 // =============================== grain ===========================================================
 
 namespace {

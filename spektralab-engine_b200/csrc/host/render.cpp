@@ -1077,6 +1077,51 @@ void gaussian_adjoint(RenderCtx& ctx, Plane& g, double sigma) {
         fail_unsupported("the transposed recursive blur needs the frame's lines in shared memory");
 }
 
+// d/dsigma of the blur of x by the Gaussian of one sigma on every channel, exact for the implemented
+// filter: on the FIR branch the derivative of the normalised taps (fixed support) in either pass,
+// dG x = H'(V x) + H(V' x); on the recursive branch the tangent of the Young-van Vliet recurrences
+// along their coefficients' derivatives, row pass then column pass.
+void gaussian_dsigma(RenderCtx& ctx, const Plane& x, double sigma, Plane& out_dot) {
+    const uint32_t w = x.w, h = x.h;
+    const Branch br = blur_branch(sigma);
+    if (br == Branch::Identity) {
+        cuda_check(cudaMemsetAsync(out_dot.data(), 0, out_dot.bytes(), ctx.stream), "memset");
+        return;
+    }
+    if (br == Branch::Fir) {
+        const bool no_iir[3] = {false, false, false};
+        const FirTaps t = fir_taps(Vec3{sigma, sigma, sigma}, no_iir);
+        FirTaps dt = t;
+        const std::vector<double> d = gaussian_kernel_dsigma(sigma, 3.0);
+        const int rd = int(d.size() / 2);
+        for (int c = 0; c < 3; ++c)
+            for (int i = -t.r; i <= t.r; ++i) dt.taps[c][t.r + i] = std::abs(i) <= rd ? f32(d[size_t(i + rd)]) : 0.0f;
+        Plane a = make_plane(ctx.pool, w, h), b = make_plane(ctx.pool, w, h);
+        const float one[3] = {1.0f, 1.0f, 1.0f};
+        dev::fir_v(x.data(), a.data(), w, h, t, ctx.stream);
+        dev::fir_h(a.data(), b.data(), b.data(), w, h, dt, ACC_NONE, one, ctx.stream);  // H'(V x)
+        dev::fir_v(x.data(), a.data(), w, h, dt, ctx.stream);
+        dev::fir_h(a.data(), out_dot.data(), b.data(), w, h, t, ACC_PLANE, one, ctx.stream);  // + H(V' x)
+        return;
+    }
+    const bool all[3] = {true, true, true};
+    const IirCoefs c = iir_coefs(Vec3{sigma, sigma, sigma}, all);
+    IirCoefs dc = c;
+    const IirCoefficients k = iir_coefficients_dsigma(sigma);
+    for (int i = 0; i < 3; ++i) {
+        dc.B[i] = k.B;
+        dc.B1[i] = k.B1;
+        dc.B2[i] = k.B2;
+        dc.B3[i] = k.B3;
+    }
+    Plane work = make_plane(ctx.pool, w, h), work_dot = make_plane(ctx.pool, w, h);
+    Plane rows = make_plane(ctx.pool, w, h), rows_dot = make_plane(ctx.pool, w, h), value = make_plane(ctx.pool, w, h);
+    dev::iir_tangent(x.data(), nullptr, work.data(), work_dot.data(), rows.data(), rows_dot.data(), w, h, false, c, dc,
+                     ctx.stream);
+    dev::iir_tangent(rows.data(), rows_dot.data(), work.data(), work_dot.data(), value.data(), out_dot.data(), w, h, true,
+                     c, dc, ctx.stream);
+}
+
 double common_sigma(const MixtureComponent& m) {
     if (!(m.sigma[0] == m.sigma[1] && m.sigma[1] == m.sigma[2]))
         fail_unsupported("the render's adjoint takes halation components with one sigma for the three channels");
@@ -1266,17 +1311,12 @@ void render_vjp(RenderCtx& ctx, const Pipeline& p, const LiveParams& live, const
     dev::vjp_develop(H3.data(), counts.as<float>(), gn.data(), g.data(), d_nodes, dp.da, w, h, ctx.stream);  // g_H3
     if (pl.bounce) {
         if (hov) {  // the override's weights and sigmas, from the exposure entering the bounce stage (H2)
-            Plane Gk = make_plane(ctx.pool, w, h), Gp = make_plane(ctx.pool, w, h);
+            Plane Gk = make_plane(ctx.pool, w, h);
             for (uint32_t k = 0; k < ncomp; ++k) {
                 const double sg = common_sigma(hov->comps[k]);
                 gaussian(ctx, H2, Gk, Vec3{sg, sg, sg});
                 dev::dot3(g.data(), Gk.data(), n, d_dots + 6 * k, ctx.stream);
-                constexpr double eps = 2e-3;
-                const double sp = sg * (1.0 + eps), sm = sg * (1.0 - eps);
-                gaussian(ctx, H2, Gk, Vec3{sp, sp, sp});
-                gaussian(ctx, H2, Gp, Vec3{sm, sm, sm});
-                const double inv = 1.0 / (sp - sm);
-                lincomb(ctx, Vec3{inv, inv, inv}, Gk, Vec3{-inv, -inv, -inv}, &Gp, Gk);
+                gaussian_dsigma(ctx, H2, sg, Gk);
                 dev::dot3(g.data(), Gk.data(), n, d_dots + 6 * k + 3, ctx.stream);
             }
         }

@@ -31,6 +31,11 @@ struct IirCoefficients {
     double B, B1, B2, B3;
 };
 IirCoefficients iir_coefficients(double sigma);         // Young and van Vliet 1995
+// Their derivatives along sigma (B', B1', B2', B3'; the render's adjoint), from q'(sigma) and the
+// quotient rule on b_i / b0.
+IirCoefficients iir_coefficients_dsigma(double sigma);
+// d/dsigma of the normalised FIR kernel on its fixed support: w_k (k^2 - sum_j w_j j^2) / sigma^3.
+std::vector<double> gaussian_kernel_dsigma(double sigma, double truncate);
 
 struct MixtureComponent {
     Vec3 weight;

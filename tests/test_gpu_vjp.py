@@ -35,33 +35,40 @@ def delta_of(p):
     return dict(DELTA, print_exposure=float(p[0]), m_filter_shift=float(p[1]), y_filter_shift=float(p[2]))
 
 
-def oracle_linear(lib, resources, img64, counts, p):
-    f64 = setup_f64(lib, resources, delta_of(p), PITCH)["f64"]
+def oracle_linear(lib, resources, img64, counts, p, pitch=PITCH):
+    f64 = setup_f64(lib, resources, delta_of(p), pitch)["f64"]
     o = oracle.Oracle(f64, seed=SEED, halation=halation(p), print_exposure=float(p[0]))
     return o.render_linear(img64, counts)
 
 
-@pytest.fixture(scope="module")
-def case(engine, lib, resources):
-    img = sc.synthetic_image(W, H, 3)
-    with engine.open(img, delta_of(PARAMS)) as s:
-        s.set_halation(*halation(PARAMS))
-        _, counts = s.develop_debug("full", SEED, W, H)
+def make_case(engine, w, h, params):
+    """The device's forward output, Poisson counts and adjoint for a w x h frame at the given parameters,
+    the loss target rendered with perturbed parameters."""
+    img = sc.synthetic_image(w, h, 3)
+    with engine.open(img, delta_of(params)) as s:
+        s.set_halation(*halation(params))
+        _, counts = s.develop_debug("full", SEED, w, h)
         y = s.render_linear(SEED)
         # the target: the same frame with perturbed parameters
-        q = PARAMS * np.array([1.1, 1.0, 1.0, 1.25, 0.8, 1.1, 0.9]) + np.array([0, 0.02, 0.03, 0, 0, 0, 0])
+        q = params * np.array([1.1, 1.0, 1.0, 1.25, 0.8, 1.1, 0.9]) + np.array([0, 0.02, 0.03, 0, 0, 0, 0])
     with engine.open(img, delta_of(q)) as s2:
         s2.set_halation(*halation(q))
         target = s2.render_linear(SEED).astype(np.float64)
-    with engine.open(img, delta_of(PARAMS)) as s:
-        s.set_halation(*halation(PARAMS))
+    with engine.open(img, delta_of(params)) as s:
+        s.set_halation(*halation(params))
         gy = (y.astype(np.float64) - target).astype(np.float32)
-        gx, gp = s.render_vjp(gy, SEED, len(PARAMS) + N_CURVE)
-    return dict(img=img, counts=counts, y=y, target=target, gx=gx, gp=gp)
+        gx, gp = s.render_vjp(gy, SEED, len(params) + N_CURVE)
+    return dict(img=img, counts=counts, y=y, target=target, gx=gx, gp=gp, params=params,
+                pitch=35000.0 / max(w, h))
+
+
+@pytest.fixture(scope="module")
+def case(engine):
+    return make_case(engine, W, H, PARAMS)
 
 
 def loss(lib, resources, case, img64, p):
-    y = oracle_linear(lib, resources, img64, case["counts"], p)
+    y = oracle_linear(lib, resources, img64, case["counts"], p, case["pitch"])
     return 0.5 * float(np.sum((y - case["target"]) ** 2))
 
 
@@ -126,3 +133,52 @@ def test_autograd_function(engine, case):
     loss_t.backward()
     np.testing.assert_allclose(img.grad.numpy(), case["gx"], rtol=1e-5, atol=1e-7)
     np.testing.assert_allclose(params.grad.numpy(), case["gp"][:len(PARAMS)], rtol=1e-5, atol=1e-9)
+
+
+# sigma 2 px takes the FIR branch (the derivative of its normalised taps), 12 px the recursive one (the
+# tangent of the Young-van Vliet recurrences)
+FIR_PARAMS = np.array([1.0, 0.05, -0.04, 0.02, 0.02, 2.0, 12.0])
+
+
+@pytest.fixture(scope="module")
+def case_fir(engine):
+    return make_case(engine, W, H, FIR_PARAMS)
+
+
+@pytest.mark.parametrize("j,step", [(5, 1e-3), (6, 1e-3)])
+def test_sigma_gradient_both_branches(lib, resources, case_fir, j, step):
+    x = case_fir["img"].astype(np.float64)
+    pp, pm = FIR_PARAMS.copy(), FIR_PARAMS.copy()
+    pp[j] += step
+    pm[j] -= step
+    fd = (loss(lib, resources, case_fir, x, pp) - loss(lib, resources, case_fir, x, pm)) / (2 * step)
+    got = float(case_fir["gp"][j])
+    assert abs(got - fd) <= TOL * abs(fd) + 1e-9, (j, got, fd)
+
+
+# the differentiation workload's size: 1024 x 1024, grain as fixed noise (seed 7), halation sigma 8 and 40 px
+@pytest.fixture(scope="module")
+def case_1024(engine):
+    return make_case(engine, 1024, 1024, PARAMS)
+
+
+def test_1024_image_direction(lib, resources, case_1024):
+    rng = np.random.default_rng(11)
+    x = case_1024["img"].astype(np.float64)
+    v = rng.standard_normal(x.shape) * x
+    eps = 1e-7
+    fd = (loss(lib, resources, case_1024, x + eps * v, PARAMS) -
+          loss(lib, resources, case_1024, x - eps * v, PARAMS)) / (2 * eps)
+    got = float(np.sum(case_1024["gx"].astype(np.float64) * v))
+    assert abs(got - fd) <= TOL * abs(fd), (got, fd)
+
+
+@pytest.mark.parametrize("j,step", [(0, 1e-4), (3, 1e-5), (5, 1e-3), (6, 1e-2)])
+def test_1024_parameter_gradient(lib, resources, case_1024, j, step):
+    x = case_1024["img"].astype(np.float64)
+    pp, pm = PARAMS.copy(), PARAMS.copy()
+    pp[j] += step
+    pm[j] -= step
+    fd = (loss(lib, resources, case_1024, x, pp) - loss(lib, resources, case_1024, x, pm)) / (2 * step)
+    got = float(case_1024["gp"][j])
+    assert abs(got - fd) <= TOL * abs(fd) + 1e-9, (j, got, fd)
