@@ -127,9 +127,31 @@ __device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
     return done != 0;
 }
 
+// the phase's completion tested without waiting
+__device__ __forceinline__ bool mbar_test(uint32_t bar, uint32_t parity) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return done != 0;
+}
+
 // Waits for the completion of the barrier's phase of the given parity; false after `limit` SM clocks
 // (kWaitCycles: about 2 s at the B200's clocks). The clock is read only once the phase was found incomplete.
+// try_wait may suspend the thread for a while by itself, so a shortened limit (the test hook) polls with
+// the non-blocking test_wait instead, and a phase still running then runs the wait out at once.
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, long long limit) {
+    if (limit < kWaitCycles) {
+        const long long t0 = clock64();
+        for (;;) {
+            if (mbar_test(bar, parity)) return true;
+            if (clock64() - t0 > limit) return false;
+        }
+    }
     if (mbar_try(bar, parity)) return true;
     const long long t0 = clock64();
     for (;;) {

@@ -4,7 +4,8 @@ The reference engine (JamesQiu2005/spektralab-engine) is compiled for the CPU fr
 oracle/Makefile (oracle/_ref/libspektralab_ref.so: its src/ stage code unmodified, its Metal kernels
 compiled as C++). This script runs it on the seeded synthetic resources and stores what it returns:
 
-  golden_renders.npz   RGBA16 renders and negatives of a 64 x 48 frame for four parameter sets
+  golden_renders.npz   RGBA16 renders and negatives of a 64 x 48 frame for five parameter sets (the last
+                       with the 4K workload's halation and scanner lens blur)
                        (render at print_exposure 1.0 and a reprint at 1.2 of the same negative)
   golden_sampler.npz   the reference's Poisson counts and lognormal values for a lambda grid
   golden_gaussian.npz  the reference's blur of a 97 x 61 plane (kernel path and same-order CPU copy)
@@ -33,12 +34,15 @@ import synth_resources  # noqa: E402
 BASE = {"film_stock": "synthetic_negative_400", "print_stock": "synthetic_paper", "auto_exposure": False,
         "dir_couplers_active": False, "glare_active": False}
 CFG1_HALATION = ([((1, 1, 1), (8, 8, 8)), ((1, 1, 1), (40, 40, 40))], (0.02, 0.02, 0.02))
+# the 4K workload's halation (sigma 20 and 120 px, weight 0.03) and scanner lens blur (1.5 px)
+CFG2_HALATION = ([((1, 1, 1), (20, 20, 20)), ((1, 1, 1), (120, 120, 120))], (0.03, 0.03, 0.03))
 
 CASES = {
     "nograin_nohalation": (dict(BASE, grain_active=False, halation_active=False), None),
     "nograin_preset": (dict(BASE, grain_active=False), None),
     "grain_preset": (dict(BASE), None),
     "grain_cfg1": (dict(BASE), CFG1_HALATION),
+    "nograin_lens_cfg2": (dict(BASE, grain_active=False, scanner_lens_blur=1.5), CFG2_HALATION),
 }
 W, H = 64, 48
 EXPOSURES = (1.0, 1.2)

@@ -161,8 +161,8 @@ def test_memory_report(lib):
         assert all(m["pool"]["audit"][k] == 0 for k in ("live_underflows", "over_releases", "reclaim_while_encoding"))
         assert sorted(m["pressure"]) == ["critical_events", "critical_pending", "idle_trim_seconds", "idle_trims",
                                          "monitor", "warn_events"]
-        assert sorted(m["pool"]) == ["audit", "buffers", "frame_high_water_bytes", "free_bytes", "live_buffers",
-                                     "live_bytes", "pending_buffers", "pending_bytes", "total_bytes"]
+        assert sorted(m["pool"]) == ["audit", "buffers", "frame_high_water_bytes", "free_buffers", "free_bytes",
+                                     "live_buffers", "live_bytes", "pending_buffers", "pending_bytes", "total_bytes"]
     pr = m1["persistent"]
     assert pr["source_bytes"] == 1200 * 900 * 12
     assert pr["source_bytes"] + pr["cached_negative_bytes"] <= pr["bytes"]

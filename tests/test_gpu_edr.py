@@ -60,4 +60,5 @@ def test_output_spaces_within_one_lsb(engine, ref, ref_engine, space):
     with engine.open(img, delta) as s:
         a, _ = s.render("full")
     st = lsb_stats(a, ref_render(ref_engine, img, delta, "full"))
-    assert st["frac_gt1"] <= 5e-4 and st["max"] <= 16, st
+    # measured: sRGB 2.6e-4 of the channels above 1 (max 4), Adobe RGB 1.2e-4 (max 11), BT.709 4e-6 (max 2)
+    assert st["frac_gt1"] <= 3e-4 and st["max"] <= 12, st

@@ -32,7 +32,7 @@ def test_highlights_fp64_gate_with_grain(engine, lib, resources):
     f64 = setup_f64(lib, resources, delta, 35000.0 / max(w, h))["f64"]
     out, _ = oracle.Oracle(f64, seed=FIRST_SEED).render(img, counts=counts)
     st = lsb_stats(a, out)
-    assert st["frac_gt1"] <= 1e-4 and st["max"] <= 64, st
+    assert st["max"] <= 1, st
 
 
 def test_boost_of_a_black_frame(engine, ref, ref_engine):

@@ -59,7 +59,7 @@ def test_auto_exposure_live_tier_within_one_lsb(engine, lib, resources, ref, ref
         assert lsb_stats(a, ref_render(ref_engine, img, delta, "live"))["max"] <= 1
         # binary32 against the float64 oracle (decode and a rotation before the develop): the FP64 gate
         st = lsb_stats(a, oracle_render_ae(lib, resources, img, delta, L)[0])
-        assert st["frac_gt1"] <= 1e-4 and st["max"] <= 8, st
+        assert st["n_gt1"] <= 4 and st["max"] <= 2, st  # measured: three channels at 2 LSB16 in 12 M
 
 
 def test_meter_rearms_on_its_key(engine):

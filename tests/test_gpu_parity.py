@@ -45,7 +45,9 @@ def test_golden_renders(engine):
             assert lsb_stats(a, ref[0])["max"] <= 1, name
             assert lsb_stats(b, ref[1])["max"] <= 1, name
         else:
-            assert lsb_stats(a, ref[0])["frac_gt1"] < 0.25, name
+            # grain against the reference's own draws: its binary32 lambdas flip a few Poisson counts
+            # against ours (the fixed-noise float64 gates hold the same renders to 1 LSB16); measured 4.4 %
+            assert lsb_stats(a, ref[0])["frac_gt1"] < 0.06, name
         assert (a[..., 3] == 65535).all()
 
 
@@ -81,9 +83,9 @@ def test_fp64_gate_fixed_noise(engine, lib, resources, case):
     o = oracle.Oracle(f64, seed=FIRST_SEED, halation=hal)
     out, neg64 = o.render(img, counts=counts)
     st = lsb_stats(a, out)
-    # binary32 device arithmetic against binary64: at most 1 LSB16 on all but a handful of pixels
-    assert st["frac_gt1"] <= 1e-4, st
-    assert st["max"] <= 64, st
+    # binary32 device arithmetic against binary64: at most 1 LSB16 on every channel but two (measured: one
+    # channel at 2 LSB16 in 786,432 without grain and with the cfg1 halation, none with the preset)
+    assert st["n_gt1"] <= 2 and st["max"] <= 2, st
     np.testing.assert_allclose(neg, neg64, rtol=0, atol=5e-5)
 
 
@@ -137,8 +139,7 @@ def test_couplers_fp64_gate_fixed_noise(engine, lib, resources):
     info = dict(st, fold=float(fold.mean()), flat=float(flat.mean()), gt1_all=int((d > 1).sum()),
                 gt1_fold=int((d[fold] > 1).sum()), gt1_flat=int((d[flat] > 1).sum()),
                 neg_flat=float(np.abs(neg - neg64)[flat].max()))
-    assert st["frac_gt1"] <= 1e-4, info
-    assert st["max"] <= 64, info
+    assert st["max"] <= 1, info
     assert fold.mean() < 0.02 and flat.mean() > 0.75, info  # the fold is a thin contour; widened, a sixth of the frame
 
 

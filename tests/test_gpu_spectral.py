@@ -130,7 +130,7 @@ def test_bf16x3_render_fp64_gate(engine, lib, resources, case):
     f64 = setup_f64(lib, resources, delta, 35000.0 / max(w, h))["f64"]
     out, _ = oracle.Oracle(f64, seed=FIRST_SEED, halation=hal).render(img, counts=counts)
     st = lsb_stats(a, out)
-    assert st["frac_gt1"] <= 1e-3 and st["max"] <= 64, st
+    assert st["max"] <= 1, st
 
 
 def test_spectral_mode_in_a_batch(engine):

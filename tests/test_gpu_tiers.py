@@ -96,8 +96,7 @@ def test_live_tier_fp64_gate_fixed_noise(engine, lib, resources):
         neg, counts = s.develop_debug("live", FIRST_SEED, a.shape[1], a.shape[0])
     out, neg64 = oracle_render(lib, resources, img, delta, 800, seed=FIRST_SEED, counts=counts)
     st = lsb_stats(a, out)
-    assert st["frac_gt1"] <= 1e-4, st
-    assert st["max"] <= 64, st
+    assert st["n_gt1"] <= 2 and st["max"] <= 2, st  # measured: one channel at 2 LSB16 in 1.2 M
     # the binary32 decode and rotated resample enter before the curves: all but a few values within the
     # plain path's 5e-5, every value within 1e-4
     dn = np.abs(neg - neg64)
