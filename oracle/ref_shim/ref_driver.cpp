@@ -167,6 +167,12 @@ int32_t fail_status(const std::exception& e) {
     return SPK_ERR_INTERNAL;
 }
 
+json::Value darr(const double* v, size_t n) {
+    json::Array a;
+    for (size_t i = 0; i < n; ++i) a.emplace_back(v[i]);
+    return json::Value(std::move(a));
+}
+
 json::Value farr(const float* v, size_t n) {
     json::Array a;
     for (size_t i = 0; i < n; ++i) a.emplace_back(double(v[i]));
@@ -371,6 +377,22 @@ __attribute__((visibility("default"))) int32_t spkref_setup_json(spk_engine* eng
         r["cam_m_to_xyz"] = farr(q.m_to_xyz, 9);
         r["cam_m_to_rgb"] = farr(q.m_to_rgb, 9);
         r["cmax"] = farr(s.cam->cmax_f32.data(), s.cam->cmax_f32.size());
+        // the binary64 values behind the narrowed ones, where the reference keeps them
+        json::Value f64;
+        f64["table"] = darr(f.table->f64.data(), f.table->f64.size());
+        f64["input_matrix"] = darr(f.input_matrix.data(), 9);
+        f64["enl_eps"] = darr(run->eps_n.data(), run->eps_n.size());
+        f64["enl_beta"] = darr(run->beta_n.data(), run->beta_n.size());
+        f64["enl_wt"] = darr(run->w_n.data(), run->w_n.size());
+        f64["enl_g"] = darr(run->g.data(), 3);
+        f64["enl_o"] = darr(run->o.data(), 3);
+        f64["scan_eps"] = darr(s.scan.eps.data(), s.scan.eps.size());
+        f64["scan_beta"] = darr(s.scan.beta.data(), s.scan.beta.size());
+        f64["scan_wt"] = darr(s.scan.wt.data(), s.scan.wt.size());
+        f64["cmax"] = darr(s.cam->cmax_f64.data(), s.cam->cmax_f64.size());
+        f64["cam_m_to_xyz"] = darr(s.cam->m_to_xyz.data(), 9);
+        f64["cam_m_to_rgb"] = darr(s.cam->m_to_rgb.data(), 9);
+        r["f64"] = std::move(f64);
         const std::string text = json::write(r);
         char* p = static_cast<char*>(std::malloc(text.size() + 1));
         std::memcpy(p, text.c_str(), text.size() + 1);
