@@ -47,10 +47,17 @@ __device__ __forceinline__ void scan_tile(const ScanArgs& a, const float* __rest
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
     // 1. the print output at (y0 - R + i, x0 - R + j), reflected; pixels more than R past an edge are
-    //    never read and load a clamped pixel
+    //    never read and load a clamped pixel. A tile whose haloed columns lie inside the frame reads each
+    //    row's floats contiguously, with no per-element reflection.
+    const bool inner_x = x0 - R >= 0 && x0 + kTW + R <= w;
     for (int i = warp; i < PR; i += kWarps) {
         const int yy = min(max(reflect_near(y0 - R + i, h), 0), h - 1);
         const float* row = rgb + size_t(yy) * size_t(w) * 3;
+        if (inner_x) {
+            const float* seg = row + 3 * (x0 - R);
+            for (int f = lane; f < PC; f += 32) A[i * PC + f] = __ldg(seg + f);
+            continue;
+        }
         for (int f = lane; f < PC; f += 32) {
             const int j = f / 3, c = f - 3 * j;
             const int xx = min(max(reflect_near(x0 - R + j, w), 0), w - 1);
@@ -77,8 +84,10 @@ __device__ __forceinline__ void scan_tile(const ScanArgs& a, const float* __rest
         const int yy = y0 - r2 + i;
         if (yy < 0 || yy >= h) continue;
         for (int fb = lane; fb < BC; fb += 32) {
-            const int xx = x0 - r2 + fb / 3;
-            if (xx < 0 || xx >= w) continue;
+            if (!inner_x) {
+                const int xx = x0 - r2 + fb / 3;
+                if (xx < 0 || xx >= w) continue;
+            }
             float acc = 0.0f;
 #pragma unroll
             for (int k = 0; k <= 2 * r1; ++k) acc += a.t1[k] * B[i * PC + fb + 3 * k];
@@ -199,9 +208,15 @@ __global__ void __launch_bounds__(kThreads) k_fir_tile(const float* __restrict__
     float* B = smem + PR * PC;
     const int x0 = blockIdx.x * kTW, y0 = blockIdx.y * kTH;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const bool inner_x = x0 - r >= 0 && x0 + kTW + r <= w;  // the haloed columns lie inside the frame
     for (int i = warp; i < PR; i += kWarps) {
         const int yy = min(max(reflect_near(y0 - r + i, h), 0), h - 1);
         const float* row = in + size_t(yy) * size_t(w) * 3;
+        if (inner_x) {
+            const float* seg = row + 3 * (x0 - r);
+            for (int f = lane; f < PC; f += 32) A[i * PC + f] = __ldg(seg + f);
+            continue;
+        }
         for (int f = lane; f < PC; f += 32) {
             const int j = f / 3, c = f - 3 * j;
             const int xx = min(max(reflect_near(x0 - r + j, w), 0), w - 1);
