@@ -343,14 +343,15 @@ def run_vjp(args):
         for _ in range(args.warmup):
             s.render_vjp(gy, VJP_SEED, VJP_PARAMS)
         fwd, bwd = [], []
-        for _ in range(args.steps):
-            t0 = time.perf_counter()
-            s.render_linear(VJP_SEED)
-            t1 = time.perf_counter()
-            gx, gp = s.render_vjp(gy, VJP_SEED, VJP_PARAMS)
-            t2 = time.perf_counter()
-            fwd.append(t1 - t0)
-            bwd.append(t2 - t1)
+        with Clocks(0) as clk:
+            for _ in range(args.steps):
+                t0 = time.perf_counter()
+                s.render_linear(VJP_SEED)
+                t1 = time.perf_counter()
+                gx, gp = s.render_vjp(gy, VJP_SEED, VJP_PARAMS)
+                t2 = time.perf_counter()
+                fwd.append(t1 - t0)
+                bwd.append(t2 - t1)
     eng.close()
     ms = 1000.0 * statistics.median(bwd)
     line = {"metric": "VJP ms/frame", "value": ms, "unit": "ms", "n_gpus": 1, "steps": args.steps,
@@ -364,7 +365,8 @@ def run_vjp(args):
             "forward_ms": 1000.0 * statistics.median(fwd),
             "note": "wall time per spk_render_vjp call with host arrays (forward recomputed inside); "
                     "gradient accuracy is checked against binary64 central differences in tests/test_gpu_vjp.py",
-            "grad_params": [float(v) for v in gp[:7]], "grad_curve_l1": float(np.abs(gp[7:]).sum()), "grad_input_l2": float(np.sqrt(np.sum(gx.astype(np.float64) ** 2)))}
+            "grad_params": [float(v) for v in gp[:7]], "grad_curve_l1": float(np.abs(gp[7:]).sum()),
+            "grad_input_l2": float(np.sqrt(np.sum(gx.astype(np.float64) ** 2))), "clocks": clk.summary()}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -550,18 +552,19 @@ def run_batch(args):
             _, tuning["reprint"] = batched(ss, True)
         for s in ss:
             s.close()
-    ss = open_all()
-    p_render, lat_pr = plain(ss, False)
-    reprint_exposures(ss)
-    p_reprint, lat_pp = plain(ss, True)
-    for s in ss:
-        s.close()
-    ss = open_all()
-    b_render, info_r = batched(ss, False)
-    reprint_exposures(ss)
-    b_reprint, info_p = batched(ss, True)
-    for s in ss:
-        s.close()
+    with Clocks(0) as clk:
+        ss = open_all()
+        p_render, lat_pr = plain(ss, False)
+        reprint_exposures(ss)
+        p_reprint, lat_pp = plain(ss, True)
+        for s in ss:
+            s.close()
+        ss = open_all()
+        b_render, info_r = batched(ss, False)
+        reprint_exposures(ss)
+        b_reprint, info_p = batched(ss, True)
+        for s in ss:
+            s.close()
     eng.close()
 
     def pct(v):
@@ -582,7 +585,8 @@ def run_batch(args):
                         "batched_ms": 1000.0 * b_reprint, "plain_ms": 1000.0 * p_reprint,
                         "latency_ms_batched": pct(info_p["frame_done_ms"]), "latency_ms_plain": pct(lat_pp),
                         "plan": info_p.get("plan"),
-                        "tuning_candidates_ms": tuning["reprint"].get("candidates_ms")}}
+                        "tuning_candidates_ms": tuning["reprint"].get("candidates_ms")},
+            "clocks": clk.summary()}
     print(json.dumps(line), flush=True)
     return 0
 
