@@ -129,8 +129,11 @@ void fir_tile(const float* in, float* out, uint32_t w, uint32_t h, int r, const 
 // items of item_px pixels (item_frame / item_first per item, ordered by frame; frames in device memory),
 // the scanner over the frames' concatenated 32 x 32 tile lists (frames in device memory, ordered by
 // first_tile; r1, r2 the radii every frame shares, or -1 for frames that differ).
+// enl and scan (host, may be null): spectral tables every frame shares, which the kernel then takes in its
+// parameters (the constant bank) instead of staging them per frame in shared memory.
 void print_batch(const BatchPrintFrame* frames, const uint32_t* item_frame, const uint32_t* item_first,
-                 uint32_t n_items, uint32_t item_px, uint32_t ctas, cudaStream_t s);
+                 uint32_t n_items, uint32_t item_px, uint32_t ctas, const SpectralPairs* enl,
+                 const SpectralPairs* scan, cudaStream_t s);
 void scan_encode_batch(const BatchScanFrame* frames, uint32_t n_frames, uint32_t n_tiles, int r1, int r2,
                        uint32_t ctas, cudaStream_t s);
 // Sets the scanner kernels' shared-memory limits on the current device (before a stream capture).

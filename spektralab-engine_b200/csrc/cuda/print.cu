@@ -68,8 +68,10 @@ __device__ __forceinline__ void spectral(const SpectralPairs& t, const float2 (&
 
 // Pixels p0 .. p0 + 2 kPairs - 1 of one frame (those below n): the spectral integrals on kPairs packed
 // pairs, the rest one pixel after the other.
-__device__ __forceinline__ void print_group(const PrintArgs& a, const float* __restrict__ neg, float* __restrict__ rgb,
-                                            uint32_t p0, uint32_t n) {
+// enl and scan: the two integrals' tables (a.enl and a.scan, or tables every frame of a batch shares)
+__device__ __forceinline__ void print_group(const PrintArgs& a, const SpectralPairs& enl, const SpectralPairs& scan,
+                                            const float* __restrict__ neg, float* __restrict__ rgb, uint32_t p0,
+                                            uint32_t n) {
     constexpr int NP = kPairs;
     float2 d[NP][3];
 #pragma unroll
@@ -81,14 +83,14 @@ __device__ __forceinline__ void print_group(const PrintArgs& a, const float* __r
     }
     float2 r[NP][3];
     if (a.printed) {
-        spectral<NP>(a.enl, d, r);
+        spectral<NP>(enl, d, r);
 #pragma unroll
         for (int i = 0; i < NP; ++i)
 #pragma unroll
             for (int c = 0; c < 3; ++c)
                 d[i][c] = make_float2(print_density(a, c, r[i][c].x), print_density(a, c, r[i][c].y));
     }
-    spectral<NP>(a.scan, d, r);
+    spectral<NP>(scan, d, r);
 #pragma unroll 1
     for (uint32_t k = 0; k < uint32_t(2 * NP); ++k) {
         if (p0 + k >= n) break;
@@ -121,7 +123,7 @@ __global__ void __launch_bounds__(kPrintThreads) k_print(const float* __restrict
                                                          const __grid_constant__ PrintArgs a) {
     const uint32_t p0 = 2 * kPairs * (blockIdx.x * blockDim.x + threadIdx.x);
     if (p0 >= a.n) return;
-    print_group(a, neg, rgb, p0, a.n);
+    print_group(a, a.enl, a.scan, neg, rgb, p0, a.n);
 }
 
 // The print stage of many frames in one persistent launch. Work item i covers `item_px` pixels of frame
@@ -153,7 +155,45 @@ __global__ void __launch_bounds__(kPrintThreads) k_print_batch(const BatchPrintF
         const uint32_t first = item_first[it];
         for (uint32_t p0 = first + 2 * kPairs * threadIdx.x; p0 < min(first + item_px, sa.n);
              p0 += 2 * kPairs * blockDim.x)
-            print_group(sa, s_neg, s_rgb, p0, sa.n);
+            print_group(sa, sa.enl, sa.scan, s_neg, s_rgb, p0, sa.n);
+    }
+}
+
+// The same with spectral tables that every frame shares (same stocks and filters: the print exposure,
+// the planes and the sizes differ), passed in the kernel's parameters so that the unrolled integrals read
+// them from the constant bank as k_print does; the per-frame arguments are staged as above (their copy of
+// the tables goes unread).
+struct SharedSpectra {
+    SpectralPairs enl, scan;
+};
+
+__global__ void __launch_bounds__(kPrintThreads) k_print_batch_shared(const BatchPrintFrame* __restrict__ frames,
+                                                                      const uint32_t* __restrict__ item_frame,
+                                                                      const uint32_t* __restrict__ item_first,
+                                                                      uint32_t n_items, uint32_t item_px,
+                                                                      const __grid_constant__ SharedSpectra t) {
+    __shared__ __align__(16) PrintArgs sa;
+    __shared__ const float* s_neg;
+    __shared__ float* s_rgb;
+    uint32_t cur = 0xFFFFFFFFu;
+    for (uint32_t it = blockIdx.x; it < n_items; it += gridDim.x) {
+        const uint32_t f = item_frame[it];
+        if (f != cur) {
+            __syncthreads();
+            const uint4* src = reinterpret_cast<const uint4*>(&frames[f].args);
+            uint4* dst = reinterpret_cast<uint4*>(&sa);
+            for (uint32_t i = threadIdx.x; i < sizeof(PrintArgs) / 16; i += blockDim.x) dst[i] = src[i];
+            if (threadIdx.x == 0) {
+                s_neg = frames[f].neg;
+                s_rgb = frames[f].rgb;
+            }
+            __syncthreads();
+            cur = f;
+        }
+        const uint32_t first = item_first[it];
+        for (uint32_t p0 = first + 2 * kPairs * threadIdx.x; p0 < min(first + item_px, sa.n);
+             p0 += 2 * kPairs * blockDim.x)
+            print_group(sa, t.enl, t.scan, s_neg, s_rgb, p0, sa.n);
     }
 }
 
@@ -167,9 +207,17 @@ void print(const float* neg, float* rgb, const PrintArgs& a, cudaStream_t s) {
 }
 
 void print_batch(const BatchPrintFrame* frames, const uint32_t* item_frame, const uint32_t* item_first,
-                 uint32_t n_items, uint32_t item_px, uint32_t ctas, cudaStream_t s) {
+                 uint32_t n_items, uint32_t item_px, uint32_t ctas, const SpectralPairs* enl,
+                 const SpectralPairs* scan, cudaStream_t s) {
     if (n_items == 0) return;
     Probe p("print_batch", s);
+    if (enl && scan) {
+        SharedSpectra t;
+        t.enl = *enl;
+        t.scan = *scan;
+        k_print_batch_shared<<<ctas, kPrintThreads, 0, s>>>(frames, item_frame, item_first, n_items, item_px, t);
+        return;
+    }
     k_print_batch<<<ctas, kPrintThreads, 0, s>>>(frames, item_frame, item_first, n_items, item_px);
 }
 

@@ -704,7 +704,19 @@ struct BatchFrame {
     std::string pid;              // the frame's progress id
 };
 
-const char* const kBatchPlans[] = {"frames:4", "frames:16", "persistent:2048:592", "persistent:8192:1184"};
+// The tuner's candidates: per-frame launches on 4 or 16 streams, and the persistent launches over a grid of
+// item sizes (pixels per print item) and CTA counts (4, 8 and 16 per SM)
+const char* const kBatchPlans[] = {"frames:4",
+                                   "frames:16",
+                                   "persistent:2048:592",
+                                   "persistent:2048:1184",
+                                   "persistent:2048:2368",
+                                   "persistent:8192:592",
+                                   "persistent:8192:1184",
+                                   "persistent:8192:2368",
+                                   "persistent:32768:592",
+                                   "persistent:32768:1184",
+                                   "persistent:32768:2368"};
 constexpr size_t kMaxWorkers = 16;
 
 // A plan string: "frames:K" (1 <= K <= 16) or "persistent:S:C" (S even, 2 .. 2^20 pixels; 1 <= C <= 65535).
@@ -861,6 +873,14 @@ void run_plan(Engine& e, const std::string& plan, const std::string& shape, std:
         if (f.sa.r1 != r1 || f.sa.r2 != r2) r1 = r2 = -1;
     }
     const uint32_t n_items = uint32_t(item_frame.size());
+    // frames of the same stocks and filters share their spectral tables: the kernel then takes them once
+    bool shared = true;
+    for (size_t slot : slots) {
+        const PrintArgs& a = fr[slot].pa;
+        const PrintArgs& a0 = fr[slots[0]].pa;
+        shared = shared && std::memcmp(&a.enl, &a0.enl, sizeof a.enl) == 0 &&
+                 std::memcmp(&a.scan, &a0.scan, sizeof a.scan) == 0;
+    }
     auto up16 = [](size_t b) { return (b + 15) / 16 * 16; };
     const size_t o_sf = up16(n * sizeof(BatchPrintFrame));
     const size_t o_if = o_sf + up16(n * sizeof(BatchScanFrame));
@@ -880,7 +900,8 @@ void run_plan(Engine& e, const std::string& plan, const std::string& shape, std:
         e, key,
         [&](cudaStream_t s) {
             dev::print_batch(reinterpret_cast<const BatchPrintFrame*>(d), reinterpret_cast<const uint32_t*>(d + o_if),
-                             reinterpret_cast<const uint32_t*>(d + o_ip), n_items, item_px, ctas, s);
+                             reinterpret_cast<const uint32_t*>(d + o_ip), n_items, item_px, ctas,
+                             shared ? &fr[slots[0]].pa.enl : nullptr, shared ? &fr[slots[0]].pa.scan : nullptr, s);
             dev::scan_encode_batch(reinterpret_cast<const BatchScanFrame*>(d + o_sf), uint32_t(n), tiles, r1, r2, ctas,
                                    s);
             for (size_t j = 0; j < n; ++j) {

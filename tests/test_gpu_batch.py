@@ -141,3 +141,28 @@ def test_batch_refusals(engine, lib):
     finally:
         s1.close()
         s2.close()
+
+
+@pytest.mark.parametrize("plan", ["persistent:2048:592", "persistent:8192:2368"])
+def test_persistent_plan_with_per_frame_filters(engine, plan):
+    """Frames whose enlarger filters differ do not share spectral tables: the persistent print then stages
+    every frame's tables itself (the frames above share theirs, which the kernel takes once). Each frame
+    still equals its single render."""
+    specs = [(300, 200, {"m_filter_shift": 0.2}), (256, 128, {"y_filter_shift": -0.3}), (512, 288, {})]
+    imgs = [sc.synthetic_image(w, h, 40 + i) for i, (w, h, _) in enumerate(specs)]
+    singles_out = []
+    for img, (w, h, extra) in zip(imgs, specs):
+        with engine.open(img, dict(BASE, **extra)) as s:
+            singles_out.append(s.render("full")[0])
+    engine.batch_plan(plan)
+    ss = [engine.open(img, dict(BASE, **extra)) for img, (w, h, extra) in zip(imgs, specs)]
+    try:
+        res, info = engine.render_batch(ss, "full")
+        arrs, _ = take(res)
+        assert info["plan"] == plan
+        for a, want in zip(arrs, singles_out):
+            assert np.array_equal(a, want), plan
+    finally:
+        engine.batch_plan(None)
+        for s in ss:
+            s.close()
