@@ -62,10 +62,10 @@ N_SM = 148
 # From the ncu capture summarised in profiles/render_kernels_2048x2048_ncu.md (one 2048 x 2048 render +
 # reprint, --set full): DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) and warp instructions
 # (smsp__inst_executed.sum) per pixel of each kernel's launch. Traffic scales with the pixels launched.
-NCU_TRAFFIC_PER_PX = {"expose": 14.20, "iir_rows": 25.09, "iir_cols": 54.05,
-                      "develop_layers": 14.39, "fir_tile": 14.46, "print": 12.94, "scan_encode": 13.29}
-NCU_WARP_INST_PER_PX = {"expose": 15.07, "iir_rows": 18.37, "iir_cols": 13.05,
-                        "develop_layers": 171.30, "fir_tile": 10.06, "print": 60.29, "scan_encode": 28.23}
+NCU_TRAFFIC_PER_PX = {"expose": 14.24, "iir_rows": 25.09, "iir_cols": 53.98,
+                      "develop_layers": 14.10, "fir_tile": 14.46, "print": 13.54, "scan_encode": 13.21}
+NCU_WARP_INST_PER_PX = {"expose": 10.73, "iir_rows": 18.37, "iir_cols": 13.05,
+                        "develop_layers": 165.51, "fir_tile": 10.06, "print": 60.34, "scan_encode": 23.01}
 
 
 def workload_name():
