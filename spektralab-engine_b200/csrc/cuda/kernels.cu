@@ -9,7 +9,6 @@
 #include <math.h>
 #include <stdint.h>
 
-#include <algorithm>
 #include <atomic>
 #include <map>
 #include <mutex>
@@ -146,13 +145,8 @@ __device__ __forceinline__ void ld32(const float* p, float* r) {
                  : "l"(p));
 }
 
-// the pixel's bicubic set-up: base indices of the patch, weights and brightness
-struct ExposeTap {
-    int ba, bb;
-    float wa[4], wb[4], bp;
-};
-
-__device__ __forceinline__ ExposeTap expose_prepare(const ExposeArgs& q, float r, float g, float b) {
+__device__ __forceinline__ void expose_pixel(const ExposeArgs& q, const float* __restrict__ patches, float r, float g,
+                                             float b, float* h) {
     if (q.apply_ae) {
         r = __fmul_rn(r, q.ae_gain);
         g = __fmul_rn(g, q.ae_gain);
@@ -166,21 +160,21 @@ __device__ __forceinline__ ExposeTap expose_prepare(const ExposeArgs& q, float r
     const float x = X / d, y = Y / d, o = 1.0f - x;
     const float t0 = fminf(fmaxf(o * o, 0.0f), 1.0f);
     const float t1 = fminf(fmaxf(y / (o > 1e-10f ? o : 1e-10f), 0.0f), 1.0f);
-    ExposeTap tp;
-    tp.bp = isnan(bs) ? 0.0f : bs;
-    mitchell_base(t0, q.L, tp.ba, tp.wa);
-    mitchell_base(t1, q.L, tp.bb, tp.wb);
-    return tp;
-}
-
-// the weighted sum over the patch's sixteen texels (t: 48 floats, RGB in loop order), normalised and scaled
-__device__ __forceinline__ void expose_finish(const ExposeArgs& q, const ExposeTap& tp, const float* t, float* h) {
+    const float bp = isnan(bs) ? 0.0f : bs;
+    int ba, bb;
+    float wa[4], wb[4];
+    mitchell_base(t0, q.L, ba, wa);
+    mitchell_base(t1, q.L, bb, wb);
+    const float* pt = patches + (size_t(ba) * (q.L - 1) + size_t(bb)) * kPatchFloats;
+    float t[kPatchFloats];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) ld32(pt + 8 * k, t + 8 * k);
     float s = 0.0f, a0 = 0.0f, a1 = 0.0f, a2 = 0.0f;
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
-            const float w = tp.wa[i] * tp.wb[j];
+            const float w = wa[i] * wb[j];
             const float* tx = t + 3 * (4 * i + j);
             s += w;
             a0 += w * tx[0];
@@ -193,7 +187,7 @@ __device__ __forceinline__ void expose_finish(const ExposeArgs& q, const ExposeT
         a1 = a1 / s;
         a2 = a2 / s;
     }
-    float h0 = tp.bp * a0, h1 = tp.bp * a1, h2 = tp.bp * a2;
+    float h0 = bp * a0, h1 = bp * a1, h2 = bp * a2;
     if (q.apply_gain) {
         h0 = h0 * q.gain;
         h1 = h1 * q.gain;
@@ -202,20 +196,6 @@ __device__ __forceinline__ void expose_finish(const ExposeArgs& q, const ExposeT
     h[0] = h0;
     h[1] = h1;
     h[2] = h2;
-}
-
-__device__ __forceinline__ const float* patch_of(const ExposeArgs& q, const float* patches, const ExposeTap& tp) {
-    return patches + (size_t(tp.ba) * (q.L - 1) + size_t(tp.bb)) * kPatchFloats;
-}
-
-__device__ __forceinline__ void expose_pixel(const ExposeArgs& q, const float* __restrict__ patches, float r, float g,
-                                             float b, float* h) {
-    const ExposeTap tp = expose_prepare(q, r, g, b);
-    const float* pt = patch_of(q, patches, tp);
-    float t[kPatchFloats];
-#pragma unroll
-    for (int k = 0; k < 6; ++k) ld32(pt + 8 * k, t + 8 * k);
-    expose_finish(q, tp, t, h);
 }
 
 constexpr uint32_t kExposeThreads = 128;
@@ -241,126 +221,6 @@ __global__ void __launch_bounds__(kExposeThreads) k_expose_patch(const float* __
         for (uint32_t p = p0; p < q.n; ++p)
             expose_pixel(q, patches, rgb[3 * size_t(p)], rgb[3 * size_t(p) + 1], rgb[3 * size_t(p) + 2],
                          hout + 3 * size_t(p));
-    }
-}
-
-// The same pass with the patches gathered by the TMA unit. A CTA takes tiles of 128 pixels, one per thread,
-// in a two-stage pipeline: each thread reads its pixel, forms its bicubic set-up and issues one 192-byte
-// bulk copy (cp.async.bulk, global -> shared, no multicast) of its patch into its shared-memory slot,
-// completing on the stage's mbarrier (128 arrivals with their byte counts); while the TMA unit fetches the
-// next tile's patches the threads weigh the current tile's from shared memory. The random 192-byte
-// gathers thus bypass the L1 data path that bounds the direct-load kernel. Slots are 208 bytes apart, so
-// a quarter-warp's 16-byte reads of its eight patches fall in distinct banks. Every wait is bounded
-// (about 1 s); a CTA whose wait gives up sets *err, waits (bounded) for its copies in flight and leaves.
-constexpr uint32_t kGatherThreads = 128;
-constexpr uint32_t kPatchSlot = 208;
-constexpr uint32_t kPatchBytes = kPatchFloats * 4;
-constexpr long long kGatherWait = 2000000000ll;
-
-__device__ __forceinline__ uint32_t smem_u32(const void* p) { return uint32_t(__cvta_generic_to_shared(p)); }
-
-__device__ __forceinline__ bool gather_wait(uint32_t bar, uint32_t parity) {
-    const long long t0 = clock64();
-    for (;;) {
-        uint32_t done;
-        asm volatile(
-            "{\n\t.reg .pred p;\n\t"
-            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-            "selp.u32 %0, 1, 0, p;\n\t}"
-            : "=r"(done)
-            : "r"(bar), "r"(parity)
-            : "memory");
-        if (done) return true;
-        if (clock64() - t0 > kGatherWait) return false;
-    }
-}
-
-// thread tid's share of tile `tile`: its pixel's set-up, and the bulk copy of its patch into its slot of
-// `stage` (a pixel past the frame copies patch 0 so that every thread arrives with the same byte count)
-__device__ __forceinline__ ExposeTap gather_issue(const ExposeArgs& q, const float* __restrict__ rgb,
-                                                  const float* __restrict__ patches, uint32_t tile, uint32_t tid,
-                                                  unsigned char* slot, uint32_t bar) {
-    const uint32_t p = tile * kGatherThreads + tid;
-    ExposeTap tp{};
-    const float* src = patches;
-    if (p < q.n) {
-        tp = expose_prepare(q, __ldcs(rgb + 3 * size_t(p)), __ldcs(rgb + 3 * size_t(p) + 1),
-                            __ldcs(rgb + 3 * size_t(p) + 2));
-        src = patch_of(q, patches, tp);
-    }
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(kPatchBytes) : "memory");
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                     smem_u32(slot)),
-                 "l"(src), "r"(kPatchBytes), "r"(bar)
-                 : "memory");
-    return tp;
-}
-
-__global__ void __launch_bounds__(kGatherThreads) k_expose_gather(const float* __restrict__ rgb, float* __restrict__ hout,
-                                                                  const float* __restrict__ patches,
-                                                                  const __grid_constant__ ExposeArgs q, uint32_t* err) {
-    extern __shared__ __align__(128) unsigned char smem[];
-    unsigned char* slots = smem;  // [stage][thread] of kPatchSlot bytes
-    const uint32_t bar0 = smem_u32(smem + 2 * kGatherThreads * kPatchSlot);
-    const uint32_t tid = threadIdx.x;
-    const uint32_t tiles = (q.n + kGatherThreads - 1) / kGatherThreads;
-    if (tid == 0) {
-        for (uint32_t s = 0; s < 2; ++s)
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar0 + 8 * s), "r"(kGatherThreads) : "memory");
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-    __syncthreads();
-    uint32_t phase = 0u, pending = 0u;  // bit s: the parity stage s waits for next; stage s has copies in flight
-    uint32_t tile = blockIdx.x;
-    ExposeTap cur{};
-    if (tile < tiles) {
-        cur = gather_issue(q, rgb, patches, tile, tid, slots + tid * kPatchSlot, bar0);
-        pending |= 1u;
-    }
-    bool failed = false;
-    for (uint32_t k = 0; tile < tiles; ++k, tile += gridDim.x) {
-        const uint32_t s = k & 1u, o = s ^ 1u;
-        ExposeTap nxt{};
-        const bool more = tile + gridDim.x < tiles;
-        if (more) {
-            nxt = gather_issue(q, rgb, patches, tile + gridDim.x, tid, slots + (o * kGatherThreads + tid) * kPatchSlot,
-                               bar0 + 8 * o);
-            pending |= 1u << o;
-        }
-        const bool mine = gather_wait(bar0 + 8 * s, (phase >> s) & 1u);
-        if (__syncthreads_or(mine ? 0 : 1)) {
-            failed = true;
-            break;
-        }
-        phase ^= 1u << s;
-        pending &= ~(1u << s);
-        const uint32_t p = tile * kGatherThreads + tid;
-        if (p < q.n) {
-            const float4* sl = reinterpret_cast<const float4*>(slots + (s * kGatherThreads + tid) * kPatchSlot);
-            float t[kPatchFloats];
-#pragma unroll
-            for (int i = 0; i < 12; ++i) {
-                const float4 v = sl[i];
-                t[4 * i] = v.x;
-                t[4 * i + 1] = v.y;
-                t[4 * i + 2] = v.z;
-                t[4 * i + 3] = v.w;
-            }
-            float h[3];
-            expose_finish(q, cur, t, h);
-            hout[3 * size_t(p)] = h[0];
-            hout[3 * size_t(p) + 1] = h[1];
-            hout[3 * size_t(p) + 2] = h[2];
-        }
-        // the slot is read before the TMA unit writes it again (next iteration but one)
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        __syncthreads();
-        cur = nxt;
-    }
-    if (failed) {
-        if (tid == 0) atomicOr(err, 1u);
-        for (uint32_t s = 0; s < 2; ++s)  // the copies still in flight land before the CTA leaves
-            if ((pending >> s) & 1u) (void)gather_wait(bar0 + 8 * s, (phase >> s) & 1u);
     }
 }
 
@@ -999,19 +859,9 @@ void set_launch_hook(LaunchHook* hook) { t_hook = hook; }
 uint64_t launch_count() { return g_launches.load(); }
 
 void expose(const float* rgb, float* h, const float* table4, const float* patches, const ExposeArgs& a,
-            uint32_t* err, cudaStream_t s) {
+            cudaStream_t s) {
     if (a.n == 0) return;
     Probe p("expose", s);
-    if (patches && err) {
-        constexpr int smem = int(2 * kGatherThreads * kPatchSlot + 16);
-        ensure_smem(reinterpret_cast<const void*>(k_expose_gather), smem);
-        int dev = 0, sms = 148;
-        if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        const uint32_t tiles = div_up(a.n, kGatherThreads);
-        const uint32_t grid = std::min<uint32_t>(tiles, uint32_t(sms) * 4u);
-        k_expose_gather<<<grid, kGatherThreads, smem, s>>>(rgb, h, patches, a, err);
-        return;
-    }
     const bool aligned = ((reinterpret_cast<uintptr_t>(rgb) | reinterpret_cast<uintptr_t>(h)) & 15u) == 0;
     if (patches && aligned) {
         k_expose_patch<<<div_up(div_up(a.n, 4), kExposeThreads), kExposeThreads, 0, s>>>(rgb, h, patches, a);

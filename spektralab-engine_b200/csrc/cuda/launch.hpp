@@ -53,11 +53,9 @@ void boost(float* p, size_t n, float x0, float r, float a, float k, cudaStream_t
 
 // RGB -> film exposure H (Mitchell bicubic of the spectral table, L x L float4 texels), times the
 // compensation gain.
-// patches (may be null): the table as 4 x 4 patches (kPatchFloats floats per base pair, (L - 1)^2 pairs).
-// With patches and err, the TMA-gather kernel runs (err: a device word or-ed with 1 when a wait gave up);
-// with patches alone the direct-load kernel, when both planes are 16-byte aligned; else the texel kernel
-// reads table4. The three compute the same values.
-void expose(const float* rgb, float* h, const float* table4, const float* patches, const ExposeArgs& a, uint32_t* err,
+// patches (may be null): the table as 4 x 4 patches (kPatchFloats floats per base pair, (L - 1)^2 pairs),
+// read by the vectorised kernel when both planes are 16-byte aligned; else the texel kernel reads table4.
+void expose(const float* rgb, float* h, const float* table4, const float* patches, const ExposeArgs& a,
             cudaStream_t s);
 
 // Separable FIR: vertical pass in -> out (no accumulation).

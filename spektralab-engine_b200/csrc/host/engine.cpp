@@ -225,8 +225,6 @@ public:
     int print_mode = -1;  // spkx_session_set_print_mode: -1 the binary32 print kernel, else a SpectralMode
     uint32_t print_bins = SPKB_NL;
     ProgressRecord progress;
-    DevBuffer err_dev;            // the develop's kernel error word, cleared before each develop
-    uint32_t* err_host = nullptr;  // its pinned copy, read after the stream's final synchronisation
     Plane meter_image;                // the frame at the meter's 1600 px long edge, kept
     std::optional<MeterValues> meter;  // until a field of the meter's key changes
 
@@ -245,7 +243,6 @@ public:
             cudaStreamDestroy(copy_stream);
         }
         for (cudaEvent_t e : band_events) cudaEventDestroy(e);
-        if (err_host) cudaFreeHost(err_host);
     }
 
     void digest(ParamSet& p, const Profile& f) const {
@@ -430,10 +427,6 @@ Session* open_session(Engine& e, const void* data, bool device_ptr, uint32_t w, 
     cuda_check(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "cudaStreamCreate");
     cuda_check(cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking), "cudaStreamCreate");
     s->pool.set_stream(s->stream);
-    s->err_dev = s->pool.persistent(16);
-    cuda_check(cudaHostAlloc(reinterpret_cast<void**>(&s->err_host), sizeof(uint32_t), cudaHostAllocDefault),
-               "cudaHostAlloc");
-    *s->err_host = 0;
     ParamSet p;
     for (const auto& [fid, v] : d.fields)
         if (fid == size_t(P::film_stock) || fid == size_t(P::print_stock)) p.set(fid, v);
@@ -493,19 +486,9 @@ void develop_tier(Session& s, Tier t, RenderCtx& ctx) {
     const uint32_t seed = s.params.b(P::grain_active) ? s.seeds.next() : kNoGrainFilmSeed;
     ctx.pitch_um = s.tier_pitch_um(ts);
     ts.applied_ev.reset();
-    cuda_check(cudaMemsetAsync(s.err_dev.ptr(), 0, sizeof(uint32_t), s.stream), "error word");
-    ctx.dev_err = s.err_dev.as<uint32_t>();
     ts.negative = develop(ctx, s.pipe, ts.source, seed, s.hal);
-    ctx.dev_err = nullptr;
-    cuda_check(cudaMemcpyAsync(s.err_host, s.err_dev.ptr(), sizeof(uint32_t), cudaMemcpyDeviceToHost, s.stream),
-               "error word");
     ts.pitch_um = ctx.pitch_um;
     ts.applied_ev = ctx.ae_ev;
-}
-
-// After the session stream's synchronisation: a develop whose gather wait gave up is a GPU failure.
-void check_develop(const Session& s) {
-    if (*s.err_host) fail_gpu("develop: a TMA gather wait of the expose pass gave up");
 }
 
 void render(Session& s, const char* tier_name, bool reprint, spk_result* out) {
@@ -541,7 +524,6 @@ void render(Session& s, const char* tier_name, bool reprint, spk_result* out) {
                        "result copy");
         cuda_check(cudaStreamSynchronize(s.stream), "render");
         cuda_check(cudaGetLastError(), "render");
-        if (developed) check_develop(s);
     } catch (...) {
         // band copies may still be writing the image's host pixels
         (void)cudaStreamSynchronize(s.copy_stream);
@@ -630,7 +612,6 @@ void preview_stock_lut(Session& s, const char* print_stock, const char* tier_nam
         dev::print_lut(ts.negative.data(), img->dev, a, s.stream);
         cuda_check(cudaMemcpyAsync(img->host, img->dev, img->bytes, cudaMemcpyDeviceToHost, s.stream), "result copy");
         cuda_check(cudaStreamSynchronize(s.stream), "print table");
-        if (developed) check_develop(s);
         cuda_check(cudaGetLastError(), "print table");
         apply_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - ta).count();
     } catch (...) {
@@ -1055,7 +1036,6 @@ void render_batch(std::vector<Session*> ss, const char* tier_name, bool reprint,
         cuda_check(cudaStreamSynchronize(bs), "batch");
         for (size_t i = 0; i < n; ++i) {
             cuda_check(cudaStreamSynchronize(ss[i]->stream), "batch");
-            if (fr[i].developed) check_develop(*ss[i]);
             float ms = 0.0f;
             if (cudaEventElapsedTime(&ms, e.start_event, e.frame_events[i]) == cudaSuccess) {
                 done_ms[i] = ms;
@@ -1148,20 +1128,12 @@ std::string session_profile(Session& s, const char* tier_name, bool reprint, uin
             ctx.print_mode = s.print_mode;
             ctx.print_bins = s.print_bins;
             cudaEventRecord(a, s.stream);
-            bool developed = false;
-            if (!reprint || !ts.negative) {  // as render's develop_tier does, error word included
+            if (!reprint || !ts.negative) {
                 ctx.ae_ev = s.session_ev();
                 ctx.pitch_um = s.tier_pitch_um(ts);
                 const uint32_t seed = s.params.b(P::grain_active) ? s.seeds.next() : kNoGrainFilmSeed;
-                cuda_check(cudaMemsetAsync(s.err_dev.ptr(), 0, sizeof(uint32_t), s.stream), "error word");
-                ctx.dev_err = s.err_dev.as<uint32_t>();
                 ts.negative = develop(ctx, s.pipe, ts.source, seed, s.hal);
-                ctx.dev_err = nullptr;
-                cuda_check(cudaMemcpyAsync(s.err_host, s.err_dev.ptr(), sizeof(uint32_t), cudaMemcpyDeviceToHost,
-                                           s.stream),
-                           "error word");
                 ts.pitch_um = ctx.pitch_um;
-                developed = true;
             }
             ctx.print_seed = s.draw_print_seed();
             ctx.pitch_um = ts.pitch_um;
@@ -1169,7 +1141,6 @@ std::string session_profile(Session& s, const char* tier_name, bool reprint, uin
             print_scan_encode(ctx, s.pipe, s.live, ts.negative, img);
             cudaEventRecord(b, s.stream);
             cuda_check(cudaStreamSynchronize(s.stream), "profile step");
-            if (developed) check_develop(s);
             float ms = 0;
             cudaEventElapsedTime(&ms, a, b);
             totals.push_back(json::Value(double(ms)));

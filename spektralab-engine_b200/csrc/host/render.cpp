@@ -633,8 +633,7 @@ Plane develop(RenderCtx& ctx, const Pipeline& p, const Plane& tier_source, uint3
             ea.ae_gain = f32(std::pow(2.0, *ctx.ae_ev));
             ea.apply_ae = 1;
         }
-        dev::expose(source.data(), H.data(), p.dev.table.as<float>(), p.dev.patches.as<float>(), ea, ctx.dev_err,
-                    ctx.stream);
+        dev::expose(source.data(), H.data(), p.dev.table.as<float>(), p.dev.patches.as<float>(), ea, ctx.stream);
     }
     if (const double bev = f.params.f(P::halation_boost_ev); bev != 0.0) {
         ctx.node("filming.boost");
@@ -1204,8 +1203,7 @@ void render_vjp(RenderCtx& ctx, const Pipeline& p, const LiveParams& live, const
     // ---- forward, keeping what the adjoint needs ----
     Plane H0 = make_plane(ctx.pool, w, h);
     const ExposeArgs ea = expose_args(f, n);
-    dev::expose(source.data(), H0.data(), p.dev.table.as<float>(), p.dev.patches.as<float>(), ea, ctx.dev_err,
-                ctx.stream);
+    dev::expose(source.data(), H0.data(), p.dev.table.as<float>(), p.dev.patches.as<float>(), ea, ctx.stream);
     const double s_lens = film_lens_blur_px(ctx, f);
     Plane H1 = H0;
     if (s_lens > 0.0) {

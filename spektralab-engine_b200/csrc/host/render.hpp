@@ -80,9 +80,6 @@ struct RenderCtx {
     int print_mode = -1;
     uint32_t print_bins = SPKB_NL;
     float* contraction_out = nullptr;
-    // a device word the TMA-gather kernels set when one of their waits gave up (null: the direct-load
-    // kernels run instead); the caller clears it before and reads it after
-    uint32_t* dev_err = nullptr;
     // the print side's copy to the output image's host pixels, in row bands on copy_stream (events from
     // band_events, grown as needed), overlapping the next band's kernels; null: no banded copy
     cudaStream_t copy_stream = nullptr;
