@@ -553,16 +553,26 @@ __global__ void k_develop(const float* __restrict__ exposure, float* __restrict_
 // counts are those of the per-lane sampler.
 
 constexpr uint32_t kDrawWarps = 4;
+// resident blocks per SM the register allocation is held to (1: no cap)
+#ifndef SPKB_DEVELOP_MIN_BLOCKS
+#define SPKB_DEVELOP_MIN_BLOCKS 1
+#endif
 constexpr uint32_t kDrawRing = 64;  // holds the < 32 left over plus one draw's 32
 
 struct DeferredDraw {
-    float lam, b, a, vr; // the squeeze's PTRS constants (kinds 1, 2); lam alone for kind 0
-    float V, k, us;      // attempt 0's full test, pending (kind 1)
-    uint32_t w2, w3;     // words z, w of Philox block 0: attempt 1's uniforms (kinds 1, 2)
-    uint32_t pixel;
-    uint32_t tag;        // kind | stream << 2 | (draw * 32 + lane) << 10
+    float lam, b, a, vr;        // the squeeze's PTRS constants (kinds 1, 2); lam alone for kind 0
+    float loglam, loginvalpha;  // the full test's constants, once formed (kTagInited)
+    float V, k, us;             // the last attempt's full test, pending (kind 1)
+    uint32_t w2, w3;            // words z, w of the last Philox block: the next attempt's uniforms when it is odd
+    uint32_t tag;               // kind | kTagInited | stream << 3 | slot << 11 | next attempt << 20
 };
-// kinds: 0 product method (lam < 10 or NaN); 1 attempt 0 needs the full test; 2 attempt 0 rejected
+// kinds: 0 product method (lam < 10 or NaN); 1 the last attempt needs the full test; 2 it was rejected.
+// slot = draw * 32 + lane: the draw's pixel is the warp's first plus the lane.
+constexpr uint32_t kResStride = kDrawWarps * 32;  // a draw's row in the block's lambda / result array
+constexpr uint32_t kTagInited = 4u;
+__device__ __forceinline__ uint32_t draw_tag(uint32_t kind, uint32_t stream, uint32_t slot, uint32_t next) {
+    return kind | (stream << 3) | (slot << 11) | (next << 20);
+}
 
 // log(k!) for k = 0 .. kLgammaTable - 1, each the sampler's own spk_lgamma_k(k + 1) computed by this
 // device once per process (k_lgamma_table): the full test's largest single cost, a table read instead.
@@ -583,53 +593,82 @@ __device__ __forceinline__ int ptrs_test_table(const spk_ptrs* p, float V, float
     return L <= Rt;
 }
 
-// The rest of a deferred draw: attempt 0's pending full test (kind 1), then attempts 1..63 exactly as
-// spk_ptrs_from runs them, with one copy of the test, the squeeze and the generator in the loop. The
-// test's own constants (log lam, 1 / alpha) are formed here, for the draws that reach it.
-__device__ __forceinline__ void finish_draw(const DeferredDraw& d, uint32_t seed, float* res) {
-    const uint32_t kind = d.tag & 3u, stream = (d.tag >> 2) & 0xFFu, slot = d.tag >> 10;
-    spk_stream g;
-    spk_stream_init(&g, d.pixel, stream, seed);
-    float value;
+// One step of a deferred draw, exactly as spk_ptrs_from runs it: the last attempt's pending full test
+// (kind 1), then, unless that accepted, the next attempt's uniforms and squeeze. Returns true once the
+// draw's count is in res; false with e holding the state to queue again (kind 1 or 2, the next attempt).
+// A product-method draw (kind 0) ends in one step. The test's constants (log lam, log 1 / alpha) are
+// formed the first time a draw reaches the test and travel with it. pixel0: the warp's first pixel; res:
+// the warp's results, draw k of lane j at res[k * kResStride + j].
+__device__ __forceinline__ bool finish_step(DeferredDraw& e, uint32_t seed, uint32_t pixel0, float* res_warp) {
+    const uint32_t kind = e.tag & 3u, stream = (e.tag >> 3) & 0xFFu, slot = (e.tag >> 11) & 0x1FFu;
+    const uint32_t it = e.tag >> 20;
+    const uint32_t pixel = pixel0 + (slot & 31u);
+    float* res = res_warp + (slot >> 5) * kResStride + (slot & 31u);
     if (kind == 0u) {
-        value = spk_poisson_product(d.lam, &g);
-    } else {
-        spk_ptrs p;
-        p.lam = d.lam;
-        p.b = d.b;
-        p.a = d.a;
-        p.vr = d.vr;
-        spk_ptrs_init_test(&p);
-        g.block.z = d.w2;
-        g.block.w = d.w3;
-        g.used = 2;
-        g.j = 1;
-        float k = d.k, us = d.us, V = d.V;
-        int state = kind == 1u ? SPK_PTRS_TEST : SPK_PTRS_REJECT;
-        for (int it = 1;; ++it) {
-            // state: the outcome of attempt it - 1's squeeze
-            if (state == SPK_PTRS_ACCEPT || (state == SPK_PTRS_TEST && ptrs_test_table(&p, V, k, us))) {
-                value = k;
-                break;
-            }
-            if (it == 64) {
-                value = SPK_FLOOR(p.lam);
-                break;
-            }
-            const float u = spk_stream_uniform(&g);
-            V = spk_stream_uniform(&g);
-            state = spk_ptrs_squeeze(&p, u, V, &k, &us);
+        spk_stream g;
+        spk_stream_init(&g, pixel, stream, seed);
+        *res = spk_poisson_product(e.lam, &g);
+        return true;
+    }
+    spk_ptrs p;
+    p.lam = e.lam;
+    p.b = e.b;
+    p.a = e.a;
+    p.vr = e.vr;
+    bool inited = (e.tag & kTagInited) != 0u;
+    if (kind == 1u) {
+        if (inited) {
+            p.loglam = e.loglam;
+            p.loginvalpha = e.loginvalpha;
+        } else {
+            spk_ptrs_init_test(&p);
+            e.loglam = p.loglam;
+            e.loginvalpha = p.loginvalpha;
+            inited = true;
+        }
+        if (ptrs_test_table(&p, e.V, e.k, e.us)) {
+            *res = e.k;
+            return true;
         }
     }
-    res[slot] = value;
+    if (it == 64u) {
+        *res = SPK_FLOOR(p.lam);
+        return true;
+    }
+    // attempt it takes uniforms 2 it and 2 it + 1: words x, y of Philox block it / 2 (it even, keeping z, w
+    // for attempt it + 1) or the kept z, w (it odd)
+    uint32_t wu = e.w2, wv = e.w3;
+    if ((it & 1u) == 0u) {
+        spk_u4 c4;
+        c4.x = pixel;
+        c4.y = stream;
+        c4.z = it >> 1;
+        c4.w = 0u;
+        const spk_u4 b = spk_philox(c4, seed, 0u);
+        wu = b.x;
+        wv = b.y;
+        e.w2 = b.z;
+        e.w3 = b.w;
+    }
+    const float V = spk_uniform(wv);
+    float k, us;
+    const int r = spk_ptrs_squeeze(&p, spk_uniform(wu), V, &k, &us);
+    if (r == SPK_PTRS_ACCEPT) {
+        *res = k;
+        return true;
+    }
+    e.V = V;
+    e.k = k;
+    e.us = us;
+    e.tag = draw_tag(r == SPK_PTRS_TEST ? 1u : 2u, stream, slot, it + 1u) | (inited ? kTagInited : 0u);
+    return false;
 }
 
-__global__ void __launch_bounds__(kDrawWarps * 32) k_develop_layers(const float* __restrict__ exposure,
+__global__ void __launch_bounds__(kDrawWarps * 32, SPKB_DEVELOP_MIN_BLOCKS) k_develop_layers(const float* __restrict__ exposure,
                                                                     float* __restrict__ out, uint32_t w,
                                                                     uint32_t blocks_per_row,
                                                                     const __grid_constant__ DevelopArgs q) {
     __shared__ DeferredDraw ring[kDrawWarps][kDrawRing];
-    __shared__ float res[kDrawWarps][9 * 32];
     __shared__ float lam[9][kDrawWarps * 32], scale[9][kDrawWarps * 32];  // [c * 3 + l][thread]
     const uint32_t lane = threadIdx.x & 31u, wi = threadIdx.x >> 5, tid = threadIdx.x;
     const uint32_t y = blockIdx.x / blocks_per_row;
@@ -656,12 +695,14 @@ __global__ void __launch_bounds__(kDrawWarps * 32) k_develop_layers(const float*
                 live ? spk_sublayer_lambda(dl[l] + q.dmin_l[lc], q.sat_d[lc], q.count[lc], q.uniformity[c], &sat)
                      : 0.0f;
             if (q.lam_out && live) q.lam_out[size_t(pixel) * 9 + c * 3 + l] = lam[c * 3 + l][tid];
-            scale[c * 3 + l][tid] = SPK_MUL(SPK_DIV(q.sat_d[lc], q.count[lc]), sat);
+            scale[c * 3 + l][tid] = SPK_MUL(q.unit[lc], sat);  // unit: SPK_DIV(sat_d, count), formed once
         }
     }
 
     DeferredDraw* ringw = ring[wi];
-    float* resw = res[wi];
+    // a draw's count replaces its lambda once the lockstep has read it: lam[k][tid] holds draw k of thread
+    // tid until its attempt 0, then its count
+    float* resw = &lam[0][wi * 32u];
     uint32_t head = 0, tail = 0;
 #pragma unroll 1
     for (uint32_t k = 0; k < 9u; ++k) {
@@ -669,7 +710,6 @@ __global__ void __launch_bounds__(kDrawWarps * 32) k_develop_layers(const float*
         bool defer = false;
         float value = 0.0f;
         DeferredDraw d{};
-        d.pixel = pixel;
         uint32_t kind = 0u;
         const float lm = lam[k][tid];
         d.lam = lm;
@@ -705,17 +745,28 @@ __global__ void __launch_bounds__(kDrawWarps * 32) k_develop_layers(const float*
         }
         const uint32_t mask = __ballot_sync(0xFFFFFFFFu, defer);
         if (defer) {
-            d.tag = kind | (stream << 2) | ((k * 32u + lane) << 10);
+            d.tag = draw_tag(kind, stream, k * 32u + lane, 1u);
             ringw[(tail + __popc(mask & ((1u << lane) - 1u))) & (kDrawRing - 1u)] = d;
         } else {
-            resw[k * 32u + lane] = value;
+            resw[k * kResStride + lane] = value;
         }
         tail += __popc(mask);
-        // finish 32 deferred draws at a time; after the last draw, whatever is left (at most 63)
+        // one step for 32 deferred draws at a time, the unfinished queued again behind the rest; after the
+        // last draw, until none is left. The ring holds at most 63: fewer than 32 left over plus 32 queued.
         while (tail - head >= 32u || (k == 8u && tail != head)) {
             __syncwarp();
-            if (lane < tail - head) finish_draw(ringw[(head + lane) & (kDrawRing - 1u)], q.seed, resw);
-            head += min(tail - head, 32u);
+            const uint32_t n = min(tail - head, 32u);
+            DeferredDraw e;
+            bool again = false;
+            if (lane < n) {
+                e = ringw[(head + lane) & (kDrawRing - 1u)];
+                again = !finish_step(e, q.seed, pixel - lane, resw);
+            }
+            head += n;
+            __syncwarp();
+            const uint32_t m = __ballot_sync(0xFFFFFFFFu, again);
+            if (again) ringw[(tail + __popc(m & ((1u << lane) - 1u))) & (kDrawRing - 1u)] = e;
+            tail += __popc(m);
             __syncwarp();
         }
     }
@@ -725,7 +776,7 @@ __global__ void __launch_bounds__(kDrawWarps * 32) k_develop_layers(const float*
         float val[3];
 #pragma unroll
         for (int l = 0; l < 3; ++l) {
-            const float cnt = resw[(c * 3 + l) * 32 + lane];
+            const float cnt = resw[(c * 3 + l) * kResStride + lane];
             if (q.counts_out) q.counts_out[size_t(pixel) * 9 + c * 3 + l] = cnt;
             val[l] = SPK_MUL(cnt, scale[c * 3 + l][tid]);
         }

@@ -494,6 +494,7 @@ DevelopPlan develop_plan(const RenderCtx& ctx, const Pipeline& p, uint32_t w, ui
             da.dmin_l[l * 3 + c] = f32(kc.dmin_l[l][c]);
             da.sat_d[l * 3 + c] = f32(kc.sat_d[l][c]);
             da.count[l * 3 + c] = f32(kc.count[l][c]);
+            da.unit[l * 3 + c] = da.sat_d[l * 3 + c] / da.count[l * 3 + c];
         }
     if (g->sublayers) {
         da.mode = 0;  // SUM

@@ -67,6 +67,7 @@ struct DevelopArgs {
     uint32_t n_sub;
     float inv_n_sub;
     float dmin_l[9], sat_d[9], count[9];
+    float unit[9];        // sat_d / count, the binary32 quotient (a draw's density per grain before saturation)
     float uniformity[3];
     float dmin_c[3];
     const float* axis;    // [k*3 + c]
