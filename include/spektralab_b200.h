@@ -130,8 +130,9 @@ SPK_API spk_status spkx_render_batch(spk_session* const* sessions, uint32_t n, c
 
 /* spkx_engine_batch_plan(engine, plan)
  *   pins the plan of every later spkx_render_batch of this engine ("frames:K", K 1..16: per-frame launches on
- *   K worker streams; "persistent:S:C": items of S pixels, S even, over C CTAs); NULL or "" restores the
- *   timed choice. SPK_ERR_INVALID_ARG for any other string.
+ *   K worker streams; "persistent:S:C": items of S pixels, S even, over C CTAs; "persistent:S:C:G": the
+ *   same in G consecutive groups of frames, G 1..1024, each group's result copies overlapping the next
+ *   group's launches); NULL or "" restores the timed choice. SPK_ERR_INVALID_ARG for any other string.
  */
 SPK_API spk_status spkx_engine_batch_plan(spk_engine* engine, const char* plan);
 

@@ -685,7 +685,9 @@ spk_status render_common(spk_session* session, const char* tier, spk_result* out
 //   frames:K          each frame's print and scanner launches on one of K worker streams (round robin),
 //                     forked from and joined to the batch stream; the frames overlap on the device;
 //   persistent:S:C    one print launch and one scanner launch for all frames: C CTAs walking items of S
-//                     pixels (print) and the frames' concatenated 32 x 32 tile lists (scanner).
+//                     pixels (print) and the frames' concatenated 32 x 32 tile lists (scanner);
+//   persistent:S:C:G  the same launches for G consecutive groups of frames (about equal pixels each), each
+//                     group's result copies on a worker stream while the next group's launches run.
 // Every plan runs the same per-pixel and per-tile code as spk_render, so the pixels are those of singles.
 // The first batch of a list of frame sizes times each candidate plan on the device and keeps the fastest.
 
@@ -704,8 +706,8 @@ struct BatchFrame {
     std::string pid;              // the frame's progress id
 };
 
-// The tuner's candidates: per-frame launches on 4 or 16 streams, and the persistent launches over a grid of
-// item sizes (pixels per print item) and CTA counts (4, 8 and 16 per SM)
+// The tuner's candidates: per-frame launches on 4 or 16 streams, the persistent launches over a grid of item
+// sizes (pixels per print item) and CTA counts (4, 8 and 16 per SM), and grouped persistent launches
 const char* const kBatchPlans[] = {"frames:4",
                                    "frames:16",
                                    "persistent:2048:592",
@@ -716,10 +718,17 @@ const char* const kBatchPlans[] = {"frames:4",
                                    "persistent:8192:2368",
                                    "persistent:32768:592",
                                    "persistent:32768:1184",
-                                   "persistent:32768:2368"};
+                                   "persistent:32768:2368",
+                                   "persistent:8192:1184:4",
+                                   "persistent:8192:1184:8",
+                                   "persistent:8192:1184:16",
+                                   "persistent:8192:2368:8",
+                                   "persistent:32768:1184:8",
+                                   "persistent:2048:1184:8"};
 constexpr size_t kMaxWorkers = 16;
 
-// A plan string: "frames:K" (1 <= K <= 16) or "persistent:S:C" (S even, 2 .. 2^20 pixels; 1 <= C <= 65535).
+// A plan string: "frames:K" (1 <= K <= 16) or "persistent:S:C[:G]" (S even, 2 .. 2^20 pixels; 1 <= C <= 65535;
+// 1 <= G <= 1024).
 bool valid_plan(const std::string& p) {
     auto number = [](const std::string& t, unsigned long lo, unsigned long hi, unsigned long& v) {
         if (t.empty() || t.size() > 9 || t.find_first_not_of("0123456789") != std::string::npos) return false;
@@ -732,7 +741,11 @@ bool valid_plan(const std::string& p) {
     const std::string rest = p.substr(11);
     const size_t c = rest.find(':');
     if (c == std::string::npos) return false;
-    return number(rest.substr(0, c), 2, 1ul << 20, a) && a % 2 == 0 && number(rest.substr(c + 1), 1, 65535, b);
+    const size_t c2 = rest.find(':', c + 1);
+    unsigned long g = 1;
+    if (c2 != std::string::npos && !number(rest.substr(c2 + 1), 1, 1024, g)) return false;
+    return number(rest.substr(0, c), 2, 1ul << 20, a) && a % 2 == 0 &&
+           number(rest.substr(c + 1, c2 == std::string::npos ? std::string::npos : c2 - c - 1), 1, 65535, b);
 }
 
 void batch_resources(Engine& e, size_t n_frames, size_t n_workers) {
@@ -843,73 +856,117 @@ void run_plan(Engine& e, const std::string& plan, const std::string& shape, std:
         return;
     }
     for (size_t slot : slots) cuda_check(cudaStreamWaitEvent(bs, fr[slot].ready, 0), "frame ready");
-    // persistent:S:C
-    const size_t c1 = plan.find(':'), c2 = plan.find(':', c1 + 1);
+    // persistent:S:C[:G]
+    const size_t c1 = plan.find(':'), c2 = plan.find(':', c1 + 1), c3 = plan.find(':', c2 + 1);
     const uint32_t item_px = uint32_t(std::stoul(plan.substr(c1 + 1, c2 - c1 - 1)));
-    const uint32_t ctas = uint32_t(std::stoul(plan.substr(c2 + 1)));
+    const uint32_t ctas = uint32_t(std::stoul(plan.substr(c2 + 1, c3 == std::string::npos ? std::string::npos : c3 - c2 - 1)));
     const size_t n = slots.size();
-    std::vector<BatchPrintFrame> pf(n);
-    std::vector<BatchScanFrame> sf(n);
-    std::vector<uint32_t> item_frame, item_first;
-    uint32_t tiles = 0;
-    int r1 = fr[slots[0]].sa.r1, r2 = fr[slots[0]].sa.r2;
-    for (size_t j = 0; j < n; ++j) {
-        BatchFrame& f = fr[slots[j]];
-        pf[j].args = f.pa;
-        pf[j].neg = f.neg;
-        pf[j].rgb = f.rgb.data();
-        for (uint32_t p = 0; p < f.pa.n; p += item_px) {
-            item_frame.push_back(uint32_t(j));
-            item_first.push_back(p);
+    const size_t G = std::min(n, c3 == std::string::npos ? size_t(1) : size_t(std::stoul(plan.substr(c3 + 1))));
+    // the frames in G consecutive groups of about equal pixel counts
+    std::vector<size_t> first(1, 0);
+    {
+        uint64_t total = 0, acc = 0;
+        for (size_t slot : slots) total += fr[slot].pa.n;
+        for (size_t j = 0; j < n && first.size() < G; ++j) {
+            acc += fr[slots[j]].pa.n;
+            if (acc * G >= total * first.size() && j + 1 < n) first.push_back(j + 1);
         }
-        sf[j].args = f.sa;
-        sf[j].rgb = f.rgb.data();
-        sf[j].out = f.img->dev;
-        sf[j].w = f.rgb.w;
-        sf[j].h = f.rgb.h;
-        sf[j].tiles_x = dev::scan_tiles_x(f.rgb.w);
-        sf[j].first_tile = tiles;
-        tiles += dev::scan_tiles(f.rgb.w, f.rgb.h);
-        if (f.sa.r1 != r1 || f.sa.r2 != r2) r1 = r2 = -1;
+        first.push_back(n);
     }
-    const uint32_t n_items = uint32_t(item_frame.size());
-    // frames of the same stocks and filters share their spectral tables: the kernel then takes them once
-    bool shared = true;
-    for (size_t slot : slots) {
-        const PrintArgs& a = fr[slot].pa;
-        const PrintArgs& a0 = fr[slots[0]].pa;
-        shared = shared && std::memcmp(&a.enl, &a0.enl, sizeof a.enl) == 0 &&
-                 std::memcmp(&a.scan, &a0.scan, sizeof a.scan) == 0;
-    }
+    // one table blob for all groups: per group its print frames, scanner frames and print items
+    struct GroupLayout {
+        size_t o_pf, o_sf, o_if, o_ip;
+        uint32_t n_items, tiles;
+        int r1, r2;
+        bool shared;
+    };
     auto up16 = [](size_t b) { return (b + 15) / 16 * 16; };
-    const size_t o_sf = up16(n * sizeof(BatchPrintFrame));
-    const size_t o_if = o_sf + up16(n * sizeof(BatchScanFrame));
-    const size_t o_ip = o_if + up16(n_items * sizeof(uint32_t));
-    const size_t bytes = o_ip + up16(n_items * sizeof(uint32_t));
-    std::vector<unsigned char> blob(bytes, 0);
-    std::memcpy(blob.data(), pf.data(), n * sizeof(BatchPrintFrame));
-    std::memcpy(blob.data() + o_sf, sf.data(), n * sizeof(BatchScanFrame));
-    std::memcpy(blob.data() + o_if, item_frame.data(), n_items * sizeof(uint32_t));
-    std::memcpy(blob.data() + o_ip, item_first.data(), n_items * sizeof(uint32_t));
+    std::vector<GroupLayout> gl(first.size() - 1);
+    std::vector<unsigned char> blob;
+    auto append = [&](const void* src, size_t bytes) {
+        const size_t o = blob.size();
+        blob.resize(o + up16(bytes), 0);
+        if (bytes) std::memcpy(blob.data() + o, src, bytes);
+        return o;
+    };
+    for (size_t g = 0; g + 1 < first.size(); ++g) {
+        const size_t j0 = first[g], j1 = first[g + 1];
+        std::vector<BatchPrintFrame> pf(j1 - j0);
+        std::vector<BatchScanFrame> sf(j1 - j0);
+        std::vector<uint32_t> item_frame, item_first;
+        GroupLayout& L = gl[g];
+        L.tiles = 0;
+        L.r1 = fr[slots[j0]].sa.r1;
+        L.r2 = fr[slots[j0]].sa.r2;
+        // frames of the same stocks and filters share their spectral tables: the kernel then takes them once
+        L.shared = true;
+        for (size_t j = j0; j < j1; ++j) {
+            BatchFrame& f = fr[slots[j]];
+            pf[j - j0].args = f.pa;
+            pf[j - j0].neg = f.neg;
+            pf[j - j0].rgb = f.rgb.data();
+            for (uint32_t q = 0; q < f.pa.n; q += item_px) {
+                item_frame.push_back(uint32_t(j - j0));
+                item_first.push_back(q);
+            }
+            sf[j - j0].args = f.sa;
+            sf[j - j0].rgb = f.rgb.data();
+            sf[j - j0].out = f.img->dev;
+            sf[j - j0].w = f.rgb.w;
+            sf[j - j0].h = f.rgb.h;
+            sf[j - j0].tiles_x = dev::scan_tiles_x(f.rgb.w);
+            sf[j - j0].first_tile = L.tiles;
+            L.tiles += dev::scan_tiles(f.rgb.w, f.rgb.h);
+            if (f.sa.r1 != L.r1 || f.sa.r2 != L.r2) L.r1 = L.r2 = -1;
+            const PrintArgs& a0 = fr[slots[j0]].pa;
+            L.shared = L.shared && std::memcmp(&f.pa.enl, &a0.enl, sizeof a0.enl) == 0 &&
+                       std::memcmp(&f.pa.scan, &a0.scan, sizeof a0.scan) == 0;
+        }
+        L.n_items = uint32_t(item_frame.size());
+        L.o_pf = append(pf.data(), pf.size() * sizeof(BatchPrintFrame));
+        L.o_sf = append(sf.data(), sf.size() * sizeof(BatchScanFrame));
+        L.o_if = append(item_frame.data(), item_frame.size() * sizeof(uint32_t));
+        L.o_ip = append(item_first.data(), item_first.size() * sizeof(uint32_t));
+    }
     Pool pool(bs);
-    tables = pool.acquire(bytes);
+    tables = pool.acquire(blob.size());
     unsigned char* d = tables.as<unsigned char>();
-    cuda_check(cudaMemcpyAsync(d, blob.data(), bytes, cudaMemcpyHostToDevice, bs), "batch tables");
+    cuda_check(cudaMemcpyAsync(d, blob.data(), blob.size(), cudaMemcpyHostToDevice, bs), "batch tables");
     // the pageable source is staged before cudaMemcpyAsync returns, so blob may go at scope exit
+    const size_t K = std::min(gl.size(), kMaxWorkers);
     launch_captured(
         e, key,
         [&](cudaStream_t s) {
-            dev::print_batch(reinterpret_cast<const BatchPrintFrame*>(d), reinterpret_cast<const uint32_t*>(d + o_if),
-                             reinterpret_cast<const uint32_t*>(d + o_ip), n_items, item_px, ctas,
-                             shared ? &fr[slots[0]].pa.enl : nullptr, shared ? &fr[slots[0]].pa.scan : nullptr, s);
-            dev::scan_encode_batch(reinterpret_cast<const BatchScanFrame*>(d + o_sf), uint32_t(n), tiles, r1, r2, ctas,
-                                   s);
-            for (size_t j = 0; j < n; ++j) {
-                BatchFrame& f = fr[slots[j]];
-                cuda_check(cudaMemcpyAsync(f.img->host, f.img->dev, f.img->bytes, cudaMemcpyDeviceToHost, s),
-                           "result copy");
-                cuda_check(cudaEventRecordWithFlags(e.frame_events[slots[j]], s, cudaEventRecordExternal), "frame");
+            for (size_t g = 0; g < gl.size(); ++g) {
+                const GroupLayout& L = gl[g];
+                const BatchFrame& f0 = fr[slots[first[g]]];
+                dev::print_batch(reinterpret_cast<const BatchPrintFrame*>(d + L.o_pf),
+                                 reinterpret_cast<const uint32_t*>(d + L.o_if),
+                                 reinterpret_cast<const uint32_t*>(d + L.o_ip), L.n_items, item_px, ctas,
+                                 L.shared ? &f0.pa.enl : nullptr, L.shared ? &f0.pa.scan : nullptr, s);
+                dev::scan_encode_batch(reinterpret_cast<const BatchScanFrame*>(d + L.o_sf),
+                                       uint32_t(first[g + 1] - first[g]), L.tiles, L.r1, L.r2, ctas, s);
+                // one group: its copies follow on the batch stream; several: the group's copies run on a
+                // worker stream while the next group's launches run
+                cudaStream_t cs = s;
+                if (gl.size() > 1) {
+                    cs = e.workers[g % K];
+                    cuda_check(cudaEventRecord(e.fork_event, s), "fork");
+                    cuda_check(cudaStreamWaitEvent(cs, e.fork_event, 0), "fork");
+                }
+                for (size_t j = first[g]; j < first[g + 1]; ++j) {
+                    BatchFrame& f = fr[slots[j]];
+                    cuda_check(cudaMemcpyAsync(f.img->host, f.img->dev, f.img->bytes, cudaMemcpyDeviceToHost, cs),
+                               "result copy");
+                    cuda_check(cudaEventRecordWithFlags(e.frame_events[slots[j]], cs, cudaEventRecordExternal),
+                               "frame");
+                }
             }
+            if (gl.size() > 1)
+                for (size_t k = 0; k < K; ++k) {
+                    cuda_check(cudaEventRecord(e.join_events[k], e.workers[k]), "join");
+                    cuda_check(cudaStreamWaitEvent(s, e.join_events[k], 0), "join");
+                }
         },
         t0, t1);
 }
@@ -1960,7 +2017,8 @@ SPK_API spk_status spkx_engine_batch_plan(spk_engine* engine, const char* plan) 
     if (!engine) return invalid("engine is NULL");
     const std::string p = plan ? plan : "";
     if (!p.empty() && !valid_plan(p))
-        return invalid("batch plan must be \"frames:K\" (K 1..16) or \"persistent:S:C\" (S even, 2..1048576; C 1..65535)");
+        return invalid("batch plan must be \"frames:K\" (K 1..16) or \"persistent:S:C[:G]\" (S even, 2..1048576; "
+                       "C 1..65535; G 1..1024)");
     return guarded([&] {
         Engine& e = *E(engine);
         std::lock_guard<std::mutex> g(e.batch_m);

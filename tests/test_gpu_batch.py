@@ -26,7 +26,8 @@ FRAMES = [
 ]
 HALATION = {0: ([(0.2, 0.1, 0.05), (3.0, 3.0, 3.0)], (0.3, 0.2, 0.1)),
             3: ([(0.1, 0.1, 0.1), (8.0, 8.0, 8.0)], (0.25, 0.25, 0.25))}
-PLANS = ["frames:1", "frames:4", "frames:16", "persistent:2048:592", "persistent:8192:1184", "persistent:2:148"]
+PLANS = ["frames:1", "frames:4", "frames:16", "persistent:2048:592", "persistent:8192:1184", "persistent:2:148",
+         "persistent:8192:1184:4", "persistent:2048:592:3", "persistent:8192:1184:64"]
 
 
 def open_all(engine):
@@ -126,7 +127,8 @@ def test_batch_refusals(engine, lib):
         with pytest.raises(sc.SpkError) as e:
             engine.render_batch([], "full")
         assert e.value.status == sc.SPK_ERR_INVALID_ARG
-        for bad in ("frames:0", "frames:17", "persistent:3:10", "persistent:2048", "persistent:2048:0", "fast"):
+        for bad in ("frames:0", "frames:17", "persistent:3:10", "persistent:2048", "persistent:2048:0", "fast",
+                    "persistent:2048:592:0", "persistent:2048:592:1025", "persistent:2048:592:", "persistent:2048:592:x"):
             with pytest.raises(sc.SpkError) as e:
                 engine.batch_plan(bad)
             assert e.value.status == sc.SPK_ERR_INVALID_ARG
@@ -143,7 +145,7 @@ def test_batch_refusals(engine, lib):
         s2.close()
 
 
-@pytest.mark.parametrize("plan", ["persistent:2048:592", "persistent:8192:2368"])
+@pytest.mark.parametrize("plan", ["persistent:2048:592", "persistent:8192:2368", "persistent:2048:592:2"])
 def test_persistent_plan_with_per_frame_filters(engine, plan):
     """Frames whose enlarger filters differ do not share spectral tables: the persistent print then stages
     every frame's tables itself (the frames above share theirs, which the kernel takes once). Each frame
