@@ -7,14 +7,16 @@
 //
 // Tensor-core modes (tcgen05): per integral the wavelengths go in chunks of 16. Each thread forms
 // T(l) = 2^(sum_c d_c e_c(l)) for its pixel on the CUDA cores (the print kernel's binary32 operations) and
-// writes its row of the A operand, 128 pixels x 16 wavelengths in the K-major layout without swizzle, into
-// one of two shared-memory stages: bf16(T) (BF16), bf16(T) and bf16(T - bf16(T)) in a second matrix
-// (BF16X3), or T in binary32 (TF32, of which the tensor core reads the TF32 part). One thread then issues
-// the chunk's MMAs, D[128 x 16] (+)= A B^T with B the pass's 16-row weight table (rows 0..2 the weights'
-// BF16 high parts, rows 3..5 their low parts), accumulating in tensor memory (32 columns per CTA), and
-// commits them to the stage's mbarrier, which releases the stage for the chunk after next. After the last
-// chunk each thread reads its pixel's row of D (tcgen05.ld): R_k = D[k] + D[k + 3] for BF16X3 (all four
-// products of the hi and lo parts), R_k = D[k] otherwise.
+// writes its row of the A operand (128 pixels x 16 wavelengths: the thread's pixel is its tensor-memory
+// lane, the wavelengths consecutive 32-bit columns) into one of three tensor-memory stages with
+// tcgen05.st: bf16(T) (BF16), bf16(T) and bf16(T - bf16(T)) in the next 8 columns (BF16X3), or T in
+// binary32 (TF32, of which the tensor core reads the TF32 part). One thread then issues the chunk's MMAs
+// with A from tensor memory, D[128 x 16] (+)= A B^T with B the pass's 16-row weight table in shared memory
+// (rows 0..2 the weights' BF16 high parts, rows 3..5 their low parts), accumulating in tensor memory, and
+// commits them to the stage's mbarrier, which releases the stage for the chunk three later. Tensor memory:
+// 64 columns per CTA, D in columns 0..15, the stages from column 16. After the last chunk each thread reads
+// its pixel's row of D (tcgen05.ld): R_k = D[k] + D[k + 3] for BF16X3 (all four products of the hi and lo
+// parts), R_k = D[k] otherwise.
 //
 // CUDA-core modes: F32 performs the print kernel's binary32 operations in its order (at the resources' 81
 // wavelengths the output equals k_print's bit for bit); F64 evaluates both integrals in binary64 from the
@@ -40,8 +42,9 @@ namespace {
 
 constexpr uint32_t kTcThreads = 128;  // the MMA's M: one pixel per thread and per TMEM lane
 constexpr uint32_t kChunk = 16;       // wavelengths per A stage
-constexpr uint32_t kStages = 2;
-constexpr uint32_t kTmemCols = 32;    // the accumulator uses 16
+constexpr uint32_t kStages = 3;
+constexpr uint32_t kTmemCols = 64;    // D in columns 0..15, the A stages in 16..63
+constexpr uint32_t kStageCols = 16;   // one A stage: 16 wavelengths of 32 bits (TF32), or BF16 hi and lo halves
 constexpr long long kWaitCycles = 4000000000ll;
 
 // instruction descriptors: D binary32 (bits 4-5 = 1), A and B format (bits 7-9, 10-12: 1 BF16, 2 TF32),
@@ -53,18 +56,12 @@ __host__ __device__ constexpr bool tc_mode(int m) {
     return m == SPKB_SPEC_TF32 || m == SPKB_SPEC_BF16 || m == SPKB_SPEC_BF16X3;
 }
 __host__ __device__ constexpr uint32_t elem_bytes(int m) { return m == SPKB_SPEC_TF32 ? 4u : 2u; }
-// one A stage: 128 x kChunk elements (BF16X3: the hi matrix, then the lo matrix)
-__host__ __device__ constexpr uint32_t stage_bytes(int m) {
-    return 128u * kChunk * elem_bytes(m) * (m == SPKB_SPEC_BF16X3 ? 2u : 1u);
-}
-constexpr uint32_t kLoOffset = 128u * kChunk * 2u;
 __host__ __device__ constexpr uint32_t round_up(uint32_t x, uint32_t a) { return (x + a - 1) / a * a; }
 
-// Dynamic shared memory of one CTA: the binary64 tables (mode F64), the B tiles and A stages of the
-// tensor-core modes, then the mbarriers (kStages stage barriers and a teardown barrier) and the
-// tensor-memory address slot.
+// Dynamic shared memory of one CTA: the binary64 tables (mode F64), the B tiles of the tensor-core modes,
+// then the mbarriers (kStages stage barriers and a teardown barrier) and the tensor-memory address slot.
 struct SmemLayout {
-    uint32_t e, w, e64, w64, b, a, bar, total;
+    uint32_t e, w, e64, w64, b, bar, total;
 };
 // At more than 96 wavelengths the spectral loops stay rolled; the binary32 CUDA-core path then reads its
 // tables from shared memory (a constant-bank operand needs a fixed index), the tensor-core paths keep them
@@ -83,8 +80,6 @@ __host__ __device__ constexpr SmemLayout smem_layout(int m, uint32_t nl_pad) {
     if (m == SPKB_SPEC_F64) off = round_up(off + 2 * nl_pad * 32, 128);
     L.b = off;
     if (tc_mode(m)) off = round_up(off + 2 * 16 * nl_pad * elem_bytes(m), 128);
-    L.a = off;
-    if (tc_mode(m)) off = round_up(off + kStages * stage_bytes(m), 128);
     L.bar = off;
     off += 8 * (kStages + 1) + 8;
     L.total = round_up(off, 128);
@@ -174,22 +169,31 @@ __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::
 // this thread's generic-proxy writes to shared memory become visible to the tensor cores' (async) proxy
 __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
-__device__ __forceinline__ void mma_bf16(uint32_t d, uint64_t a, uint64_t b, uint32_t acc) {
+// D (+)= A B^T with A in tensor memory (a: the tile's column address, lane 0) and B in shared memory
+__device__ __forceinline__ void mma_bf16(uint32_t d, uint32_t a, uint64_t b, uint32_t acc) {
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
         "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d),
-        "l"(a), "l"(b), "r"(kIdescBf16), "r"(acc)
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, p;\n\t}" ::"r"(d),
+        "r"(a), "l"(b), "r"(kIdescBf16), "r"(acc)
         : "memory");
 }
-__device__ __forceinline__ void mma_tf32(uint32_t d, uint64_t a, uint64_t b, uint32_t acc) {
+__device__ __forceinline__ void mma_tf32(uint32_t d, uint32_t a, uint64_t b, uint32_t acc) {
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
         "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(d),
-        "l"(a), "l"(b), "r"(kIdescTf32), "r"(acc)
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, p;\n\t}" ::"r"(d),
+        "r"(a), "l"(b), "r"(kIdescTf32), "r"(acc)
         : "memory");
 }
+// this thread's 8 consecutive 32-bit columns of its lane, from the column address taddr (the warp's 32
+// lanes start at taddr's lane field); tmem_wait_st waits for this thread's stores to complete
+__device__ __forceinline__ void tmem_st8(uint32_t taddr, const uint32_t r[8]) {
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"r"(taddr),
+                 "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7])
+                 : "memory");
+}
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 // the barrier's arrival once every MMA this thread issued before it has completed
 __device__ __forceinline__ void mma_commit(uint32_t bar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
@@ -221,9 +225,6 @@ __device__ __forceinline__ uint32_t bf16x2(float lo, float hi) {
     return r;
 }
 
-__device__ __forceinline__ void st_shared16(unsigned char* p, uint32_t a, uint32_t b, uint32_t c, uint32_t d) {
-    *reinterpret_cast<uint4*>(p) = make_uint4(a, b, c, d);
-}
 
 __device__ __forceinline__ void copy16(unsigned char* dst, const void* src, uint32_t bytes) {
     const uint4* s = reinterpret_cast<const uint4*>(src);
@@ -264,67 +265,62 @@ __device__ __forceinline__ void transmittance8(const SpectralParams<NLP>& p, con
     }
 }
 
-// T over wavelengths j*kChunk .. j*kChunk + kChunk - 1 for this thread's pixel, into its row of the A stage:
-//   TF32    T (binary32);
-//   BF16    bf16(T), rounded to nearest;
-//   BF16X3  hi = T truncated to BF16 and lo = bf16(T - hi) (T - hi is exact in binary32), in two matrices.
+// T over wavelengths j*kChunk .. j*kChunk + kChunk - 1 for this thread's pixel, into its lane of the A stage
+// at tensor-memory column address `stage` (the warp's lanes):
+//   TF32    T (binary32), columns 0..15;
+//   BF16    bf16(T), rounded to nearest, wavelength pairs in columns 0..7 (the lower wavelength in the low half);
+//   BF16X3  hi = T truncated to BF16 in columns 0..7 and lo = bf16(T - hi) in columns 8..15 (T - hi is exact
+//           in binary32).
 template <int M, int NLP, uint32_t PASS>
 __device__ __forceinline__ void produce(const SpectralParams<NLP>& p, const float* smem_e, uint32_t j, float2 D0,
-                                        float2 D1, float2 D2, unsigned char* A, uint32_t row) {
-    constexpr uint32_t cm_per_row = kChunk * elem_bytes(M) / 16;  // core matrices along K in one stage
-    unsigned char* R = A + (row >> 3) * cm_per_row * 128 + (row & 7) * 16;
+                                        float2 D1, float2 D2, uint32_t stage) {
+    uint32_t h[kChunk / 2], l[kChunk / 2];
 #pragma unroll
     for (uint32_t q = 0; q < kChunk / 8; ++q) {
         float T[8];
         transmittance8<NLP, PASS, false>(p, smem_e, j * kChunk + q * 8, D0, D1, D2, T);
         if constexpr (M == SPKB_SPEC_TF32) {
-            st_shared16(R + (2 * q) * 128, __float_as_uint(T[0]), __float_as_uint(T[1]), __float_as_uint(T[2]),
-                        __float_as_uint(T[3]));
-            st_shared16(R + (2 * q + 1) * 128, __float_as_uint(T[4]), __float_as_uint(T[5]), __float_as_uint(T[6]),
-                        __float_as_uint(T[7]));
-        } else if constexpr (M == SPKB_SPEC_BF16) {
-            st_shared16(R + q * 128, bf16x2(T[0], T[1]), bf16x2(T[2], T[3]), bf16x2(T[4], T[5]), bf16x2(T[6], T[7]));
+            uint32_t t[8];
+#pragma unroll
+            for (uint32_t i = 0; i < 8; ++i) t[i] = __float_as_uint(T[i]);
+            tmem_st8(stage + 8 * q, t);
         } else {
-            uint32_t h[4], l[4];
 #pragma unroll
             for (uint32_t i = 0; i < 4; ++i) {
                 const float a = T[2 * i], b = T[2 * i + 1];
-                h[i] = upper_halves(a, b);
-                // T - hi = T + (-1) hi, exact
-                const float2 hi2 = make_float2(__uint_as_float(__float_as_uint(a) & 0xFFFF0000u),
-                                               __uint_as_float(__float_as_uint(b) & 0xFFFF0000u));
-                const float2 rem = __ffma2_rn(hi2, make_float2(-1.0f, -1.0f), make_float2(a, b));
-                l[i] = bf16x2(rem.x, rem.y);
+                if constexpr (M == SPKB_SPEC_BF16) {
+                    h[4 * q + i] = bf16x2(a, b);
+                } else {
+                    h[4 * q + i] = upper_halves(a, b);
+                    // T - hi = T + (-1) hi, exact
+                    const float2 hi2 = make_float2(__uint_as_float(__float_as_uint(a) & 0xFFFF0000u),
+                                                   __uint_as_float(__float_as_uint(b) & 0xFFFF0000u));
+                    const float2 rem = __ffma2_rn(hi2, make_float2(-1.0f, -1.0f), make_float2(a, b));
+                    l[4 * q + i] = bf16x2(rem.x, rem.y);
+                }
             }
-            st_shared16(R + q * 128, h[0], h[1], h[2], h[3]);
-            st_shared16(R + kLoOffset + q * 128, l[0], l[1], l[2], l[3]);
         }
     }
+    if constexpr (M != SPKB_SPEC_TF32) tmem_st8(stage, h);
+    if constexpr (M == SPKB_SPEC_BF16X3) tmem_st8(stage + 8, l);
 }
 
-// the MMAs of chunk j: A the stage at a_saddr, B the pass's table at b_saddr (16 x NLP)
+// the MMAs of chunk j: A the stage at tensor-memory column address a_tmem, B the pass's table at b_saddr
+// (16 x NLP)
 template <int M, int NLP>
-__device__ __forceinline__ void issue(uint32_t tmem, uint32_t a_saddr, uint32_t b_saddr, uint32_t j) {
+__device__ __forceinline__ void issue(uint32_t tmem, uint32_t a_tmem, uint32_t b_saddr, uint32_t j) {
     if constexpr (M == SPKB_SPEC_TF32) {
         constexpr uint32_t sbo_b = (NLP * 4 / 16) * 128;
 #pragma unroll
-        for (uint32_t s = 0; s < kChunk / 8; ++s) {  // K = 8 per MMA
-            const uint64_t a = smem_desc(a_saddr + s * 256, 128, (kChunk * 4 / 16) * 128);
+        for (uint32_t s = 0; s < kChunk / 8; ++s) {  // K = 8 per MMA: 8 columns
             const uint64_t b = smem_desc(b_saddr + (j * (kChunk * 4 / 16) + 2 * s) * 128, 128, sbo_b);
-            mma_tf32(tmem, a, b, (j | s) != 0);
+            mma_tf32(tmem, a_tmem + 8 * s, b, (j | s) != 0);
         }
     } else {
         constexpr uint32_t sbo_b = (NLP * 2 / 16) * 128;
-#pragma unroll
-        for (uint32_t s = 0; s < kChunk / 16; ++s) {  // K = 16 per MMA
-            const uint64_t a = smem_desc(a_saddr + s * 256, 128, (kChunk * 2 / 16) * 128);
-            const uint64_t b = smem_desc(b_saddr + (j * (kChunk * 2 / 16) + 2 * s) * 128, 128, sbo_b);
-            mma_bf16(tmem, a, b, (j | s) != 0);
-            if constexpr (M == SPKB_SPEC_BF16X3) {
-                const uint64_t al = smem_desc(a_saddr + kLoOffset + s * 256, 128, (kChunk * 2 / 16) * 128);
-                mma_bf16(tmem, al, b, 1u);
-            }
-        }
+        const uint64_t b = smem_desc(b_saddr + j * (kChunk * 2 / 16) * 128, 128, sbo_b);  // K = 16 per MMA
+        mma_bf16(tmem, a_tmem, b, j != 0);
+        if constexpr (M == SPKB_SPEC_BF16X3) mma_bf16(tmem, a_tmem + 8, b, 1u);
     }
 }
 
@@ -336,6 +332,7 @@ __device__ __forceinline__ void contract_tc(const SpectralParams<NLP>& p, unsign
                                             const float d[3], float R[3], uint32_t& g, bool& ok) {
     constexpr SmemLayout L = smem_layout(M, NLP);
     const uint32_t tid = threadIdx.x;
+    const uint32_t lanes = (32u * (tid / 32u)) << 16;  // this warp's 32 lanes
     const float2 D0 = make_float2(d[0], d[0]), D1 = make_float2(d[1], d[1]), D2 = make_float2(d[2], d[2]);
     const uint32_t b_saddr = smem_addr(smem + L.b) + PASS * 16 * NLP * elem_bytes(M);
     const uint32_t bar0 = smem_addr(smem + L.bar);
@@ -345,17 +342,20 @@ __device__ __forceinline__ void contract_tc(const SpectralParams<NLP>& p, unsign
 #pragma unroll kUnroll
     for (uint32_t j = 0; j < NLP / kChunk; ++j, ++g) {
         const uint32_t st = g % kStages;
-        unsigned char* A = smem + L.a + st * stage_bytes(M);
+        const uint32_t stage = tmem + 16u + st * kStageCols;
         // the MMAs of chunk g - kStages read this stage
         bool mine = ok;
         if (g >= kStages && mine) mine = mbar_wait(bar0 + 8 * st, ((g / kStages) - 1) & 1u, p.wait_limit);
-        if (mine) produce<M, NLP, PASS>(p, reinterpret_cast<const float*>(smem + L.e), j, D0, D1, D2, A, tid);
-        fence_async_smem();
+        if (mine) {
+            tc_fence_after();
+            produce<M, NLP, PASS>(p, reinterpret_cast<const float*>(smem + L.e), j, D0, D1, D2, stage + lanes);
+            tmem_wait_st();
+        }
         tc_fence_before();
         ok = __syncthreads_or(mine ? 0 : 1) == 0;
         if (tid == 0 && ok) {
             tc_fence_after();
-            issue<M, NLP>(tmem, smem_addr(A), b_saddr, j);
+            issue<M, NLP>(tmem, stage, b_saddr, j);
             mma_commit(bar0 + 8 * st);
         }
     }
@@ -369,7 +369,7 @@ __device__ __forceinline__ void contract_tc(const SpectralParams<NLP>& p, unsign
     }
     tc_fence_after();
     float v[8];
-    tmem_ld8(tmem + ((32u * (tid / 32u)) << 16), v);
+    tmem_ld8(tmem + lanes, v);
 #pragma unroll
     for (int k = 0; k < 3; ++k) R[k] = M == SPKB_SPEC_BF16X3 ? v[k] + v[k + 3] : v[k];
 }
@@ -553,7 +553,10 @@ long long g_wait_limit = 0;  // spkx_test_set_tc_wait_limit: 0 the full limit
 template <int M, int NLP>
 void launch_spectral(const PrintArgs& a, const SpectralTablesN& host_tab, const SpectralTablesN* tab, const float* neg,
                      float* rgb, uint32_t n, float* contraction, uint32_t* err, cudaStream_t s) {
-    constexpr uint32_t smem = smem_layout(M, NLP).total;
+    // a tensor-core CTA takes at least 25 KB of shared memory, so that no more than 8 are resident on an SM:
+    // with 64 tensor-memory columns each, 8 fill the SM's 512, and a ninth would wait in tcgen05.alloc
+    constexpr uint32_t smem = tc_mode(M) && smem_layout(M, NLP).total < 25u * 1024u ? 25u * 1024u
+                                                                                 : smem_layout(M, NLP).total;
     auto kernel = k_print_spectral<M, NLP>;
     ensure_smem(reinterpret_cast<const void*>(kernel), int(smem));
     cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout, int(cudaSharedmemCarveoutMaxShared));
@@ -581,11 +584,14 @@ void launch_spectral(const PrintArgs& a, const SpectralTablesN& host_tab, const 
         (void)cudaGetLastError();
         per_sm = 0;
     }
-    // resident CTAs by shared memory (228 KB per SM, 1 KB reserved per CTA) and threads (2048 per SM); a
-    // CTA beyond the resident ones only starts later, no CTA waits on another
+    // resident CTAs by shared memory (228 KB per SM, 1 KB reserved per CTA), threads (2048 per SM) and, in
+    // the tensor-core modes, tensor memory (512 columns per SM); a CTA beyond the resident ones only starts
+    // later, no CTA waits on another
     const int by_smem = int((228u * 1024u) / (smem + 1024u));
     const int fit = by_smem < 16 ? by_smem : 16;
     if (per_sm < fit) per_sm = fit;
+    if (tc_mode(M) && per_sm > int(512u / kTmemCols)) per_sm = int(512u / kTmemCols);
+    static_assert(512u / kTmemCols == 8u, "the shared-memory floor above holds 8 CTAs per SM");
     const uint64_t tiles = (uint64_t(n) + kTcThreads - 1) / kTcThreads;
     const uint64_t resident = uint64_t(sms > 0 ? sms : 1) * uint64_t(per_sm > 0 ? per_sm : 1);
     const uint32_t grid = uint32_t(tiles < resident ? tiles : resident);
