@@ -552,7 +552,10 @@ __global__ void k_develop(const float* __restrict__ exposure, float* __restrict_
 // draw consumes the same uniforms in the same order and with the same arithmetic as spk_poisson, so the
 // counts are those of the per-lane sampler.
 
-constexpr uint32_t kDrawWarps = 4;
+#ifndef SPKB_DEVELOP_WARPS
+#define SPKB_DEVELOP_WARPS 4
+#endif
+constexpr uint32_t kDrawWarps = SPKB_DEVELOP_WARPS;  // warps per block
 // resident blocks per SM the register allocation is held to (1: no cap)
 #ifndef SPKB_DEVELOP_MIN_BLOCKS
 #define SPKB_DEVELOP_MIN_BLOCKS 1

@@ -66,6 +66,68 @@ __device__ __forceinline__ void scan_tile(const ScanArgs& a, const float* __rest
     }
     __syncthreads();
 
+    if constexpr (R1 >= 0 && R2 >= 0) {
+        // 2. lens blur, vertical, with register windows: a thread takes kVRows consecutive output rows of
+        //    one column and reads each input row once; every output is still sum_k t1[k] A[i + k] from 0,
+        //    k ascending
+        constexpr int T1 = 2 * R1 + 1, PCc = 3 * (kTW + 2 * (R1 + R2)), PRc = kTH + 2 * (R1 + R2);
+        constexpr int BRc = kTH + 2 * R2, BCc = 3 * (kTW + 2 * R2);
+        constexpr int kVRows = 6, NB = (BRc + kVRows - 1) / kVRows;
+        for (int item = threadIdx.x; item < PCc * NB; item += kThreads) {
+            const int f = item % PCc, i0 = (item / PCc) * kVRows;
+            float acc[kVRows];
+#pragma unroll
+            for (int o = 0; o < kVRows; ++o) acc[o] = 0.0f;
+#pragma unroll
+            for (int j = 0; j < kVRows + T1 - 1; ++j) {
+                if (i0 + j < PRc) {
+                    const float v = A[(i0 + j) * PCc + f];
+#pragma unroll
+                    for (int o = 0; o < kVRows; ++o)
+                        if (j - o >= 0 && j - o < T1) acc[o] += a.t1[j - o] * v;
+                }
+            }
+#pragma unroll
+            for (int o = 0; o < kVRows; ++o) {
+                const int i = i0 + o, yy = y0 - R2 + i;
+                if (i < BRc && yy >= 0 && yy < h) B[i * PCc + f] = acc[o];
+            }
+        }
+        __syncthreads();
+
+        // 3. lens blur, horizontal, with register windows: a thread takes kHPix consecutive output pixels
+        //    of one channel in one row
+        constexpr int kHPix = 4, NG = (kTW + 2 * R2 + kHPix - 1) / kHPix;
+        for (int item = threadIdx.x; item < BRc * 3 * NG; item += kThreads) {
+            const int i = item / (3 * NG), rem = item - i * (3 * NG), c = rem % 3, j0 = (rem / 3) * kHPix;
+            const int yy = y0 - R2 + i;
+            if (yy < 0 || yy >= h) continue;
+            float acc[kHPix];
+#pragma unroll
+            for (int o = 0; o < kHPix; ++o) acc[o] = 0.0f;
+            const float* brow = B + i * PCc + c;
+#pragma unroll
+            for (int q = 0; q < kHPix + T1 - 1; ++q) {
+                if (j0 + q < kTW + 2 * (R1 + R2)) {
+                    const float v = brow[3 * (j0 + q)];
+#pragma unroll
+                    for (int o = 0; o < kHPix; ++o)
+                        if (q - o >= 0 && q - o < T1) acc[o] += a.t1[q - o] * v;
+                }
+            }
+#pragma unroll
+            for (int o = 0; o < kHPix; ++o) {
+                const int jb = j0 + o;
+                if (jb >= kTW + 2 * R2) break;
+                if (!inner_x) {
+                    const int xx = x0 - R2 + jb;
+                    if (xx < 0 || xx >= w) continue;
+                }
+                A[i * BCc + 3 * jb + c] = acc[o];
+            }
+        }
+        __syncthreads();
+    } else {
     // 2. lens blur, vertical: rows y0 - r2 + i inside the image, every column of the tile
     for (int i = warp; i < BR; i += kWarps) {
         const int yy = y0 - r2 + i;
@@ -95,6 +157,7 @@ __device__ __forceinline__ void scan_tile(const ScanArgs& a, const float* __rest
         }
     }
     __syncthreads();
+    }
 
     if (r2 > 0) {
         // 4. the border up to r2 past an edge takes the lens-blurred value of the reflected pixel
@@ -116,6 +179,29 @@ __device__ __forceinline__ void scan_tile(const ScanArgs& a, const float* __rest
             __syncthreads();
         }
         // 5. unsharp blur, vertical: the tile's rows inside the image, every column of the blurred tile
+        if constexpr (R2 >= 0) {
+            // register windows of kURows rows per thread, as in step 2
+            constexpr int T2 = 2 * R2 + 1, BCc = 3 * (kTW + 2 * R2), BRc = kTH + 2 * R2;
+            constexpr int kURows = 8, NU = kTH / kURows;
+            for (int item = threadIdx.x; item < BCc * NU; item += kThreads) {
+                const int fb = item % BCc, i0 = (item / BCc) * kURows;
+                float acc[kURows];
+#pragma unroll
+                for (int o = 0; o < kURows; ++o) acc[o] = 0.0f;
+#pragma unroll
+                for (int j = 0; j < kURows + T2 - 1; ++j) {
+                    if (i0 + j < BRc) {
+                        const float v = A[(i0 + j) * BCc + fb];
+#pragma unroll
+                        for (int o = 0; o < kURows; ++o)
+                            if (j - o >= 0 && j - o < T2) acc[o] += a.t2[j - o] * v;
+                    }
+                }
+#pragma unroll
+                for (int o = 0; o < kURows; ++o)
+                    if (y0 + i0 + o < h) B[(i0 + o) * BCc + fb] = acc[o];
+            }
+        } else {
         for (int i = warp; i < kTH; i += kWarps) {
             if (y0 + i >= h) break;
             for (int fb = lane; fb < BC; fb += 32) {
@@ -124,6 +210,7 @@ __device__ __forceinline__ void scan_tile(const ScanArgs& a, const float* __rest
                 for (int k = 0; k <= 2 * r2; ++k) acc += a.t2[k] * A[(i + k) * BC + fb];
                 B[i * BC + fb] = acc;
             }
+        }
         }
         __syncthreads();
     }
