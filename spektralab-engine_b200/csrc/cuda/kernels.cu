@@ -329,43 +329,73 @@ __device__ __forceinline__ void iir_line(const float* src, float* work, float* d
 //   backward: y'[i] = dB u[i] + B u'[i] + sum_j (dB_j y[i+j] + B_j y'[i+j]), y'[n..n+2] = u'[n-1]
 // with u = the forward pass rounded to binary32 (its tangent is not rounded). Work planes: the forward
 // pass's value and tangent.
-__device__ __forceinline__ void iir_line_tangent(const float* src, const float* src_dot, float* work, float* work_dot,
-                                                 float* dst, float* dst_dot, size_t base, size_t stride, uint32_t n,
-                                                 const IirCoefs& q, const IirCoefs& dq, int c) {
+__device__ __forceinline__ void iir_line_tangent(const float* __restrict__ src, const float* __restrict__ src_dot,
+                                                 float* __restrict__ work, float* __restrict__ work_dot,
+                                                 float* __restrict__ dst, float* __restrict__ dst_dot, size_t base,
+                                                 size_t stride, uint32_t n, const IirCoefs& q, const IirCoefs& dq,
+                                                 int c) {
+    // the line's samples go in chunks of kTanChunk: a chunk's loads are issued together, ahead of its
+    // recurrence steps, so that a step waits on the previous step and not on memory
+    constexpr uint32_t kTanChunk = 8;
     const double B = q.B[c], B1 = q.B1[c], B2 = q.B2[c], B3 = q.B3[c];
     const double dB = dq.B[c], dB1 = dq.B1[c], dB2 = dq.B2[c], dB3 = dq.B3[c];
     double w1 = double(src[base]), w2 = w1, w3 = w1;
     double t1 = src_dot ? double(src_dot[base]) : 0.0, t2 = t1, t3 = t1;
-    for (uint32_t i = 0; i < n; ++i) {
-        const size_t o = base + i * stride;
-        const double x = double(src[o]), xd = src_dot ? double(src_dot[o]) : 0.0;
-        const double v = ((B * x + B1 * w1) + B2 * w2) + B3 * w3;
-        const double vd = dB * x + B * xd + (dB1 * w1 + B1 * t1) + (dB2 * w2 + B2 * t2) + (dB3 * w3 + B3 * t3);
-        w3 = w2;
-        w2 = w1;
-        w1 = v;
-        t3 = t2;
-        t2 = t1;
-        t1 = vd;
-        work[o] = float(v);
-        work_dot[o] = float(vd);
+    for (uint32_t i0 = 0; i0 < n; i0 += kTanChunk) {
+        float xs[kTanChunk], xds[kTanChunk];
+#pragma unroll
+        for (uint32_t j = 0; j < kTanChunk; ++j) {
+            const size_t o = base + size_t(i0 + j) * stride;
+            xs[j] = i0 + j < n ? src[o] : 0.0f;
+            xds[j] = i0 + j < n && src_dot ? src_dot[o] : 0.0f;
+        }
+#pragma unroll
+        for (uint32_t j = 0; j < kTanChunk; ++j) {
+            if (i0 + j >= n) break;
+            const size_t o = base + size_t(i0 + j) * stride;
+            const double x = double(xs[j]), xd = double(xds[j]);
+            // the newest state enters last: one multiply-add latency per sample on each recurrence
+            const double v = fma(B1, w1, fma(B2, w2, fma(B3, w3, B * x)));
+            const double vd = fma(B1, t1, fma(dB1, w1, fma(B2, t2, fma(dB2, w2, fma(B3, t3, fma(dB3, w3, fma(B, xd, dB * x)))))));
+            w3 = w2;
+            w2 = w1;
+            w1 = v;
+            t3 = t2;
+            t2 = t1;
+            t1 = vd;
+            work[o] = float(v);
+            work_dot[o] = float(vd);
+        }
     }
     const size_t last = base + size_t(n - 1) * stride;
     double y1 = double(work[last]), y2 = y1, y3 = y1;
     double s1 = double(work_dot[last]), s2 = s1, s3 = s1;
-    for (uint32_t k = n; k-- > 0;) {
-        const size_t o = base + k * stride;
-        const double u = double(work[o]), ud = double(work_dot[o]);
-        const double v = ((B * u + B1 * y1) + B2 * y2) + B3 * y3;
-        const double vd = dB * u + B * ud + (dB1 * y1 + B1 * s1) + (dB2 * y2 + B2 * s2) + (dB3 * y3 + B3 * s3);
-        y3 = y2;
-        y2 = y1;
-        y1 = v;
-        s3 = s2;
-        s2 = s1;
-        s1 = vd;
-        dst[o] = float(v);
-        dst_dot[o] = float(vd);
+    for (uint32_t k0 = n; k0 > 0;) {
+        const uint32_t m = k0 < kTanChunk ? k0 : kTanChunk;  // samples k0 - 1 down to k0 - m
+        float us[kTanChunk], uds[kTanChunk];
+#pragma unroll
+        for (uint32_t j = 0; j < kTanChunk; ++j) {
+            const size_t o = base + size_t(k0 - 1 - (j < m ? j : 0)) * stride;
+            us[j] = work[o];
+            uds[j] = work_dot[o];
+        }
+#pragma unroll
+        for (uint32_t j = 0; j < kTanChunk; ++j) {
+            if (j >= m) break;
+            const size_t o = base + size_t(k0 - 1 - j) * stride;
+            const double u = double(us[j]), ud = double(uds[j]);
+            const double v = fma(B1, y1, fma(B2, y2, fma(B3, y3, B * u)));
+            const double vd = fma(B1, s1, fma(dB1, y1, fma(B2, s2, fma(dB2, y2, fma(B3, s3, fma(dB3, y3, fma(B, ud, dB * u)))))));
+            y3 = y2;
+            y2 = y1;
+            y1 = v;
+            s3 = s2;
+            s2 = s1;
+            s1 = vd;
+            dst[o] = float(v);
+            dst_dot[o] = float(vd);
+        }
+        k0 -= m;
     }
 }
 
@@ -929,8 +959,9 @@ void iir_tangent(const float* in, const float* in_dot, float* work, float* work_
     const uint32_t lines = vertical ? 3u * w : 3u * h;
     if (lines == 0) return;
     Probe p("iir_tangent", s);
-    k_iir_tangent<<<div_up(lines, 128), 128, 0, s>>>(in, in_dot, work, work_dot, out, out_dot, w, h, vertical ? 1 : 0,
-                                                     c, dc);
+    // a thread per line and few lines (3 per row or column): 32-thread CTAs spread them over more SMs
+    k_iir_tangent<<<div_up(lines, 32), 32, 0, s>>>(in, in_dot, work, work_dot, out, out_dot, w, h, vertical ? 1 : 0, c,
+                                                   dc);
 }
 
 void fir_v(const float* in, float* out, uint32_t w, uint32_t h, const FirTaps& t, cudaStream_t s) {
