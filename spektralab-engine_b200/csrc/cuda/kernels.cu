@@ -399,6 +399,114 @@ __device__ __forceinline__ void iir_line_tangent(const float* __restrict__ src, 
     }
 }
 
+// The same per-line tangent with the lines staged in shared memory: a CTA takes one row (3 lines, vertical
+// = 0) or a strip of `px` pixel columns (3 px lines, vertical = 1), loads them with coalesced reads, runs
+// each line's forward and backward recurrences in place in shared memory (a thread per line; the forward
+// pass's binary32 value and tangent replace the input as iir_line_tangent's work planes hold them) and
+// stores the result. Line j, sample i at [i * nl + j]. The arithmetic is iir_line_tangent's, operation for
+// operation.
+__global__ void k_iir_tangent_smem(const float* __restrict__ in, const float* __restrict__ in_dot,
+                                   float* __restrict__ out, float* __restrict__ out_dot, uint32_t w, uint32_t h,
+                                   int vertical, uint32_t px, const __grid_constant__ IirCoefs q,
+                                   const __grid_constant__ IirCoefs dq) {
+    extern __shared__ float tsm[];
+    const uint32_t n = vertical ? h : w;
+    const uint32_t x0 = vertical ? blockIdx.x * px : 0;
+    const uint32_t npx = vertical ? min(px, w - x0) : 1;  // pixel columns in this strip
+    const uint32_t nl = 3 * (vertical ? px : 1);           // the strip's line pitch
+    const uint32_t nv = 3 * npx;                             // valid lines
+    float* val = tsm;
+    float* dot = tsm + size_t(n) * nl;
+    // global index of line j (pixel x0 + j / 3, channel j % 3), sample i
+    auto gidx = [&](uint32_t i, uint32_t j) -> size_t {
+        return vertical ? (size_t(i) * w + x0) * 3 + j : (size_t(blockIdx.x) * w + i) * 3 + j;
+    };
+    // the whole CTA loads (a thread per line would wait on memory for each sample); four loads in flight
+#pragma unroll 4
+    for (uint32_t e = threadIdx.x; e < n * nl; e += blockDim.x) {
+        const uint32_t i = e / nl, j = e - i * nl;
+        if (j >= nv) continue;
+        const size_t g = gidx(i, j);
+        val[e] = in[g];
+        dot[e] = in_dot ? in_dot[g] : 0.0f;
+    }
+    __syncthreads();
+    const uint32_t t = threadIdx.x;
+    const int c = int(t % 3u);
+    if (t < nv && ((q.mask >> c) & 1u) != 0u) {
+        constexpr uint32_t kTanChunk = 8;
+        const double B = q.B[c], B1 = q.B1[c], B2 = q.B2[c], B3 = q.B3[c];
+        const double dB = dq.B[c], dB1 = dq.B1[c], dB2 = dq.B2[c], dB3 = dq.B3[c];
+        double w1 = double(val[t]), w2 = w1, w3 = w1;
+        double t1 = double(dot[t]), t2 = t1, t3 = t1;
+        for (uint32_t i0 = 0; i0 < n; i0 += kTanChunk) {
+            float xs[kTanChunk], xds[kTanChunk];
+#pragma unroll
+            for (uint32_t j = 0; j < kTanChunk; ++j) {
+                const uint32_t i = i0 + j < n ? i0 + j : n - 1;
+                xs[j] = val[size_t(i) * nl + t];
+                xds[j] = dot[size_t(i) * nl + t];
+            }
+#pragma unroll
+            for (uint32_t j = 0; j < kTanChunk; ++j) {
+                if (i0 + j >= n) break;
+                const double x = double(xs[j]), xd = double(xds[j]);
+                const double v = fma(B1, w1, fma(B2, w2, fma(B3, w3, B * x)));
+                const double vd =
+                    fma(B1, t1, fma(dB1, w1, fma(B2, t2, fma(dB2, w2, fma(B3, t3, fma(dB3, w3, fma(B, xd, dB * x)))))));
+                w3 = w2;
+                w2 = w1;
+                w1 = v;
+                t3 = t2;
+                t2 = t1;
+                t1 = vd;
+                val[size_t(i0 + j) * nl + t] = float(v);
+                dot[size_t(i0 + j) * nl + t] = float(vd);
+            }
+        }
+        const size_t last = size_t(n - 1) * nl + t;
+        double y1 = double(val[last]), y2 = y1, y3 = y1;
+        double s1 = double(dot[last]), s2 = s1, s3 = s1;
+        for (uint32_t k0 = n; k0 > 0;) {
+            const uint32_t m = k0 < kTanChunk ? k0 : kTanChunk;  // samples k0 - 1 down to k0 - m
+            float us[kTanChunk], uds[kTanChunk];
+#pragma unroll
+            for (uint32_t j = 0; j < kTanChunk; ++j) {
+                const size_t o = size_t(k0 - 1 - (j < m ? j : 0)) * nl + t;
+                us[j] = val[o];
+                uds[j] = dot[o];
+            }
+#pragma unroll
+            for (uint32_t j = 0; j < kTanChunk; ++j) {
+                if (j >= m) break;
+                const size_t o = size_t(k0 - 1 - j) * nl + t;
+                const double u = double(us[j]), ud = double(uds[j]);
+                const double v = fma(B1, y1, fma(B2, y2, fma(B3, y3, B * u)));
+                const double vd =
+                    fma(B1, s1, fma(dB1, y1, fma(B2, s2, fma(dB2, y2, fma(B3, s3, fma(dB3, y3, fma(B, ud, dB * u)))))));
+                y3 = y2;
+                y2 = y1;
+                y1 = v;
+                s3 = s2;
+                s2 = s1;
+                s1 = vd;
+                val[o] = float(v);
+                dot[o] = float(vd);
+            }
+            k0 -= m;
+        }
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (uint32_t e = threadIdx.x; e < n * nl; e += blockDim.x) {
+        const uint32_t i = e / nl, j = e - i * nl;
+        if (j >= nv) continue;
+        const size_t g = gidx(i, j);
+        out[g] = val[e];
+        out_dot[g] = dot[e];
+    }
+}
+
 // the blur's tangent along sigma, one thread per line: rows (vertical = 0) or columns (vertical = 1); a
 // channel outside q.mask passes its value and tangent through
 __global__ void k_iir_tangent(const float* __restrict__ in, const float* in_dot, float* work, float* work_dot,
@@ -959,6 +1067,21 @@ void iir_tangent(const float* in, const float* in_dot, float* work, float* work_
     const uint32_t lines = vertical ? 3u * w : 3u * h;
     if (lines == 0) return;
     Probe p("iir_tangent", s);
+    // lines staged in shared memory where they fit (a row, or a strip of 4, 2 or 1 pixel columns); the
+    // lines in global memory otherwise
+    int dev = 0, optin = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    const size_t n = vertical ? h : w;
+    for (uint32_t px : {4u, 2u, 1u}) {
+        const uint32_t nl = 3 * (vertical ? px : 1u);
+        const size_t smem = 2 * n * nl * sizeof(float);
+        if (smem > size_t(optin)) continue;
+        ensure_smem(reinterpret_cast<const void*>(k_iir_tangent_smem), int(smem));
+        const uint32_t ctas = vertical ? div_up(w, px) : h;
+        k_iir_tangent_smem<<<ctas, 256, smem, s>>>(in, in_dot, out, out_dot, w, h, vertical ? 1 : 0, px, c, dc);
+        return;
+    }
     // a thread per line and few lines (3 per row or column): 32-thread CTAs spread them over more SMs
     k_iir_tangent<<<div_up(lines, 32), 32, 0, s>>>(in, in_dot, work, work_dot, out, out_dot, w, h, vertical ? 1 : 0, c,
                                                    dc);

@@ -347,7 +347,13 @@ __device__ void gamut_d(const VjpPrintArgs& pa, DP& r, DP& g, DP& b) {
     dmat(q.m_to_rgb, x100 / 100.0f, y100 / 100.0f, z100 / 100.0f, r, g, b);
 }
 
-__global__ void __launch_bounds__(128) k_vjp_print(const float* __restrict__ neg, const float* __restrict__ g_p,
+// threads per CTA of the print's adjoint
+#ifndef SPKB_VJP_PRINT_THREADS
+#define SPKB_VJP_PRINT_THREADS 128
+#endif
+constexpr uint32_t kVjpPrintThreads = SPKB_VJP_PRINT_THREADS;
+
+__global__ void __launch_bounds__(kVjpPrintThreads) k_vjp_print(const float* __restrict__ neg, const float* __restrict__ g_p,
                                                    float* __restrict__ g_neg, double* __restrict__ grad_params,
                                                    const __grid_constant__ VjpPrintArgs a) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -440,7 +446,8 @@ void vjp_print(const float* neg, const float* g_print, float* g_neg, double* gra
                cudaStream_t s) {
     if (a.n == 0) return;
     Probe p("vjp_print", s);
-    k_vjp_print<<<(a.n + 127) / 128, 128, 0, s>>>(neg, g_print, g_neg, grad_params, a);
+    k_vjp_print<<<(a.n + kVjpPrintThreads - 1) / kVjpPrintThreads, kVjpPrintThreads, 0, s>>>(neg, g_print, g_neg,
+                                                                                             grad_params, a);
 }
 
 void vjp_develop(const float* exposure, const float* counts, const float* g_neg, float* g_exposure,
