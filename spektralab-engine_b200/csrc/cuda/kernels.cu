@@ -399,8 +399,8 @@ __device__ __forceinline__ void iir_line_tangent(const float* __restrict__ src, 
     }
 }
 
-// The same per-line tangent with the lines staged in shared memory: a CTA takes one row (3 lines, vertical
-// = 0) or a strip of `px` pixel columns (3 px lines, vertical = 1), loads them with coalesced reads, runs
+// The same per-line tangent with the lines staged in shared memory: a CTA takes `px` rows (3 px lines,
+// vertical = 0) or a strip of `px` pixel columns (3 px lines, vertical = 1), loads them with coalesced reads, runs
 // each line's forward and backward recurrences in place in shared memory (a thread per line; the forward
 // pass's binary32 value and tangent replace the input as iir_line_tangent's work planes hold them) and
 // stores the result. Line j, sample i at [i * nl + j]. The arithmetic is iir_line_tangent's, operation for
@@ -411,24 +411,24 @@ __global__ void k_iir_tangent_smem(const float* __restrict__ in, const float* __
                                    const __grid_constant__ IirCoefs dq) {
     extern __shared__ float tsm[];
     const uint32_t n = vertical ? h : w;
-    const uint32_t x0 = vertical ? blockIdx.x * px : 0;
-    const uint32_t npx = vertical ? min(px, w - x0) : 1;  // pixel columns in this strip
-    const uint32_t nl = 3 * (vertical ? px : 1);           // the strip's line pitch
+    const uint32_t z0 = blockIdx.x * px;                    // the first pixel column, or row
+    const uint32_t npx = min(px, (vertical ? w : h) - z0);  // columns (rows) in this strip
+    const uint32_t nl = 3 * px;                              // the strip's line pitch
     const uint32_t nv = 3 * npx;                             // valid lines
     float* val = tsm;
     float* dot = tsm + size_t(n) * nl;
-    // global index of line j (pixel x0 + j / 3, channel j % 3), sample i
-    auto gidx = [&](uint32_t i, uint32_t j) -> size_t {
-        return vertical ? (size_t(i) * w + x0) * 3 + j : (size_t(blockIdx.x) * w + i) * 3 + j;
-    };
-    // the whole CTA loads (a thread per line would wait on memory for each sample); four loads in flight
+    // the whole CTA loads (a thread per line would wait on memory for each sample), in the frame's order:
+    // element e of the strip's rows (vertical: row i, 3 npx floats from column z0; else row z0 + e / (3 n),
+    // float e % (3 n)) to line j, sample i
+    const uint32_t span = vertical ? nv : 3 * n;  // contiguous floats per strip row
+    const uint32_t total = vertical ? n * nv : npx * 3 * n;
 #pragma unroll 4
-    for (uint32_t e = threadIdx.x; e < n * nl; e += blockDim.x) {
-        const uint32_t i = e / nl, j = e - i * nl;
-        if (j >= nv) continue;
-        const size_t g = gidx(i, j);
-        val[e] = in[g];
-        dot[e] = in_dot ? in_dot[g] : 0.0f;
+    for (uint32_t e = threadIdx.x; e < total; e += blockDim.x) {
+        const uint32_t r = e / span, f = e - r * span;
+        const size_t g = vertical ? (size_t(r) * w + z0) * 3 + f : (size_t(z0 + r) * w) * 3 + f;
+        const uint32_t i = vertical ? r : f / 3, j = vertical ? f : 3 * r + f % 3;
+        val[size_t(i) * nl + j] = in[g];
+        dot[size_t(i) * nl + j] = in_dot ? in_dot[g] : 0.0f;
     }
     __syncthreads();
     const uint32_t t = threadIdx.x;
@@ -498,12 +498,12 @@ __global__ void k_iir_tangent_smem(const float* __restrict__ in, const float* __
     }
     __syncthreads();
 #pragma unroll 4
-    for (uint32_t e = threadIdx.x; e < n * nl; e += blockDim.x) {
-        const uint32_t i = e / nl, j = e - i * nl;
-        if (j >= nv) continue;
-        const size_t g = gidx(i, j);
-        out[g] = val[e];
-        out_dot[g] = dot[e];
+    for (uint32_t e = threadIdx.x; e < total; e += blockDim.x) {
+        const uint32_t r = e / span, f = e - r * span;
+        const size_t g = vertical ? (size_t(r) * w + z0) * 3 + f : (size_t(z0 + r) * w) * 3 + f;
+        const uint32_t i = vertical ? r : f / 3, j = vertical ? f : 3 * r + f % 3;
+        out[g] = val[size_t(i) * nl + j];
+        out_dot[g] = dot[size_t(i) * nl + j];
     }
 }
 
@@ -1067,18 +1067,19 @@ void iir_tangent(const float* in, const float* in_dot, float* work, float* work_
     const uint32_t lines = vertical ? 3u * w : 3u * h;
     if (lines == 0) return;
     Probe p("iir_tangent", s);
-    // lines staged in shared memory where they fit (a row, or a strip of 4, 2 or 1 pixel columns); the
-    // lines in global memory otherwise
+    // lines staged in shared memory where they fit (strips of up to 9 rows or 4 pixel columns: a line's
+    // recurrence is a chain of dependent steps, so an SM is kept busy by the lines it holds, up to a warp's
+    // worth); the lines in global memory otherwise
     int dev = 0, optin = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     const size_t n = vertical ? h : w;
-    for (uint32_t px : {4u, 2u, 1u}) {
-        const uint32_t nl = 3 * (vertical ? px : 1u);
-        const size_t smem = 2 * n * nl * sizeof(float);
+    for (uint32_t px : {9u, 8u, 4u, 2u, 1u}) {
+        if (vertical && px > 4u) continue;
+        const size_t smem = 2 * n * (3 * px) * sizeof(float);
         if (smem > size_t(optin)) continue;
         ensure_smem(reinterpret_cast<const void*>(k_iir_tangent_smem), int(smem));
-        const uint32_t ctas = vertical ? div_up(w, px) : h;
+        const uint32_t ctas = div_up(vertical ? w : h, px);
         k_iir_tangent_smem<<<ctas, 256, smem, s>>>(in, in_dot, out, out_dot, w, h, vertical ? 1 : 0, px, c, dc);
         return;
     }

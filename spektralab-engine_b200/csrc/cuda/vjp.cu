@@ -347,9 +347,9 @@ __device__ void gamut_d(const VjpPrintArgs& pa, DP& r, DP& g, DP& b) {
     dmat(q.m_to_rgb, x100 / 100.0f, y100 / 100.0f, z100 / 100.0f, r, g, b);
 }
 
-// threads per CTA of the print's adjoint
+// threads per CTA of the print's adjoint (VJP at 1024x1024: 5.02 ms at 128, 4.64 at 256, 5.91 at 512)
 #ifndef SPKB_VJP_PRINT_THREADS
-#define SPKB_VJP_PRINT_THREADS 128
+#define SPKB_VJP_PRINT_THREADS 256
 #endif
 constexpr uint32_t kVjpPrintThreads = SPKB_VJP_PRINT_THREADS;
 
