@@ -399,27 +399,58 @@ __device__ __forceinline__ void iir_line_tangent(const float* __restrict__ src, 
     }
 }
 
-// The same per-line tangent with the lines staged in shared memory: a CTA takes `px` rows (3 px lines,
-// vertical = 0) or a strip of `px` pixel columns (3 px lines, vertical = 1), loads them with coalesced reads, runs
-// each line's forward and backward recurrences in place in shared memory (a thread per line; the forward
-// pass's binary32 value and tangent replace the input as iir_line_tangent's work planes hold them) and
-// stores the result. Line j, sample i at [i * nl + j]. The arithmetic is iir_line_tangent's, operation for
-// operation.
-__global__ void k_iir_tangent_smem(const float* __restrict__ in, const float* __restrict__ in_dot,
-                                   float* __restrict__ out, float* __restrict__ out_dot, uint32_t w, uint32_t h,
-                                   int vertical, uint32_t px, const __grid_constant__ IirCoefs q,
-                                   const __grid_constant__ IirCoefs dq) {
-    extern __shared__ float tsm[];
+// The same tangent with the lines staged in shared memory and each line cut into kTanSegs segments of L
+// samples, a thread per (line, segment). A CTA takes `px` rows (3 px lines, vertical = 0) or a strip of
+// `px` pixel columns (3 px lines, vertical = 1); the whole CTA loads and stores them in the frame's order.
+// Line j, sample i at [i * nl + j]. The value and its tangent form one linear recurrence on the state
+// (w1, w2, w3, t1, t2, t3) (the last three values and tangents), so a segment is solved block-parallel as
+// the blur itself is: every segment runs from a zero state (the first from the line's edge state) and
+// keeps its end state e_s; one thread per line chains the true entry states, S_{s+1} = A^L S_s + e_s, with
+// A^L the homogeneous L-step map (TangentMaps, binary64, formed on the host); every segment then reruns
+// from its true entry state and stores float(value) and float(tangent) in place. The backward direction
+// cuts its segments from the line's end. The state is binary64 throughout.
+constexpr uint32_t kTanSegs = 8;
+struct TangentMaps {
+    double AL[3][36];  // per channel, row-major over (w1, w2, w3, t1, t2, t3)
+    uint32_t L;        // segment length
+};
+
+struct TanState {
+    double w1, w2, w3, t1, t2, t3;
+};
+
+// one step of the recurrence on the sample at smem offset o (x and its tangent), the newest state last in
+// each multiply-add chain; writes float(value), float(tangent) back when `store`
+__device__ __forceinline__ void tan_step(TanState& st, const double* k, float* val, float* dot, size_t o, bool store) {
+    const double x = double(val[o]), xd = double(dot[o]);
+    const double v = fma(k[1], st.w1, fma(k[2], st.w2, fma(k[3], st.w3, k[0] * x)));
+    const double vd = fma(k[1], st.t1, fma(k[5], st.w1, fma(k[2], st.t2, fma(k[6], st.w2,
+                      fma(k[3], st.t3, fma(k[7], st.w3, fma(k[0], xd, k[4] * x)))))));
+    st.w3 = st.w2;
+    st.w2 = st.w1;
+    st.w1 = v;
+    st.t3 = st.t2;
+    st.t2 = st.t1;
+    st.t1 = vd;
+    if (store) {
+        val[o] = float(v);
+        dot[o] = float(vd);
+    }
+}
+
+__global__ void k_iir_tangent_seg(const float* __restrict__ in, const float* __restrict__ in_dot,
+                                  float* __restrict__ out, float* __restrict__ out_dot, uint32_t w, uint32_t h,
+                                  int vertical, uint32_t px, const __grid_constant__ IirCoefs q,
+                                  const __grid_constant__ IirCoefs dq, const __grid_constant__ TangentMaps maps) {
+    extern __shared__ __align__(16) unsigned char tsm_raw[];
     const uint32_t n = vertical ? h : w;
     const uint32_t z0 = blockIdx.x * px;                    // the first pixel column, or row
     const uint32_t npx = min(px, (vertical ? w : h) - z0);  // columns (rows) in this strip
     const uint32_t nl = 3 * px;                              // the strip's line pitch
     const uint32_t nv = 3 * npx;                             // valid lines
-    float* val = tsm;
-    float* dot = tsm + size_t(n) * nl;
-    // the whole CTA loads (a thread per line would wait on memory for each sample), in the frame's order:
-    // element e of the strip's rows (vertical: row i, 3 npx floats from column z0; else row z0 + e / (3 n),
-    // float e % (3 n)) to line j, sample i
+    double* carry = reinterpret_cast<double*>(tsm_raw);      // [line][segment][6]
+    float* val = reinterpret_cast<float*>(carry + size_t(nl) * kTanSegs * 6);
+    float* dot = val + size_t(n) * nl;
     const uint32_t span = vertical ? nv : 3 * n;  // contiguous floats per strip row
     const uint32_t total = vertical ? n * nv : npx * 3 * n;
 #pragma unroll 4
@@ -431,72 +462,81 @@ __global__ void k_iir_tangent_smem(const float* __restrict__ in, const float* __
         dot[size_t(i) * nl + j] = in_dot ? in_dot[g] : 0.0f;
     }
     __syncthreads();
-    const uint32_t t = threadIdx.x;
-    const int c = int(t % 3u);
-    if (t < nv && ((q.mask >> c) & 1u) != 0u) {
-        constexpr uint32_t kTanChunk = 8;
-        const double B = q.B[c], B1 = q.B1[c], B2 = q.B2[c], B3 = q.B3[c];
-        const double dB = dq.B[c], dB1 = dq.B1[c], dB2 = dq.B2[c], dB3 = dq.B3[c];
-        double w1 = double(val[t]), w2 = w1, w3 = w1;
-        double t1 = double(dot[t]), t2 = t1, t3 = t1;
-        for (uint32_t i0 = 0; i0 < n; i0 += kTanChunk) {
-            float xs[kTanChunk], xds[kTanChunk];
-#pragma unroll
-            for (uint32_t j = 0; j < kTanChunk; ++j) {
-                const uint32_t i = i0 + j < n ? i0 + j : n - 1;
-                xs[j] = val[size_t(i) * nl + t];
-                xds[j] = dot[size_t(i) * nl + t];
+
+    const uint32_t line = threadIdx.x / kTanSegs, seg = threadIdx.x % kTanSegs;
+    const int c = int(line % 3u);
+    const bool active = line < nv && ((q.mask >> c) & 1u) != 0u;
+    const double k[8] = {q.B[c], q.B1[c], q.B2[c], q.B3[c], dq.B[c], dq.B1[c], dq.B2[c], dq.B3[c]};
+    const uint32_t L = maps.L;
+    double* cs = carry + (size_t(line) * kTanSegs + seg) * 6;
+    for (int dir = 0; dir < 2; ++dir) {
+        // this segment's samples: forward [a, b) ascending; backward [a, b) descending, cut from the end
+        uint32_t a, b;
+        if (dir == 0) {
+            a = min(n, seg * L);
+            b = min(n, a + L);
+        } else {
+            b = n > seg * L ? n - seg * L : 0u;
+            a = b > L ? b - L : 0u;
+        }
+        // the line's edge state: x[0] (forward) or the forward result u[n-1] (backward)
+        TanState edge{};
+        if (active) {
+            const size_t o0 = size_t(dir == 0 ? 0u : n - 1u) * nl + line;
+            const double e0 = double(val[o0]), d0 = double(dot[o0]);
+            edge = TanState{e0, e0, e0, d0, d0, d0};
+        }
+        // pass 1: zero-state run (the first segment from the edge state), its end state kept
+        if (active && a < b) {
+            TanState st = seg == 0 ? edge : TanState{};
+            if (dir == 0) {
+                for (uint32_t i = a; i < b; ++i) tan_step(st, k, val, dot, size_t(i) * nl + line, false);
+            } else {
+                for (uint32_t i = b; i-- > a;) tan_step(st, k, val, dot, size_t(i) * nl + line, false);
             }
-#pragma unroll
-            for (uint32_t j = 0; j < kTanChunk; ++j) {
-                if (i0 + j >= n) break;
-                const double x = double(xs[j]), xd = double(xds[j]);
-                const double v = fma(B1, w1, fma(B2, w2, fma(B3, w3, B * x)));
-                const double vd =
-                    fma(B1, t1, fma(dB1, w1, fma(B2, t2, fma(dB2, w2, fma(B3, t3, fma(dB3, w3, fma(B, xd, dB * x)))))));
-                w3 = w2;
-                w2 = w1;
-                w1 = v;
-                t3 = t2;
-                t2 = t1;
-                t1 = vd;
-                val[size_t(i0 + j) * nl + t] = float(v);
-                dot[size_t(i0 + j) * nl + t] = float(vd);
+            cs[0] = st.w1;
+            cs[1] = st.w2;
+            cs[2] = st.w3;
+            cs[3] = st.t1;
+            cs[4] = st.t2;
+            cs[5] = st.t3;
+        }
+        __syncthreads();
+        // the true entry states, one thread per line: segment s + 1 enters with A^L S_s + e_s (segment 0's
+        // end state is already true); a segment's slot takes its entry state
+        if (active && seg == 0) {
+            double S[6];
+            double* c0 = carry + size_t(line) * kTanSegs * 6;
+            for (int m = 0; m < 6; ++m) S[m] = c0[m];
+            for (uint32_t sg = 1; sg < kTanSegs && sg * L < n; ++sg) {
+                double* cg = c0 + sg * 6;
+                double e[6];
+                for (int m = 0; m < 6; ++m) {
+                    e[m] = cg[m];
+                    cg[m] = S[m];
+                }
+                const double* A = maps.AL[c];
+                double T[6];
+                for (int r = 0; r < 6; ++r) {
+                    double acc = e[r];
+                    for (int m = 0; m < 6; ++m) acc = fma(A[r * 6 + m], S[m], acc);
+                    T[r] = acc;
+                }
+                for (int m = 0; m < 6; ++m) S[m] = T[m];
             }
         }
-        const size_t last = size_t(n - 1) * nl + t;
-        double y1 = double(val[last]), y2 = y1, y3 = y1;
-        double s1 = double(dot[last]), s2 = s1, s3 = s1;
-        for (uint32_t k0 = n; k0 > 0;) {
-            const uint32_t m = k0 < kTanChunk ? k0 : kTanChunk;  // samples k0 - 1 down to k0 - m
-            float us[kTanChunk], uds[kTanChunk];
-#pragma unroll
-            for (uint32_t j = 0; j < kTanChunk; ++j) {
-                const size_t o = size_t(k0 - 1 - (j < m ? j : 0)) * nl + t;
-                us[j] = val[o];
-                uds[j] = dot[o];
+        __syncthreads();
+        // pass 2: every segment from its true entry state, storing
+        if (active && a < b) {
+            TanState st = seg == 0 ? edge : TanState{cs[0], cs[1], cs[2], cs[3], cs[4], cs[5]};
+            if (dir == 0) {
+                for (uint32_t i = a; i < b; ++i) tan_step(st, k, val, dot, size_t(i) * nl + line, true);
+            } else {
+                for (uint32_t i = b; i-- > a;) tan_step(st, k, val, dot, size_t(i) * nl + line, true);
             }
-#pragma unroll
-            for (uint32_t j = 0; j < kTanChunk; ++j) {
-                if (j >= m) break;
-                const size_t o = size_t(k0 - 1 - j) * nl + t;
-                const double u = double(us[j]), ud = double(uds[j]);
-                const double v = fma(B1, y1, fma(B2, y2, fma(B3, y3, B * u)));
-                const double vd =
-                    fma(B1, s1, fma(dB1, y1, fma(B2, s2, fma(dB2, y2, fma(B3, s3, fma(dB3, y3, fma(B, ud, dB * u)))))));
-                y3 = y2;
-                y2 = y1;
-                y1 = v;
-                s3 = s2;
-                s2 = s1;
-                s1 = vd;
-                val[o] = float(v);
-                dot[o] = float(vd);
-            }
-            k0 -= m;
         }
+        __syncthreads();
     }
-    __syncthreads();
 #pragma unroll 4
     for (uint32_t e = threadIdx.x; e < total; e += blockDim.x) {
         const uint32_t r = e / span, f = e - r * span;
@@ -1067,20 +1107,46 @@ void iir_tangent(const float* in, const float* in_dot, float* work, float* work_
     const uint32_t lines = vertical ? 3u * w : 3u * h;
     if (lines == 0) return;
     Probe p("iir_tangent", s);
-    // lines staged in shared memory where they fit (strips of up to 9 rows or 4 pixel columns: a line's
-    // recurrence is a chain of dependent steps, so an SM is kept busy by the lines it holds, up to a warp's
-    // worth); the lines in global memory otherwise
+    // lines staged in shared memory where they fit, kTanSegs threads per line (strips of up to 10 rows or 4
+    // pixel columns, at most 32 lines for the 256-thread CTA); the lines in global memory otherwise
     int dev = 0, optin = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     const size_t n = vertical ? h : w;
-    for (uint32_t px : {9u, 8u, 4u, 2u, 1u}) {
+    TangentMaps maps{};
+    maps.L = uint32_t((n + kTanSegs - 1) / kTanSegs);
+    for (int ch = 0; ch < 3; ++ch) {
+        // the homogeneous one-step map A of (w1, w2, w3, t1, t2, t3), raised to the L-th power by squaring
+        double A[36] = {0}, R[36] = {0}, T[36];
+        A[0] = c.B1[ch], A[1] = c.B2[ch], A[2] = c.B3[ch];
+        A[6] = 1.0;
+        A[13] = 1.0;
+        A[18] = dc.B1[ch], A[19] = dc.B2[ch], A[20] = dc.B3[ch], A[21] = c.B1[ch], A[22] = c.B2[ch], A[23] = c.B3[ch];
+        A[27] = 1.0;
+        A[34] = 1.0;
+        for (int i = 0; i < 6; ++i) R[i * 7] = 1.0;
+        auto mul = [&](const double* X, const double* Y, double* Z) {
+            for (int r = 0; r < 6; ++r)
+                for (int q2 = 0; q2 < 6; ++q2) {
+                    double acc = 0.0;
+                    for (int m = 0; m < 6; ++m) acc += X[r * 6 + m] * Y[m * 6 + q2];
+                    T[r * 6 + q2] = acc;
+                }
+            for (int i = 0; i < 36; ++i) Z[i] = T[i];
+        };
+        for (uint32_t e = maps.L; e > 0; e >>= 1) {
+            if (e & 1u) mul(R, A, R);
+            mul(A, A, A);
+        }
+        for (int i = 0; i < 36; ++i) maps.AL[ch][i] = R[i];
+    }
+    for (uint32_t px : {10u, 8u, 4u, 2u, 1u}) {
         if (vertical && px > 4u) continue;
-        const size_t smem = 2 * n * (3 * px) * sizeof(float);
+        const size_t smem = size_t(3 * px) * kTanSegs * 6 * sizeof(double) + 2 * n * (3 * px) * sizeof(float);
         if (smem > size_t(optin)) continue;
-        ensure_smem(reinterpret_cast<const void*>(k_iir_tangent_smem), int(smem));
+        ensure_smem(reinterpret_cast<const void*>(k_iir_tangent_seg), int(smem));
         const uint32_t ctas = div_up(vertical ? w : h, px);
-        k_iir_tangent_smem<<<ctas, 256, smem, s>>>(in, in_dot, out, out_dot, w, h, vertical ? 1 : 0, px, c, dc);
+        k_iir_tangent_seg<<<ctas, 256, smem, s>>>(in, in_dot, out, out_dot, w, h, vertical ? 1 : 0, px, c, dc, maps);
         return;
     }
     // a thread per line and few lines (3 per row or column): 32-thread CTAs spread them over more SMs

@@ -208,27 +208,55 @@ __global__ void k_vjp_develop(const float* __restrict__ exposure, const float* _
 constexpr int NP = 3 + kVjpPrintParams;  // tangents: the three negative densities, then the parameters
 using DP = Dual<NP>;
 
-// a table entry with its parameter tangents (t: [param][entry], stride = table length)
-__device__ __forceinline__ DP table_d(float v, const float* t, int stride, int i) {
-    DP r = dconst<NP>(v);
-    if (t)
-#pragma unroll
-        for (int j = 0; j < kVjpPrintParams; ++j) r.d[3 + j] = t[j * stride + i];
-    return r;
-}
 
-// R_k = sum_l 10^-(d . eps(l) + beta(l)) wt_k(l), ascending l
+// R_k = sum_l 10^-(d . eps(l) + beta(l)) wt_k(l), ascending l, with its tangents written out rather than
+// carried through dual products (most of a dual product's terms are zero here): per wavelength
+//   x = d . eps + beta,  x' = d' . eps + d . eps' + beta',  T = 10^-x,  T' = -ln(10) T x',
+//   R_k += T wt_k,  R_k' += T' wt_k + T wt_k'
+// with eps', beta', wt' the print parameters' tangents (components 3..; none where t_* is null), each
+// stored [parameter][index] with the strides of the tables.
 __device__ void spectral_d(const float* eps, const float* beta, const float* wt, const float* t_eps,
                            const float* t_beta, const float* t_wt, const DP* d, DP* R) {
-    R[0] = R[1] = R[2] = dconst<NP>(0.0f);
-    for (int l = 0; l < SPKB_NL; ++l) {
-        const DP e0 = table_d(eps[3 * l], t_eps, 3 * SPKB_NL, 3 * l);
-        const DP e1 = table_d(eps[3 * l + 1], t_eps, 3 * SPKB_NL, 3 * l + 1);
-        const DP e2 = table_d(eps[3 * l + 2], t_eps, 3 * SPKB_NL, 3 * l + 2);
-        const DP D = ((d[0] * e0 + d[1] * e1) + d[2] * e2) + table_d(beta[l], t_beta, SPKB_NL, l);
-        const DP T = dexp10(-D);
+    float r[3] = {0.0f, 0.0f, 0.0f};
+    float rd[3][NP];
 #pragma unroll
-        for (int k = 0; k < 3; ++k) R[k] = R[k] + T * table_d(wt[3 * l + k], t_wt, 3 * SPKB_NL, 3 * l + k);
+    for (int k = 0; k < 3; ++k)
+#pragma unroll
+        for (int i = 0; i < NP; ++i) rd[k][i] = 0.0f;
+#pragma unroll 3
+    for (int l = 0; l < SPKB_NL; ++l) {
+        const float e0 = eps[3 * l], e1 = eps[3 * l + 1], e2 = eps[3 * l + 2];
+        const float x = ((d[0].v * e0 + d[1].v * e1) + d[2].v * e2) + beta[l];
+        float xd[NP];
+#pragma unroll
+        for (int i = 0; i < NP; ++i) xd[i] = (d[0].d[i] * e0 + d[1].d[i] * e1) + d[2].d[i] * e2;
+        if (t_eps) {
+#pragma unroll
+            for (int j = 0; j < kVjpPrintParams; ++j) {
+                const float* te = t_eps + j * 3 * SPKB_NL + 3 * l;
+                xd[3 + j] += ((d[0].v * te[0] + d[1].v * te[1]) + d[2].v * te[2]) + t_beta[j * SPKB_NL + l];
+            }
+        }
+        const float T = exp10f(-x);
+        const float cT = -2.30258509299404568f * T;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const float wk = wt[3 * l + k];
+            r[k] += T * wk;
+            const float cw = cT * wk;
+#pragma unroll
+            for (int i = 0; i < NP; ++i) rd[k][i] += cw * xd[i];
+            if (t_wt) {
+#pragma unroll
+                for (int j = 0; j < kVjpPrintParams; ++j) rd[k][3 + j] += T * t_wt[j * 3 * SPKB_NL + 3 * l + k];
+            }
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        R[k].v = r[k];
+#pragma unroll
+        for (int i = 0; i < NP; ++i) R[k].d[i] = rd[k][i];
     }
 }
 
