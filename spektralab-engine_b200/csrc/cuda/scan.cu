@@ -311,6 +311,27 @@ __global__ void __launch_bounds__(kThreads) k_fir_tile(const float* __restrict__
         }
     }
     __syncthreads();
+    if constexpr (R >= 0) {
+        // register windows: a thread takes kFRows consecutive rows of one column and reads each input row
+        // once; every output is still sum_k t[k] A[i + k] from 0, k ascending
+        constexpr int T = 2 * R + 1, PCc = 3 * (kTW + 2 * R), kFRows = 8, NB = kTH / kFRows;
+        for (int item = threadIdx.x; item < PCc * NB; item += kThreads) {
+            const int f = item % PCc, i0 = (item / PCc) * kFRows;
+            float acc[kFRows];
+#pragma unroll
+            for (int o = 0; o < kFRows; ++o) acc[o] = 0.0f;
+#pragma unroll
+            for (int j = 0; j < kFRows + T - 1; ++j) {
+                const float v = A[(i0 + j) * PCc + f];
+#pragma unroll
+                for (int o = 0; o < kFRows; ++o)
+                    if (j - o >= 0 && j - o < T) acc[o] += a.t1[j - o] * v;
+            }
+#pragma unroll
+            for (int o = 0; o < kFRows; ++o)
+                if (y0 + i0 + o < h) B[(i0 + o) * PCc + f] = acc[o];
+        }
+    } else {
     for (int i = warp; i < kTH; i += kWarps) {
         if (y0 + i >= h) break;
         for (int f = lane; f < PC; f += 32) {
@@ -319,6 +340,7 @@ __global__ void __launch_bounds__(kThreads) k_fir_tile(const float* __restrict__
             for (int k = 0; k <= 2 * r; ++k) acc += a.t1[k] * A[(i + k) * PC + f];
             B[i * PC + f] = acc;
         }
+    }
     }
     __syncthreads();
     const int OC = 3 * kTW;
