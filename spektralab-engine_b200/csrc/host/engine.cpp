@@ -115,7 +115,54 @@ public:
     std::map<std::string, cudaGraphExec_t> graphs;
     static constexpr size_t kGraphCache = 16;
 
+    // A session's two streams and its row-band events, returned here when it is released and reused by
+    // the next session (creating and destroying them cost an open-render-release cycle about 0.1 ms)
+    struct SessionStreams {
+        cudaStream_t stream = nullptr, copy = nullptr;
+        std::vector<cudaEvent_t> band_events;
+    };
+    std::mutex streams_m;
+    std::vector<SessionStreams> idle_streams;
+    static constexpr size_t kIdleStreams = 16;
+
+    SessionStreams take_streams() {
+        {
+            std::lock_guard<std::mutex> g(streams_m);
+            if (!idle_streams.empty()) {
+                SessionStreams t = std::move(idle_streams.back());
+                idle_streams.pop_back();
+                return t;
+            }
+        }
+        SessionStreams t;
+        cuda_check(cudaStreamCreateWithFlags(&t.stream, cudaStreamNonBlocking), "cudaStreamCreate");
+        const cudaError_t err = cudaStreamCreateWithFlags(&t.copy, cudaStreamNonBlocking);
+        if (err != cudaSuccess) {
+            cudaStreamDestroy(t.stream);
+            cuda_check(err, "cudaStreamCreate");
+        }
+        return t;
+    }
+    // s's streams are idle (synchronised by the caller)
+    void give_streams(SessionStreams s) {
+        {
+            std::lock_guard<std::mutex> g(streams_m);
+            if (idle_streams.size() < kIdleStreams) {
+                idle_streams.push_back(std::move(s));
+                return;
+            }
+        }
+        destroy_streams(s);
+    }
+    static void destroy_streams(SessionStreams& s) {
+        for (cudaEvent_t e : s.band_events) cudaEventDestroy(e);
+        if (s.copy) cudaStreamDestroy(s.copy);
+        if (s.stream) cudaStreamDestroy(s.stream);
+        s = SessionStreams{};
+    }
+
     ~Engine() {
+        for (SessionStreams& t : idle_streams) destroy_streams(t);
         if (batch_stream) cudaStreamSynchronize(batch_stream);
         for (auto& [k, g] : graphs) cudaGraphExecDestroy(g);
         for (cudaStream_t w : workers) cudaStreamDestroy(w);
@@ -234,15 +281,17 @@ public:
         meter_image = Plane{};
         source = Plane{};
         pipe = Pipeline{};
-        if (stream) {
-            cudaStreamSynchronize(stream);
-            cudaStreamDestroy(stream);
+        // idle streams go back to the engine for the next session; a stream that reports an error is
+        // destroyed with its events instead
+        Engine::SessionStreams t{stream, copy_stream, std::move(band_events)};
+        const bool idle = (!stream || cudaStreamSynchronize(stream) == cudaSuccess) &&
+                          (!copy_stream || cudaStreamSynchronize(copy_stream) == cudaSuccess);
+        if (idle && stream && copy_stream && engine) {
+            engine->give_streams(std::move(t));
+        } else {
+            (void)cudaGetLastError();
+            Engine::destroy_streams(t);
         }
-        if (copy_stream) {
-            cudaStreamSynchronize(copy_stream);
-            cudaStreamDestroy(copy_stream);
-        }
-        for (cudaEvent_t e : band_events) cudaEventDestroy(e);
     }
 
     void digest(ParamSet& p, const Profile& f) const {
@@ -424,8 +473,12 @@ Session* open_session(Engine& e, const void* data, bool device_ptr, uint32_t w, 
     auto s = std::make_unique<Session>();
     s->engine = &e;
     s->product_defaults = d.product_defaults.value_or(false);
-    cuda_check(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "cudaStreamCreate");
-    cuda_check(cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    {
+        Engine::SessionStreams t = e.take_streams();
+        s->stream = t.stream;
+        s->copy_stream = t.copy;
+        s->band_events = std::move(t.band_events);
+    }
     s->pool.set_stream(s->stream);
     ParamSet p;
     for (const auto& [fid, v] : d.fields)
