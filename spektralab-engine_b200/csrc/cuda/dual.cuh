@@ -35,21 +35,45 @@ __device__ __forceinline__ Dual<N> dvar(float v, int i) {
     return r;
 }
 
+// With an even number of tangents the tangent arithmetic runs on packed f32x2 operations, tangents i and
+// i + 1 in the two halves (half the instructions; each half is the same IEEE operation as the scalar form).
+template <int N>
+__device__ __forceinline__ float2 dpair(const Dual<N>& a, int i) {
+    return make_float2(a.d[i], a.d[i + 1]);
+}
+template <int N>
+__device__ __forceinline__ void dset(Dual<N>& r, int i, float2 v) {
+    r.d[i] = v.x;
+    r.d[i + 1] = v.y;
+}
+__device__ __forceinline__ float2 dsplat(float v) { return make_float2(v, v); }
+
 // r = a + b, a - b, a * b, a / b
 template <int N>
 __device__ __forceinline__ Dual<N> operator+(const Dual<N>& a, const Dual<N>& b) {
     Dual<N> r;
     r.v = a.v + b.v;
+    if constexpr (N % 2 == 0) {
 #pragma unroll
-    for (int i = 0; i < N; ++i) r.d[i] = a.d[i] + b.d[i];
+        for (int i = 0; i < N; i += 2) dset(r, i, __fadd2_rn(dpair(a, i), dpair(b, i)));
+    } else {
+#pragma unroll
+        for (int i = 0; i < N; ++i) r.d[i] = a.d[i] + b.d[i];
+    }
     return r;
 }
 template <int N>
 __device__ __forceinline__ Dual<N> operator-(const Dual<N>& a, const Dual<N>& b) {
     Dual<N> r;
     r.v = a.v - b.v;
+    if constexpr (N % 2 == 0) {
+        // a - b as fma(b, -1, a): the product is exact, so one rounding as in the scalar subtraction
 #pragma unroll
-    for (int i = 0; i < N; ++i) r.d[i] = a.d[i] - b.d[i];
+        for (int i = 0; i < N; i += 2) dset(r, i, __ffma2_rn(dpair(b, i), dsplat(-1.0f), dpair(a, i)));
+    } else {
+#pragma unroll
+        for (int i = 0; i < N; ++i) r.d[i] = a.d[i] - b.d[i];
+    }
     return r;
 }
 template <int N>
@@ -64,8 +88,14 @@ template <int N>
 __device__ __forceinline__ Dual<N> operator*(const Dual<N>& a, const Dual<N>& b) {
     Dual<N> r;
     r.v = a.v * b.v;
+    if constexpr (N % 2 == 0) {
 #pragma unroll
-    for (int i = 0; i < N; ++i) r.d[i] = a.d[i] * b.v + a.v * b.d[i];
+        for (int i = 0; i < N; i += 2)
+            dset(r, i, __ffma2_rn(dpair(a, i), dsplat(b.v), __fmul2_rn(dsplat(a.v), dpair(b, i))));
+    } else {
+#pragma unroll
+        for (int i = 0; i < N; ++i) r.d[i] = a.d[i] * b.v + a.v * b.d[i];
+    }
     return r;
 }
 template <int N>
@@ -73,8 +103,14 @@ __device__ __forceinline__ Dual<N> operator/(const Dual<N>& a, const Dual<N>& b)
     Dual<N> r;
     r.v = a.v / b.v;
     const float ib = 1.0f / b.v;
+    if constexpr (N % 2 == 0) {
 #pragma unroll
-    for (int i = 0; i < N; ++i) r.d[i] = (a.d[i] - r.v * b.d[i]) * ib;
+        for (int i = 0; i < N; i += 2)
+            dset(r, i, __fmul2_rn(__ffma2_rn(dpair(b, i), dsplat(-r.v), dpair(a, i)), dsplat(ib)));
+    } else {
+#pragma unroll
+        for (int i = 0; i < N; ++i) r.d[i] = (a.d[i] - r.v * b.d[i]) * ib;
+    }
     return r;
 }
 // with a constant
@@ -106,8 +142,13 @@ template <int N>
 __device__ __forceinline__ Dual<N> operator*(const Dual<N>& a, float b) {
     Dual<N> r;
     r.v = a.v * b;
+    if constexpr (N % 2 == 0) {
 #pragma unroll
-    for (int i = 0; i < N; ++i) r.d[i] = a.d[i] * b;
+        for (int i = 0; i < N; i += 2) dset(r, i, __fmul2_rn(dpair(a, i), dsplat(b)));
+    } else {
+#pragma unroll
+        for (int i = 0; i < N; ++i) r.d[i] = a.d[i] * b;
+    }
     return r;
 }
 template <int N>
@@ -132,8 +173,13 @@ template <int N>
 __device__ __forceinline__ Dual<N> dchain(const Dual<N>& a, float fv, float fd) {
     Dual<N> r;
     r.v = fv;
+    if constexpr (N % 2 == 0) {
 #pragma unroll
-    for (int i = 0; i < N; ++i) r.d[i] = fd * a.d[i];
+        for (int i = 0; i < N; i += 2) dset(r, i, __fmul2_rn(dsplat(fd), dpair(a, i)));
+    } else {
+#pragma unroll
+        for (int i = 0; i < N; ++i) r.d[i] = fd * a.d[i];
+    }
     return r;
 }
 
@@ -201,8 +247,15 @@ __device__ __forceinline__ Dual<N> datan2(const Dual<N>& y, const Dual<N>& x) {
     r.v = atan2f(y.v, x.v);
     const float q = x.v * x.v + y.v * y.v;
     const float iq = q > 0.0f ? 1.0f / q : 0.0f;
+    if constexpr (N % 2 == 0) {
 #pragma unroll
-    for (int i = 0; i < N; ++i) r.d[i] = (x.v * y.d[i] - y.v * x.d[i]) * iq;
+        for (int i = 0; i < N; i += 2)
+            dset(r, i, __fmul2_rn(__ffma2_rn(dpair(x, i), dsplat(-y.v), __fmul2_rn(dsplat(x.v), dpair(y, i))),
+                                  dsplat(iq)));
+    } else {
+#pragma unroll
+        for (int i = 0; i < N; ++i) r.d[i] = (x.v * y.d[i] - y.v * x.d[i]) * iq;
+    }
     return r;
 }
 // sign(a) as a constant
