@@ -15,7 +15,7 @@
 // State and the carries are binary64 (the reference keeps double-float state on its GPU and double
 // state on its host copy); x, u and y are stored as binary32 exactly as there.
 //
-// k_iir_rows: one CTA per image row, 3 lines x 128 segments; the row (3 w floats) in shared memory,
+// k_iir_rows: one CTA per image row, 3 lines x kSegRows segments; the row (3 w floats) in shared memory,
 //             loaded afresh for every mixture component, blurred and written to the component's plane.
 // k_iir_cols: one CTA per strip of 4 pixel columns (12 lines); every component's row result blurred
 //             down the columns in turn; the mixture accumulated as the reference's fused passes do
@@ -31,11 +31,19 @@ namespace spkb::dev {
 
 namespace {
 
-constexpr int kSegRows = 128;      // segments per channel line in a row
+#ifndef SPKB_IIR_SEG_ROWS
+#define SPKB_IIR_SEG_ROWS 64
+#endif
+constexpr int kSegRows = SPKB_IIR_SEG_ROWS;  // segments per channel line in a row (4K rows: 0.185 ms at 128, 0.152 at 64)
+static_assert(kSegRows <= (1 << kIirScanSteps), "the carry scan composes at most 2^kIirScanSteps segments");
 constexpr int kRowThreads = 3 * kSegRows;
 constexpr int kColPixels = 4;       // pixels per column strip
 constexpr int kColLines = 3 * kColPixels;
-constexpr int kSegCols = 32;        // segments per column line (two 4K strips per SM)
+#ifndef SPKB_IIR_SEG_COLS
+#define SPKB_IIR_SEG_COLS 32
+#endif
+constexpr int kSegCols = SPKB_IIR_SEG_COLS;  // segments per column line (32: two 4K strips per SM)
+static_assert(kSegCols <= (1 << kIirScanSteps), "the carry scan composes at most 2^kIirScanSteps segments");
 constexpr int kColThreads = kColLines * kSegCols;
 
 struct Coef {
