@@ -198,7 +198,10 @@ __device__ __forceinline__ void expose_pixel(const ExposeArgs& q, const float* _
     h[2] = h2;
 }
 
-constexpr uint32_t kExposeThreads = 128;
+#ifndef SPKB_EXPOSE_THREADS
+#define SPKB_EXPOSE_THREADS 128
+#endif
+constexpr uint32_t kExposeThreads = SPKB_EXPOSE_THREADS;
 
 __global__ void __launch_bounds__(kExposeThreads) k_expose_patch(const float* __restrict__ rgb, float* __restrict__ hout,
                                                                  const float* __restrict__ patches,
