@@ -20,7 +20,7 @@
 // k_iir_cols: one CTA per strip of 4 pixel columns (12 lines); every component's row result blurred
 //             down the columns in turn; the mixture accumulated as the reference's fused passes do
 //             (acc = 0 + w0 y0, acc = acc + w_k y_k) and the halation mix raw := a raw + b acc written
-//             in place of raw.
+//             in place of raw; a plain blur (one component) stores its lines as they are.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -280,7 +280,21 @@ __global__ void __launch_bounds__(kColThreads) k_iir_cols(float* raw, IirPlanes 
         __syncthreads();
         blur_lines(strip, kColLines, kColLines, n, kSegCols, mix.cols, c, carry, false);
         const bool first = c == 0, last = c + 1 == int(mix.ncomp);
-        if (vec) {
+        if (mix.plain) {
+            // a plain blur (one component): the blurred lines as they are
+            if (vec) {
+                for (int i = threadIdx.x; i < n * kQuads; i += blockDim.x) {
+                    const int r = i / kQuads, qd = i - r * kQuads;
+                    *reinterpret_cast<float4*>(raw + size_t(r) * pitch + off + 4 * qd) =
+                        *reinterpret_cast<const float4*>(strip + size_t(r) * kColLines + 4 * qd);
+                }
+            } else {
+                for (int i = threadIdx.x; i < n * kColLines; i += blockDim.x) {
+                    const int r = i / kColLines, j = i % kColLines;
+                    if (j < nl) raw[size_t(r) * pitch + off + j] = strip[i];
+                }
+            }
+        } else if (vec) {
             for (int i = threadIdx.x; i < n * kQuads; i += blockDim.x) {
                 const int r = i / kQuads, qd = i - r * kQuads;
                 const size_t o = size_t(r) * pitch + off + 4 * qd;
@@ -366,8 +380,8 @@ bool iir_mixture_fits(uint32_t w, uint32_t h) {
     return iir_rows_smem(w) <= size_t(optin) && iir_cols_smem(h) <= size_t(optin);
 }
 
-void iir_mixture(float* raw, float* const* tmp, float* acc, uint32_t w, uint32_t h, const IirMixture& m,
-                 cudaStream_t s) {
+void iir_mixture(const float* src, float* raw, float* const* tmp, float* acc, uint32_t w, uint32_t h,
+                 const IirMixture& m, cudaStream_t s) {
     IirPlanes planes{};
     for (uint32_t c = 0; c < m.ncomp; ++c) planes.p[c] = tmp[c];
     const size_t sr = iir_rows_smem(w), sc = iir_cols_smem(h);
@@ -375,7 +389,7 @@ void iir_mixture(float* raw, float* const* tmp, float* acc, uint32_t w, uint32_t
     ensure_smem(reinterpret_cast<const void*>(k_iir_cols), int(sc));
     {
         Probe p("iir_rows", s);
-        k_iir_rows<<<h, kRowThreads, sr, s>>>(raw, planes, w, h, m);
+        k_iir_rows<<<h, kRowThreads, sr, s>>>(src, planes, w, h, m);
     }
     {
         Probe p("iir_cols", s);

@@ -31,6 +31,9 @@ struct IirLaunch {
 
 struct IirMixture {
     uint32_t ncomp;
+    // 1: a plain blur, raw := G_0(src) with one component (weight, mix_a and mix_b unused); the column
+    // pass stores the blurred lines as they are and never reads raw
+    uint32_t plain;
     float weight[SPKB_MAX_COMPONENTS][3];
     float mix_a[3], mix_b[3];  // raw := mix_a raw + mix_b sum_k weight_k G_k(raw)
     IirLaunch rows, cols;
@@ -46,9 +49,11 @@ int iir_row_seg_len(uint32_t w);  // segment length of the row and column passes
 int iir_col_seg_len(uint32_t h);
 bool iir_mixture_fits(uint32_t w, uint32_t h);  // both kernels' lines fit in shared memory
 
-// raw := mix_a raw + mix_b sum_k weight_k G_k(raw), every component recursive on every channel.
-// tmp: ncomp planes for the row results; acc: one plane for the running sum (unused for one component).
-void iir_mixture(float* raw, float* const* tmp, float* acc, uint32_t w, uint32_t h, const IirMixture& m,
-                 cudaStream_t s);
+// raw := mix_a raw + mix_b sum_k weight_k G_k(src), every component recursive on every active channel
+// (an inactive channel's lines pass through G_k unchanged); src is raw itself or, for a plain blur, any
+// plane (raw := G_0(src)). tmp: ncomp planes for the row results; acc: one plane for the running sum
+// (unused for one component).
+void iir_mixture(const float* src, float* raw, float* const* tmp, float* acc, uint32_t w, uint32_t h,
+                 const IirMixture& m, cudaStream_t s);
 
 }  // namespace spkb::dev

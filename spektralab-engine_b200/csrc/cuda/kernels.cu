@@ -5,6 +5,7 @@
 // fx_grain.metal): binary32 arithmetic in the same bracketing; recursive-filter state in binary64
 // (the reference keeps it in double-float on its GPU and in double on its host copy); the grain
 // sampler from grain_sampler.h, which the host checker compiles too.
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
@@ -1078,14 +1079,41 @@ Probe::~Probe() {
     if (t_hook) t_hook->after(s);
 }
 
+unsigned long long current_context_id() {
+    using GetCurrent = CUresult (*)(CUcontext*);
+    using GetId = CUresult (*)(CUcontext, unsigned long long*);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* f0 = nullptr;
+        void* f1 = nullptr;
+        cudaDriverEntryPointQueryResult q0{}, q1{};
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f0, 12000, cudaEnableDefault, &q0) != cudaSuccess ||
+            cudaGetDriverEntryPointByVersion("cuCtxGetId", &f1, 12000, cudaEnableDefault, &q1) != cudaSuccess ||
+            !f0 || !f1)
+            return;
+        get_current = reinterpret_cast<GetCurrent>(f0);
+        get_id = reinterpret_cast<GetId>(f1);
+    });
+    CUcontext ctx = nullptr;
+    unsigned long long id = 0;
+    if (!get_current || !get_id || get_current(&ctx) != CUDA_SUCCESS || !ctx || get_id(ctx, &id) != CUDA_SUCCESS)
+        return 0;
+    return id;
+}
+
 void ensure_smem(const void* kernel, int bytes) {
     static std::mutex m;
-    static std::map<std::pair<const void*, int>, int> done;
-    int dev = 0;
-    cudaGetDevice(&dev);
+    static std::map<std::pair<const void*, unsigned long long>, int> done;
+    unsigned long long ctx = current_context_id();
+    if (ctx == 0) {  // no context yet: make the device's primary one current first
+        cudaFree(nullptr);
+        ctx = current_context_id();
+    }
     std::lock_guard<std::mutex> g(m);
-    int& cur = done[{kernel, dev}];
-    if (bytes <= cur) return;
+    int& cur = done[{kernel, ctx}];
+    if (ctx != 0 && bytes <= cur) return;
     cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     cur = bytes;
 }

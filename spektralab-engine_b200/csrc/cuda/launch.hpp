@@ -27,9 +27,13 @@ struct Probe {
     ~Probe();
 };
 
-// Raises a kernel's dynamic shared-memory limit to `bytes` on the current device, once (a later call asking
-// no more is a no-op), so that launches inside a stream capture make no attribute call.
+// Raises a kernel's dynamic shared-memory limit to `bytes` in the current context, once (a later call in
+// the same context asking no more is a no-op), so that launches inside a stream capture make no attribute
+// call. A new context (a host's own driver context, or one after a device reset) sets it afresh.
 void ensure_smem(const void* kernel, int bytes);
+
+// The driver's unique id of the current CUDA context; 0 when none is current or the driver cannot say.
+unsigned long long current_context_id();
 
 // Tier downscale: the vertical prefilter src -> dst (same size), then the horizontal prefilter at the
 // bilinear sample points fused with the blend, v (in_w x in_h) -> dst (out_w x out_h).

@@ -36,39 +36,12 @@ namespace {
 constexpr size_t kMaxFloats = size_t(1) << 21;  // one plane: 2,097,152 floats (8 MiB)
 __device__ __align__(256) float g_scratch[2 * kMaxFloats];
 
-using CtxGetCurrent = CUresult (*)(CUcontext*);
-using CtxGetId = CUresult (*)(CUcontext, unsigned long long*);
-
 std::mutex g_mutex;
-CtxGetCurrent g_get_current = nullptr;
-CtxGetId g_get_id = nullptr;
 std::vector<std::pair<unsigned long long, float*>> g_address;  // (driver context id, address of g_scratch)
-
-// The driver's id of the current context (0 when none is current or the driver cannot say).
-unsigned long long current_context_id() {
-    CUcontext ctx = nullptr;
-    unsigned long long id = 0;
-    if (g_get_current(&ctx) != CUDA_SUCCESS || !ctx || g_get_id(ctx, &id) != CUDA_SUCCESS) return 0;
-    return id;
-}
 
 // The device address of g_scratch in the current context, looked up once per context. The caller holds
 // g_mutex.
 float* scratch_address(cudaError_t* err) {
-    if (!g_get_current || !g_get_id) {
-        void* f0 = nullptr;
-        void* f1 = nullptr;
-        cudaDriverEntryPointQueryResult q0{}, q1{};
-        *err = cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f0, 12000, cudaEnableDefault, &q0);
-        if (*err == cudaSuccess)
-            *err = cudaGetDriverEntryPointByVersion("cuCtxGetId", &f1, 12000, cudaEnableDefault, &q1);
-        if (*err != cudaSuccess || !f0 || !f1) {
-            if (*err == cudaSuccess) *err = cudaErrorNotSupported;
-            return nullptr;
-        }
-        g_get_current = reinterpret_cast<CtxGetCurrent>(f0);
-        g_get_id = reinterpret_cast<CtxGetId>(f1);
-    }
     unsigned long long id = current_context_id();
     for (const auto& [ctx, p] : g_address)
         if (id != 0 && ctx == id) return p;
@@ -138,15 +111,19 @@ extern "C" SPK_API spk_status spkx_gaussian_noalloc(const float* in, float* out,
             dev::fir_h(s0, out, out, w, h, taps, ACC_NONE, one, st);
         }
     } else {
-        const IirCoefs coefs = blur_iir_coefs(sigma3, iir);
         const float* src = in;
         if (n_iir < 3 && taps.r > 0) {  // FIR channels first, the recursive ones pass through as a delta
             dev::fir_v(in, s0, w, h, taps, st);
             dev::fir_h(s0, s1, s1, w, h, taps, ACC_NONE, one, st);
             src = s1;
         }
-        dev::iir_h(src, s0, w, h, coefs, st);
-        dev::iir_v(s0, out, out, w, h, coefs, ACC_NONE, one, st);
+        // the block-parallel kernels where the lines fit in shared memory (the other channels pass
+        // through), else one thread per line
+        if (!blur_iir_block(src, out, s0, w, h, sigma3, iir, st)) {
+            const IirCoefs coefs = blur_iir_coefs(sigma3, iir);
+            dev::iir_h(src, s0, w, h, coefs, st);
+            dev::iir_v(s0, out, out, w, h, coefs, ACC_NONE, one, st);
+        }
     }
     e = cudaGetLastError();
     if (e != cudaSuccess) {

@@ -299,13 +299,14 @@ bool iir_mixture_mix(RenderCtx& ctx, const Plane& raw, const std::vector<Mixture
 }  // namespace
 
 void gaussian(RenderCtx& ctx, const Plane& in, const Plane& dst, const Vec3& sigma) {
-    // one recursive sigma on every channel: the block-parallel kernels, as a one-component mixture
-    // dst := 0 dst + 1 G(dst) (the same recurrence as the line kernels, evaluated by segments)
-    if (sigma[0] == sigma[1] && sigma[1] == sigma[2] && blur_branch(sigma[0]) == Branch::Iir &&
-        dev::iir_mixture_fits(in.w, in.h)) {
-        if (!same(in, dst)) dev::copy(in.data(), dst.data(), in.pixels(), ctx.stream);
-        const std::vector<MixtureComponent> one{MixtureComponent{Vec3{1.0, 1.0, 1.0}, sigma}};
-        if (iir_mixture_mix(ctx, dst, one, Vec3{0.0, 0.0, 0.0}, Vec3{1.0, 1.0, 1.0})) return;
+    // every channel recursive: the block-parallel kernels as a plain one-component blur, dst := G(in)
+    // (the same recurrence as the line kernels, evaluated by segments; in == dst allowed)
+    if (blur_branch(sigma[0]) == Branch::Iir && blur_branch(sigma[1]) == Branch::Iir &&
+        blur_branch(sigma[2]) == Branch::Iir && dev::iir_mixture_fits(in.w, in.h)) {
+        const double s3[3] = {sigma[0], sigma[1], sigma[2]};
+        const bool all[3] = {true, true, true};
+        Plane tmp = make_plane(ctx.pool, in.w, in.h);
+        if (blur_iir_block(in.data(), dst.data(), tmp.data(), in.w, in.h, s3, all, ctx.stream)) return;
     }
     encode_blur(ctx, in, dst, sigma, Fuse{});
 }
@@ -346,11 +347,16 @@ void entry_map(const IirCoefficients& k, int L, double M[3][3]) {
     }
 }
 
-void fill_launch(dev::IirLaunch& q, const std::vector<MixtureComponent>& comps, int L) {
+// active: the channels that blur (null: all three); the others pass through
+void fill_launch(dev::IirLaunch& q, const std::vector<MixtureComponent>& comps, int L, const bool* active = nullptr) {
     q.seg_len = L;
     for (size_t c = 0; c < comps.size(); ++c)
         for (int ch = 0; ch < 3; ++ch) {
             dev::IirChannel& d = q.ch[3 * c + ch];
+            if (active && !active[ch]) {
+                d = dev::IirChannel{};
+                continue;
+            }
             const IirCoefficients k = iir_coefficients(comps[c].sigma[ch]);
             d.B = k.B;
             d.B1 = k.B1;
@@ -394,11 +400,27 @@ bool iir_mixture_mix(RenderCtx& ctx, const Plane& raw, const std::vector<Mixture
         tp[c] = tmp.back().data();
     }
     Plane acc = comps.size() > 1 ? make_plane(ctx.pool, raw.w, raw.h) : Plane{};
-    dev::iir_mixture(raw.data(), tp, acc ? acc.data() : nullptr, raw.w, raw.h, q, ctx.stream);
+    dev::iir_mixture(raw.data(), raw.data(), tp, acc ? acc.data() : nullptr, raw.w, raw.h, q, ctx.stream);
     return true;
 }
 
 }  // namespace
+
+bool blur_iir_block(const float* src, float* dst, float* tmp, uint32_t w, uint32_t h, const double sigma[3],
+                    const bool iir[3], cudaStream_t s) {
+    // the kernels move whole rows and strips in 16-byte pieces from the planes' bases
+    auto aligned = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; };
+    if (!aligned(src) || !aligned(dst) || !aligned(tmp) || !dev::iir_mixture_fits(w, h)) return false;
+    dev::IirMixture q{};
+    q.ncomp = 1;
+    q.plain = 1;
+    const std::vector<MixtureComponent> one{MixtureComponent{Vec3{1.0, 1.0, 1.0}, Vec3{sigma[0], sigma[1], sigma[2]}}};
+    fill_launch(q.rows, one, dev::iir_row_seg_len(w), iir);
+    fill_launch(q.cols, one, dev::iir_col_seg_len(h), iir);
+    float* tp[SPKB_MAX_COMPONENTS] = {tmp};
+    dev::iir_mixture(src, dst, tp, nullptr, w, h, q, s);
+    return true;
+}
 
 void check_supported(const ParamSet&) {
     // every field of the reference's parameter schema has its stage in this build: nothing is refused

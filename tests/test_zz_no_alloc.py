@@ -5,7 +5,8 @@ callback (their memory is budgeted by the host application's own allocator, or c
 synchronisation are not allowed there): they pass device buffers and the blur's intermediate planes
 come from a fixed scratch array inside the library. This test gives it device buffers it allocated
 itself (through torch) and checks two calls in a row against the allocating entry point, spkx_gaussian,
-within the tolerances the other blur tests use: separate and in-place buffers, and a recursive channel
+within the tolerances the other blur tests use: separate and in-place buffers, buffers that start off a
+16-byte boundary, and a recursive channel
 beside channels of zero sigma, which must come back unchanged. It runs last (file name) so that a failure here never
 stops the rest of the suite, and it passes alone in a fresh process as well.
 """
@@ -37,16 +38,21 @@ def test_noalloc_matches_allocating_entry_point(lib):
     fn.restype, fn.argtypes = NOALLOC
     rng = np.random.default_rng(42)
     stream = torch.cuda.Stream()
-    # (0, 8, 0): a recursive channel beside two channels that no pass may change; in_place: out == in
-    cases = [((300, 257), (0.65, 1.5, 2.9), False), ((480, 640), (3.0, 20.0, 120.0), False),
-             ((61, 97), (2.5, 8.0, 0.0), False), ((200, 150), (0.0, 8.0, 0.0), False),
-             ((300, 257), (0.65, 1.5, 2.9), True), ((480, 640), (3.0, 20.0, 120.0), True),
-             ((120, 90), (0.0, 8.0, 0.0), True)]
-    for (h, w), sigma, in_place in cases:
+    # (0, 8, 0): a recursive channel beside two channels that no pass may change; in_place: out == in;
+    # shift: the buffers start 4 bytes past a 16-byte boundary (the recursive channels then take the
+    # one-thread-per-line kernels instead of the block-parallel ones)
+    cases = [((300, 257), (0.65, 1.5, 2.9), False, 0), ((480, 640), (3.0, 20.0, 120.0), False, 0),
+             ((61, 97), (2.5, 8.0, 0.0), False, 0), ((200, 150), (0.0, 8.0, 0.0), False, 0),
+             ((300, 257), (0.65, 1.5, 2.9), True, 0), ((480, 640), (3.0, 20.0, 120.0), True, 0),
+             ((120, 90), (0.0, 8.0, 0.0), True, 0), ((480, 640), (3.0, 20.0, 120.0), False, 1),
+             ((61, 97), (2.5, 8.0, 0.0), True, 1), ((64, 48), (8.0, 8.0, 8.0), False, 1)]
+    for (h, w), sigma, in_place, shift in cases:
         for call in range(2):  # two calls in a row share the scratch array
             plane = (rng.random((h, w, 3), dtype=np.float32) + 0.1 * (call + 1)).astype(np.float32)
-            d_in = torch.from_numpy(plane).cuda()
-            d_out = d_in if in_place else torch.empty_like(d_in)
+            n = h * w * 3
+            d_in = torch.empty(n + shift, device="cuda")[shift:].view(h, w, 3)
+            d_in.copy_(torch.from_numpy(plane))
+            d_out = d_in if in_place else torch.empty(n + shift, device="cuda")[shift:].view(h, w, 3)
             st = fn(ctypes.cast(d_in.data_ptr(), sc.FP), ctypes.cast(d_out.data_ptr(), sc.FP), w, h,
                     (ctypes.c_double * 3)(*sigma), ctypes.c_void_p(stream.cuda_stream))
             assert st == sc.SPK_OK, lib.last_error()
