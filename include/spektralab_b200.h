@@ -200,7 +200,10 @@ SPK_API spk_status spk_render_vjp(spk_session* session, const char* tier, uint32
  *   keeps it for later calls in the same context (keyed by the driver's context id, so a new context or a
  *   reset device gets a fresh lookup); make that first call before any stream capture. All calls in a
  *   context share the one array and leave their data in it, so calls whose work overlaps on the GPU race:
- *   order them on one stream, or wait for one before starting the next on another.
+ *   order them on one stream, or wait for one before starting the next on another. Buffers that start on
+ *   16-byte boundaries (as cudaMalloc's do) let the recursive channels (sigma >= 3) run the block-parallel
+ *   kernels; other buffers take slower one-thread-per-line kernels (the same recurrence, rounded in a
+ *   different order: results agree within the blur's tolerances).
  */
 SPK_API spk_status spkx_gaussian_noalloc(const float* in, float* out, uint32_t w, uint32_t h, const double* sigma3,
                                          void* stream);
