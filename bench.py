@@ -91,9 +91,9 @@ def film_format_for_grains(lib, resources, long_edge):
 def hbm_peak():
     try:
         with open(MEASURED_PEAKS) as f:
-            return float(json.load(f)["hbm_gbs"]), "measured"
+            return float(json.load(f)["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
     except (OSError, KeyError, ValueError):
-        return FALLBACK_HBM_GBS, "fallback"
+        return FALLBACK_HBM_GBS, "fallback (no MEASURED_PEAKS.json: an earlier copy measurement on this B200 type)"
 
 
 class Clocks:
@@ -459,9 +459,9 @@ def run_precision(args):
     head_key = "bf16x3@81" if "bf16x3@81" in table else next(iter(table))
     try:
         with open(MEASURED_PEAKS) as f:
-            tpeak, tkind = float(json.load(f)["bf16_tflops"]), "measured (MEASURED_PEAKS bf16_tflops)"
+            tpeak, tkind = float(json.load(f)["bf16_tflops"]), "measured (MEASURED_PEAKS.json bf16_tflops)"
     except (OSError, KeyError, ValueError):
-        tpeak, tkind = 1590.0, "fallback"
+        tpeak, tkind = 1590.0, "fallback (no MEASURED_PEAKS.json: an earlier cuBLAS bf16 measurement on this B200 type)"
     line = {"metric": "print Mpx/s, split-BF16 tensor cores, 81 wavelengths" if head_key == "bf16x3@81"
             else f"print Mpx/s, {head_key}", "value": head["mpx_s"],
             "unit": "Mpx/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
@@ -679,7 +679,7 @@ def main():
     traffic = NCU_TRAFFIC_PER_PX.get(dom)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": traffic * W * H if traffic else None, "kernel": dom,
-                "algorithmic_bytes_per_launch": bytes_launch, "peak_source": f"{peak_kind} (MEASURED_PEAKS hbm_gbs)",
+                "algorithmic_bytes_per_launch": bytes_launch, "peak_source": peak_kind,
                 # the render kernels are instruction-bound, not HBM-bound: the fraction of the SMs' issue
                 # rate the kernel sustains (warp instructions per pixel from its ncu capture, the launch time
                 # measured here, peak = 4 warp instructions per SM per clock at the sampled SM clock)
