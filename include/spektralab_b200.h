@@ -107,6 +107,15 @@ SPK_API spk_status spkx_philox(const uint32_t* counters, const uint32_t* keys, u
  * SPK_ERR_GPU with the context still usable. Process-wide; set it back to 0 afterwards. */
 SPK_API spk_status spkx_test_set_tc_wait_limit(int64_t cycles);
 
+/* Test hooks of the recursive blur's column pass (no counterpart in the reference engine), which loads its
+ * strips by TMA and waits on an mbarrier. spkx_test_set_iir_wait_limit: the SM clocks a strip wait may
+ * take before it gives up (0: the normal limit, about 2 s; process-wide, set it back to 0 afterwards). A
+ * wait that gives up is counted, then waits again under the normal limit for the copies in flight, and
+ * the blur's result is unchanged. spkx_test_take_iir_waits_given_up: the count since the last call, reset
+ * to 0. */
+SPK_API spk_status spkx_test_set_iir_wait_limit(int64_t cycles);
+SPK_API spk_status spkx_test_take_iir_waits_given_up(uint32_t* count);
+
 /* the Gaussian blur of a w x h RGB float plane (3 floats per pixel) with per-channel sigma in pixels,
  * by the engine's FIR / recursive branch rule */
 SPK_API spk_status spkx_gaussian(const float* in, float* out, uint32_t w, uint32_t h, const double* sigma3);

@@ -21,8 +21,17 @@
 //             down the columns in turn; the mixture accumulated as the reference's fused passes do
 //             (acc = 0 + w0 y0, acc = acc + w_k y_k) and the halation mix raw := a raw + b acc written
 //             in place of raw; a plain blur (one component) stores its lines as they are.
+//             A full strip (frame width a multiple of 4) comes into shared memory by TMA: the component's
+//             plane is a 2-D tensor (3 w floats x h rows), and the strip is a column of 12-float boxes of up
+//             to 256 rows, all completing on one mbarrier. Its waits are bounded: one that gives up counts
+//             itself (g_iir_gave_up), waits again under the full limit for the copies in flight, and if
+//             even they never land the CTA loads this and every later strip with plain copies.
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
+
+#include <atomic>
+#include <mutex>
 
 #include "../kernel_args.h"
 #include "iir.hpp"
@@ -45,6 +54,90 @@ constexpr int kColLines = 3 * kColPixels;
 constexpr int kSegCols = SPKB_IIR_SEG_COLS;  // segments per column line (32: two 4K strips per SM)
 static_assert(kSegCols <= (1 << kIirScanSteps), "the carry scan composes at most 2^kIirScanSteps segments");
 constexpr int kColThreads = kColLines * kSegCols;
+
+// The column pass's tensor maps, one per component plane, and the strip's box geometry: `boxes` boxes of
+// `box_rows` rows (a multiple of 8, at most 256) cover the frame's rows; the strip buffer holds
+// boxes * box_rows rows, and the rows past the frame are zero-filled by the copy and never read.
+struct IirColMaps {
+    CUtensorMap map[SPKB_MAX_COMPONENTS];
+    long long wait_limit;  // SM clocks a strip wait may take before it gives up
+    uint32_t box_rows, boxes;
+    uint32_t use_tma;      // 0: plain copies (a width that is not a multiple of 4, or no tensor map)
+};
+
+#ifndef SPKB_IIR_COL_TMA
+#define SPKB_IIR_COL_TMA 1
+#endif
+constexpr bool kColTma = SPKB_IIR_COL_TMA != 0;  // 0: every strip by plain 16-byte copies
+
+constexpr long long kWaitCycles = 4000000000LL;  // about 2 s at the B200's clocks
+__device__ unsigned int g_iir_gave_up;           // strip waits that gave up, since the last read
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return uint32_t(__cvta_generic_to_shared(p)); }
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+
+// this thread's earlier shared-memory accesses ordered before the asynchronous (TMA) proxy's next ones
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return done != 0;
+}
+
+// the phase's completion tested without waiting
+__device__ __forceinline__ bool mbar_test(uint32_t bar, uint32_t parity) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return done != 0;
+}
+
+// the barrier's phase of the given parity completed; false once `limit` SM clocks have passed without it.
+// try_wait may suspend the thread for a while by itself, so a shortened limit (the test hook) polls with
+// the non-blocking test_wait instead.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, long long limit) {
+    if (limit < kWaitCycles) {
+        const long long t0 = clock64();
+        for (;;) {
+            if (mbar_test(bar, parity)) return true;
+            if (clock64() - t0 > limit) return false;
+        }
+    }
+    if (mbar_try(bar, parity)) return true;
+    const long long t0 = clock64();
+    for (;;) {
+        if (mbar_try(bar, parity)) return true;
+        if (clock64() - t0 > limit) return false;
+    }
+}
+
+// one box of a 2-D tensor map at element coordinates (x, y) into shared memory, completing on `bar`
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int x, int y, uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
+        : "memory");
+}
 
 struct Coef {
     double B, B1, B2, B3;
@@ -219,7 +312,7 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 
 __global__ void __launch_bounds__(kRowThreads) k_iir_rows(const float* __restrict__ in, IirPlanes outs, uint32_t w,
                                                           uint32_t h, const __grid_constant__ IirMixture mix) {
-    extern __shared__ __align__(16) unsigned char smem[];
+    extern __shared__ __align__(128) unsigned char smem[];
     const uint32_t y = blockIdx.x;
     if (y >= h) return;
     const int n3 = int(3 * w);
@@ -250,22 +343,57 @@ __global__ void __launch_bounds__(kRowThreads) k_iir_rows(const float* __restric
 }
 
 __global__ void __launch_bounds__(kColThreads) k_iir_cols(float* raw, IirPlanes hs, float* acc, uint32_t w, uint32_t h,
-                                                          const __grid_constant__ IirMixture mix) {
-    extern __shared__ __align__(16) unsigned char smem[];
+                                                          const __grid_constant__ IirMixture mix,
+                                                          const __grid_constant__ IirColMaps maps) {
+    extern __shared__ __align__(128) unsigned char smem[];
     const uint32_t x0 = blockIdx.x * kColPixels;
     const int px = min(kColPixels, int(w) - int(x0));
     const int nl = 3 * px;  // valid lines in this strip
     const int n = int(h);
-    float* strip = reinterpret_cast<float*>(smem);  // [row][kColLines]
-    double* carry = reinterpret_cast<double*>(strip + size_t(n) * kColLines);
+    // [row][kColLines], boxes * box_rows rows (each box's first row 128-byte aligned: box_rows is a
+    // multiple of 8 and a row is 48 bytes), then the carries, then the strip's mbarrier
+    const size_t rows_alloc = size_t(maps.box_rows) * maps.boxes;
+    float* strip = reinterpret_cast<float*>(smem);
+    double* carry = reinterpret_cast<double*>(strip + rows_alloc * kColLines);
+    const uint32_t bar = smem_addr(carry + size_t(kColLines) * kSegCols * 3);
     const size_t pitch = 3 * size_t(w);
     const size_t off = 3 * size_t(x0);
     // a full strip of a frame whose width is a multiple of 4: every strip row is three aligned float4
     const bool vec = px == kColPixels && (w & 3u) == 0;
     constexpr int kQuads = kColLines / 4;
+    bool tma = vec && maps.use_tma != 0;  // the same in every thread of the CTA
+    if (tma) {
+        if (threadIdx.x == 0) {
+            mbar_init(bar, 1);
+            fence_mbar_init();
+        }
+        __syncthreads();
+    }
     for (int c = 0; c < int(mix.ncomp); ++c) {
         const float* src = hs.p[c];
-        if (vec) {
+        if (tma) {
+            if (threadIdx.x == 0) {
+                fence_proxy_async();  // the previous component's reads and writes of the strip come first
+                mbar_arrive_expect_tx(bar, maps.boxes * maps.box_rows * uint32_t(kColLines * sizeof(float)));
+                for (uint32_t k = 0; k < maps.boxes; ++k)
+                    tma_load_2d(smem_addr(strip + size_t(k) * maps.box_rows * kColLines), &maps.map[c], int(off),
+                                int(k * maps.box_rows), bar);
+            }
+            // component c completes the barrier's phase c
+            const uint32_t parity = uint32_t(c) & 1u;
+            bool gave_up = false, landed = true;
+            if (!mbar_wait(bar, parity, maps.wait_limit)) {
+                gave_up = true;
+                landed = mbar_wait(bar, parity, kWaitCycles);
+            }
+            const int any_gave_up = __syncthreads_or(gave_up);
+            const int all_landed = __syncthreads_and(landed);
+            if (threadIdx.x == 0 && any_gave_up) atomicAdd(&g_iir_gave_up, 1u);
+            if (!all_landed) tma = false;  // this strip and every later one by plain copies
+        }
+        if (tma) {
+            // the strip is in place
+        } else if (vec) {
             for (int i = threadIdx.x; i < n * kQuads; i += blockDim.x) {
                 const int r = i / kQuads, qd = i - r * kQuads;
                 cp_async16(strip + size_t(r) * kColLines + 4 * qd, src + size_t(r) * pitch + off + 4 * qd);
@@ -348,8 +476,22 @@ size_t iir_rows_smem(uint32_t w) {
     return n3r * sizeof(float) + size_t(3) * kSegRows * 3 * sizeof(double);
 }
 
+namespace {
+// The strip's boxes: ceil(h / 256) of them, each a multiple of 8 rows (at most 256) and together at least h.
+struct ColBoxes {
+    uint32_t rows, boxes;
+};
+ColBoxes col_boxes(uint32_t h) {
+    const uint32_t boxes = h > 0 ? (h + 255u) / 256u : 1u;
+    const uint32_t per = (h + boxes - 1u) / boxes;
+    return {(per + 7u) & ~7u, boxes};
+}
+}  // namespace
+
 size_t iir_cols_smem(uint32_t h) {
-    return size_t(h) * kColLines * sizeof(float) + size_t(kColLines) * kSegCols * 3 * sizeof(double);
+    const ColBoxes cb = col_boxes(h);
+    return size_t(cb.rows) * cb.boxes * kColLines * sizeof(float) + size_t(kColLines) * kSegCols * 3 * sizeof(double) +
+           sizeof(uint64_t);
 }
 
 // The column segment length: at least n / nseg, and with nlines L = nlines (mod 32), so that a warp's
@@ -380,6 +522,67 @@ bool iir_mixture_fits(uint32_t w, uint32_t h) {
     return iir_rows_smem(w) <= size_t(optin) && iir_cols_smem(h) <= size_t(optin);
 }
 
+namespace {
+using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                 const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+// cuTensorMapEncodeTiled from the driver, looked up once (null when the driver cannot give it)
+EncodeTiled encode_tiled() {
+    static EncodeTiled fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &f, 12000, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiled>(f);
+    });
+    return fn;
+}
+
+std::atomic<long long> g_wait_limit{0};  // set_iir_wait_limit: 0 the full limit
+
+// The tensor maps of the column pass's component planes: each a 2-D tensor of 3 w floats x h rows (row
+// pitch 12 w bytes), read in 12 x box_rows boxes. False (plain copies) for a width that is not a multiple
+// of 4 (the rows and the strips' x coordinates would leave 16-byte alignment), a plane not on a 16-byte
+// boundary, or a map the driver refuses.
+bool col_maps(IirColMaps& maps, const IirPlanes& planes, uint32_t ncomp, uint32_t w, uint32_t h) {
+    const ColBoxes cb = col_boxes(h);
+    maps.box_rows = cb.rows;
+    maps.boxes = cb.boxes;
+    const long long lim = g_wait_limit.load();
+    maps.wait_limit = lim > 0 ? lim : kWaitCycles;
+    maps.use_tma = 0;
+    const EncodeTiled enc = encode_tiled();
+    if (!kColTma || !enc || (w & 3u) != 0u) return false;
+    const cuuint64_t dims[2] = {cuuint64_t(3) * w, h};
+    const cuuint64_t strides[1] = {cuuint64_t(3) * w * sizeof(float)};
+    const cuuint32_t box[2] = {cuuint32_t(kColLines), cb.rows};
+    const cuuint32_t estr[2] = {1, 1};
+    for (uint32_t c = 0; c < ncomp; ++c) {
+        if ((reinterpret_cast<uintptr_t>(planes.p[c]) & 15u) != 0u) return false;
+        if (enc(&maps.map[c], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, planes.p[c], dims, strides, box, estr,
+                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+            return false;
+    }
+    maps.use_tma = 1;
+    return true;
+}
+}  // namespace
+
+void set_iir_wait_limit(long long cycles) { g_wait_limit.store(cycles); }
+
+uint32_t take_iir_waits_given_up(cudaStream_t s) {
+    unsigned int v = 0, zero = 0;
+    cudaMemcpyFromSymbolAsync(&v, g_iir_gave_up, sizeof(v), 0, cudaMemcpyDeviceToHost, s);
+    cudaMemcpyToSymbolAsync(g_iir_gave_up, &zero, sizeof(zero), 0, cudaMemcpyHostToDevice, s);
+    cudaStreamSynchronize(s);
+    return v;
+}
+
 void iir_mixture(const float* src, float* raw, float* const* tmp, float* acc, uint32_t w, uint32_t h,
                  const IirMixture& m, cudaStream_t s) {
     IirPlanes planes{};
@@ -387,13 +590,15 @@ void iir_mixture(const float* src, float* raw, float* const* tmp, float* acc, ui
     const size_t sr = iir_rows_smem(w), sc = iir_cols_smem(h);
     ensure_smem(reinterpret_cast<const void*>(k_iir_rows), int(sr));
     ensure_smem(reinterpret_cast<const void*>(k_iir_cols), int(sc));
+    IirColMaps maps{};
+    col_maps(maps, planes, m.ncomp, w, h);
     {
         Probe p("iir_rows", s);
         k_iir_rows<<<h, kRowThreads, sr, s>>>(src, planes, w, h, m);
     }
     {
         Probe p("iir_cols", s);
-        k_iir_cols<<<(w + kColPixels - 1) / kColPixels, kColThreads, sc, s>>>(raw, planes, acc, w, h, m);
+        k_iir_cols<<<(w + kColPixels - 1) / kColPixels, kColThreads, sc, s>>>(raw, planes, acc, w, h, m, maps);
     }
 }
 

@@ -56,4 +56,10 @@ bool iir_mixture_fits(uint32_t w, uint32_t h);  // both kernels' lines fit in sh
 void iir_mixture(const float* src, float* raw, float* const* tmp, float* acc, uint32_t w, uint32_t h,
                  const IirMixture& m, cudaStream_t s);
 
+// Test hooks of the column pass's bounded TMA waits: the SM clocks a strip wait may take before it gives
+// up (0: the full limit, about 2 s; process-wide), and the number of waits that gave up since the last
+// call (read and reset on stream s, which is synchronised).
+void set_iir_wait_limit(long long cycles);
+uint32_t take_iir_waits_given_up(cudaStream_t s);
+
 }  // namespace spkb::dev

@@ -16,6 +16,7 @@
 #include <mutex>
 #include <set>
 
+#include "../cuda/iir.hpp"
 #include "../cuda/launch.hpp"
 #include "device.hpp"
 #include "render.hpp"
@@ -2559,6 +2560,19 @@ SPK_API spk_status spkx_test_set_tc_wait_limit(int64_t cycles) {
     if (cycles < 0) return invalid("a wait limit is a count of SM clocks, 0 or more");
     dev::set_tc_wait_limit(cycles);
     return SPK_OK;
+}
+
+SPK_API spk_status spkx_test_set_iir_wait_limit(int64_t cycles) {
+    last_error::clear();
+    if (cycles < 0) return invalid("a wait limit is a count of SM clocks, 0 or more");
+    dev::set_iir_wait_limit(cycles);
+    return SPK_OK;
+}
+
+SPK_API spk_status spkx_test_take_iir_waits_given_up(uint32_t* count) {
+    last_error::clear();
+    if (!count) return invalid("count is NULL");
+    return with_scratch_stream([&](cudaStream_t s) { *count = dev::take_iir_waits_given_up(s); });
 }
 
 SPK_API spk_status spkx_gaussian(const float* in, float* out, uint32_t w, uint32_t h, const double* sigma3) {

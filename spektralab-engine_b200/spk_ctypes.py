@@ -109,6 +109,8 @@ EXT = {
     "spkx_session_set_print_mode": (I32, [P, C, U32]),
     "spkx_print_negative": (I32, [P, P, U32, U32, P, U32, P, ctypes.POINTER(ctypes.c_double)]),
     "spkx_test_set_tc_wait_limit": (I32, [ctypes.c_int64]),
+    "spkx_test_set_iir_wait_limit": (I32, [ctypes.c_int64]),
+    "spkx_test_take_iir_waits_given_up": (I32, [UP]),
 }
 
 REF_EXT = {

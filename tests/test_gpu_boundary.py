@@ -1,5 +1,6 @@
 """The ABI's control surface under load (marked gpu: needs a B200): cancellation from a second thread,
-the progress record, the memory report, and the tensor-core kernel's failure path.
+the progress record, the memory report, and the failure paths of the tensor-core kernel's and the
+recursive blur's bounded mbarrier waits.
 
 Reference behaviour:
   * cancel: tests/session_check.py:287-306 -- a render polled with spk_cancel returns SPK_ERR_CANCELLED,
@@ -191,3 +192,33 @@ def test_tensor_core_wait_runs_out(engine, lib):
         got, meta = s.reprint("full")
         assert meta["reprint"] == 1 and np.array_equal(got, want)
     assert lib.lib.spkx_test_set_tc_wait_limit(-1) == sc.SPK_ERR_INVALID_ARG
+
+
+HALATION = ([((1, 1, 1), (8, 8, 8)), ((1, 1, 1), (40, 40, 40))], (0.03, 0.03, 0.03))
+
+
+def test_iir_column_wait_runs_out(engine, lib):
+    """The recursive blur's column pass loads its strips by TMA and waits on an mbarrier. With the wait cut
+    to one SM clock the strip waits give up at once: each CTA counts the event, waits again under the full
+    limit for the copies in flight and goes on, so the render (width a multiple of 4: the TMA path) is the
+    image a fresh session renders under the normal limit, and no wait gives up under that limit."""
+    img = sc.synthetic_image(512, 384, 6)
+    n = ctypes.c_uint32(0)
+    lib.check(lib.lib.spkx_test_take_iir_waits_given_up(ctypes.byref(n)))
+    with engine.open(img, BASE) as s:
+        s.set_halation(*HALATION)
+        want, _ = s.render("full")
+    lib.check(lib.lib.spkx_test_take_iir_waits_given_up(ctypes.byref(n)))
+    assert n.value == 0
+    lib.check(lib.lib.spkx_test_set_iir_wait_limit(1))
+    try:
+        with engine.open(img, BASE) as s:
+            s.set_halation(*HALATION)
+            got, _ = s.render("full")
+        lib.check(lib.lib.spkx_test_take_iir_waits_given_up(ctypes.byref(n)))
+    finally:
+        lib.check(lib.lib.spkx_test_set_iir_wait_limit(0))
+    assert n.value > 0
+    assert np.array_equal(got, want)
+    assert lib.lib.spkx_test_set_iir_wait_limit(-1) == sc.SPK_ERR_INVALID_ARG
+    assert lib.lib.spkx_test_take_iir_waits_given_up(None) == sc.SPK_ERR_INVALID_ARG
