@@ -108,3 +108,14 @@ def test_delta_validation(lib, resources, delta, needle):
 def test_valid_delta_builds(lib, resources):
     st, msg = _setup(lib, resources, BASE)
     assert st == sc.SPK_OK, msg
+
+
+def test_wait_limit_hooks_check_their_arguments(lib):
+    """The failure-path test hooks refuse bad arguments before any CUDA call (so here, with no GPU)."""
+    L = lib.lib
+    assert L.spkx_test_set_tc_wait_limit(-1) == sc.SPK_ERR_INVALID_ARG
+    assert L.spkx_test_set_iir_wait_limit(-1) == sc.SPK_ERR_INVALID_ARG
+    assert "SM clocks" in lib.last_error()
+    assert L.spkx_test_take_iir_waits_given_up(None) == sc.SPK_ERR_INVALID_ARG
+    assert "count is NULL" in lib.last_error()
+    assert L.spkx_test_set_iir_wait_limit(0) == sc.SPK_OK
