@@ -62,9 +62,9 @@ N_SM = 148
 # From the ncu capture summarised in profiles/render_kernels_2048x2048_ncu.md (one 2048 x 2048 render +
 # reprint, --set full): DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) and warp instructions
 # (smsp__inst_executed.sum) per pixel of each kernel's launch. Traffic scales with the pixels launched.
-NCU_TRAFFIC_PER_PX = {"expose": 14.24, "iir_rows": 25.09, "iir_cols": 53.98,
+NCU_TRAFFIC_PER_PX = {"expose": 14.24, "iir_rows": 25.09, "iir_cols": 53.66,
                       "develop_layers": 13.98, "fir_tile": 14.42, "print": 13.08, "scan_encode": 13.39}
-NCU_WARP_INST_PER_PX = {"expose": 10.73, "iir_rows": 18.37, "iir_cols": 13.05,
+NCU_WARP_INST_PER_PX = {"expose": 10.73, "iir_rows": 18.37, "iir_cols": 11.89,
                         "develop_layers": 149.67, "fir_tile": 6.90, "print": 60.34, "scan_encode": 18.96}
 
 
